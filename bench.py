@@ -1,0 +1,356 @@
+#!/usr/bin/env python
+"""Benchmark of the per-step lattice Boltzmann path (MLUPS).
+
+Workload (one bench step = INNER lattice Boltzmann time steps of the fused
+kernel on one resident simulation): the nonuniform-grid two-layer case,
+1024 x 256 cells, uniform x, tanh-stretched z (spacing ratio ~4), D2Q9 MRT +
+D2Q5 salinity, 3-point upwind-biased quadratic interpolated streaming,
+bounce-back walls, FP32 (see ip_cu_lbm_b200/workloads.py).
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+N > 1 runs one independent replica per GPU (torchrun, one process per GPU):
+the path has no exchange step, so no data-path collective is used; the
+timing is a barrier + synchronize on both sides and the max over ranks.
+Between timed steps L2 is flushed by writing a 256 MiB buffer (the 36 MB
+state is L2-resident inside a step). Rank 0 prints one JSON line.
+
+--impl reference times the reference's own implementation of this path,
+its CUDA kernel library built unmodified for sm_100a (oracle/_ref), running
+the LockExchange kernel chain on the closest workload it supports: the same
+262,144 cells with the stretched axis along x (the reference interpolates
+x only), Q9 scalar, its 5-point stencil.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+INNER = 100
+METRIC = "MLUPS"
+
+
+def env_int(k, d):
+    try:
+        return int(os.environ.get(k, d))
+    except ValueError:
+        return d
+
+
+class Clocks:
+    """Samples SM clocks and throttle reasons with nvidia-smi during the timed region."""
+
+    def __init__(self, index):
+        self.index, self.samples, self.proc = index, [], None
+
+    def __enter__(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 7:
+                self.samples.append(parts)
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples for i in range(4) if s[3 + i].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def dist_setup(n_gpus):
+    import torch
+
+    rank, world = env_int("RANK", 0), env_int("WORLD_SIZE", 1)
+    local = env_int("LOCAL_RANK", 0)
+    torch.cuda.set_device(local)
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+        pg = dist
+    return rank, world, local, pg
+
+
+def barrier_sync(pg):
+    import torch
+
+    torch.cuda.synchronize()
+    if pg is not None:
+        pg.barrier()
+    torch.cuda.synchronize()
+
+
+def max_over_ranks(pg, v):
+    import torch
+
+    if pg is None:
+        return v
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def cpu_baseline(params, S0, meta, budget_s=12.0):
+    """The FP64 structured-grid oracle (numpy port of the path) on the same
+    workload, single host thread, bounded number of steps."""
+    from ip_cu_lbm_b200.cases import d2q9_mrt
+    from oracle.structured import Box
+
+    M, Minv, S = d2q9_mrt()
+    p = dict(params)
+    for k in ("storage", "s_ref", "mrt"):
+        p.pop(k, None)
+    b = Box(meta["nx"], meta["nz"], M=M, Minv=Minv, S=S, **p)
+    b.S = S0.copy()
+    b.g = np.array([1 / 3] + [1 / 6] * 4)[:, None, None] * S0[None]
+    b.step(1)  # warm
+    n, t0 = 0, time.perf_counter()
+    while time.perf_counter() - t0 < budget_s and n < 50:
+        b.step(1)
+        n += 1
+    dt = time.perf_counter() - t0
+    return {"value": round(meta["nx"] * meta["nz"] * n / dt / 1e6, 4), "unit": METRIC, "cores": 1, "kind": "port",
+            "sample": f"{n} steps of the {meta['nx']}x{meta['nz']} workload, FP64 numpy oracle (oracle/structured.py)"}
+
+
+def run_ours(args):
+    import torch
+
+    from ip_cu_lbm_b200 import Sim, workloads
+
+    rank, world, local, pg = dist_setup(args.gpus)
+    params, S0, meta = workloads.stratified_nonuniform(storage=args.storage)
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.current_stream(dev)
+    sim = Sim(meta["nx"], meta["nz"], s0=S0.ravel(), stream=stream.cuda_stream, **params)
+    N = sim.N
+    inner = args.inner
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    for w in range(args.warmup):
+        flush.fill_(float(w))
+        sim.step_graph(inner, chunk=inner)
+    barrier_sync(pg)
+    times = []
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    with Clocks(local) as clk:
+        for k in range(args.steps):
+            flush.fill_(float(k))  # L2 flush between timed steps (not timed)
+            ev[k][0].record(stream)
+            sim.step_graph(inner, chunk=inner)
+            ev[k][1].record(stream)
+        barrier_sync(pg)
+    times = [a.elapsed_time(b) for a, b in ev]
+    total_ms = max_over_ranks(pg, sum(times))
+    assert sim.status() == 0, "non-finite state"
+    value = world * N * inner * args.steps / (total_ms / 1e3) / 1e6
+    launch_ms = total_ms / (args.steps * inner)
+    bpc = sim.bytes_per_cell()
+    peak, peak_src = load_peaks()
+    achieved = N * bpc / (launch_ms / 1e3) / 1e9
+
+    # end to end through the C ABI with pinned host buffers: upload the state,
+    # advance INNER steps, read S, u_x, u_z back
+    esz = sim.storage_bytes()
+    hdt = torch.float32 if esz == 4 else torch.float16
+    hf = torch.empty(9 * N, dtype=hdt, pin_memory=True)
+    hg = torch.empty(5 * N, dtype=hdt, pin_memory=True)
+    hm = torch.empty(3 * N, dtype=torch.float32, pin_memory=True)
+    sim.download(hf, hg, hm)
+    sim.sync()
+    e2e_steps = max(3, args.steps)
+    barrier_sync(pg)
+    t0 = time.perf_counter()
+    for k in range(e2e_steps):
+        sim.upload(hf, hg, hm)
+        sim.step_graph(inner, chunk=inner)
+        sim.download(None, None, hm)
+        sim.sync()
+    barrier_sync(pg)
+    e2e_s = max_over_ranks(pg, time.perf_counter() - t0)
+    e2e = world * N * inner * e2e_steps / e2e_s / 1e6
+
+    line = {
+        "metric": METRIC, "value": round(value, 2), "unit": METRIC, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(total_ms / args.steps, 4), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32" if args.storage == "f32" else f"{args.storage}-storage/f32",
+        "data": "synthetic (seeded two-layer tanh interface)",
+        "config": {"workload": f"nonuniform two-layer, {meta['nx']}x{meta['nz']} D2Q9 MRT + D2Q5, tanh-stretched z "
+                               f"(ratio {meta['spacing_ratio']:.2f}), 3-point upwind flux form, bounce-back",
+                   "lbm_steps_per_step": inner, "cells": N, "storage": args.storage,
+                   "parallelism": f"replicas x{world}",
+                   "l2": "flushed (256 MiB write) between timed steps; the 36 MB state is L2-resident within a step"},
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4), "traffic": None,
+                     "bytes_per_cell": bpc, "peak_source": f"{peak_src} (MEASURED_PEAKS.json hbm_gbs)",
+                     "note": "algorithmic bytes (each stored value read once and written once) / mean launch time"},
+        "e2e": {"value": round(e2e, 2), "unit": METRIC, "h2d_bytes_per_step": int(N * (14 * esz + 12)),
+                "d2h_bytes_per_step": int(N * 12)},
+        "gpu_launches": args.steps * inner,
+        "clocks": clk.summary(),
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            line["cpu_baseline"] = cpu_baseline(params, S0, meta)
+        except Exception as e:  # reported, not fatal
+            line["cpu_baseline"] = {"value": None, "error": str(e)[:200]}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    sim.close()
+    if pg is not None:
+        pg.destroy_process_group()
+
+
+def run_reference(args):
+    """The reference's CUDA kernel chain (oracle/_ref) on the closest
+    supported workload; rank 0 only."""
+    rank = env_int("RANK", 0)
+    if rank != 0:
+        return
+    from oracle import oracle as _o
+
+    if not _o.ref_available():
+        print(json.dumps({"impl": "reference", "unavailable": "reference build oracle/_ref/libipcu_ref.so missing"}))
+        return
+    import torch
+
+    from ip_cu_lbm_b200 import cases, workloads
+
+    dev = torch.device("cuda", env_int("LOCAL_RANK", 0))
+    torch.cuda.set_device(dev)
+    params, S0, meta = workloads.stratified_nonuniform()
+    nzs, nxs = meta["nz"], meta["nx"]  # stretched axis becomes the reference's x axis
+    c = cases.box_case(Q=9, nx0=nzs, nz=nxs, dx=1.0, dt=1.0, prec="f32")
+    # stretched x coordinates (the reference accepts any posx/delX >= dz)
+    xs, ws = np.asarray(params["z"]), np.asarray(params["wz"])
+    nc, own = c["nc"], c["owner"]
+    px = np.repeat(xs, nxs)
+    dX = np.repeat(ws, nxs)
+    c["posx"] = np.concatenate([px, px[own]]).astype(np.float32)
+    c["delX"] = np.concatenate([dX, dX[own]]).astype(np.float32)
+    Q, nt = 9, c["nt"]
+    # S[z, x] -> reference cell (i = z, l = x); scaled by 1e-3 because the
+    # reference hard-codes g = 9.81 and rho ~ 1000 (function/collision.cu:78)
+    Sg = 1e-3 * S0.T.reshape(-1)
+    w9 = c["w"]
+    g = (w9[None, :] * Sg[:, None]).astype(np.float32)
+    ext = lambda a: np.concatenate([a, a[own]])
+    st = dict(f=np.zeros(nt * Q, np.float32), g=np.concatenate([g, np.zeros((len(own), Q), np.float32)]).ravel(),
+              p=np.zeros(nt, np.float32), sal=ext(Sg.astype(np.float32)), phi=np.ones(nt, np.float32),
+              u=np.zeros(nt, np.float32), v=np.zeros(nt, np.float32), w=np.zeros(nt, np.float32),
+              tau=np.full(nt, params["tau"], np.float32), taus=np.full(nt, params["taus"], np.float32))
+    st["rho"] = (1000.0 + st["sal"].astype(np.float64) * 0.824493).astype(np.float32)
+    M, Minv, S = cases.d2q9_mrt()
+    _, S, _, MM = cases.set_M(9, M, S, Minv)
+    host = dict(items=c["items"], neib=c["neib"], nextB=c["nextB"], nextK=c["nextK"], posx=c["posx"],
+                posy=c["posy"], posz=c["posz"], delX=c["delX"], delY=c["delY"], M=M.ravel(), Minv=Minv.ravel(),
+                S=S, MM=MM.ravel(), ftmp=st["f"], fout=st["f"], feq=np.zeros(nt * Q), Fk=np.zeros(nt * Q),
+                Fx=np.zeros(nt), Fy=np.zeros(nt), Fz=np.zeros(nt), **st)
+    for a in range(6):
+        wl = c["walls"][a]
+        host[f"w{a + 1}"] = wl if len(wl) else np.zeros(1, np.int32)
+    T = {k: torch.as_tensor(np.ascontiguousarray(v), device=dev,
+                            dtype=torch.float32 if np.asarray(v).dtype.kind == "f" else torch.int32)
+         for k, v in host.items()}
+    import ctypes
+
+    slots = (ctypes.c_void_p * len(_o.REF_BUFS))(*[T[k].data_ptr() if k in T else None for k in _o.REF_BUFS])
+    ip = (ctypes.c_longlong * 16)(nt, INNER, 1, 1, 1, 0, 1, *[len(w) for w in c["walls"]], nt, 0)
+    fp = (ctypes.c_float * 2)(1.0, 1000.0)
+    R = _o.ref()
+    for _ in range(args.warmup):
+        assert R.lib.ref_le_steps_f32(slots, ip, fp) == 0
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    torch.cuda.synchronize()
+    total = 0.0
+    with Clocks(dev.index or 0) as clk:
+        for k in range(args.steps):
+            flush.fill_(float(k))
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            assert R.lib.ref_le_steps_f32(slots, ip, fp) == 0
+            e1.record()
+            torch.cuda.synchronize()
+            total += e0.elapsed_time(e1)
+    value = nc * INNER * args.steps / (total / 1e3) / 1e6
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": round(value, 2), "unit": METRIC, "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(total / args.steps, 4),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"reference LockExchange kernel chain, {nzs}x{nxs} cells (stretched axis along x, "
+                               "5-point stencil, Q9 scalar, MRT, bounce-back), reference CUDA built for sm_100a",
+                   "lbm_steps_per_step": INNER, "cells": nc},
+        "cpu_baseline": {"value": round(value, 2), "unit": METRIC, "kind": "reference", "cores": 0,
+                         "sample": "the reference's own CUDA build on the GPU (it has no CPU implementation)"},
+        "e2e": {"value": round(value, 2), "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "clocks": clk.summary(),
+    }), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--storage", default="f32", choices=["f32", "f16", "bf16"])
+    ap.add_argument("--inner", type=int, default=INNER)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,98 @@
+/*
+ * ipcu_sim.h -- structured-grid solver of libipcu (included by ipcu.h).
+ *
+ * One simulation = one rectangular box of nx x nz cells (2-D, x-z plane,
+ * D2Q9 flow) with a passive salinity lattice (D2Q5 or the reference's Q9
+ * scalar), rectilinear coordinates and one interpolated axis. Each step is
+ * the reference's LockExchange step (ref: LockExchange/LockExchange.cu:
+ * 220-236 without the wall model): equilibrium, force, MRT/SRT collision,
+ * conservative interpolated streaming of f, regularised scalar collision
+ * and streaming of g, then the moments -- fused into one kernel launch that
+ * reads each stored value once and writes it once.
+ *
+ * Storage: structure-of-arrays, x fastest, ping-pong buffers resident in
+ * HBM; distributions in FP32 or in FP16/BF16 (the pressure-form f is a
+ * deviation; g is stored shifted by w_k*S_ref), macroscopic S, u_x, u_z in
+ * FP32. Counts are exact int64.
+ */
+#ifndef IPCU_SIM_H
+#define IPCU_SIM_H
+#include <stdint.h>
+
+/* grid kinds for the interpolated streaming */
+#define IPCU_GEO_UNIFORM 0 /* exact shift */
+#define IPCU_GEO_X5 1      /* x nonuniform, 5-point Lagrange flux form (reference scheme) */
+#define IPCU_GEO_X3 2      /* x nonuniform, 3-point upwind-biased quadratic flux form */
+#define IPCU_GEO_Z5 3      /* z nonuniform, 5-point */
+#define IPCU_GEO_Z3 4      /* z nonuniform, 3-point quadratic upwind */
+
+#define IPCU_STORE_F32 0
+#define IPCU_STORE_F16 1
+#define IPCU_STORE_BF16 2
+
+#define IPCU_WALL_SLIP 0 /* specular reflection, reference set_bound2D tables */
+#define IPCU_WALL_BB 1   /* halfway bounce-back */
+
+typedef struct ipcu_sim_config {
+  int32_t nx, nz;       /* cells */
+  int32_t q_scalar;     /* 0 none, 5 D2Q5, 9 reference Q9 scalar */
+  int32_t geometry;     /* IPCU_GEO_* */
+  int32_t storage;      /* IPCU_STORE_* */
+  int32_t wall;         /* IPCU_WALL_* on all four walls */
+  int32_t mrt;          /* 1 MRT (matrices below), 0 SRT */
+  int32_t reserved;
+  double dz;            /* lattice spacing; c = dz/dt */
+  double dt;
+  const double *x;      /* host, nx cell centres (NULL: (i+0.5)*dz) */
+  const double *z;      /* host, nz cell centres (NULL: (l+0.5)*dz) */
+  const double *wx;     /* host, nx cell widths (NULL: dz) */
+  const double *wz;     /* host, nz cell widths (NULL: dz) */
+  double tau, taus;     /* relaxation times of f and g */
+  double rhoL, rhoH, phi; /* rho = rhoL + (rhoH-rhoL)*phi + rho_sal*S */
+  double rho_sal;       /* reference: 0.824493 */
+  double g_bouss;       /* buoyancy Fz = -g_bouss*S (reference: 0.824493*9.81) */
+  double s_ref;         /* salinity shift for reduced-precision g storage */
+  const double *M;      /* host 9x9 moment matrix (row-major), MRT only */
+  const double *Minv;   /* host 9x9 inverse */
+  const double *S;      /* host 9 relaxation rates (shear entries 7,8 are replaced by 1/tau) */
+} ipcu_sim_config;
+
+typedef struct ipcu_sim ipcu_sim;
+
+/* Creates a simulation on the current device and stream. Initial state:
+ * f = equilibrium of p*=0, u=0 (zero), g = equilibrium of S, S given per
+ * cell in s0 (host, nx*nz, x fastest; NULL = 0). Returns a status. */
+int ipcu_sim_create(const ipcu_sim_config *cfg, const double *s0, ipcu_stream_t stream, ipcu_sim **out);
+void ipcu_sim_destroy(ipcu_sim *sim);
+/* Advances nsteps (asynchronous on the sim's stream). */
+int ipcu_sim_step(ipcu_sim *sim, int64_t nsteps);
+/* Same steps recorded once into a CUDA graph of `chunk` steps and replayed. */
+int ipcu_sim_step_graph(ipcu_sim *sim, int64_t nsteps, int32_t chunk);
+/* Field names: "f" (9*N), "g" (q_scalar*N), "S", "ux", "uz", "p", "rho"
+ * (N each). Host output in FP64, x fastest, population-major for f/g.
+ * Synchronises the sim's stream. */
+int ipcu_sim_get(ipcu_sim *sim, const char *field, double *host_out, int64_t n);
+/* Overwrites the state from host FP64 arrays (f: 9*N, g: q*N, S/ux/uz: N). */
+int ipcu_sim_set_state(ipcu_sim *sim, const double *f, const double *g, const double *S, const double *ux,
+                       const double *uz);
+/* Sticky error flags (bit 0: non-finite moment seen). Synchronises. */
+int ipcu_sim_status(ipcu_sim *sim, uint32_t *flags);
+/* Raw state transfer in the storage layout, asynchronous on the sim's
+ * stream (host buffers should be pinned): f (9*N values of the storage
+ * type, already scaled), g (q_scalar*N, scaled and shifted), mac (FP32
+ * [3][N]: S, u_x, u_z). NULL skips a buffer. */
+int ipcu_sim_upload(ipcu_sim *sim, const void *f, const void *g, const float *mac);
+int ipcu_sim_download(ipcu_sim *sim, void *f, void *g, float *mac);
+int ipcu_sim_sync(ipcu_sim *sim);
+/* Bytes of one stored distribution value (4 FP32, 2 FP16/BF16). */
+int32_t ipcu_sim_storage_bytes(const ipcu_sim *sim);
+int64_t ipcu_sim_cells(const ipcu_sim *sim);
+/* Device pointers of the current state buffers (for zero-copy consumers). */
+int ipcu_sim_device_state(ipcu_sim *sim, void **f, void **g, float **mac);
+/* Bytes each stored value moves per cell and step (algorithmic traffic). */
+int64_t ipcu_sim_bytes_per_cell(const ipcu_sim *sim);
+/* FP64 domain sums of S and p* weighted by cell area (dx*dz/dz^2), the
+ * reference's conservation diagnostic (ref: function/basic.cu:9-15). */
+int ipcu_sim_totals(ipcu_sim *sim, double *sum_p, double *sum_s);
+
+#endif /* IPCU_SIM_H */

@@ -1,0 +1,44 @@
+// Parameters of the fused 2-D step kernel (fused2d.cu).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "ipcu.h"
+
+namespace ipcu {
+namespace f2d {
+
+constexpr int kTX = 64;  // tile width along x (two warps per row)
+constexpr int kTZ = 8;   // tile height along z
+constexpr int kThreads = 256;
+
+struct Params {
+  int nx, nz;
+  int mrt, wall;
+  const void *f_in;
+  void *f_out;
+  const void *g_in;
+  void *g_out;
+  const float *mac_in;  // [3][N]: S, ux, uz
+  float *mac_out;
+  // interpolated axis: weights [2][NA][NS], fin scale [2][NA], fout scale [NA]
+  const float *wA, *scin, *scout;
+  // 1/(x_{i+1} - x_{i-1} + dz/1000) with clamped neighbours (density gradient)
+  const float *ginvx, *ginvz;
+  float c, dt, tau, taus;
+  float rhoL, rhoH, phi;
+  double rho_sal, g_bouss;
+  float fscale, inv_fscale, gscale, inv_gscale, s_ref;
+  float MM[81];   // Minv diag(S) M with the shear rates zeroed
+  float Ms[18];   // shear rows 7, 8 of M
+  float Mis[18];  // shear columns 7, 8 of Minv, [a][2]
+  int8_t slipB9[16 * 9], slipK9[16 * 9];  // per wall class: owner neighbour and population
+  int8_t slipB5[16 * 9], slipK5[16 * 9];
+  unsigned *status;
+};
+
+// prepare_only: set the kernel's shared-memory attribute (call once before any capture)
+int launch_step(const Params &p, int storage, int qs, int geo, cudaStream_t s, bool prepare_only = false);
+
+}  // namespace f2d
+}  // namespace ipcu

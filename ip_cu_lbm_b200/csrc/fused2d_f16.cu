@@ -1,0 +1,17 @@
+// Instantiations of the fused 2-D step for __half distribution storage.
+#include "fused2d_impl.cuh"
+
+namespace ipcu {
+namespace f2d {
+
+int launch_f16(const Params &p, int qs, int geo, cudaStream_t s, bool prep) {
+  switch (qs) {
+    case 0: return launch_g<__half, 0>(p, geo, s, prep);
+    case 5: return launch_g<__half, 5>(p, geo, s, prep);
+    case 9: return launch_g<__half, 9>(p, geo, s, prep);
+  }
+  return IPCU_ERR_UNSUPPORTED;
+}
+
+}  // namespace f2d
+}  // namespace ipcu

@@ -1,0 +1,130 @@
+"""Python front end of the structured-grid solver (ipcu_sim_* in libipcu.so)."""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _lib
+from .cases import d2q9_mrt
+
+GEOMETRY = {"uniform": 0, "x5": 1, "x3": 2, "z5": 3, "z3": 4}
+STORAGE = {"f32": 0, "f16": 1, "bf16": 2}
+WALL = {"slip": 0, "bb": 1}
+
+# the reference's constants (ref: function/collision.cu:78,251)
+REF_RHO_SAL = 0.824493
+REF_G_BOUSS = 0.824493 * 9.81
+
+
+class Sim:
+    """A 2-D box (x-z plane) advanced by the fused sm_100a step kernel.
+
+    Fields are returned as numpy arrays shaped [nz, nx] (x fastest), or
+    [q, nz, nx] for the distributions f and g.
+    """
+
+    def __init__(self, nx, nz, *, q_scalar=5, geometry="uniform", storage="f32", wall="bb", mrt=True,
+                 dz=1.0, dt=1.0, x=None, z=None, wx=None, wz=None, tau=0.53, taus=0.503,
+                 rhoL=1.0, rhoH=1.0, phi=1.0, rho_sal=0.0, g_bouss=1e-4, s_ref=0.5,
+                 M=None, Minv=None, S=None, s0=None, stream=None):
+        L = _lib.lib()
+        self.nx, self.nz, self.q_scalar = int(nx), int(nz), int(q_scalar)
+        self._keep = []
+
+        def arr(a, n):
+            if a is None:
+                return None
+            a = np.ascontiguousarray(a, dtype=np.float64)
+            if a.size != n:
+                raise ValueError(f"expected {n} values, got {a.size}")
+            self._keep.append(a)
+            return a.ctypes.data
+
+        if mrt and M is None:
+            M, Minv, S = d2q9_mrt()
+        cfg = _lib.SimConfig()
+        cfg.nx, cfg.nz, cfg.q_scalar = self.nx, self.nz, self.q_scalar
+        cfg.geometry = GEOMETRY[geometry] if isinstance(geometry, str) else int(geometry)
+        cfg.storage = STORAGE[storage] if isinstance(storage, str) else int(storage)
+        cfg.wall = WALL[wall] if isinstance(wall, str) else int(wall)
+        cfg.mrt = 1 if mrt else 0
+        cfg.dz, cfg.dt = dz, dt
+        cfg.x, cfg.z, cfg.wx, cfg.wz = arr(x, nx), arr(z, nz), arr(wx, nx), arr(wz, nz)
+        cfg.tau, cfg.taus = tau, taus
+        cfg.rhoL, cfg.rhoH, cfg.phi = rhoL, rhoH, phi
+        cfg.rho_sal, cfg.g_bouss, cfg.s_ref = rho_sal, g_bouss, s_ref
+        if mrt:
+            cfg.M, cfg.Minv, cfg.S = arr(M, 81), arr(Minv, 81), arr(S, 9)
+        s0p = arr(s0, nx * nz)
+        h = ctypes.c_void_p()
+        _lib.check(L.ipcu_sim_create(ctypes.byref(cfg), s0p, stream, ctypes.byref(h)), "ipcu_sim_create")
+        self._h = h
+        self.N = self.nx * self.nz
+        self.storage = storage
+
+    # ---------------------------------------------------------------- lifecycle
+    def close(self):
+        if getattr(self, "_h", None):
+            _lib.lib().ipcu_sim_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ---------------------------------------------------------------- stepping
+    def step(self, n=1):
+        _lib.check(_lib.lib().ipcu_sim_step(self._h, int(n)), "ipcu_sim_step")
+
+    def step_graph(self, n, chunk=64):
+        _lib.check(_lib.lib().ipcu_sim_step_graph(self._h, int(n), int(chunk)), "ipcu_sim_step_graph")
+
+    # ---------------------------------------------------------------- fields
+    def get(self, field):
+        n = self.N * (9 if field == "f" else (self.q_scalar if field == "g" else 1))
+        out = np.zeros(n)
+        _lib.check(_lib.lib().ipcu_sim_get(self._h, field.encode(), out.ctypes.data, n), f"get {field}")
+        if field in ("f", "g"):
+            return out.reshape(-1, self.nz, self.nx)
+        return out.reshape(self.nz, self.nx)
+
+    def set_state(self, f=None, g=None, S=None, ux=None, uz=None):
+        keep = [None if a is None else np.ascontiguousarray(a, dtype=np.float64).reshape(-1) for a in (f, g, S, ux, uz)]
+        p = [None if a is None else a.ctypes.data for a in keep]
+        _lib.check(_lib.lib().ipcu_sim_set_state(self._h, *p), "ipcu_sim_set_state")
+
+    def status(self):
+        fl = ctypes.c_uint32()
+        _lib.lib().ipcu_sim_status(self._h, ctypes.byref(fl))
+        return fl.value
+
+    def totals(self):
+        a, b = ctypes.c_double(), ctypes.c_double()
+        _lib.check(_lib.lib().ipcu_sim_totals(self._h, ctypes.byref(a), ctypes.byref(b)), "ipcu_sim_totals")
+        return a.value, b.value
+
+    def bytes_per_cell(self):
+        return int(_lib.lib().ipcu_sim_bytes_per_cell(self._h))
+
+    def upload(self, f=None, g=None, mac=None):
+        """Asynchronous raw upload from (ideally pinned) host buffers in the storage layout."""
+        P = lambda a: None if a is None else (a.data_ptr() if hasattr(a, "data_ptr") else a.ctypes.data)
+        _lib.check(_lib.lib().ipcu_sim_upload(self._h, P(f), P(g), P(mac)), "ipcu_sim_upload")
+
+    def download(self, f=None, g=None, mac=None):
+        P = lambda a: None if a is None else (a.data_ptr() if hasattr(a, "data_ptr") else a.ctypes.data)
+        _lib.check(_lib.lib().ipcu_sim_download(self._h, P(f), P(g), P(mac)), "ipcu_sim_download")
+
+    def sync(self):
+        _lib.check(_lib.lib().ipcu_sim_sync(self._h), "ipcu_sim_sync")
+
+    def storage_bytes(self):
+        return int(_lib.lib().ipcu_sim_storage_bytes(self._h))
+
+    def device_state(self):
+        f, g, m = ctypes.c_void_p(), ctypes.c_void_p(), ctypes.c_void_p()
+        _lib.check(_lib.lib().ipcu_sim_device_state(self._h, ctypes.byref(f), ctypes.byref(g), ctypes.byref(m)))
+        return f.value, g.value, m.value

@@ -1,0 +1,75 @@
+"""Synthetic workloads of the benchmark configurations (seeded; no datasets).
+
+`stratified_nonuniform` is the nonuniform-grid two-layer case: 1024 x 256
+cells in the x-z plane, uniform in x, tanh-stretched in z
+    z(xi) = H zh(xi)/zh(1),  zh(xi) = xi - (gamma/beta) tanh(beta (xi - xi_c)),
+beta = 2.0, gamma = 0.812, xi_c so that z(xi_c) = 0.6 H, spacing scaled so the
+finest cell equals the lattice spacing (CFL <= 1 on the stretched axis).
+Lattice units (dz = dt = 1). D2Q9 MRT with nu = 0.005 (tau = 3 nu + 1/2),
+D2Q5 salinity with kappa = 0.0005 (tau_s = kappa/c_s^2 + 1/2), two layers
+S = [1 - tanh((z - z_i(x))/delta)]/2 with a 3-cell interface, a 2 % density
+difference and an interface tilt of 0.1 H over the tank, g' = 1e-4,
+bounce-back walls.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+
+def tanh_stretched_axis(n, beta=2.0, gamma=0.812, frac=0.6):
+    """Cell centres and widths of n cells on a tanh-clustered axis, finest width 1."""
+    xi_e = np.linspace(0.0, 1.0, n + 1)
+
+    def zh(xi, xc):
+        return xi - (gamma / beta) * np.tanh(beta * (xi - xc))
+
+    # xi_c such that z(xi_c)/H = frac (bisection; z(xi_c)/H = zh(xi_c)/zh(1))
+    lo, hi = 0.0, 1.0
+    for _ in range(200):
+        xc = 0.5 * (lo + hi)
+        if zh(xc, xc) / zh(1.0, xc) < frac:
+            lo = xc
+        else:
+            hi = xc
+    xc = 0.5 * (lo + hi)
+    edges = zh(xi_e, xc)
+    edges = edges - edges[0]
+    w = np.diff(edges)
+    w = w / w.min()
+    e = np.concatenate([[0.0], np.cumsum(w)])
+    return 0.5 * (e[1:] + e[:-1]), w, xc
+
+
+def stratified_nonuniform(nx=1024, nz=256, storage="f32", seed=20261203):
+    z, wz, xc = tanh_stretched_axis(nz)
+    H = z[-1] + wz[-1] / 2
+    x = (np.arange(nx) + 0.5)
+    L = float(nx)
+    rng = np.random.default_rng(seed)
+    zi = 0.6 * H + 0.1 * H * (x / L - 0.5)
+    delta = 1.5 * wz.min()  # 3-cell interface at the finest spacing
+    S = 0.5 * (1 - np.tanh((z[:, None] - zi[None, :]) / delta))
+    S = S + 1e-4 * rng.uniform(-1, 1, S.shape) * (np.abs(z[:, None] - zi[None, :]) < 2 * delta)
+    nu, kappa = 0.005, 0.0005
+    params = dict(q_scalar=5, geometry="z3", storage=storage, wall="bb", mrt=True, dz=1.0, dt=1.0, z=z, wz=wz,
+                  tau=3 * nu + 0.5, taus=3 * kappa + 0.5, rhoL=1.0, rhoH=1.0, phi=1.0, rho_sal=0.02, g_bouss=1e-4,
+                  s_ref=0.5)
+    meta = dict(nx=nx, nz=nz, spacing_ratio=float(wz.max() / wz.min()), xi_c=float(xc), H=float(H), nu=nu,
+                kappa=kappa, g_prime=1e-4, density_difference=0.02)
+    return params, S, meta
+
+
+def lock_exchange_uniform(nx=512, nz=64, seed=20261203):
+    """Uniform 512 x 64 lock exchange: S = 1 for x < nx/2 with seeded
+    U(-1e-4, 1e-4) noise on the interface columns; g' = 1e-4, nu = 0.01,
+    kappa = 0.001 on D2Q5, bounce-back walls."""
+    rng = np.random.default_rng(seed)
+    x = np.arange(nx)
+    S = np.where(x[None, :] < nx // 2, 1.0, 0.0) * np.ones((nz, 1))
+    band = np.abs(x + 0.5 - nx / 2) <= 1.0
+    S[:, band] += rng.uniform(-1e-4, 1e-4, (nz, band.sum()))
+    nu, kappa = 0.01, 0.001
+    params = dict(q_scalar=5, geometry="uniform", storage="f32", wall="bb", mrt=True, dz=1.0, dt=1.0,
+                  tau=3 * nu + 0.5, taus=3 * kappa + 0.5, rhoL=1.0, rhoH=1.0, phi=1.0, rho_sal=1e-4, g_bouss=1e-4,
+                  s_ref=0.5)
+    return params, S, dict(nx=nx, nz=nz)

@@ -1,0 +1,1104 @@
+// ORACLE -- test infrastructure only, never part of the product path.
+//
+// A plain-loop CPU restatement of the reference's per-step lattice Boltzmann
+// kernels (Kasahara1341/IP_CU_LBM, function/*.cu), templated on float and
+// double. Every entry point follows one reference kernel and keeps its
+// argument order, its array-of-structures layout f[cell*Q+k] over the
+// compacted, indirectly addressed cell list, and its in-place buffer
+// contracts (e.g. the collision zeroing f and feq). Atomic scatters of the
+// reference become sequential adds in cell order.
+//
+// Only tests/, __graft_entry__.smoke() and bench.py's cpu_baseline / reference
+// legs load this library (oracle/_build/libipcu_oracle.so).
+//
+// Parity pin: the library is checked against outputs of the reference CUDA
+// itself, built from the reference sources by oracle/Makefile into
+// oracle/_ref/ and run on the GPU (fixtures in tests/golden/, generated by
+// tests/golden/make_golden.py).
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <vector>
+
+namespace {
+
+// Parameter-block layout (ref: itemIndex.hpp:4-33).
+enum {
+  I_dz = 0, I_dt, I_c, I_nx, I_ny, I_nz, I_Q, I_ratiox, I_ratioy, I_PFthick, I_num_calc,
+  I_num_wall, I_num_IBPoints, I_dIBM, I_nu, I_alpha, I_sigma, I_tau, I_taus,
+  I_vec = 25
+};
+
+// Direction tables of the reference lattices (ref: function/basic.cu:112-153).
+struct Dirs {
+  int kinv[27], cp[27], cm[27], cip[27], cim[27], cxp[27], cxm[27], cyp[27], cym[27];
+  explicit Dirs(int Q) {
+    std::memset(this, 0, sizeof(*this));
+    if (Q == 9) {
+      static const int ki[9] = {0, 3, 4, 1, 2, 7, 8, 5, 6};
+      std::memcpy(kinv, ki, sizeof ki);
+      // upwind partner along x for the x-moving directions (ref: basic.cu:123-126)
+      const int xm[6] = {1, 3, 5, 6, 7, 8}, p[6] = {1, 3, 1, 3, 3, 1};
+      for (int i = 0; i < 6; i++) {
+        cp[xm[i]] = p[i];
+        cm[xm[i]] = (p[i] == 1) ? 3 : 1;
+      }
+    } else {
+      static const int ki[27] = {0, 3, 4, 1, 2, 6, 5, 10, 9, 8, 7, 14, 13, 12,
+                                 11, 18, 17, 16, 15, 26, 25, 24, 23, 22, 21, 20, 19};
+      std::memcpy(kinv, ki, sizeof ki);
+      static const int p[27] = {0, 1, 2, 3, 4, 0, 0, 7, 8, 9, 10, 1, 1, 3,
+                                3, 2, 2, 4, 4, 7, 7, 8, 8, 9, 9, 10, 10};
+      std::memcpy(cp, p, sizeof p);
+      for (int k = 0; k < 27; k++) cm[k] = kinv[cp[k]];
+      static const int ip_[8] = {8, 8, 7, 7, 10, 10, 9, 9}, im_[8] = {9, 9, 10, 10, 7, 7, 8, 8};
+      for (int i = 0; i < 8; i++) {
+        cip[19 + i] = ip_[i];
+        cim[19 + i] = im_[i];
+      }
+    }
+    // axis partners used by the xy tensor stencil (ref: basic.cu:139-153)
+    static const int xp[27] = {0, 1, 0, 3, 0, 0, 0, 1, 1, 3, 3, 1, 1, 3, 3, 0, 0, 0, 0, 1, 1, 1, 1, 3, 3, 3, 3};
+    static const int yp[27] = {0, 0, 2, 0, 4, 0, 0, 2, 4, 2, 4, 0, 0, 0, 0, 2, 2, 4, 4, 2, 2, 4, 4, 2, 2, 4, 4};
+    for (int k = 0; k < 27; k++) {
+      cxp[k] = xp[k];
+      cxm[k] = xp[k] == 1 ? 3 : (xp[k] == 3 ? 1 : 0);
+      cyp[k] = yp[k];
+      cym[k] = yp[k] == 2 ? 4 : (yp[k] == 4 ? 2 : 0);
+    }
+  }
+};
+
+template <class T>
+struct P {
+  const T *it;
+  int Q;
+  long nc, nw;
+  T dz, dt, c;
+  explicit P(const T *items)
+      : it(items), Q((int)items[I_Q]), nc((long)items[I_num_calc]), nw((long)items[I_num_wall]),
+        dz(items[I_dz]), dt(items[I_dt]), c(items[I_c]) {}
+  T w(int k) const { return it[I_vec + k]; }
+  T cx(int k) const { return it[I_vec + Q + k]; }
+  T cy(int k) const { return it[I_vec + 2 * Q + k]; }
+  T cz(int k) const { return it[I_vec + 3 * Q + k]; }
+};
+
+template <class T>
+inline T equil(const P<T> &p, int k, T base, T lead, T u, T v, T w) {
+  // w_k * base * (lead + 3 eu + 4.5 eu^2 - 1.5 u^2) in units of c (ref: collision.cu:10-11,23-24)
+  T eu = (p.cx(k) * u + p.cy(k) * v + p.cz(k) * w) / (p.c * p.c);
+  return p.w(k) * base * (lead + 3.0 * eu + 4.5 * eu * eu - 1.5 * (u * u + v * v + w * w) / (p.c * p.c));
+}
+
+// Stencil-node clamp next to walls (ref: function/adv.cu:16-28): ghost nodes
+// inherit their owner's coordinate; they are pushed one lattice spacing dz
+// beyond the previous node on each side.
+template <class T>
+inline void clamp_nodes(T *pl, T s, T dz) {
+  if (s == (T)1) {
+    pl[1] = std::min(pl[1], pl[2] - dz);
+    pl[0] = std::min(pl[0], pl[1] - dz);
+    pl[3] = std::max(pl[3], pl[2] + dz);
+    pl[4] = std::max(pl[4], pl[3] + dz);
+  } else if (s == (T)-1) {
+    pl[1] = std::max(pl[1], pl[2] + dz);
+    pl[0] = std::max(pl[0], pl[1] + dz);
+    pl[3] = std::min(pl[3], pl[2] - dz);
+    pl[4] = std::min(pl[4], pl[3] - dz);
+  } else {
+    for (int i = 0; i < 5; i++) pl[i] = 0;
+  }
+}
+
+// n-point Lagrange weights at xa (ref: function/adv.cu:41-48)
+template <class T>
+inline void lagrange(T *cf, const T *pl, T xa, int n) {
+  for (int i = 0; i < n; i++) {
+    T a = 1;
+    for (int j = 0; j < n; j++)
+      if (j != i) a *= (xa - pl[j]) / (pl[i] - pl[j]);
+    cf[i] = a;
+  }
+}
+
+// Peskin-type 4-point kernel used by the reference IBM (ref: function/ibm.cu:61-66)
+inline float peskin4(float dx, float x, float xl) {
+  float r = std::fabs(x - xl) / dx;
+  if (r < 1.0f) return (3.0f - 2.0f * r + std::sqrt(1.0f + 4.0f * r - 4.0f * r * r)) / 8.0f;
+  if (r <= 2.0f) return (5.0f - 2.0f * r - std::sqrt(-7.0f + 12.0f * r - 4.0f * r * r)) / 8.0f;
+  return 0.0f;
+}
+
+// rotation matrix of a quaternion (ref: function/ibm.cu:16-29)
+template <class T>
+inline void quat_rot(T q0, T q1, T q2, T q3, T *R) {
+  R[0] = q0 * q0 - q2 * q2 - q3 * q3 + q1 * q1;
+  R[1] = 2 * (q1 * q2 - q0 * q3);
+  R[2] = 2 * (q1 * q3 + q0 * q2);
+  R[3] = 2 * (q1 * q2 + q0 * q3);
+  R[4] = q0 * q0 - q3 * q3 - q1 * q1 + q2 * q2;
+  R[5] = 2 * (q2 * q3 - q0 * q1);
+  R[6] = 2 * (q1 * q3 - q0 * q2);
+  R[7] = 2 * (q2 * q3 + q0 * q1);
+  R[8] = q0 * q0 - q1 * q1 - q2 * q2 + q3 * q3;
+}
+
+// ======================================================================= collision.cu
+template <class T>
+void o_equ_f(const T *it, T *feq, const T *pr, const T *u, const T *v, const T *w) {  // collision.cu:3-14
+  P<T> p(it);
+  for (long i = 0; i < p.nc; i++)
+    for (int k = 0; k < p.Q; k++) feq[i * p.Q + k] = equil<T>(p, k, 1, pr[i], u[i], v[i], w[i]);
+}
+template <class T>
+void o_equ_g(const T *it, T *feq, const T *s, const T *u, const T *v, const T *w) {  // collision.cu:16-27
+  P<T> p(it);
+  for (long i = 0; i < p.nc; i++)
+    for (int k = 0; k < p.Q; k++) feq[i * p.Q + k] = equil<T>(p, k, s[i], 1, u[i], v[i], w[i]);
+}
+
+// Spalding wall model (ref: collision.cu:28-55)
+template <class T>
+void o_wall_function(const T *it, const T *dX, const T *dY, int x, int y, int z, int nw, const int *wall,
+                     const T *u, const T *v, const T *w, T *Fx, T *Fy, const T *rho) {
+  P<T> p(it);
+  const T nu = it[I_nu];
+  for (int e = 0; e < nw; e++) {
+    int id = wall[e];
+    T vol = dX[id] * dY[id] * p.dz;
+    T au = std::sqrt(u[id] * u[id] + v[id] * v[id] + w[id] * w[id]);
+    T eta = au * (T)1e-7f + (T)1e-20f;
+    const T kap = (T)0.41, B = (T)5.5;
+    T yd = x * dX[id] / 2.0 + y * dY[id] / 2.0 + z * p.dz / 2.0;
+    T area = vol / (yd * 2.0);
+    T ut = au * (T)0.11;
+    const T eb = std::exp(-kap * B);
+    for (int i = 0; i < 15; i++) {
+      T t = kap * au / (ut + eta);
+      T et = std::exp(t);
+      T fval = au / (ut + eta) - yd * ut / nu + eb * (et - 1.0 - t - t * t / 2.0 - t * t * t / 6.0);
+      T dval = -yd / nu - au / (ut * ut + eta) + eb * t / (ut + eta) * (-et + 1.0 + t + t * t / 2.0) + eta;
+      ut += -(fval / dval);
+    }
+    Fx[id] += -u[id] / (au + eta) * ut * ut * rho[id] * (area / vol);
+    Fy[id] += -v[id] / (au + eta) * ut * ut * rho[id] * (area / vol);
+  }
+}
+
+// Surface tension + buoyancy + pressure-gradient force and its lattice
+// projection Fk (ref: collision.cu:57-112)
+template <class T>
+void o_Force(const T *it, int bouss, const int *nb, const T *, const T *, const T *, T *Fk, T *Fx,
+             T *Fy, T *Fz, const T *pr, const T *rho, const T *sal, const T *phi, const T *u,
+             const T *v, const T *w, const T *dX, const T *, const T *px, const T *py, const T *pz) {
+  P<T> p(it);
+  const int Q = p.Q, up = (Q == 27) ? 5 : 2, dn = (Q == 27) ? 6 : 4;
+  const T reg = p.dz / 1000;
+  const T sig = it[I_sigma], W = it[I_PFthick];
+  for (long i = 0; i < p.nc; i++) {
+    const int *n = nb + i * Q;
+    auto grad = [&](const T *a, const T *pos, int d1, int d2) {
+      return (a[n[d1]] - a[n[d2]]) / (pos[n[d1]] - pos[n[d2]] + reg);
+    };
+    T gx = grad(phi, px, 1, 3), gy = (Q == 27) ? grad(phi, py, 2, 4) : 0, gz = grad(phi, pz, up, dn);
+    T lap = (phi[n[1]] - 2 * phi[i] + phi[n[3]]) / (dX[i] * dX[i]) +
+            (phi[n[2]] - 2 * phi[i] + phi[n[4]]) / (p.dz * p.dz);
+    T beta = 12.0 * sig / W, kap = 3.0 * sig * W / 2.0;
+    T st = 4 * beta * phi[i] * (phi[i] - 1.0) * (phi[i] - 0.5) - kap * lap;
+    Fx[i] += st * gx;
+    Fy[i] += st * gy;
+    Fz[i] += st * gz;
+    if (bouss)
+      Fz[i] += -sal[i] * 0.824493 * 9.81;
+    else
+      Fz[i] += -rho[i] * 9.81;
+    gx = grad(rho, px, 1, 3);
+    gy = (Q == 27) ? grad(rho, py, 2, 4) : 0;
+    gz = grad(rho, pz, up, dn);
+    T pc = pr[i] * p.c * p.c / 3.0;
+    Fx[i] += -pc * gx;
+    Fy[i] += -pc * gy;
+    Fz[i] += -pc * gz;
+    for (int k = 0; k < Q; k++)
+      Fk[i * Q + k] = p.w(k) * p.dt * (p.cx(k) * Fx[i] + p.cy(k) * Fy[i] + p.cz(k) * Fz[i]) /
+                      (rho[i] * p.c * p.c / 3.0);
+  }
+}
+
+// MRT collision with per-cell shear relaxation (ref: collision.cu:115-150).
+// Leaves the post-collision state in ftmp and zeroes f and feq.
+template <class T>
+void o_col_f_MRT(const T *it, const T *tau, T *f, T *ftmp, T *feq, const T *Fk, const T *M,
+                 const T *Mi, const T *, const T *MM) {
+  P<T> p(it);
+  const int Q = p.Q, s0 = (Q == 27) ? 5 : 7, ns = (Q == 27) ? 5 : 2;
+  std::vector<T> d(Q), mles(Q);
+  for (long i = 0; i < p.nc; i++) {
+    T *fi = f + i * Q;
+    for (int k = 0; k < Q; k++) d[k] = fi[k] - feq[i * Q + k] + Fk[i * Q + k] / 2.0;
+    for (int a = 0; a < Q; a++) {
+      for (int k = 0; k < Q; k++) {
+        T m = 0;
+        for (int l = 0; l < ns; l++) m += Mi[a * Q + s0 + l] * M[(s0 + l) * Q + k] / tau[i];
+        mles[k] = m;
+      }
+      T acc = 0;
+      for (int k = 0; k < Q; k++) acc += (MM[a * Q + k] + mles[k]) * d[k];
+      fi[a] = fi[a] - acc + Fk[i * Q + a];
+      ftmp[i * Q + a] = fi[a];
+    }
+    for (int k = 0; k < Q; k++) {
+      feq[i * Q + k] = 0;
+      fi[k] = 0;
+    }
+  }
+}
+
+// BGK with forcing (ref: collision.cu:151-165)
+template <class T>
+void o_col_f_SRT(const T *it, const T *tau, T *f, T *ftmp, T *feq, const T *Fk) {
+  P<T> p(it);
+  for (long i = 0; i < p.nc; i++)
+    for (int k = 0; k < p.Q; k++) {
+      long j = i * p.Q + k;
+      f[j] = f[j] - (f[j] - feq[j] + Fk[j] / 2.0) / tau[i] + Fk[j];
+      ftmp[j] = f[j];
+    }
+  for (long i = 0; i < p.nc; i++)
+    for (int k = 0; k < p.Q; k++) f[i * p.Q + k] = feq[i * p.Q + k] = 0;
+}
+
+// Regularised BGK for a passive scalar (ref: collision.cu:167-188)
+template <class T>
+void o_col_g_reg(const T *it, const T *taus, T *g, T *gtmp, T *geq, const T *s, const T *u,
+                 const T *v, const T *w) {
+  P<T> p(it);
+  const int Q = p.Q;
+  for (long i = 0; i < p.nc; i++) {
+    T jx = 0, jy = 0, jz = 0;
+    for (int k = 0; k < Q; k++) {
+      long j = i * Q + k;
+      geq[j] = equil<T>(p, k, s[i], 1, u[i], v[i], w[i]);
+      gtmp[j] = g[j] - geq[j];
+      jx += gtmp[j] * p.cx(k);
+      jy += gtmp[j] * p.cy(k);
+      jz += gtmp[j] * p.cz(k);
+    }
+    for (int k = 0; k < Q; k++) {
+      long j = i * Q + k;
+      T neq = p.w(k) * 3 * (jx * p.cx(k) + jy * p.cy(k) + jz * p.cz(k)) / (p.c * p.c);
+      gtmp[j] = geq[j] + (1.0 - 1.0 / taus[i]) * neq;
+      geq[j] = 0;
+      g[j] = 0;
+    }
+  }
+}
+
+// Conservative Allen-Cahn phase-field collision (ref: collision.cu:190-223)
+template <class T>
+void o_col_PF(const T *it, const int *nb, const T *, T *g, T *gtmp, T *geq, const T *phi, const T *u,
+              const T *v, const T *w, T *phio, T *uo, T *vo, T *wo, const T *px, const T *py,
+              const T *pz) {
+  P<T> p(it);
+  const int Q = p.Q, up = (Q == 27) ? 5 : 2, dn = (Q == 27) ? 6 : 4;
+  const T reg = p.dz / 1000, W = it[I_PFthick];
+  for (long i = 0; i < p.nc; i++) {
+    const int *n = nb + i * Q;
+    T gx = (phi[n[1]] - phi[n[3]]) / (px[n[1]] - px[n[3]] + reg);
+    T gy = (Q == 27) ? (phi[n[2]] - phi[n[4]]) / (py[n[2]] - py[n[4]] + reg) : 0;
+    T gz = (phi[n[up]] - phi[n[dn]]) / (pz[n[up]] - pz[n[dn]] + reg);
+    T du = (phi[i] * u[i] - phio[i] * uo[i]) / p.dt;
+    T dv = (phi[i] * v[i] - phio[i] * vo[i]) / p.dt;
+    T dw = (phi[i] * w[i] - phio[i] * wo[i]) / p.dt;
+    phio[i] = phi[i];
+    uo[i] = u[i];
+    vo[i] = v[i];
+    wo[i] = w[i];
+    T gn = std::sqrt(gx * gx + gy * gy + gz * gz + (T)1e-8f);
+    for (int k = 0; k < Q; k++) {
+      long j = i * Q + k;
+      geq[j] = equil<T>(p, k, phi[i], 1, u[i], v[i], w[i]);
+      T src = p.dt * p.w(k) *
+              ((1.0 - 4.0 * (phi[i] - 0.5) * (phi[i] - 0.5)) / W * (p.cx(k) * gx + p.cy(k) * gy + p.cz(k) * gz) / gn +
+               3 * (p.cx(k) * du + p.cy(k) * dv + p.cz(k) * dw) / (p.c * p.c));
+      gtmp[j] = g[j] - (g[j] - geq[j] - src * 0.08) / (0.5 + 0.08);
+      geq[j] = 0;
+      g[j] = 0;
+    }
+  }
+}
+
+template <class T>
+void o_update_scalar(const T *it, const T *g, T *s) {  // collision.cu:225-236
+  P<T> p(it);
+  for (long i = 0; i < p.nc; i++) {
+    T a = 0;
+    for (int k = 0; k < p.Q; k++) a += g[i * p.Q + k];
+    s[i] = a;
+  }
+}
+
+// moments p*, u (+F dt / 2 rho) and density from phi and salinity (ref: collision.cu:238-257)
+template <class T>
+void o_update_rho(const T *it, T rhoL, T rhoH, const T *f, const T *Fx, const T *Fy, const T *Fz, T *pr,
+                  const T *sal, const T *phi, T *rho, T *u, T *v, T *w) {
+  P<T> p(it);
+  for (long i = 0; i < p.nc; i++) {
+    T a = 0, b = 0, c = 0, d = 0;
+    for (int k = 0; k < p.Q; k++) {
+      T fk = f[i * p.Q + k];
+      a += fk;
+      b += p.cx(k) * fk;
+      c += p.cy(k) * fk;
+      d += p.cz(k) * fk;
+    }
+    pr[i] = a;
+    rho[i] = rhoL + (rhoH - rhoL) * phi[i] + sal[i] * 0.824493;
+    u[i] = b + Fx[i] * p.dt / (2.0 * rho[i]);
+    v[i] = c + Fy[i] * p.dt / (2.0 * rho[i]);
+    w[i] = d + Fz[i] * p.dt / (2.0 * rho[i]);
+  }
+}
+
+template <class T>
+void o_resetF(const T *, T *Fx, T *Fy, T *Fz, int n) {  // collision.cu:258-264
+  for (int i = 0; i < n; i++) Fx[i] = Fy[i] = Fz[i] = 0;
+}
+
+// ======================================================================= adv.cu / propagation.cu / set_bound.cu
+template <class T>
+void o_set_wall_f(const T *it, const int *nb, T *f) {  // adv.cu:3-13 (ghost <- owner copy)
+  P<T> p(it);
+  for (long g = p.nc; g < p.nc + p.nw; g++) {
+    long o = nb[g * p.Q];
+    for (int k = 0; k < p.Q; k++) f[g * p.Q + k] = f[o * p.Q + k];
+  }
+}
+
+// Conservative interpolated streaming fluxes (ref: adv.cu:50-147)
+template <class T>
+void o_set_out(const T *it, const int *nb, const T *ftmp, T *fout, T *fin, T *finy, const T *px,
+               const T *py, const T *dX, const T *dY) {
+  P<T> p(it);
+  const int Q = p.Q;
+  Dirs D(Q);
+  auto N = [&](long cell, int d) -> long { return nb[cell * Q + d]; };
+  int kx[6], ky[6], kd[12], nx_ = 6, ny_ = 6, nd = 12;
+  if (Q == 9) {
+    const int a[6] = {1, 3, 5, 6, 7, 8};
+    std::memcpy(kx, a, sizeof a);
+    ny_ = nd = 0;
+  } else {
+    const int a[6] = {1, 3, 11, 13, 12, 14}, b[6] = {2, 4, 15, 17, 16, 18};
+    std::memcpy(kx, a, sizeof a);
+    std::memcpy(ky, b, sizeof b);
+    for (int k = 0; k < 4; k++) {
+      kd[k] = 7 + k;
+      kd[k + 4] = 19 + k;
+      kd[k + 8] = 23 + k;
+    }
+  }
+  for (long i = 0; i < p.nc; i++) {
+    const long b = i * Q;
+    if (Q == 9) {
+      for (int k : {0, 2, 4}) fout[b + k] = fin[b + k] = ftmp[b + k];
+    } else {
+      for (int k : {0, 5, 6}) fout[b + k] = fin[b + k] = ftmp[b + k];
+    }
+    auto axis = [&](int k, const T *pos, const T *del, T s) {
+      long a1 = N(i, D.cm[k]), b1 = N(i, D.cp[k]);
+      long a2 = N(a1, D.cm[k]), b2 = N(b1, D.cp[k]);
+      T xa = pos[i] + s * (del[i] - p.dz) / 2.0;
+      T pl[5] = {pos[a2], pos[a1], pos[i], pos[b1], pos[b2]};
+      clamp_nodes(pl, s, p.dz);
+      T cf[5];
+      lagrange(cf, pl, xa, 5);
+      T val = cf[0] * ftmp[a2 * Q + k] + cf[1] * ftmp[a1 * Q + k] + cf[2] * ftmp[b + k] +
+              cf[3] * ftmp[b1 * Q + k] + cf[4] * ftmp[b2 * Q + k];
+      fin[b + k] = val * (p.dz / del[b1]);
+      fout[b + k] = val * (p.dz / del[i]);
+    };
+    for (int e = 0; e < nx_; e++) axis(kx[e], px, dX, p.cx(kx[e]) / p.c);
+    for (int e = 0; e < ny_; e++) axis(ky[e], py, dY, p.cy(ky[e]) / p.c);
+    for (int e = 0; e < nd; e++) {  // xy-diagonal: 5x5 tensor stencil (ref: adv.cu:100-145)
+      const int k = kd[e];
+      long id[25];
+      id[12] = i;
+      id[13] = N(i, D.cxp[k]);
+      id[14] = N(id[13], D.cxp[k]);
+      id[11] = N(i, D.cxm[k]);
+      id[10] = N(id[11], D.cxm[k]);
+      id[17] = N(i, D.cyp[k]);
+      id[22] = N(id[17], D.cyp[k]);
+      id[7] = N(i, D.cym[k]);
+      id[2] = N(id[7], D.cym[k]);
+      id[18] = N(i, D.cp[k]);
+      id[24] = N(id[18], D.cp[k]);
+      id[6] = N(i, D.cm[k]);
+      id[0] = N(id[6], D.cm[k]);
+      id[8] = N(i, D.cip[k]);
+      id[4] = N(id[8], D.cip[k]);
+      id[16] = N(i, D.cim[k]);
+      id[20] = N(id[16], D.cim[k]);
+      id[19] = N(id[14], D.cyp[k]);
+      id[9] = N(id[14], D.cym[k]);
+      id[15] = N(id[10], D.cyp[k]);
+      id[5] = N(id[10], D.cym[k]);
+      id[23] = N(id[22], D.cxp[k]);
+      id[21] = N(id[22], D.cxm[k]);
+      id[3] = N(id[2], D.cxp[k]);
+      id[1] = N(id[2], D.cxm[k]);
+      T sx = p.cx(k) / p.c, sy = p.cy(k) / p.c;
+      T pl[5] = {px[id[10]], px[id[11]], px[i], px[id[13]], px[id[14]]};
+      clamp_nodes(pl, sx, p.dz);
+      T cxw[5], cyw[5];
+      lagrange(cxw, pl, (T)(px[i] + sx * (dX[i] - p.dz) / 2.0), 5);
+      T fx = 0, fy = 0, fxy = 0;
+      for (int a = 0; a < 5; a++) fx += cxw[a] * ftmp[id[10 + a] * Q + k];
+      T ql[5] = {py[id[2]], py[id[7]], py[i], py[id[17]], py[id[22]]};
+      clamp_nodes(ql, sy, p.dz);
+      lagrange(cyw, ql, (T)(py[i] + sy * (dY[i] - p.dz) / 2.0), 5);
+      for (int a = 0; a < 5; a++) fy += cyw[a] * ftmp[id[2 + a * 5] * Q + k];
+      for (int a = 0; a < 5; a++)
+        for (int c = 0; c < 5; c++) fxy += cxw[a] * cyw[c] * ftmp[id[a + c * 5] * Q + k];
+      fout[b + k] = fx * p.dz / dX[i] + fy * p.dz / dY[i] - fxy * (p.dz * p.dz) / (dX[i] * dY[i]);
+      fin[b + k] += fxy * (p.dz * p.dz) / (dX[id[13]] * dY[id[17]]);
+      fin[N(i, D.cxm[k]) * Q + k] += (fy - fxy * p.dz / dX[id[17]]) * p.dz / dY[id[17]];
+      finy[N(i, D.cym[k]) * Q + k] += (fx - fxy * p.dz / dY[id[13]]) * p.dz / dX[id[13]];
+    }
+  }
+}
+
+// Q27 only: fluxes that landed on ghost cells are handed back to the
+// neighbouring fluid cell (ref: adv.cu:148-175)
+template <class T>
+void o_set_fin(const T *it, const int *nb, const int *, T *fin, T *finy) {
+  P<T> p(it);
+  if (p.Q != 27) return;
+  const int Q = 27;
+  static const int nk[8] = {9, 8, 10, 7, 7, 10, 8, 9}, nkz[8] = {19, 20, 21, 22, 23, 24, 25, 26},
+                   nn[8] = {1, 2, 1, 4, 3, 2, 3, 4};
+  int k3[12];
+  for (int k = 0; k < 4; k++) {
+    k3[k] = 7 + k;
+    k3[k + 4] = 19 + 2 * k;
+    k3[k + 8] = 20 + 2 * k;
+  }
+  for (long g = p.nc; g < p.nc + p.nw; g++) {
+    const long b = g * Q;
+    for (int k = 0; k < 4; k++) {
+      long A = nb[b + nn[2 * k]];
+      T fa = (T)(1 - A / g);
+      int d0 = nk[2 * (k3[k] - 7)];
+      fin[A * Q + d0] += fin[b + k3[k]] * fa;
+      fin[A * Q + nkz[2 * (d0 - 7)]] += fin[b + k3[k + 4]] * fa;
+      fin[A * Q + nkz[2 * (d0 - 7) + 1]] += fin[b + k3[k + 8]] * fa;
+      long B = nb[b + nn[2 * k + 1]];
+      T fb = (T)(1 - B / g);
+      int d1 = nk[2 * (k3[k] - 7) + 1];
+      finy[B * Q + d1] += finy[b + k3[k]] * fb;
+      finy[B * Q + nkz[2 * (d1 - 7)]] += finy[b + k3[k + 4]] * fb;
+      finy[B * Q + nkz[2 * (d1 - 7) + 1]] += finy[b + k3[k + 8]] * fb;
+    }
+  }
+}
+
+template <class T>
+void o_reset_f(const T *it, const T *ftmp, T *fin, T *f) {  // adv.cu:176-187
+  P<T> p(it);
+  for (long j = 0; j < p.nc * p.Q; j++) {
+    fin[j] += f[j];
+    f[j] = ftmp[j];
+  }
+}
+
+// ghost <- mirror of the owner across the x wall (ref: adv.cu:188-232)
+template <class T>
+void o_set_wall_f_inv(const T *it, const int *nb, const int *nextB, const int *nextK, T *f) {
+  P<T> p(it);
+  const int Q = p.Q;
+  for (long g = p.nc; g < p.nc + p.nw; g++) {
+    const long b = g * Q, o = nb[b];
+    if (Q == 9) {
+      static const int mx[9] = {0, 3, 0, 1, 0, 6, 5, 8, 7};
+      for (int k = 1; k < 9; k++) f[b + k] = f[o * Q + mx[k]];
+    } else {
+      Dirs D(27);
+      static const int nkz[8] = {20, 19, 22, 21, 24, 23, 26, 25};
+      static const int mxy[19] = {0, 3, 4, 1, 2, 0, 0, 0, 0, 0, 0, 13, 14, 11, 12, 17, 18, 15, 16};
+      int k1[15];
+      for (int k = 0; k < 7; k++) {
+        k1[k] = k;
+        k1[k + 7] = 11 + k;
+      }
+      k1[14] = 18;
+      for (int e = 0; e < 15; e++) f[b + k1[e]] = f[o * Q + mxy[k1[e]]];
+      int k3[12];
+      for (int k = 0; k < 4; k++) {
+        k3[k] = 7 + k;
+        k3[k + 4] = 19 + 2 * k;
+        k3[k + 8] = 20 + 2 * k;
+      }
+      const long wb = (g - p.nc) * Q;
+      for (int k = 0; k < 4; k++) {
+        int nk = D.kinv[nextK[wb + D.kinv[k3[k]]]], neB = nextB[wb + D.kinv[k3[k]]];
+        long s = nb[o * Q + neB];
+        f[b + k3[k]] = f[s * Q + nk];
+        f[b + k3[k + 4]] = f[s * Q + nkz[2 * (nk - 7) + 1]];
+        f[b + k3[k + 8]] = f[s * Q + nkz[2 * (nk - 7)]];
+      }
+    }
+  }
+}
+
+// new post-stream candidate: f(c+) + fin(c) - fout(c+) (ref: adv.cu:234-244)
+template <class T>
+void o_set_tmp(const T *it, const int *nb, const T *f, T *ftmp, const T *fout, const T *fin) {
+  P<T> p(it);
+  Dirs D(p.Q);
+  for (long i = 0; i < p.nc; i++)
+    for (int k = 0; k < p.Q; k++) {
+      long s = nb[i * p.Q + D.cp[k]];
+      ftmp[i * p.Q + k] = f[s * p.Q + k] + (fin[i * p.Q + k] - fout[s * p.Q + k]);
+    }
+}
+
+// ghost populations: bounce-back (1) or specular slip (0) (ref: set_bound.cu:164-183)
+template <class T>
+void o_set_wall_propagation(const T *it, int bc, const int *nb, const int *nextK, const int *nextB,
+                            T *ftmp) {
+  P<T> p(it);
+  const int Q = p.Q;
+  Dirs D(Q);
+  for (long g = p.nc; g < p.nc + p.nw; g++) {
+    const long b = g * Q, o = nb[b], wb = (g - p.nc) * Q;
+    if (bc == 1) {
+      for (int k = 1; k < Q; k++) ftmp[b + k] = ftmp[o * Q + D.kinv[k]];
+    } else if (bc == 0) {
+      for (int k = 1; k < Q; k++) {
+        long s = nb[o * Q + nextB[wb + k]];
+        ftmp[b + k] = ftmp[s * Q + nextK[wb + k]];
+      }
+    }
+  }
+}
+
+template <class T>
+void o_propagation(const T *it, const int *nb, T *f, const T *ftmp) {  // propagation.cu:2-12
+  P<T> p(it);
+  Dirs D(p.Q);
+  for (long i = 0; i < p.nc; i++)
+    for (int k = 0; k < p.Q; k++) f[i * p.Q + k] = ftmp[(long)nb[i * p.Q + D.kinv[k]] * p.Q + k];
+}
+
+template <class T>
+void o_reset_wall_fin(const T *it, T *fin, T *finy) {  // basic.cu:274-284
+  P<T> p(it);
+  for (long j = p.nc * p.Q; j < (p.nc + p.nw) * p.Q; j++) fin[j] = finy[j] = 0;
+}
+
+template <class T>
+void o_set_wall_rho(const T *it, const int *nb, T *rho) {  // basic.cu:254-261
+  P<T> p(it);
+  for (long g = p.nc; g < p.nc + p.nw; g++) rho[g] = rho[nb[g * p.Q]];
+}
+
+// The ten-launch streaming pass (ref: adv.cu:245-257)
+template <class T>
+void o_IP_process(const T *it, const int *nb, T *f, T *feq, T *ftmp, T *fout, const int *nextB,
+                  const int *nextK, const T *px, const T *py, const T *dX, const T *dY, int slip) {
+  o_set_wall_f(it, nb, ftmp);
+  o_set_out(it, nb, ftmp, fout, feq, f, px, py, dX, dY);
+  o_set_fin(it, nb, nextK, feq, f);
+  o_reset_f(it, ftmp, feq, f);
+  o_set_wall_f_inv(it, nb, nextB, nextK, f);
+  o_set_wall_f_inv(it, nb, nextB, nextK, fout);
+  o_set_tmp(it, nb, f, ftmp, fout, feq);
+  o_set_wall_propagation(it, slip, nb, nextK, nextB, ftmp);
+  o_propagation(it, nb, f, ftmp);
+  o_reset_wall_fin(it, feq, f);
+}
+
+template <class T>
+void o_reset_pressure(const T *it, T *pr, T *f, const T *u, const T *v, const T *w, T alpha) {  // basic.cu:262-273
+  P<T> p(it);
+  for (long i = 0; i < p.nc; i++) {
+    pr[i] /= alpha * alpha;
+    for (int k = 0; k < p.Q; k++) f[i * p.Q + k] = equil<T>(p, k, 1, pr[i], u[i], v[i], w[i]);
+  }
+}
+
+// Coherent-structure Smagorinsky model (ref: basic.cu:285-339)
+template <class T>
+void o_LES(const T *it, const int *nb, T *tau, T *taus, const T *phi, const T *rho, T muL, T muH,
+           const T *u, const T *v, const T *w, const T *px, const T *py, const T *pz) {
+  P<T> p(it);
+  const int Q = p.Q, up = (Q == 27) ? 5 : 2, dn = (Q == 27) ? 6 : 2;
+  const T reg = p.dz / 1000;
+  for (long i = 0; i < p.nc; i++) {
+    const int *n = nb + i * Q;
+    T g[3][3] = {{0}};
+    const T *vel[3] = {u, v, w};
+    for (int a = 0; a < 3; a++) {
+      g[0][a] = (vel[a][n[1]] - vel[a][n[3]]) / (px[n[1]] - px[n[3]] + reg);
+      if (Q == 27) g[1][a] = (vel[a][n[2]] - vel[a][n[4]]) / (py[n[2]] - py[n[4]] + reg);
+      g[2][a] = (vel[a][n[up]] - vel[a][n[dn]]) / (pz[n[up]] - pz[n[dn]] + reg);
+    }
+    T S = 0, Qc = 0, sum = 0;
+    for (int a = 0; a < 3; a++)
+      for (int b = 0; b < 3; b++) {
+        T sab = (g[a][b] + g[b][a]) / 2.0;
+        S += std::sqrt((T)(2.0 * sab * sab));
+        Qc += g[a][b] * g[b][a];
+        sum += g[a][b];
+      }
+    Qc *= -0.5;
+    T E = 1.0 / (2.0 * sum * sum + (T)1e-40f);
+    T Fcs = std::max((T)-1.0, std::min(Qc / E, (T)1.0));
+    T C = 0.05 * std::pow(std::fabs(Fcs), (T)1.5);
+    tau[i] = 3.0 * ((muL + phi[i] * (muH - muL)) / rho[i] + C * S * p.dz * p.dz) / (p.c * p.c * p.dt) + 0.5;
+    taus[i] = 3.0 * ((T)1e-9f + C * S * p.dz * p.dz / 1000) / (p.c * p.c * p.dt) + 0.5;
+  }
+}
+
+// ======================================================================= ibm.cu
+template <class T>
+struct IbIdx {
+  int t[3][3][3];
+  explicit IbIdx(int Q) {
+    std::memset(t, 0, sizeof t);
+    if (Q == 9) {
+      // (x-index, -, z-index) -> direction (ref: ibm.cu:133-137)
+      t[0][1][2] = 6; t[1][1][2] = 2; t[2][1][2] = 5;
+      t[0][1][1] = 3; t[1][1][1] = 0; t[2][1][1] = 1;
+      t[0][1][0] = 5; t[1][1][0] = 4; t[2][1][0] = 8;
+    } else {
+      // direction with velocity (i-1, j-1, l-1) (ref: ibm.cu:138-142)
+      static const int c[27][3] = {{0, 0, 0}, {1, 0, 0}, {0, 1, 0}, {-1, 0, 0}, {0, -1, 0}, {0, 0, 1},
+                                   {0, 0, -1}, {1, 1, 0}, {1, -1, 0}, {-1, 1, 0}, {-1, -1, 0}, {1, 0, 1},
+                                   {1, 0, -1}, {-1, 0, 1}, {-1, 0, -1}, {0, 1, 1}, {0, 1, -1}, {0, -1, 1},
+                                   {0, -1, -1}, {1, 1, 1}, {1, 1, -1}, {1, -1, 1}, {1, -1, -1}, {-1, 1, 1},
+                                   {-1, 1, -1}, {-1, -1, 1}, {-1, -1, -1}};
+      for (int k = 0; k < 27; k++) t[c[k][0] + 1][c[k][1] + 1][c[k][2] + 1] = k;
+    }
+  }
+};
+
+// Stress-jump IBM force of Suzuki & Yoshino, interpolate + spread
+// (ref: ibm.cu:124-274)
+template <class T>
+void o_get_IBMGw2(const T *it, const int *lid, const int *nb, const T *f, const T *tau, const T *px,
+                  const T *py, const T *pz, const T *posw, const T *, const T *nB, const T *, const T *,
+                  const T *, const T *velw, T *Fx, T *Fy, T *Fz, T *Gw, T rhof) {
+  P<T> p(it);
+  const int Q = p.Q;
+  const long np = (long)it[I_num_IBPoints];
+  const T dIBM = it[I_dIBM];
+  Dirs D(Q);
+  IbIdx<T> X(Q);
+  const int j0 = (Q == 9) ? 1 : 0, j1 = (Q == 9) ? 2 : 3, dim = (Q == 9) ? 2 : 3;
+  std::vector<T> fw(Q), fw1(Q), fw2(Q);
+  for (long m = 0; m < np; m++) {
+    const long L = lid[m];
+    auto N = [&](int d) -> long { return nb[L * Q + d]; };
+    const T uw = velw[m * 3], vw = velw[m * 3 + 1], ww = velw[m * 3 + 2];
+    T cx[3], cy[3], cz[3];
+    const int xs[3] = {3, 0, 1};
+    for (int a = 0; a < 3; a++)
+      cx[a] = (T)peskin4((float)p.dz, (float)posw[m * 3], (float)px[N(xs[a])]) * (T)(N(xs[a]) < p.nc);
+    if (Q == 27) {
+      T pl[3] = {py[N(4)], py[N(0)], py[N(2)]};
+      lagrange(cy, pl, posw[m * 3 + 1], 3);
+      T ql[3] = {pz[N(6)], pz[N(0)], pz[N(5)]};
+      lagrange(cz, ql, posw[m * 3 + 2], 3);
+    } else {
+      cy[0] = 0; cy[1] = 1; cy[2] = 0;
+      const int zs[3] = {4, 0, 2};
+      for (int a = 0; a < 3; a++)
+        cz[a] = (T)peskin4((float)p.dz, (float)posw[m * 3 + 2], (float)pz[N(zs[a])]) * (T)(N(zs[a]) < p.nc);
+      T s = cx[0] + cx[1] + cx[2];
+      for (int a = 0; a < 3; a++) cx[a] /= s;
+      s = cz[0] + cz[1] + cz[2];
+      for (int a = 0; a < 3; a++) cz[a] /= s;
+    }
+    std::fill(fw.begin(), fw.end(), (T)0);
+    for (int i = 0; i < 3; i++)
+      for (int j = j0; j < j1; j++)
+        for (int l = 0; l < 3; l++) {
+          long id = N(X.t[i][j][l]);
+          if (id < p.nc)
+            for (int k = 0; k < Q; k++) fw[k] += cx[i] * cy[j] * cz[l] * f[id * Q + k];
+        }
+    const T alpha = 22.5 / 180.0 * 3.14159;
+    for (int k = 0; k < Q; k++) {
+      T t = (nB[m * 3] * p.cx(k) + nB[m * 3 + 1] * p.cy(k) + nB[m * 3 + 2] * p.cz(k)) / p.c;
+      T t2 = std::sqrt(p.cx(k) * p.cx(k) + p.cy(k) * p.cy(k) + p.cz(k) * p.cz(k)) / p.c * std::sin(alpha);
+      T t3 = 6.0 * p.w(k) * (p.cx(k) * uw + p.cy(k) * vw + p.cz(k) * ww) / (p.c * p.c);
+      T be = std::fabs(t) / (t2 + (T)1e-10f);
+      T mix = (1.0 - be) * fw[k] + be * (fw[D.kinv[k]] + t3), refl = fw[D.kinv[k]] + t3;
+      fw1[k] = (t <= 0) ? fw[k] : ((t <= t2) ? mix : refl);
+      fw2[k] = (t >= 0) ? fw[k] : ((t >= -t2) ? mix : refl);
+    }
+    const T tl = tau[L];
+    const T uvec[3] = {uw, vw, ww};
+    auto ccomp = [&](int a, int k) { return a == 0 ? p.cx(k) : (a == 1 ? p.cy(k) : p.cz(k)); };
+    auto stress = [&](int a, bool jump, T *sig) {
+      for (int b = 0; b < 3; b++) sig[b] = 0;
+      for (int k = 0; k < Q; k++) {
+        T df = jump ? fw1[k] - fw2[k] : fw1[k];
+        for (int b = 0; b < 3; b++)
+          sig[b] -= 0.5 / tl * df * (T)(a == b) +
+                    (1.0 - 0.5 / tl) * 3 *
+                        (df * (ccomp(a, k) - uvec[a]) * (ccomp(b, k) - uvec[b]) - (1 * df - p.w(k)) * uvec[a] * uvec[b]) /
+                        (p.c * p.c);
+      }
+    };
+    T sig[3];
+    for (int a = 0; a < 3; a++) {
+      stress(a, true, sig);
+      Gw[m * 3 + a] = -(sig[0] * nB[m * 3] + sig[1] * nB[m * 3 + 1] + sig[2] * nB[m * 3 + 2]);
+    }
+    const T sc = std::pow((float)(dIBM / p.dz), (float)(dim - 1)) / p.dz;
+    for (int i = 0; i < 3; i++)
+      for (int j = j0; j < j1; j++)
+        for (int l = 0; l < 3; l++) {
+          long id = N(X.t[i][j][l]);
+          if (id < p.nc) {
+            T wgt = cx[i] * cy[j] * cz[l];
+            Fx[id] += Gw[m * 3] * sc * wgt;
+            Fy[id] += Gw[m * 3 + 1] * sc * wgt;
+            Fz[id] += Gw[m * 3 + 2] * sc * wgt;
+          }
+        }
+    for (int a = 0; a < 3; a++) {
+      stress(a, false, sig);
+      Gw[m * 3 + a] = sig[0] * nB[m * 3] + sig[1] * nB[m * 3 + 1] + sig[2] * nB[m * 3 + 2];
+    }
+    const T gs = rhof * p.c * p.c / 3.0 * std::pow((float)dIBM, (float)(dim - 1));
+    for (int a = 0; a < 3; a++) Gw[m * 3 + a] *= gs;
+  }
+}
+
+// Classic direct forcing, float only in the reference (ref: ibm.cu:276-344)
+void o_IB_directForcing(const float *it, const int *lid, const int *nb, const float *px, const float *py,
+                        const float *pz, const float *posw, const float *u, const float *v, const float *w,
+                        const float *velw, float *Fx, float *Fy, float *Fz, float *Gw) {
+  P<float> p(it);
+  const int Q = p.Q;
+  const long np = (long)it[I_num_IBPoints];
+  IbIdx<float> X(Q);
+  const int j0 = (Q == 9) ? 1 : 0, j1 = (Q == 9) ? 2 : 3, dim = (Q == 9) ? 2 : 3;
+  const float *vel[3] = {u, v, w};
+  float *F[3] = {Fx, Fy, Fz};
+  for (long m = 0; m < np; m++) {
+    const long L = lid[m];
+    auto N = [&](int d) -> long { return nb[L * Q + d]; };
+    float cx[3], cy[3], cz[3];
+    float pl[3] = {px[N(3)], px[N(0)], px[N(1)]};
+    lagrange(cx, pl, posw[m * 3], 3);
+    if (Q == 27) {
+      float a[3] = {py[N(4)], py[N(0)], py[N(2)]};
+      lagrange(cy, a, posw[m * 3 + 1], 3);
+      float b[3] = {pz[N(6)], pz[N(0)], pz[N(5)]};
+      lagrange(cz, b, posw[m * 3 + 2], 3);
+    } else {
+      cy[0] = 0; cy[1] = 1; cy[2] = 0;
+      float b[3] = {pz[N(4)], pz[N(0)], pz[N(2)]};
+      lagrange(cz, b, posw[m * 3 + 2], 3);
+    }
+    float uw[3] = {0, 0, 0};
+    for (int i = 0; i < 3; i++)
+      for (int j = j0; j < j1; j++)
+        for (int l = 0; l < 3; l++) {
+          long id = N(X.t[i][j][l]);
+          if (id < p.nc)
+            for (int a = 0; a < 3; a++) uw[a] += cx[i] * cy[j] * cz[l] * vel[a][id];
+        }
+    float gw[3];
+    for (int a = 0; a < 3; a++) gw[a] = (velw[m * 3 + a] - uw[a]) / p.dt;
+    const float sc = std::pow(it[I_dIBM] / p.dz, (float)(dim - 1)) * 3.0f / (p.c * p.c);
+    for (int i = 0; i < 3; i++)
+      for (int j = j0; j < j1; j++)
+        for (int l = 0; l < 3; l++) {
+          long id = N(X.t[i][j][l]);
+          if (id < p.nc)
+            for (int a = 0; a < 3; a++) F[a][id] += gw[a] * sc * cx[i] * cy[j] * cz[l];
+        }
+    for (int a = 0; a < 3; a++) Gw[m * 3 + a] += -gw[a] * 1000 * std::pow(it[I_dIBM], (float)(dim - 1)) * p.dz;
+  }
+}
+
+// post-stream forcing and moment update (ref: ibm.cu:346-365)
+template <class T>
+void o_update_velIBM(const T *it, const int *, T *f, const T *, T *pr, const T *, T *u, T *v, T *w,
+                     const T *, const T *, const T *, const T *Fx, const T *Fy, const T *Fz) {
+  P<T> p(it);
+  for (long i = 0; i < p.nc; i++) {
+    T a = 0, b = 0, c = 0, d = 0;
+    for (int k = 0; k < p.Q; k++) {
+      long j = i * p.Q + k;
+      f[j] = f[j] + p.w(k) * p.dt * (p.cx(k) * Fx[i] + p.cy(k) * Fy[i] + p.cz(k) * Fz[i]);
+      a += f[j];
+      b += p.cx(k) * f[j];
+      c += p.cy(k) * f[j];
+      d += p.cz(k) * f[j];
+    }
+    pr[i] = a;
+    u[i] = b;
+    v[i] = c;
+    w[i] = d;
+  }
+}
+
+// Rigid body: force/torque sums, AB2 translation/rotation, quaternion AB2
+// (ref: ibm.cu:367-424). quatold is read at offset 0 as in the reference.
+template <class T>
+void o_update_IBbody(const T *it, int ib, const T *massB, const T *densB, const T *inertia, T *FB, T *posB,
+                     T *Tq, T *velB, T *quat, T *quaS, T *angleVB, const T *posw, const T *Gw, T *quatold,
+                     T rhof) {
+  const long np = (long)it[I_num_IBPoints];
+  const T dt = it[I_dt];
+  T Ro[9], Fo[3], To[3], vo[3], wo[3];
+  quat_rot(quatold[ib * 4], quatold[ib * 4 + 1], quatold[ib * 4 + 2], quatold[ib * 4 + 3], Ro);
+  for (int a = 0; a < 3; a++) {
+    Fo[a] = FB[ib * 3 + a];
+    FB[ib * 3 + a] = 0;
+    To[a] = Tq[ib * 3 + a];
+    Tq[ib * 3 + a] = 0;
+    vo[a] = velB[ib * 3 + a];
+    wo[a] = angleVB[ib * 3 + a];
+  }
+  for (long m = 0; m < np; m++) {
+    const T *g = Gw + m * 3, *x = posw + m * 3, *c = posB + ib * 3;
+    FB[ib * 3] += g[0];
+    FB[ib * 3 + 1] += g[1];
+    FB[ib * 3 + 2] += g[2];
+    Tq[ib * 3] += (x[1] - c[1]) * g[2] - (x[2] - c[2]) * g[1];
+    Tq[ib * 3 + 1] += (x[2] - c[2]) * g[0] - (x[0] - c[0]) * g[2];
+    Tq[ib * 3 + 2] += (x[0] - c[0]) * g[1] - (x[1] - c[1]) * g[0];
+  }
+  FB[ib * 3 + 2] += (1.0 - rhof / densB[ib]) * massB[ib] * 9.81;
+  for (int a = 0; a < 3; a++) {
+    velB[ib * 3 + a] += dt * (3.0 * FB[ib * 3 + a] - Fo[a]) / massB[ib] / 2.0;
+    posB[ib * 3 + a] += dt * (3.0 * velB[ib * 3 + a] - vo[a]) / 2.0;
+  }
+  for (int a = 0; a < 3; a++)
+    for (int b = 0; b < 3; b++)
+      angleVB[ib * 3 + a] +=
+          dt * (3.0 * quaS[ib * 3 + b * 3 + a] * Tq[ib * 3 + b] - Ro[b * 3 + a] * To[b]) / inertia[ib * 3 + a] / 2.0;
+  T q[4], w[3];
+  for (int a = 0; a < 4; a++) q[a] = quat[ib * 4 + a];
+  for (int a = 0; a < 3; a++) w[a] = angleVB[ib * 3 + a];
+  T *Q = quat + ib * 4;
+  Q[0] += dt * 3.0 * (-w[0] * q[1] - w[1] * q[2] - w[2] * q[3]) / 4.0;
+  Q[1] += dt * 3.0 * (w[0] * q[0] + w[2] * q[2] - w[1] * q[3]) / 4.0;
+  Q[2] += dt * 3.0 * (w[1] * q[0] - w[2] * q[1] + w[0] * q[3]) / 4.0;
+  Q[3] += dt * 3.0 * (w[2] * q[0] + w[1] * q[1] - w[0] * q[2]) / 4.0;
+  const T *qo = quatold;
+  Q[0] -= dt * (-wo[0] * qo[1] - wo[1] * qo[2] - wo[2] * qo[3]) / 4.0;
+  Q[1] -= dt * (wo[0] * qo[0] + wo[2] * qo[2] - wo[1] * qo[3]) / 4.0;
+  Q[2] -= dt * (wo[1] * qo[0] - wo[2] * qo[1] + wo[0] * qo[3]) / 4.0;
+  Q[3] -= dt * (wo[2] * qo[0] + wo[1] * qo[1] - wo[0] * qo[2]) / 4.0;
+  for (int a = 0; a < 4; a++) quatold[ib * 4 + a] = q[a];
+  quat_rot(Q[0], Q[1], Q[2], Q[3], quaS);
+}
+
+// marker kinematics (ref: ibm.cu:426-447)
+template <class T>
+void o_update_IBpoint(const T *it, int ib, const T *posB, const T *velB, const T *om, const T *R, T *posw,
+                      const T *op, T *nB, const T *onB, T *velw) {
+  const long np = (long)it[I_num_IBPoints];
+  const T *Rb = R + ib * 9, *w = om + ib * 3;
+  for (long m = 0; m < np; m++) {
+    const T *r = op + m * 3;
+    for (int a = 0; a < 3; a++) {
+      posw[m * 3 + a] = posB[ib * 3 + a];
+      velw[m * 3 + a] = velB[ib * 3 + a];
+      nB[m * 3 + a] = 0;
+      for (int b = 0; b < 3; b++) {
+        posw[m * 3 + a] += Rb[a * 3 + b] * r[b];
+        nB[m * 3 + a] += Rb[a * 3 + b] * onB[m * 3 + b];
+      }
+    }
+    const T wr[3] = {w[1] * r[2] - w[2] * r[1], w[2] * r[0] - w[0] * r[2], w[0] * r[1] - w[1] * r[0]};
+    for (int a = 0; a < 3; a++) velw[m * 3 + a] += Rb[a * 3] * wr[0] + Rb[a * 3 + 1] * wr[1] + Rb[a * 3 + 2] * wr[2];
+  }
+}
+
+// nearest of the Q neighbours (ref: ibm.cu:449-463)
+template <class T>
+void o_search_IBlattice(const T *it, int, int *lid, const int *nb, const T *px, const T *py, const T *pz,
+                        const T *posw) {
+  P<T> p(it);
+  const long np = (long)it[I_num_IBPoints];
+  for (long m = 0; m < np; m++) {
+    long id = lid[m], best = id;
+    auto d2 = [&](long c) {
+      T a = px[c] - posw[m * 3], b = py[c] - posw[m * 3 + 1], e = pz[c] - posw[m * 3 + 2];
+      return a * a + b * b + e * e;
+    };
+    T d1 = d2(id);
+    for (int k = 1; k < p.Q; k++) {
+      long n = nb[id * p.Q + k];
+      T dd = d2(n);
+      if (dd < d1) {
+        best = n;
+        d1 = dd;
+      }
+    }
+    lid[m] = (int)best;
+  }
+}
+
+// smoothed-profile forcing of a disc (ref: ibm.cu:44-49,68-85)
+template <class T>
+void o_SPM(const T *it, T R, const T *posB, T *f, T *ftmp, const T *, const T *px, const T *py, T *Fx, T *Fy,
+           T *Fz, const T *u, const T *v, const T *w, const T *velw) {
+  P<T> p(it);
+  for (long i = 0; i < p.nc; i++) {
+    float dz = (float)p.dz;
+    float r = (float)R - 0.5f * dz - std::sqrt((float)((px[i] - posB[0]) * (px[i] - posB[0]) + (py[i] - posB[1]) * (py[i] - posB[1])));
+    float prof = (r < -0.5f * dz) ? 0.0f : (std::fabs(r) <= 0.5f * dz ? 0.5f * (std::sin(3.14159f * r / dz) + 1.0f) : 1.0f);
+    Fx[i] = prof * (velw[0] - u[i]) / p.dz;
+    Fy[i] = prof * (velw[1] - v[i]) / p.dz;
+    Fz[i] = prof * (velw[2] - w[i]) / p.dz;
+    for (int k = 0; k < p.Q; k++) {
+      long j = i * p.Q + k;
+      f[j] = ftmp[j] + p.w(k) * p.dt * 3.0 * (p.cx(k) * Fx[i] + p.cy(k) * Fy[i] + p.cz(k) * Fz[i]) / (p.c * p.c);
+      ftmp[j] = f[j];
+    }
+    Fx[i] = Fy[i] = Fz[i] = 0;
+  }
+}
+
+}  // namespace
+
+// ======================================================================= C ABI
+#define ORACLE_BOTH(X) X(float, f32) X(double, f64)
+#define DEF(T, S)                                                                                        \
+  extern "C" void oracle_equ_f_##S(const T *a, T *b, const T *c, const T *d, const T *e, const T *f) {  \
+    o_equ_f<T>(a, b, c, d, e, f);                                                                       \
+  }                                                                                                      \
+  extern "C" void oracle_equ_g_##S(const T *a, T *b, const T *c, const T *d, const T *e, const T *f) {  \
+    o_equ_g<T>(a, b, c, d, e, f);                                                                       \
+  }                                                                                                      \
+  extern "C" void oracle_wall_function_##S(const T *it, const T *dX, const T *dY, int x, int y, int z,  \
+                                           int nw, const int *wall, const T *u, const T *v, const T *w, \
+                                           T *Fx, T *Fy, const T *rho) {                                 \
+    o_wall_function<T>(it, dX, dY, x, y, z, nw, wall, u, v, w, Fx, Fy, rho);                            \
+  }                                                                                                      \
+  extern "C" void oracle_Force_##S(const T *it, int bf, const int *nb, const T *f, const T *feq,        \
+                                   const T *tau, T *Fk, T *Fx, T *Fy, T *Fz, const T *p, const T *rho,   \
+                                   const T *sal, const T *phi, const T *u, const T *v, const T *w,       \
+                                   const T *dX, const T *dY, const T *px, const T *py, const T *pz) {    \
+    o_Force<T>(it, bf, nb, f, feq, tau, Fk, Fx, Fy, Fz, p, rho, sal, phi, u, v, w, dX, dY, px, py, pz);  \
+  }                                                                                                      \
+  extern "C" void oracle_col_f_MRT_##S(const T *it, const T *tau, T *f, T *ftmp, T *feq, const T *Fk,   \
+                                       const T *M, const T *Mi, const T *Sv, const T *MM) {             \
+    o_col_f_MRT<T>(it, tau, f, ftmp, feq, Fk, M, Mi, Sv, MM);                                           \
+  }                                                                                                      \
+  extern "C" void oracle_col_f_SRT_##S(const T *it, const T *tau, T *f, T *ftmp, T *feq,                \
+                                       const T *Fk) {                                                   \
+    o_col_f_SRT<T>(it, tau, f, ftmp, feq, Fk);                                                          \
+  }                                                                                                      \
+  extern "C" void oracle_col_g_reg_##S(const T *it, const T *taus, T *g, T *gtmp, T *geq, const T *s,   \
+                                       const T *u, const T *v, const T *w) {                            \
+    o_col_g_reg<T>(it, taus, g, gtmp, geq, s, u, v, w);                                                 \
+  }                                                                                                      \
+  extern "C" void oracle_col_PF_##S(const T *it, const int *nb, const T *taus, T *g, T *gtmp, T *geq,   \
+                                    const T *phi, const T *u, const T *v, const T *w, T *po, T *uo,     \
+                                    T *vo, T *wo, const T *px, const T *py, const T *pz) {              \
+    o_col_PF<T>(it, nb, taus, g, gtmp, geq, phi, u, v, w, po, uo, vo, wo, px, py, pz);                  \
+  }                                                                                                      \
+  extern "C" void oracle_update_scalar_##S(const T *it, const T *g, T *s) { o_update_scalar<T>(it, g, s); } \
+  extern "C" void oracle_update_rho_##S(const T *it, T rl, T rh, const T *f, const T *Fx, const T *Fy,  \
+                                        const T *Fz, T *p, const T *sal, const T *phi, T *rho, T *u,    \
+                                        T *v, T *w) {                                                   \
+    o_update_rho<T>(it, rl, rh, f, Fx, Fy, Fz, p, sal, phi, rho, u, v, w);                              \
+  }                                                                                                      \
+  extern "C" void oracle_resetF_##S(const T *it, T *a, T *b, T *c, int n) { o_resetF<T>(it, a, b, c, n); } \
+  extern "C" void oracle_set_wall_f_##S(const T *it, const int *nb, T *f) { o_set_wall_f<T>(it, nb, f); }  \
+  extern "C" void oracle_set_out_##S(const T *it, const int *nb, const T *ftmp, T *fout, T *fin, T *finy, \
+                                     const T *px, const T *py, const T *dX, const T *dY) {              \
+    o_set_out<T>(it, nb, ftmp, fout, fin, finy, px, py, dX, dY);                                        \
+  }                                                                                                      \
+  extern "C" void oracle_set_fin_##S(const T *it, const int *nb, const int *nk, T *fin, T *finy) {      \
+    o_set_fin<T>(it, nb, nk, fin, finy);                                                                \
+  }                                                                                                      \
+  extern "C" void oracle_reset_f_##S(const T *it, const T *ftmp, T *fin, T *f) { o_reset_f<T>(it, ftmp, fin, f); } \
+  extern "C" void oracle_set_wall_f_inv_##S(const T *it, const int *nb, const int *nB, const int *nK,    \
+                                            T *f) {                                                     \
+    o_set_wall_f_inv<T>(it, nb, nB, nK, f);                                                             \
+  }                                                                                                      \
+  extern "C" void oracle_set_tmp_##S(const T *it, const int *nb, const T *f, T *ftmp, const T *fout,     \
+                                     const T *fin) {                                                    \
+    o_set_tmp<T>(it, nb, f, ftmp, fout, fin);                                                           \
+  }                                                                                                      \
+  extern "C" void oracle_set_wall_propagation_##S(const T *it, int bc, const int *nb, const int *nK,     \
+                                                  const int *nB, T *ftmp) {                             \
+    o_set_wall_propagation<T>(it, bc, nb, nK, nB, ftmp);                                                \
+  }                                                                                                      \
+  extern "C" void oracle_propagation_##S(const T *it, const int *nb, T *f, const T *ftmp) {             \
+    o_propagation<T>(it, nb, f, ftmp);                                                                  \
+  }                                                                                                      \
+  extern "C" void oracle_reset_wall_fin_##S(const T *it, T *fin, T *finy) { o_reset_wall_fin<T>(it, fin, finy); } \
+  extern "C" void oracle_set_wall_rho_##S(const T *it, const int *nb, T *rho) { o_set_wall_rho<T>(it, nb, rho); } \
+  extern "C" void oracle_IP_process_##S(const T *it, const int *nb, T *f, T *feq, T *ftmp, T *fout,      \
+                                        const int *nB, const int *nK, const T *px, const T *py,         \
+                                        const T *dX, const T *dY, int slip) {                           \
+    o_IP_process<T>(it, nb, f, feq, ftmp, fout, nB, nK, px, py, dX, dY, slip);                          \
+  }                                                                                                      \
+  extern "C" void oracle_reset_pressure_##S(const T *it, T *p, T *f, const T *u, const T *v, const T *w, \
+                                            T alpha) {                                                  \
+    o_reset_pressure<T>(it, p, f, u, v, w, alpha);                                                      \
+  }                                                                                                      \
+  extern "C" void oracle_LES_##S(const T *it, const int *nb, T *tau, T *taus, const T *phi, const T *rho, \
+                                 T muL, T muH, const T *u, const T *v, const T *w, const T *px,         \
+                                 const T *py, const T *pz) {                                            \
+    o_LES<T>(it, nb, tau, taus, phi, rho, muL, muH, u, v, w, px, py, pz);                               \
+  }                                                                                                      \
+  extern "C" void oracle_get_IBMGw2_##S(const T *it, const int *lid, const int *nb, const T *f,          \
+                                        const T *tau, const T *px, const T *py, const T *pz,            \
+                                        const T *posw, const T *posB, const T *nB, const T *u,          \
+                                        const T *v, const T *w, const T *velw, T *Fx, T *Fy, T *Fz,     \
+                                        T *Gw, T rhof) {                                                \
+    o_get_IBMGw2<T>(it, lid, nb, f, tau, px, py, pz, posw, posB, nB, u, v, w, velw, Fx, Fy, Fz, Gw, rhof); \
+  }                                                                                                      \
+  extern "C" void oracle_update_velIBM_##S(const T *it, const int *lid, T *f, const T *ftmp, T *p,       \
+                                           const T *tau, T *u, T *v, T *w, const T *uo, const T *vo,    \
+                                           const T *wo, const T *Fx, const T *Fy, const T *Fz) {         \
+    o_update_velIBM<T>(it, lid, f, ftmp, p, tau, u, v, w, uo, vo, wo, Fx, Fy, Fz);                      \
+  }                                                                                                      \
+  extern "C" void oracle_update_IBbody_##S(const T *it, int ib, const T *massB, const T *densB,          \
+                                           const T *inertia, T *FB, T *posB, T *Tq, T *velB, T *quat,   \
+                                           T *quaS, T *angleVB, const T *posw, const T *Gw, T *quatold, \
+                                           T rhof) {                                                    \
+    o_update_IBbody<T>(it, ib, massB, densB, inertia, FB, posB, Tq, velB, quat, quaS, angleVB, posw, Gw, \
+                       quatold, rhof);                                                                  \
+  }                                                                                                      \
+  extern "C" void oracle_update_IBpoint_##S(const T *it, int ib, const T *posB, const T *velB,           \
+                                            const T *om, const T *R, T *posw, const T *op, T *nB,       \
+                                            const T *onB, T *velw) {                                    \
+    o_update_IBpoint<T>(it, ib, posB, velB, om, R, posw, op, nB, onB, velw);                            \
+  }                                                                                                      \
+  extern "C" void oracle_search_IBlattice_##S(const T *it, int ib, int *lid, const int *nb, const T *px,  \
+                                              const T *py, const T *pz, const T *posw) {                \
+    o_search_IBlattice<T>(it, ib, lid, nb, px, py, pz, posw);                                           \
+  }                                                                                                      \
+  extern "C" void oracle_SPM_##S(const T *it, T R, const T *posB, T *f, T *ftmp, const T *tau,           \
+                                 const T *px, const T *py, T *Fx, T *Fy, T *Fz, const T *u, const T *v,  \
+                                 const T *w, const T *velw) {                                           \
+    o_SPM<T>(it, R, posB, f, ftmp, tau, px, py, Fx, Fy, Fz, u, v, w, velw);                             \
+  }
+ORACLE_BOTH(DEF)
+#undef DEF
+
+extern "C" void oracle_IB_directForcing_f32(const float *it, const int *lid, const int *nb, const float *px,
+                                            const float *py, const float *pz, const float *posw,
+                                            const float *u, const float *v, const float *w,
+                                            const float *velw, float *Fx, float *Fy, float *Fz,
+                                            float *Gw) {
+  o_IB_directForcing(it, lid, nb, px, py, pz, posw, u, v, w, velw, Fx, Fy, Fz, Gw);
+}
