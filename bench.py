@@ -36,15 +36,11 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-INNER = 100
+INNER = 1000
 METRIC = "MLUPS"
 
 
-def env_int(k, d):
-    try:
-        return int(os.environ.get(k, d))
-    except ValueError:
-        return d
+from ip_cu_lbm_b200.replicas import env_int  # noqa: E402
 
 
 class Clocks:
@@ -59,8 +55,8 @@ class Clocks:
              "clocks_event_reasons.sw_power_cap")
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
-                                          "--format=csv,noheader,nounits", "-lms", "100"],
-                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
         except OSError:
@@ -71,7 +67,12 @@ class Clocks:
         for line in self.proc.stdout:
             parts = [p.strip() for p in line.split(",")]
             if len(parts) >= 7:
-                self.samples.append(parts)
+                self.samples.append((time.perf_counter(), parts))
+
+    def window(self, t0, t1):
+        """Keep the samples taken between t0 and t1 (the timed region)."""
+        inside = [s for s in self.samples if t0 <= s[0] <= t1]
+        self.kept = inside if inside else self.samples[-1:]
 
     def __exit__(self, *a):
         if self.proc:
@@ -82,14 +83,21 @@ class Clocks:
                 self.proc.kill()
 
     def summary(self):
-        if not self.samples:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
-        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        samples = [p for _, p in getattr(self, "kept", self.samples)]
+        if not samples:
+            err = ""
+            if self.proc is not None and self.proc.stderr is not None:
+                try:
+                    err = self.proc.stderr.read()[:200]
+                except Exception:
+                    pass
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "error": err}
+        sm = [float(s[0]) for s in samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in samples if s[1].replace(".", "").isdigit()]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for s in self.samples for i in range(4) if s[3 + i].lower() == "active"})
+        reasons = sorted({names[i] for s in samples for i in range(4) if s[3 + i].lower() == "active"})
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(self.samples)}
+                "reasons": reasons, "samples": len(samples)}
 
 
 def load_peaks():
@@ -98,43 +106,6 @@ def load_peaks():
         d = json.load(open(p))
         return float(d["hbm_gbs"]), "measured"
     return 6650.0, "fallback"
-
-
-def dist_setup(n_gpus):
-    import torch
-
-    rank, world = env_int("RANK", 0), env_int("WORLD_SIZE", 1)
-    local = env_int("LOCAL_RANK", 0)
-    torch.cuda.set_device(local)
-    pg = None
-    if world > 1:
-        import datetime
-
-        import torch.distributed as dist
-
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                device_id=torch.device("cuda", local))
-        pg = dist
-    return rank, world, local, pg
-
-
-def barrier_sync(pg):
-    import torch
-
-    torch.cuda.synchronize()
-    if pg is not None:
-        pg.barrier()
-    torch.cuda.synchronize()
-
-
-def max_over_ranks(pg, v):
-    import torch
-
-    if pg is None:
-        return v
-    t = torch.tensor([v], dtype=torch.float64, device="cuda")
-    pg.all_reduce(t, op=pg.ReduceOp.MAX)
-    return float(t.item())
 
 
 def cpu_baseline(params, S0, meta, budget_s=12.0):
@@ -164,8 +135,10 @@ def run_ours(args):
     import torch
 
     from ip_cu_lbm_b200 import Sim, workloads
+    from ip_cu_lbm_b200.replicas import Replicas
 
-    rank, world, local, pg = dist_setup(args.gpus)
+    R = Replicas("nccl")
+    rank, world, local = R.rank, R.world, R.local
     params, S0, meta = workloads.stratified_nonuniform(storage=args.storage)
     dev = torch.device("cuda", local)
     stream = torch.cuda.current_stream(dev)
@@ -173,21 +146,24 @@ def run_ours(args):
     N = sim.N
     inner = args.inner
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
-    for w in range(args.warmup):
-        flush.fill_(float(w))
-        sim.step_graph(inner, chunk=inner)
-    barrier_sync(pg)
-    times = []
+    chunk = min(inner, 200)
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     with Clocks(local) as clk:
+        time.sleep(0.3)  # let the sampler start
+        for w in range(args.warmup):
+            flush.fill_(float(w))
+            sim.step_graph(inner, chunk=chunk)
+        R.barrier()
+        t_start = time.perf_counter()
         for k in range(args.steps):
             flush.fill_(float(k))  # L2 flush between timed steps (not timed)
             ev[k][0].record(stream)
-            sim.step_graph(inner, chunk=inner)
+            sim.step_graph(inner, chunk=chunk)
             ev[k][1].record(stream)
-        barrier_sync(pg)
+        R.barrier()
+        clk.window(t_start, time.perf_counter())
     times = [a.elapsed_time(b) for a, b in ev]
-    total_ms = max_over_ranks(pg, sum(times))
+    total_ms = R.max(sum(times))
     assert sim.status() == 0, "non-finite state"
     value = world * N * inner * args.steps / (total_ms / 1e3) / 1e6
     launch_ms = total_ms / (args.steps * inner)
@@ -205,15 +181,15 @@ def run_ours(args):
     sim.download(hf, hg, hm)
     sim.sync()
     e2e_steps = max(3, args.steps)
-    barrier_sync(pg)
+    R.barrier()
     t0 = time.perf_counter()
     for k in range(e2e_steps):
         sim.upload(hf, hg, hm)
-        sim.step_graph(inner, chunk=inner)
+        sim.step_graph(inner, chunk=chunk)
         sim.download(None, None, hm)
         sim.sync()
-    barrier_sync(pg)
-    e2e_s = max_over_ranks(pg, time.perf_counter() - t0)
+    R.barrier()
+    e2e_s = R.max(time.perf_counter() - t0)
     e2e = world * N * inner * e2e_steps / e2e_s / 1e6
 
     line = {
@@ -243,8 +219,7 @@ def run_ours(args):
     if rank == 0:
         print(json.dumps(line), flush=True)
     sim.close()
-    if pg is not None:
-        pg.destroy_process_group()
+    R.close()
 
 
 def run_reference(args):
@@ -310,6 +285,7 @@ def run_reference(args):
     torch.cuda.synchronize()
     total = 0.0
     with Clocks(dev.index or 0) as clk:
+        t_start = time.perf_counter()
         for k in range(args.steps):
             flush.fill_(float(k))
             torch.cuda.synchronize()
@@ -319,6 +295,7 @@ def run_reference(args):
             e1.record()
             torch.cuda.synchronize()
             total += e0.elapsed_time(e1)
+        clk.window(t_start, time.perf_counter())
     value = nc * INNER * args.steps / (total / 1e3) / 1e6
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": round(value, 2), "unit": METRIC, "n_gpus": 1,

@@ -125,3 +125,66 @@ def compact_to_grid(case, a):
 
 def grid_to_compact(case, g):
     return np.asarray(g).T.reshape(-1).copy()
+
+
+def ellipse_points(n, a=1.0, b=0.5, samples=10000):
+    """n points at equal arc length on the ellipse (a cos t, b sin t),
+    starting at t = 0 (the marker layout of the reference's ellipse case,
+    EllipticalFall2/make_ellipce.py): the arc length is accumulated on a fine
+    parameter grid and inverted by linear interpolation."""
+    t = np.linspace(0.0, 2 * np.pi, samples)
+    ds = np.hypot(-a * np.sin(t), b * np.cos(t))
+    s = np.cumsum(ds) * (2 * np.pi / samples)
+    s -= s[0]
+    target = np.linspace(0.0, s[-1], n, endpoint=False)
+    tt = np.interp(target, s, t)
+    return np.stack([a * np.cos(tt), np.zeros(n), b * np.sin(tt)], axis=1)
+
+
+def quat_rot(q):
+    q0, q1, q2, q3 = q
+    return np.array([[q0 * q0 - q2 * q2 - q3 * q3 + q1 * q1, 2 * (q1 * q2 - q0 * q3), 2 * (q1 * q3 + q0 * q2)],
+                     [2 * (q1 * q2 + q0 * q3), q0 * q0 - q3 * q3 - q1 * q1 + q2 * q2, 2 * (q2 * q3 - q0 * q1)],
+                     [2 * (q1 * q3 - q0 * q2), 2 * (q2 * q3 + q0 * q1), q0 * q0 - q1 * q1 - q2 * q2 + q3 * q3]])
+
+
+def ibm_ellipse_case(nx0=40, nz=60, n_markers=24, dx=1e-3, dt=1e-3, tilt_deg=45.0, rho_ratio=1.1, rhoH=1000.0,
+                     nu=1e-6, center=(0.5, 0.5), prec="f32", a_frac=1 / 8):
+    """Settling-ellipse case in the reference driver's set-up
+    (ref: EllipticalFall2/EllipticalFallxz.cu:45-46,188-256): semi-axes
+    a = H/8, b = a/2 with H = nx*dx, markers at equal arc length, body
+    rotated about y by the tilt, radial marker normals (2x, 0, 2z)/|.|,
+    mass and inertia of the 2-D ellipse, each marker's lattice cell the
+    nearest fluid cell. Returns (case, body) with host arrays."""
+    c = box_case(Q=9, nx0=nx0, nz=nz, dx=dx, dt=dt, prec=prec, n_ib=n_markers, nu=nu)
+    dtp = c["dtype"]
+    H = dx * nx0
+    a = H * a_frac
+    b = a / 2
+    op = ellipse_points(n_markers, 1.0, 0.5) * a
+    ang = np.deg2rad(tilt_deg) / 2
+    q = np.array([np.cos(ang), 0.0, np.sin(ang), 0.0])
+    R = quat_rot(q)
+    posB = np.array([center[0] * nx0 * dx, dx * 1 / 2.0, center[1] * nz * dx])
+    onB = np.stack([2 * op[:, 0], np.zeros(n_markers), 2 * op[:, 2]], axis=1)
+    onB /= np.linalg.norm(onB, axis=1)[:, None]
+    posw = posB[None, :] + op @ R.T
+    nB = onB @ R.T
+    length = np.sum(np.hypot(np.diff(op[:, 0]), np.diff(op[:, 2])))
+    nc = c["nc"]
+    P = np.stack([c["posx"][:nc], c["posy"][:nc], c["posz"][:nc]], axis=1).astype(np.float64)
+    lid = np.array([int(np.argmin(np.linalg.norm(P - pw[None, :], axis=1))) for pw in posw], np.int32)
+    densB = rho_ratio * rhoH
+    massB = densB * a * b * np.pi
+    inertia = np.full(3, massB * (a * a + b * b) / 4)
+    items = c["items"].astype(np.float64)
+    items[IDX["num_IBPoints"]] = n_markers
+    items[IDX["dIBM"]] = length / n_markers
+    c["items"] = items.astype(dtp)
+    c["n_ib"] = n_markers
+    f32 = lambda v: np.ascontiguousarray(v, dtype=dtp).ravel()
+    body = dict(lid=lid, massB=f32([massB]), densB=f32([densB]), inertia=f32(inertia), FB=f32(np.zeros(3)),
+                posB=f32(posB), Torque=f32(np.zeros(3)), velB=f32(np.zeros(3)), quat=f32(q), quaS=f32(R.ravel()),
+                angleVB=f32(np.zeros(3)), posw=f32(posw), oposw=f32(op), Gw=f32(np.zeros(3 * n_markers)),
+                velw=f32(np.zeros(3 * n_markers)), nB=f32(nB), onB=f32(onB), quatold=f32(q))
+    return c, body

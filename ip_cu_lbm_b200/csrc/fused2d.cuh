@@ -8,13 +8,14 @@
 namespace ipcu {
 namespace f2d {
 
-constexpr int kTX = 64;  // tile width along x (two warps per row)
-constexpr int kTZ = 8;   // tile height along z
+constexpr int kTX = 32;  // tile width along x (one warp per row)
+constexpr int kTZ = 16;  // tile height along z
 constexpr int kThreads = 256;
+constexpr int kMinBlocks = 4;  // resident CTAs per SM the register budget is sized for
 
 struct Params {
   int nx, nz;
-  int mrt, wall;
+  int mrt, wall;  // mrt: 0 BGK, 1 general MRT, 2 MRT with unit non-shear rates (two-moment form)
   const void *f_in;
   void *f_out;
   const void *g_in;

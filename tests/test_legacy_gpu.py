@@ -14,9 +14,10 @@ from helpers import gpu_chain, mrt_mats, oracle_chain, random_state, rel_l2
 pytestmark = pytest.mark.gpu
 
 CASES = {
-    "q9": dict(Q=9, nx0=10, nz=7, divx=[1, 1, 2, 3, 1, 1, 2, 1, 1, 1], dx=1.0, dt=1.0),
+    "q9": dict(Q=9, nx0=10, nz=7, divx=[1, 1, 2, 4, 1, 1, 2, 1, 1, 1], ratiox=4.0, dx=1.0, dt=1.0),
     "q9u": dict(Q=9, nx0=12, nz=6, dx=1.0, dt=1.0),
-    "q27": dict(Q=27, nx0=5, ny0=4, nz=5, divx=[1, 2, 2, 1, 1], divy=[1, 2, 1, 1], dx=1.0, dt=1.0),
+    "q27": dict(Q=27, nx0=5, ny0=4, nz=5, divx=[1, 2, 4, 1, 1], divy=[1, 2, 1, 1], ratiox=4.0, ratioy=2.0,
+                dx=1.0, dt=1.0),
 }
 
 # name, arguments (buffer keys or literal scalars), outputs
