@@ -188,6 +188,35 @@ int64_t ipcu_build_box_grid(int Q, int nx0, int ny0, int nz, double dx, double r
                             const int *divx, const int *divy, int *lnum, int *neib, double *posx, double *posy,
                             double *posz, double *delX, double *delY);
 
+/* ---------------------------------------------------------------------
+ * Device geometry set-up (all array pointers are DEVICE pointers; divx and
+ * divy are host arrays). Replaces the case drivers' host loops.
+ * --------------------------------------------------------------------- */
+/* LockExchange/LockExchange.cu:55-127 + basic.cu:203-237 on the GPU: box
+ * numbering lnum[NX*NY*nz], neighbour table neib[cap*Q] with one ghost per
+ * open cell (ghost numbering in the reference's scan order), cell geometry
+ * pos*, del* (cap entries; ghosts copy their owner), owner[num_wall].
+ * Returns IPCU_ERR_CAPACITY when num_calc + num_wall > cap. Synchronises
+ * `stream`; allocates small temporaries. */
+int ipcu_build_box_device_f32(int Q, int nx0, int ny0, int nz, double dx, double ratiox, double ratioy,
+                              const int *divx, const int *divy, int *lnum, int *neib, float *posx, float *posy,
+                              float *posz, float *delX, float *delY, int64_t cap, int *owner, int64_t *num_calc,
+                              int64_t *num_wall, ipcu_stream_t stream);
+int ipcu_build_box_device_f64(int Q, int nx0, int ny0, int nz, double dx, double ratiox, double ratioy,
+                              const int *divx, const int *divy, int *lnum, int *neib, double *posx, double *posy,
+                              double *posz, double *delX, double *delY, int64_t cap, int *owner,
+                              int64_t *num_calc, int64_t *num_wall, ipcu_stream_t stream);
+/* SphereFallSuzuki2018/SphereSuzuki.cu:268-275: lattice_id[m] = the fluid
+ * cell (index < num_calc) nearest marker m (posw[3m..3m+2]); first index
+ * among equal distances. Asynchronous on `stream`. */
+int ipcu_nearest_cells_f32(const float *posx, const float *posy, const float *posz, int64_t num_calc,
+                           const float *posw, int num_markers, int *lattice_id, ipcu_stream_t stream);
+int ipcu_nearest_cells_f64(const double *posx, const double *posy, const double *posz, int64_t num_calc,
+                           const double *posw, int num_markers, int *lattice_id, ipcu_stream_t stream);
+
+/* pybind_LockExchange/kernel.cu:4-17 (the prototype's kernel): data[i] += value */
+int ipcu_add_scalar_f32(float *data, int64_t n, float value, ipcu_stream_t stream);
+
 /* ======================================================================
  * 2. Structured-grid solver (fused B200 path)
  * ====================================================================== */

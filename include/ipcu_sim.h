@@ -84,6 +84,15 @@ int ipcu_sim_status(ipcu_sim *sim, uint32_t *flags);
 int ipcu_sim_upload(ipcu_sim *sim, const void *f, const void *g, const float *mac);
 int ipcu_sim_download(ipcu_sim *sim, void *f, void *g, float *mac);
 int ipcu_sim_sync(ipcu_sim *sim);
+/* Time steps taken since creation or restore. */
+int64_t ipcu_sim_steps(const ipcu_sim *sim);
+/* Versioned binary snapshot (configuration, geometry, MRT matrices, step
+ * count, raw state) and its restore into a new simulation; a restored run
+ * continues bit-identically (replaces basic.cu:31-56 save_status). */
+int ipcu_sim_save(ipcu_sim *sim, const char *path);
+int ipcu_sim_load(const char *path, ipcu_stream_t stream, ipcu_sim **out);
+/* Field CSV in the reference's column order and cell order (basic.cu:16-28). */
+int ipcu_sim_write_csv(ipcu_sim *sim, const char *path);
 /* Bytes of one stored distribution value (4 FP32, 2 FP16/BF16). */
 int32_t ipcu_sim_storage_bytes(const ipcu_sim *sim);
 int64_t ipcu_sim_cells(const ipcu_sim *sim);
@@ -94,5 +103,18 @@ int64_t ipcu_sim_bytes_per_cell(const ipcu_sim *sim);
 /* FP64 domain sums of S and p* weighted by cell area (dx*dz/dz^2), the
  * reference's conservation diagnostic (ref: function/basic.cu:9-15). */
 int ipcu_sim_totals(ipcu_sim *sim, double *sum_p, double *sum_s);
+
+/* Batched stepping of many resident simulations (continuous-batching
+ * serving): each call advances every listed simulation by nsteps with one
+ * launch per step per kernel class (storage, scalar lattice, geometry); CTAs
+ * walk a device work list of (simulation, tile). A simulation's arithmetic is
+ * the same tile by tile as when it runs alone. Synchronous; the simulations'
+ * own streams must be idle. */
+typedef struct ipcu_batch ipcu_batch;
+int ipcu_batch_create(ipcu_stream_t stream, ipcu_batch **out);
+void ipcu_batch_destroy(ipcu_batch *batch);
+int ipcu_batch_step(ipcu_batch *batch, ipcu_sim *const *sims, int n, int64_t nsteps);
+/* Device bytes a simulation holds (state, ping-pong, tables). */
+int64_t ipcu_sim_device_bytes(const ipcu_sim *sim);
 
 #endif /* IPCU_SIM_H */

@@ -106,6 +106,21 @@ def _declare(L: ctypes.CDLL) -> None:
         "ipcu_sim_download": ([P, P, P, P], I),
         "ipcu_sim_sync": ([P], I),
         "ipcu_sim_storage_bytes": ([P], ctypes.c_int32),
+        "ipcu_sim_steps": ([P], I64),
+        "ipcu_sim_save": ([P, ctypes.c_char_p], I),
+        "ipcu_sim_load": ([ctypes.c_char_p, P, ctypes.POINTER(P)], I),
+        "ipcu_sim_write_csv": ([P, ctypes.c_char_p], I),
+        "ipcu_add_scalar_f32": ([P, I64, ctypes.c_float, P], I),
+        "ipcu_batch_create": ([P, ctypes.POINTER(P)], I),
+        "ipcu_batch_destroy": ([P], None),
+        "ipcu_batch_step": ([P, P, I, I64], I),
+        "ipcu_sim_device_bytes": ([P], I64),
+        "ipcu_build_box_device_f32": ([I, I, I, I, D, D, D, P, P, P, P, P, P, P, P, P, I64, P,
+                                       ctypes.POINTER(I64), ctypes.POINTER(I64), P], I),
+        "ipcu_build_box_device_f64": ([I, I, I, I, D, D, D, P, P, P, P, P, P, P, P, P, I64, P,
+                                       ctypes.POINTER(I64), ctypes.POINTER(I64), P], I),
+        "ipcu_nearest_cells_f32": ([P, P, P, I64, P, I, P, P], I),
+        "ipcu_nearest_cells_f64": ([P, P, P, I64, P, I, P, P], I),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)

@@ -116,6 +116,49 @@ def box_case(Q=9, nx0=16, nz=8, ny0=1, divx=None, divy=None, dx=1.0, dt=1.0, rat
                 lnum=lnum, c=c, tau=tau, taus=taus, w=w, cx=cx, cy=cy, cz=cz, dtype=dtype)
 
 
+def box_grid_device(Q=9, nx0=16, nz=8, ny0=1, divx=None, divy=None, dx=1.0, ratiox=1.0, ratioy=1.0,
+                    prec="f32", device="cuda", stream=None):
+    """Box numbering, neighbour table with ghosts and cell geometry built on
+    the GPU (ipcu_build_box_device_*); the same arrays as box_case's host
+    path, as torch tensors on `device`."""
+    import torch
+
+    L = _lib.lib()
+    tdt = torch.float32 if prec == "f32" else torch.float64
+    divx = np.asarray(divx if divx is not None else [1] * nx0, np.int32)
+    divy = np.asarray(divy if divy is not None else [1] * ny0, np.int32)
+    NX, NY = int(divx.sum()), int(divy.sum())
+    ncell = NX * NY * nz
+    cap = 2 * ncell + 8
+    lnum = torch.empty(ncell, dtype=torch.int32, device=device)
+    neib = torch.empty(cap * Q, dtype=torch.int32, device=device)
+    owner = torch.empty(cap, dtype=torch.int32, device=device)
+    geo = [torch.empty(cap, dtype=tdt, device=device) for _ in range(5)]
+    nc, nw = ctypes.c_int64(), ctypes.c_int64()
+    fn = getattr(L, f"ipcu_build_box_device_{prec}")
+    _lib.check(fn(Q, len(divx), len(divy), nz, dx, ratiox, ratioy, divx.ctypes.data, divy.ctypes.data,
+                  lnum.data_ptr(), neib.data_ptr(), *[g.data_ptr() for g in geo], cap, owner.data_ptr(),
+                  ctypes.byref(nc), ctypes.byref(nw), stream), "ipcu_build_box_device")
+    nt = nc.value + nw.value
+    posx, posy, posz, delX, delY = (g[:nt] for g in geo)
+    return dict(Q=Q, nc=nc.value, nw=nw.value, nt=nt, NX=NX, NY=NY, nz=nz, lnum=lnum, neib=neib[: nt * Q],
+                owner=owner[: nw.value], posx=posx, posy=posy, posz=posz, delX=delX, delY=delY)
+
+
+def nearest_cells(posx, posy, posz, num_calc, posw, stream=None):
+    """lattice_id of each marker (posw: [n, 3] device tensor) on the GPU."""
+    import torch
+
+    prec = "f32" if posx.dtype == torch.float32 else "f64"
+    posw = posw.contiguous()
+    n = posw.numel() // 3
+    lid = torch.empty(n, dtype=torch.int32, device=posw.device)
+    _lib.check(getattr(_lib.lib(), f"ipcu_nearest_cells_{prec}")(
+        posx.data_ptr(), posy.data_ptr(), posz.data_ptr(), int(num_calc), posw.data_ptr(), n, lid.data_ptr(),
+        stream), "ipcu_nearest_cells")
+    return lid
+
+
 def compact_to_grid(case, a):
     """Fluid values of a 2-D (ny=1) case in compact x-major/z-fastest order ->
     [nz, nx] array (x fastest), the structured solver's layout."""

@@ -81,3 +81,20 @@ extern "C" const char *ipcu_status_string(int code) {
 }
 
 extern "C" const char *ipcu_last_cuda_error(void) { return cudaGetErrorString(cudaPeekAtLastError()); }
+
+// The pybind prototype's kernel: add a constant to every element
+// (ref: pybind_LockExchange/kernel.cu:4-9, which adds 5.0f).
+namespace {
+__global__ void k_add_scalar(float *d, long long n, float v) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    d[i] += v;
+}
+}  // namespace
+
+extern "C" int ipcu_add_scalar_f32(float *data, int64_t n, float value, ipcu_stream_t stream) {
+  if (n < 0 || (n > 0 && !data)) return IPCU_ERR_ARG;
+  if (n == 0) return IPCU_OK;
+  ipcu::Launch L = ipcu::launch_for(n);
+  k_add_scalar<<<L.grid, L.block, 0, (cudaStream_t)stream>>>(data, n, value);
+  return ipcu::status_from_cuda(cudaGetLastError());
+}

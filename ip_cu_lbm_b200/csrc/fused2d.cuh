@@ -16,12 +16,11 @@ constexpr int kMinBlocks = 4;  // resident CTAs per SM the register budget is si
 struct Params {
   int nx, nz;
   int mrt, wall;  // mrt: 0 BGK, 1 general MRT, 2 MRT with unit non-shear rates (two-moment form)
-  const void *f_in;
-  void *f_out;
-  const void *g_in;
-  void *g_out;
-  const float *mac_in;  // [3][N]: S, ux, uz
-  float *mac_out;
+  // ping-pong state; a step reads buffer (cur ^ parity) and writes the other
+  void *fbuf[2];
+  void *gbuf[2];
+  float *mbuf[2];  // [3][N]: S, ux, uz
+  int cur;
   // interpolated axis: weights [2][NA][NS], fin scale [2][NA], fout scale [NA]
   const float *wA, *scin, *scout;
   // 1/(x_{i+1} - x_{i-1} + dz/1000) with clamped neighbours (density gradient)
@@ -40,6 +39,17 @@ struct Params {
 
 // prepare_only: set the kernel's shared-memory attribute (call once before any capture)
 int launch_step(const Params &p, int storage, int qs, int geo, cudaStream_t s, bool prepare_only = false);
+
+// One work item of a batched step: simulation index and tile coordinates.
+struct WorkItem {
+  int sim, tx, tz, pad;
+};
+// Advances every simulation referenced by `work` (all of the same storage,
+// scalar lattice and geometry) by one step; `params` and `work` are device
+// arrays; `parity` flips the ping-pong buffers of all of them. `grid` CTAs
+// loop over the work list.
+int launch_batched(const Params *params, const WorkItem *work, int nwork, int parity, int storage, int qs, int geo,
+                   int grid, cudaStream_t s, bool prepare_only = false);
 
 }  // namespace f2d
 }  // namespace ipcu

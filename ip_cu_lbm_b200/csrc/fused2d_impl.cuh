@@ -69,10 +69,25 @@ struct Geo {
   static constexpr int WREC = NS + 2;             // NS weights, fin scale, fout scale
 };
 
+// FP32 storage stages the raw tile (f, g, u_x, u_z) into shared memory with
+// asynchronous copies before colliding it in place; reduced-precision storage
+// loads through registers (cp.async moves 4, 8 or 16 bytes, not 2).
+template <class ST>
+constexpr bool kStageAsync = sizeof(ST) == 4;
+
 template <class ST, int QS, int GEO>
 constexpr size_t smem_bytes() {
   using G = Geo<GEO>;
-  return sizeof(float) * ((9 + QS) * G::NE + 2 * G::SX * G::SZ + 2 * kTX * kTZ + 2 * G::NWA * G::WREC);
+  return sizeof(float) * ((9 + QS + (kStageAsync<ST> ? 2 : 0)) * G::NE + 2 * G::SX * G::SZ + 2 * kTX * kTZ +
+                          2 * G::NWA * G::WREC);
+}
+
+__device__ __forceinline__ void cp_async4(float *dst, const float *src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
 }
 
 // storage conversion: value = stored*inv_scale
@@ -129,35 +144,56 @@ struct Fast {
   }
 };
 
+// One tile of one step; shared by the single-simulation kernel (parameters in
+// the kernel's constant bank) and the batched kernel (parameters in global memory).
 template <class ST, int QS, int GEO>
-__global__ void __launch_bounds__(kThreads, kMinBlocks) step_kernel(const Params p) {
+__device__ __forceinline__ void step_tile(const Params &p, int parity, int tile_x, int tile_z, float *smem) {
   using G = Geo<GEO>;
   constexpr int HX = G::HX, HZ = G::HZ, EX = G::EX, NE = G::NE, SX = G::SX, SZ = G::SZ;
   constexpr int NWA = G::NWA, WREC = G::WREC;
-  extern __shared__ float smem[];
   float *sf = smem;                       // [9][EZ][EX] post-collision f
   float *sg = sf + 9 * NE;                // [QS][EZ][EX] post-collision g
   float *sS = sg + QS * NE;               // [SZ][SX] salinity
   float *sR = sS + SZ * SX;               // [SZ][SX] density
   float *sF = sR + SZ * SX;               // [2][kTZ][kTX] interior force
   float *sW = sF + 2 * kTX * kTZ;         // [2][WREC][NWA] axis weights
+  float *sU = sW + 2 * WREC * NWA;        // [2][EZ][EX] staged u_x, u_z (FP32 storage)
 
   const int nx = p.nx, nz = p.nz;
   const long long N = (long long)nx * nz;
-  const int x0 = blockIdx.x * kTX, z0 = blockIdx.y * kTZ;
+  const int x0 = tile_x * kTX, z0 = tile_z * kTZ;
   const int ox = x0 - HX, oz = z0 - HZ;  // global coords of local (0,0)
   const int tid = threadIdx.x;
-  const ST *__restrict__ f_in = static_cast<const ST *>(p.f_in);
-  const ST *__restrict__ g_in = static_cast<const ST *>(p.g_in);
-  ST *__restrict__ f_out = static_cast<ST *>(p.f_out);
-  ST *__restrict__ g_out = static_cast<ST *>(p.g_out);
-  const float *__restrict__ mac_in = p.mac_in;
+  const int bi = p.cur ^ parity, bo = bi ^ 1;
+  const ST *__restrict__ f_in = static_cast<const ST *>(p.fbuf[bi]);
+  const ST *__restrict__ g_in = static_cast<const ST *>(p.gbuf[bi]);
+  ST *__restrict__ f_out = static_cast<ST *>(p.fbuf[bo]);
+  ST *__restrict__ g_out = static_cast<ST *>(p.gbuf[bo]);
+  const float *__restrict__ mac_in = p.mbuf[bi];
+  float *__restrict__ mac_out = p.mbuf[bo];
 
   // density as the reference forms it: float base plus a double salinity
   // term, rounded once (ref: collision.cu:251)
   const float rho0 = p.rhoL + (p.rhoH - p.rhoL) * p.phi;
 
-  // ---- phase 0: salinity/density ring and the interpolation weights
+  // ---- phase 0: start the asynchronous copy of the raw tile + halo (FP32
+  // storage), then stage the salinity/density ring and the axis weights
+  if constexpr (kStageAsync<ST>) {
+    const float *fin32 = reinterpret_cast<const float *>(f_in);
+    const float *gin32 = reinterpret_cast<const float *>(g_in);
+    for (int e = tid; e < NE; e += kThreads) {
+      const int lz = e / EX, lx = e - lz * EX;
+      const int gx = ox + lx, gz = oz + lz;
+      if (gx < 0 || gx >= nx || gz < 0 || gz >= nz) continue;
+      const long long ci = (long long)gz * nx + gx;
+#pragma unroll
+      for (int k = 0; k < 9; k++) cp_async4(sf + k * NE + e, fin32 + k * N + ci);
+#pragma unroll
+      for (int k = 0; k < QS; k++) cp_async4(sg + k * NE + e, gin32 + k * N + ci);
+      cp_async4(sU + e, mac_in + N + ci);
+      cp_async4(sU + NE + e, mac_in + 2 * N + ci);
+    }
+  }
   for (int e = tid; e < SX * SZ; e += kThreads) {
     const int lz = e / SX, lx = e - lz * SX;
     const int gx = min(max(ox - 1 + lx, 0), nx - 1), gz = min(max(oz - 1 + lz, 0), nz - 1);
@@ -177,6 +213,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) step_kernel(const Params
       sW[e] = v;
     }
   }
+  if constexpr (kStageAsync<ST>) cp_async_wait_all();
   __syncthreads();
 
   const float c = p.c, c2 = c * c, ic = 1.0f / c, dt = p.dt;
@@ -189,14 +226,23 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) step_kernel(const Params
     const int lz = e / EX, lx = e - lz * EX;
     const int gx = ox + lx, gz = oz + lz;
     if (gx < 0 || gx >= nx || gz < 0 || gz >= nz) continue;
-    const long long ci = (long long)gz * nx + gx;
-    float f[9];
+    float f[9], g[QS > 0 ? QS : 1], u, w;
+    if constexpr (kStageAsync<ST>) {
 #pragma unroll
-    for (int k = 0; k < 9; k++) f[k] = ld(f_in, k * N + ci, ifs);
-    float g[QS > 0 ? QS : 1];
+      for (int k = 0; k < 9; k++) f[k] = sf[k * NE + e];
 #pragma unroll
-    for (int k = 0; k < QS; k++) g[k] = ld(g_in, k * N + ci, igs) + wq<QS>(k) * p.s_ref;
-    const float u = mac_in[N + ci], w = mac_in[2 * N + ci];
+      for (int k = 0; k < QS; k++) g[k] = sg[k * NE + e];
+      u = sU[e];
+      w = sU[NE + e];
+    } else {
+      const long long ci = (long long)gz * nx + gx;
+#pragma unroll
+      for (int k = 0; k < 9; k++) f[k] = ld(f_in, k * N + ci, ifs);
+#pragma unroll
+      for (int k = 0; k < QS; k++) g[k] = ld(g_in, k * N + ci, igs) + wq<QS>(k) * p.s_ref;
+      u = mac_in[N + ci];
+      w = mac_in[2 * N + ci];
+    }
     const int rs = (lz + 1) * SX + lx + 1;
     const float S = sS[rs], rho = sR[rs];
     // p* (ref: collision.cu:244-246)
@@ -386,11 +432,52 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) step_kernel(const Params
     const float rho = (float)((double)rho0 + (double)S * p.rho_sal);
     const float h = dt / (2.0f * rho);
     const float ux = c * jx + sF[e] * h, uz = c * jz + sF[kTX * kTZ + e] * h;
-    p.mac_out[ci] = S;
-    p.mac_out[N + ci] = ux;
-    p.mac_out[2 * N + ci] = uz;
+    mac_out[ci] = S;
+    mac_out[N + ci] = ux;
+    mac_out[2 * N + ci] = uz;
     if (!(isfinite(ux) && isfinite(uz) && isfinite(S) && isfinite(pr))) atomicOr(p.status, 1u);
   }
+}
+
+template <class ST, int QS, int GEO>
+__global__ void __launch_bounds__(kThreads, kMinBlocks) step_kernel(const __grid_constant__ Params p) {
+  extern __shared__ float smem[];
+  step_tile<ST, QS, GEO>(p, 0, blockIdx.x, blockIdx.y, smem);
+}
+
+template <class ST, int QS, int GEO>
+__global__ void __launch_bounds__(kThreads, kMinBlocks)
+    step_kernel_batched(const Params *__restrict__ ps, const WorkItem *__restrict__ work, int nwork, int parity) {
+  extern __shared__ float smem[];
+  for (int i = blockIdx.x; i < nwork; i += gridDim.x) {
+    const WorkItem w = work[i];
+    step_tile<ST, QS, GEO>(ps[w.sim], parity, w.tx, w.tz, smem);
+    __syncthreads();  // the next item reuses shared memory
+  }
+}
+
+template <class ST, int QS, int GEO>
+int launch_b(const Params *ps, const WorkItem *work, int nwork, int parity, int grid, cudaStream_t s, bool prep) {
+  constexpr size_t sm = smem_bytes<ST, QS, GEO>();
+  if (prep)
+    return status_from_cuda(cudaFuncSetAttribute(step_kernel_batched<ST, QS, GEO>,
+                                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  if (nwork <= 0) return IPCU_OK;
+  step_kernel_batched<ST, QS, GEO><<<grid, kThreads, sm, s>>>(ps, work, nwork, parity);
+  return status_from_cuda(cudaGetLastError());
+}
+
+template <class ST, int QS>
+int launch_bg(const Params *ps, const WorkItem *work, int nwork, int parity, int geo, int grid, cudaStream_t s,
+              bool prep) {
+  switch (geo) {
+    case IPCU_GEO_UNIFORM: return launch_b<ST, QS, IPCU_GEO_UNIFORM>(ps, work, nwork, parity, grid, s, prep);
+    case IPCU_GEO_X5: return launch_b<ST, QS, IPCU_GEO_X5>(ps, work, nwork, parity, grid, s, prep);
+    case IPCU_GEO_X3: return launch_b<ST, QS, IPCU_GEO_X3>(ps, work, nwork, parity, grid, s, prep);
+    case IPCU_GEO_Z5: return launch_b<ST, QS, IPCU_GEO_Z5>(ps, work, nwork, parity, grid, s, prep);
+    case IPCU_GEO_Z3: return launch_b<ST, QS, IPCU_GEO_Z3>(ps, work, nwork, parity, grid, s, prep);
+  }
+  return IPCU_ERR_UNSUPPORTED;
 }
 
 template <class ST, int QS, int GEO>

@@ -5,6 +5,7 @@
 #include <cuda_fp16.h>
 
 #include <algorithm>
+#include <tuple>
 #include <cmath>
 #include <cstring>
 #include <string>
@@ -32,6 +33,8 @@ struct ipcu_sim {
   cudaGraphExec_t graph[2] = {nullptr, nullptr};  // per starting parity
   int graph_chunk = 0;
   std::vector<double> X, Z, DX, DZ;
+  std::vector<double> M, Minv, Srates;  // MRT matrices as given (for snapshots)
+  long long steps = 0;                  // time steps taken since creation / restore
 };
 
 namespace {
@@ -257,6 +260,11 @@ extern "C" int ipcu_sim_create(const ipcu_sim_config *cfg, const double *s0, ipc
   s->stream = (cudaStream_t)stream;
   s->esz = c.storage == IPCU_STORE_F32 ? 4 : 2;
   const double dz = c.dz;
+  if (c.mrt) {
+    s->M.assign(c.M, c.M + 81);
+    s->Minv.assign(c.Minv, c.Minv + 81);
+    s->Srates.assign(c.S, c.S + 9);
+  }
   s->X.resize(c.nx);
   s->Z.resize(c.nz);
   s->DX.resize(c.nx);
@@ -381,6 +389,11 @@ extern "C" int ipcu_sim_create(const ipcu_sim_config *cfg, const double *s0, ipc
   slip_tables(9, P.slipB9, P.slipK9);
   slip_tables(5, P.slipB5, P.slipK5);
   P.status = s->status;
+  for (int i = 0; i < 2; i++) {
+    P.fbuf[i] = s->f[i];
+    P.gbuf[i] = s->g[i];
+    P.mbuf[i] = s->mac[i];
+  }
   st = f2d::launch_step(P, c.storage, c.q_scalar, c.geometry, s->stream, true);
   if (st != IPCU_OK) {
     free_sim(s);
@@ -409,14 +422,12 @@ extern "C" void ipcu_sim_destroy(ipcu_sim *sim) {
 
 static int launch_one(ipcu_sim *s) {
   f2d::Params P = s->P;
-  P.f_in = s->f[s->cur];
-  P.f_out = s->f[1 - s->cur];
-  P.g_in = s->g[s->cur];
-  P.g_out = s->g[1 - s->cur];
-  P.mac_in = s->mac[s->cur];
-  P.mac_out = s->mac[1 - s->cur];
+  P.cur = s->cur;
   int st = f2d::launch_step(P, s->cfg.storage, s->cfg.q_scalar, s->cfg.geometry, s->stream);
-  if (st == IPCU_OK) s->cur ^= 1;
+  if (st == IPCU_OK) {
+    s->cur ^= 1;
+    s->steps++;
+  }
   return st;
 }
 
@@ -460,12 +471,14 @@ extern "C" int ipcu_sim_step_graph(ipcu_sim *sim, int64_t nsteps, int32_t chunk)
       sim->stream = keep;
       cudaStreamDestroy(cs);
       sim->cur = par;  // capture does not execute
+      sim->steps -= chunk;
       if (st != IPCU_OK || e != cudaSuccess) return IPCU_ERR_CUDA;
       e = cudaGraphInstantiate(&sim->graph[par], gr, 0);
       cudaGraphDestroy(gr);
       if (e != cudaSuccess) return IPCU_ERR_CUDA;
     }
     if (cudaGraphLaunch(sim->graph[par], sim->stream) != cudaSuccess) return IPCU_ERR_CUDA;
+    sim->steps += chunk;
     left -= chunk;
   }
   return ipcu_sim_step(sim, left);
@@ -638,3 +651,239 @@ extern "C" int ipcu_sim_sync(ipcu_sim *s) {
 }
 
 extern "C" int32_t ipcu_sim_storage_bytes(const ipcu_sim *s) { return s ? (int32_t)s->esz : 0; }
+
+// ---------------------------------------------------------------------------
+// Checkpoint / restore: a versioned binary snapshot of the configuration,
+// the axis geometry, the MRT matrices, the step count and the raw state in
+// its storage format (replaces the reference's unused text save_status,
+// ref: function/basic.cu:31-56, which had no reader).
+namespace {
+constexpr char kMagic[8] = {'I', 'P', 'C', 'U', 'S', 'I', 'M', '1'};
+constexpr int32_t kSnapVersion = 1;
+template <class T>
+bool wr(FILE *f, const T *p, size_t n) { return fwrite(p, sizeof(T), n, f) == n; }
+template <class T>
+bool rd(FILE *f, T *p, size_t n) { return fread(p, sizeof(T), n, f) == n; }
+}  // namespace
+
+extern "C" int64_t ipcu_sim_steps(const ipcu_sim *s) { return s ? s->steps : -1; }
+
+extern "C" int ipcu_sim_save(ipcu_sim *s, const char *path) {
+  if (!s || !path) return IPCU_ERR_ARG;
+  if (cudaStreamSynchronize(s->stream) != cudaSuccess) return IPCU_ERR_CUDA;
+  const long long N = s->N;
+  const int q = s->cfg.q_scalar;
+  std::vector<unsigned char> fb(s->esz * 9 * N), gb(s->esz * (size_t)q * N);
+  std::vector<float> mb(3 * N);
+  if (cudaMemcpy(fb.data(), s->f[s->cur], fb.size(), cudaMemcpyDeviceToHost) != cudaSuccess) return IPCU_ERR_CUDA;
+  if (q && cudaMemcpy(gb.data(), s->g[s->cur], gb.size(), cudaMemcpyDeviceToHost) != cudaSuccess) return IPCU_ERR_CUDA;
+  if (cudaMemcpy(mb.data(), s->mac[s->cur], sizeof(float) * 3 * N, cudaMemcpyDeviceToHost) != cudaSuccess)
+    return IPCU_ERR_CUDA;
+  FILE *f = fopen(path, "wb");
+  if (!f) return IPCU_ERR_IO;
+  ipcu_sim_config c = s->cfg;
+  c.x = c.z = c.wx = c.wz = c.M = c.Minv = c.S = nullptr;
+  bool ok = wr(f, kMagic, 8) && wr(f, &kSnapVersion, 1) && wr(f, &c, 1) && wr(f, &s->steps, 1) &&
+            wr(f, s->X.data(), s->X.size()) && wr(f, s->Z.data(), s->Z.size()) && wr(f, s->DX.data(), s->DX.size()) &&
+            wr(f, s->DZ.data(), s->DZ.size());
+  if (ok && c.mrt) ok = wr(f, s->M.data(), 81) && wr(f, s->Minv.data(), 81) && wr(f, s->Srates.data(), 9);
+  ok = ok && wr(f, fb.data(), fb.size()) && wr(f, gb.data(), gb.size()) && wr(f, mb.data(), mb.size());
+  ok = (fclose(f) == 0) && ok;
+  return ok ? IPCU_OK : IPCU_ERR_IO;
+}
+
+extern "C" int ipcu_sim_load(const char *path, ipcu_stream_t stream, ipcu_sim **out) {
+  if (!path || !out) return IPCU_ERR_ARG;
+  *out = nullptr;
+  FILE *f = fopen(path, "rb");
+  if (!f) return IPCU_ERR_IO;
+  char mg[8];
+  int32_t ver = 0;
+  ipcu_sim_config c;
+  long long steps = 0;
+  bool ok = rd(f, mg, 8) && std::memcmp(mg, kMagic, 8) == 0 && rd(f, &ver, 1) && ver == kSnapVersion && rd(f, &c, 1) &&
+            rd(f, &steps, 1) && c.nx > 0 && c.nz > 0;
+  std::vector<double> X(ok ? c.nx : 0), Z(ok ? c.nz : 0), DX(X.size()), DZ(Z.size()), M(81), Mi(81), S(9);
+  ok = ok && rd(f, X.data(), X.size()) && rd(f, Z.data(), Z.size()) && rd(f, DX.data(), DX.size()) &&
+       rd(f, DZ.data(), DZ.size());
+  if (ok && c.mrt) ok = rd(f, M.data(), 81) && rd(f, Mi.data(), 81) && rd(f, S.data(), 9);
+  if (!ok) {
+    fclose(f);
+    return IPCU_ERR_IO;
+  }
+  c.x = X.data();
+  c.z = Z.data();
+  c.wx = DX.data();
+  c.wz = DZ.data();
+  c.M = c.mrt ? M.data() : nullptr;
+  c.Minv = c.mrt ? Mi.data() : nullptr;
+  c.S = c.mrt ? S.data() : nullptr;
+  ipcu_sim *s = nullptr;
+  int st = ipcu_sim_create(&c, nullptr, stream, &s);
+  if (st != IPCU_OK) {
+    fclose(f);
+    return st;
+  }
+  const long long N = s->N;
+  const int q = c.q_scalar;
+  std::vector<unsigned char> fb(s->esz * 9 * N), gb(s->esz * (size_t)q * N);
+  std::vector<float> mb(3 * N);
+  ok = rd(f, fb.data(), fb.size()) && rd(f, gb.data(), gb.size()) && rd(f, mb.data(), mb.size());
+  fclose(f);
+  if (!ok) {
+    ipcu_sim_destroy(s);
+    return IPCU_ERR_IO;
+  }
+  if (cudaMemcpy(s->f[s->cur], fb.data(), fb.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
+      (q && cudaMemcpy(s->g[s->cur], gb.data(), gb.size(), cudaMemcpyHostToDevice) != cudaSuccess) ||
+      cudaMemcpy(s->mac[s->cur], mb.data(), sizeof(float) * 3 * N, cudaMemcpyHostToDevice) != cudaSuccess) {
+    ipcu_sim_destroy(s);
+    return IPCU_ERR_CUDA;
+  }
+  s->steps = steps;
+  *out = s;
+  return IPCU_OK;
+}
+
+// Field CSV in the reference's column order (ref: function/basic.cu:16-28):
+// "num_calc,N" then x,y,z,delx,dely,pressure,salinity,phi,rho,u,v,w,Fx,Fy,Fz
+// per cell in the reference's cell order (x-major, z fastest). Fx, Fz are the
+// force the next step applies to the current state (buoyancy + pressure
+// gradient); the reference wrote the one applied to the previous state.
+extern "C" int ipcu_sim_write_csv(ipcu_sim *s, const char *path) {
+  if (!s || !path) return IPCU_ERR_ARG;
+  const long long N = s->N;
+  std::vector<double> p(N), S(N), ux(N), uz(N), rho(N);
+  int st;
+  if ((st = ipcu_sim_get(s, "p", p.data(), N)) || (st = ipcu_sim_get(s, "S", S.data(), N)) ||
+      (st = ipcu_sim_get(s, "ux", ux.data(), N)) || (st = ipcu_sim_get(s, "uz", uz.data(), N)) ||
+      (st = ipcu_sim_get(s, "rho", rho.data(), N)))
+    return st;
+  FILE *f = fopen(path, "w");
+  if (!f) return IPCU_ERR_IO;
+  const int nx = s->nx, nz = s->nz;
+  const double c2 = (double)s->P.c * s->P.c, reg = s->cfg.dz / 1000.0;
+  fprintf(f, "num_calc,%lld\n", N);
+  fprintf(f, "x       ,y       ,z       ,delx    ,dely    ,pressure,salinity ,phi     ,rho     ,u       ,v       ,w       ,Fx      ,Fy      ,Fz      \n");
+  for (int i = 0; i < nx; i++)
+    for (int l = 0; l < nz; l++) {
+      const long long c = (long long)l * nx + i;
+      const int ip = std::min(i + 1, nx - 1), im = std::max(i - 1, 0), lp = std::min(l + 1, nz - 1), lm = std::max(l - 1, 0);
+      const double pc = p[c] * c2 / 3.0;
+      const double Fx = -pc * (rho[(long long)l * nx + ip] - rho[(long long)l * nx + im]) / (s->X[ip] - s->X[im] + reg);
+      const double Fz = -S[c] * s->cfg.g_bouss -
+                        pc * (rho[(long long)lp * nx + i] - rho[(long long)lm * nx + i]) / (s->Z[lp] - s->Z[lm] + reg);
+      fprintf(f, "%f,%f,%f,%f,%f,%f,%f,%f,%f,%f,%f,%f,%f,%f,%f\n", s->X[i], 0.5 * s->cfg.dz, s->Z[l], s->DX[i],
+              s->cfg.dz, p[c], S[c], s->cfg.phi, rho[c], ux[c], 0.0, uz[c], Fx, 0.0, Fz);
+    }
+  return fclose(f) == 0 ? IPCU_OK : IPCU_ERR_IO;
+}
+
+// ---------------------------------------------------------------------------
+// Batched stepping: many resident simulations advanced together, one launch
+// per step for each (storage, scalar lattice, geometry) class, CTAs walking a
+// device work list of (simulation, tile) items. Each simulation's arithmetic
+// is the single-run kernel's, tile by tile, so a simulation's result does not
+// depend on what it is batched with.
+struct ipcu_batch {
+  cudaStream_t stream;
+  f2d::Params *d_params = nullptr;
+  f2d::WorkItem *d_work = nullptr;
+  size_t cap_params = 0, cap_work = 0;
+  int grid_cap = 0;
+};
+
+extern "C" int ipcu_batch_create(ipcu_stream_t stream, ipcu_batch **out) {
+  if (!out) return IPCU_ERR_ARG;
+  ipcu_batch *b = new ipcu_batch();
+  b->stream = (cudaStream_t)stream;
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  b->grid_cap = sms * f2d::kMinBlocks;
+  *out = b;
+  return IPCU_OK;
+}
+
+extern "C" void ipcu_batch_destroy(ipcu_batch *b) {
+  if (!b) return;
+  cudaStreamSynchronize(b->stream);
+  cudaFree(b->d_params);
+  cudaFree(b->d_work);
+  delete b;
+}
+
+extern "C" int ipcu_batch_step(ipcu_batch *b, ipcu_sim *const *sims, int n, int64_t nsteps) {
+  if (!b || (n > 0 && !sims) || nsteps < 0) return IPCU_ERR_ARG;
+  if (n == 0 || nsteps == 0) return IPCU_OK;
+  for (int i = 0; i < n; i++) {
+    if (!sims[i]) return IPCU_ERR_ARG;
+    // the batch stream takes over: the simulation's own work must be finished
+    if (cudaStreamSynchronize(sims[i]->stream) != cudaSuccess) return IPCU_ERR_CUDA;
+  }
+  // group by kernel class, keeping order
+  std::vector<int> order(n);
+  for (int i = 0; i < n; i++) order[i] = i;
+  std::stable_sort(order.begin(), order.end(), [&](int a, int c) {
+    const ipcu_sim_config &A = sims[a]->cfg, &C = sims[c]->cfg;
+    return std::make_tuple(A.storage, A.q_scalar, A.geometry) < std::make_tuple(C.storage, C.q_scalar, C.geometry);
+  });
+  std::vector<f2d::Params> hp(n);
+  std::vector<f2d::WorkItem> hw;
+  struct Group { int storage, qs, geo, w0, w1; };
+  std::vector<Group> groups;
+  for (int oi = 0; oi < n; oi++) {
+    ipcu_sim *s = sims[order[oi]];
+    hp[oi] = s->P;
+    hp[oi].cur = s->cur;
+    const ipcu_sim_config &c = s->cfg;
+    if (groups.empty() || groups.back().storage != c.storage || groups.back().qs != c.q_scalar ||
+        groups.back().geo != c.geometry)
+      groups.push_back({c.storage, c.q_scalar, c.geometry, (int)hw.size(), (int)hw.size()});
+    const int tx = (s->nx + f2d::kTX - 1) / f2d::kTX, tz = (s->nz + f2d::kTZ - 1) / f2d::kTZ;
+    for (int z = 0; z < tz; z++)
+      for (int x = 0; x < tx; x++) hw.push_back({oi, x, z, 0});
+    groups.back().w1 = (int)hw.size();
+  }
+  if (hp.size() > b->cap_params) {
+    cudaFree(b->d_params);
+    if (cudaMalloc((void **)&b->d_params, sizeof(f2d::Params) * hp.size()) != cudaSuccess) return IPCU_ERR_NOMEM;
+    b->cap_params = hp.size();
+  }
+  if (hw.size() > b->cap_work) {
+    cudaFree(b->d_work);
+    if (cudaMalloc((void **)&b->d_work, sizeof(f2d::WorkItem) * hw.size()) != cudaSuccess) return IPCU_ERR_NOMEM;
+    b->cap_work = hw.size();
+  }
+  if (cudaMemcpyAsync(b->d_params, hp.data(), sizeof(f2d::Params) * hp.size(), cudaMemcpyHostToDevice, b->stream) !=
+          cudaSuccess ||
+      cudaMemcpyAsync(b->d_work, hw.data(), sizeof(f2d::WorkItem) * hw.size(), cudaMemcpyHostToDevice, b->stream) !=
+          cudaSuccess)
+    return IPCU_ERR_CUDA;
+  for (const Group &g : groups) {
+    int st = f2d::launch_batched(nullptr, nullptr, 0, 0, g.storage, g.qs, g.geo, 0, b->stream, true);
+    if (st) return st;
+  }
+  for (int64_t k = 0; k < nsteps; k++) {
+    for (const Group &g : groups) {
+      const int nw = g.w1 - g.w0;
+      const int grid = std::min(nw, b->grid_cap);
+      int st = f2d::launch_batched(b->d_params, b->d_work + g.w0, nw, (int)(k & 1), g.storage, g.qs, g.geo, grid,
+                                   b->stream, false);
+      if (st) return st;
+    }
+  }
+  if (cudaStreamSynchronize(b->stream) != cudaSuccess) return IPCU_ERR_CUDA;
+  for (int i = 0; i < n; i++) {
+    sims[i]->cur ^= (int)(nsteps & 1);
+    sims[i]->steps += nsteps;
+  }
+  return IPCU_OK;
+}
+
+extern "C" int64_t ipcu_sim_device_bytes(const ipcu_sim *s) {
+  if (!s) return 0;
+  const long long N = s->N;
+  return 2 * ((long long)s->esz * (9 + std::max(s->cfg.q_scalar, 1)) * N + 4LL * 3 * N) +
+         4LL * (3 * (s->nx + s->nz) + 2 * 5 * std::max(s->nx, s->nz)) + 2048;
+}

@@ -124,6 +124,37 @@ class Sim:
     def storage_bytes(self):
         return int(_lib.lib().ipcu_sim_storage_bytes(self._h))
 
+    def device_bytes(self):
+        return int(_lib.lib().ipcu_sim_device_bytes(self._h))
+
+    def steps(self):
+        return int(_lib.lib().ipcu_sim_steps(self._h))
+
+    def save(self, path):
+        _lib.check(_lib.lib().ipcu_sim_save(self._h, str(path).encode()), "ipcu_sim_save")
+
+    @classmethod
+    def load(cls, path, stream=None):
+        """Restores a simulation saved with `save`."""
+        h = ctypes.c_void_p()
+        _lib.check(_lib.lib().ipcu_sim_load(str(path).encode(), stream, ctypes.byref(h)), "ipcu_sim_load")
+        obj = cls.__new__(cls)
+        obj._h, obj._keep = h, []
+        obj.N = int(_lib.lib().ipcu_sim_cells(h))
+        obj._dims_from_file(path)
+        return obj
+
+    def _dims_from_file(self, path):
+        # snapshot header: 8-byte magic, int32 version, then the configuration struct
+        with open(path, "rb") as fh:
+            head = fh.read(8 + 4 + ctypes.sizeof(_lib.SimConfig))
+        cfg = _lib.SimConfig.from_buffer_copy(head[12:])
+        self.nx, self.nz, self.q_scalar = cfg.nx, cfg.nz, cfg.q_scalar
+        self.storage = {0: "f32", 1: "f16", 2: "bf16"}[cfg.storage]
+
+    def write_csv(self, path):
+        _lib.check(_lib.lib().ipcu_sim_write_csv(self._h, str(path).encode()), "ipcu_sim_write_csv")
+
     def device_state(self):
         f, g, m = ctypes.c_void_p(), ctypes.c_void_p(), ctypes.c_void_p()
         _lib.check(_lib.lib().ipcu_sim_device_state(self._h, ctypes.byref(f), ctypes.byref(g), ctypes.byref(m)))

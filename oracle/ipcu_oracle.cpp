@@ -1102,3 +1102,24 @@ extern "C" void oracle_IB_directForcing_f32(const float *it, const int *lid, con
                                             float *Gw) {
   o_IB_directForcing(it, lid, nb, px, py, pz, posw, u, v, w, velw, Fx, Fy, Fz, Gw);
 }
+
+// Nearest fluid cell of each marker as the case drivers search it at set-up
+// (ref: SphereFallSuzuki2018/SphereSuzuki.cu:268-275): float differences
+// squared through pow() in double, sqrt rounded to float, strict '<' against
+// the running minimum (starting at 100) so the first minimum wins.
+extern "C" void oracle_nearest_cells_f32(const float *px, const float *py, const float *pz, long long nc,
+                                         const float *posw, int nm, int *lid) {
+  for (int k = 0; k < nm; k++) {
+    float dist1 = 100;
+    int near_id = 0;
+    for (long long i = 0; i < nc; i++) {
+      const float dist2 = (float)std::sqrt(std::pow(px[i] - posw[k * 3 + 0], 2) + std::pow(py[i] - posw[k * 3 + 1], 2) +
+                                           std::pow(pz[i] - posw[k * 3 + 2], 2));
+      if (dist1 > dist2) {
+        dist1 = dist2;
+        near_id = (int)i;
+      }
+    }
+    lid[k] = near_id;
+  }
+}

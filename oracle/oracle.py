@@ -16,6 +16,8 @@ import ctypes
 import os
 import sys
 
+import numpy as np
+
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 if ROOT not in sys.path:
@@ -42,9 +44,19 @@ class Oracle:
             f = getattr(self.lib, f"oracle_IP_process_{prec}")
             f.argtypes = [P] * 12 + [I]
             f.restype = None
+        self.lib.oracle_nearest_cells_f32.argtypes = [P, P, P, ctypes.c_longlong, P, I, P]
+        self.lib.oracle_nearest_cells_f32.restype = None
 
     def __call__(self, name, prec, *args):
         return self.b(name, prec, *args)
+
+    def nearest_cells(self, px, py, pz, nc, posw):
+        """lattice_id per marker as the case drivers search it (float32 inputs)."""
+        posw = np.ascontiguousarray(posw, np.float32).ravel()
+        xyz = [np.ascontiguousarray(a, np.float32) for a in (px, py, pz)]
+        lid = np.zeros(posw.size // 3, np.int32)
+        self.lib.oracle_nearest_cells_f32(*[ptr(a) for a in xyz], int(nc), ptr(posw), posw.size // 3, ptr(lid))
+        return lid
 
     def IP_process(self, prec, items, neib, f, feq, ftmp, fout, nextB, nextK, px, py, dX, dY, slip):
         getattr(self.lib, f"oracle_IP_process_{prec}")(
