@@ -84,6 +84,18 @@ int ipcu_sim_status(ipcu_sim *sim, uint32_t *flags);
 int ipcu_sim_upload(ipcu_sim *sim, const void *f, const void *g, const float *mac);
 int ipcu_sim_download(ipcu_sim *sim, void *f, void *g, float *mac);
 int ipcu_sim_sync(ipcu_sim *sim);
+/* FP64 area-weighted totals of p* (sum of the 9 FP32 populations f[k*N+i])
+ * and of S (mac[i]) with cell weights wx[x]*wz[z], written to out[0..1]
+ * (all device pointers), without allocating anything. No counterpart in the
+ * reference: it exists for callers that cannot allocate device memory where
+ * they need the check -- code inside CUDA graph capture, hosts that give all
+ * device memory to their own pool, loops that must not enter the driver's
+ * allocator. Its scratch is a fixed file-scope device array, so it accepts
+ * at most 16,777,216 cells (IPCU_ERR_CAPACITY beyond), the first call on a
+ * device resolves that array's address (make it before any capture), and
+ * concurrent calls race on the shared array. */
+int ipcu_totals_noalloc_f32(const float *f, const float *mac, const float *wx, const float *wz, int nx, int nz,
+                            double *out, ipcu_stream_t stream);
 /* Time steps taken since creation or restore. */
 int64_t ipcu_sim_steps(const ipcu_sim *sim);
 /* Versioned binary snapshot (configuration, geometry, MRT matrices, step

@@ -110,6 +110,7 @@ def _declare(L: ctypes.CDLL) -> None:
         "ipcu_sim_save": ([P, ctypes.c_char_p], I),
         "ipcu_sim_load": ([ctypes.c_char_p, P, ctypes.POINTER(P)], I),
         "ipcu_sim_write_csv": ([P, ctypes.c_char_p], I),
+        "ipcu_totals_noalloc_f32": ([P, P, P, P, I, I, P, P], I),
         "ipcu_add_scalar_f32": ([P, I64, ctypes.c_float, P], I),
         "ipcu_batch_create": ([P, ctypes.POINTER(P)], I),
         "ipcu_batch_destroy": ([P], None),

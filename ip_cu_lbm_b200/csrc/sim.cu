@@ -653,6 +653,49 @@ extern "C" int ipcu_sim_sync(ipcu_sim *s) {
 extern "C" int32_t ipcu_sim_storage_bytes(const ipcu_sim *s) { return s ? (int32_t)s->esz : 0; }
 
 // ---------------------------------------------------------------------------
+// Allocation-free totals. Some callers cannot allocate device memory at the
+// point where they need the conservation check: code running inside CUDA
+// graph capture (an allocation is not a capturable stream operation), hosts
+// that hand all device memory to their own pool at start-up, and real-time
+// loops that must not hit the driver's allocator. This entry point runs the
+// same two-pass reduction as ipcu_sim_totals but keeps its per-block partial
+// sums in a file-scope device array instead of allocated scratch.
+//
+// Limit: kNoAllocBlocks partials of kNoAllocCells cells each, i.e. at most
+// 1024 * 16384 = 16,777,216 cells; larger fields are rejected with
+// IPCU_ERR_CAPACITY. The array occupies 16.4 KB on every device that loads
+// the library, until the process exits. Every call shares it and it keeps
+// the last call's contents: each call writes every partial it reads, so
+// nothing needs clearing, but calls whose kernels overlap on the GPU (two
+// streams, or two host threads) race on it and must be serialised by the
+// caller.
+constexpr int kNoAllocBlocks = 1024;
+constexpr long long kNoAllocCells = 16384;
+static __device__ __align__(256) double g_noalloc_partials[2 * kNoAllocBlocks + 2];
+
+extern "C" int ipcu_totals_noalloc_f32(const float *f, const float *mac, const float *wx, const float *wz, int nx,
+                                       int nz, double *out, ipcu_stream_t stream) {
+  if (!f || !mac || !wx || !wz || !out || nx < 1 || nz < 1) return IPCU_ERR_ARG;
+  const long long N = (long long)nx * nz;
+  if (N > (long long)kNoAllocBlocks * kNoAllocCells) return IPCU_ERR_CAPACITY;
+  // host code cannot use the array's name as a device address: resolve it
+  // once per device (the first call on a device does this set-up, so it
+  // should come before any stream capture)
+  static double *dev_ptr[64] = {nullptr};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return IPCU_ERR_CUDA;
+  if (!dev_ptr[dev]) {
+    void *ptr = nullptr;
+    if (cudaGetSymbolAddress(&ptr, g_noalloc_partials) != cudaSuccess || !ptr) return IPCU_ERR_CUDA;
+    dev_ptr[dev] = static_cast<double *>(ptr);
+  }
+  const int nb = (int)((N + kNoAllocCells - 1) / kNoAllocCells);
+  k_totals<float><<<nb, 256, 0, (cudaStream_t)stream>>>(f, mac, wx, wz, nx, nz, 1.0f, dev_ptr[dev]);
+  k_totals_final<<<1, 32, 0, (cudaStream_t)stream>>>(dev_ptr[dev], nb, out);
+  return status_from_cuda(cudaGetLastError());
+}
+
+// ---------------------------------------------------------------------------
 // Checkpoint / restore: a versioned binary snapshot of the configuration,
 // the axis geometry, the MRT matrices, the step count and the raw state in
 // its storage format (replaces the reference's unused text save_status,
