@@ -21,11 +21,13 @@ struct Params {
   void *gbuf[2];
   float *mbuf[2];  // [3][N]: S, ux, uz
   int cur;
-  // interpolated axis: weights [2][NA][NS], fin scale [2][NA], fout scale [NA]
-  const float *wA, *scin, *scout;
+  // interpolated axis: weights [2][NA][NS], fin scale [2][NA], fout scale [NA],
+  // and the interior cells' combined flux weights [2][NS+1][NA]
+  const float *wA, *scin, *scout, *wC;
   // 1/(x_{i+1} - x_{i-1} + dz/1000) with clamped neighbours (density gradient)
   const float *ginvx, *ginvz;
   float c, dt, tau, taus;
+  float fk3, hdt;  // 3 dt / c (forcing term per unit density) and dt / 2
   float rhoL, rhoH, phi;
   double rho_sal, g_bouss;
   float fscale, inv_fscale, gscale, inv_gscale, s_ref;

@@ -69,25 +69,11 @@ struct Geo {
   static constexpr int WREC = NS + 2;             // NS weights, fin scale, fout scale
 };
 
-// FP32 storage stages the raw tile (f, g, u_x, u_z) into shared memory with
-// asynchronous copies before colliding it in place; reduced-precision storage
-// loads through registers (cp.async moves 4, 8 or 16 bytes, not 2).
-template <class ST>
-constexpr bool kStageAsync = sizeof(ST) == 4;
-
 template <class ST, int QS, int GEO>
 constexpr size_t smem_bytes() {
   using G = Geo<GEO>;
-  return sizeof(float) * ((9 + QS + (kStageAsync<ST> ? 2 : 0)) * G::NE + 2 * G::SX * G::SZ + 2 * kTX * kTZ +
-                          2 * G::NWA * G::WREC);
-}
-
-__device__ __forceinline__ void cp_async4(float *dst, const float *src) {
-  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(src) : "memory");
-}
-__device__ __forceinline__ void cp_async_wait_all() {
-  asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
+  return sizeof(float) * ((9 + QS) * G::NE + 2 * G::SX * G::SZ + 2 * kTX * kTZ + 2 * G::NWA * G::WREC +
+                          2 * G::NWA * (G::NS + 1));
 }
 
 // storage conversion: value = stored*inv_scale
@@ -112,34 +98,28 @@ __device__ __forceinline__ void st(ST *p, long long i, float v, float scale) {
   }
 }
 
-// Clamp-free pull for an interior cell. lc: local index of the cell; la:
-// its local index along the interpolated axis; sW layout [s][m][la].
-template <int GEO, int K, bool AMOVE>
+// Clamp-free pull for an interior cell: lc is the cell's local index; W
+// holds the combined flux weights of its axis position for both signs of
+// the axis velocity (see axis_tables on the host), so the flux form is one
+// dot product over the NS+1 nodes around the source cell.
+template <int GEO, int K>
 struct Fast {
   using G = Geo<GEO>;
   static constexpr int DA = G::AX == 0 ? 1 : G::EX;   // one cell along the interpolated axis
   static constexpr int A = G::AX == 0 ? ex(K) : (G::AX == 1 ? ez(K) : 0);
   static constexpr int BX = G::AX == 0 ? 0 : ex(K);   // shift-axis part of e_K
   static constexpr int BZ = G::AX == 1 ? 0 : ez(K);
-  __device__ __forceinline__ static float pull(const float *arr, int lc, int la, const float *sW) {
+  __device__ __forceinline__ static float pull(const float *arr, int lc, const float (&W)[2][G::NS + 1]) {
     constexpr int NE = G::NE;
     if constexpr (G::AX < 0 || A == 0) {
       return arr[K * NE + lc - ex(K) - ez(K) * G::EX];
     } else {
       constexpr int s = A > 0 ? 0 : 1, sg = A > 0 ? 1 : -1, h = G::NS / 2;
-      const int cp = lc - BX - BZ * G::EX;  // c' = c - (shift part of e_K)
-      float v[G::NS + 1];
+      const float *src = arr + K * NE + lc - BX - BZ * G::EX;  // c' = c - (shift part of e_K)
+      float acc = 0.f;
 #pragma unroll
-      for (int q = 0; q <= G::NS; q++) v[q] = arr[K * NE + cp + sg * (q - h - 1) * DA];
-      const float *wj = sW + (s * G::WREC) * G::NWA + (la - A);  // weights of j = c' - a
-      const float *wc = sW + (s * G::WREC) * G::NWA + la;        // weights of c'
-      float Ij = 0.f, Ic = 0.f;
-#pragma unroll
-      for (int m = 0; m < G::NS; m++) {
-        Ij += wj[m * G::NWA] * v[m];
-        Ic += wc[m * G::NWA] * v[m + 1];
-      }
-      return v[h + 1] + (Ij * wj[G::NS * G::NWA] - Ic * wc[(G::NS + 1) * G::NWA]);
+      for (int q = 0; q <= G::NS; q++) acc = fmaf(W[s][q], src[sg * (q - h - 1) * DA], acc);
+      return acc;
     }
   }
 };
@@ -157,7 +137,7 @@ __device__ __forceinline__ void step_tile(const Params &p, int parity, int tile_
   float *sR = sS + SZ * SX;               // [SZ][SX] density
   float *sF = sR + SZ * SX;               // [2][kTZ][kTX] interior force
   float *sW = sF + 2 * kTX * kTZ;         // [2][WREC][NWA] axis weights
-  float *sU = sW + 2 * WREC * NWA;        // [2][EZ][EX] staged u_x, u_z (FP32 storage)
+  float *sC = sW + 2 * WREC * NWA;        // [2][NS+1][NWA] combined interior weights
 
   const int nx = p.nx, nz = p.nz;
   const long long N = (long long)nx * nz;
@@ -176,24 +156,7 @@ __device__ __forceinline__ void step_tile(const Params &p, int parity, int tile_
   // term, rounded once (ref: collision.cu:251)
   const float rho0 = p.rhoL + (p.rhoH - p.rhoL) * p.phi;
 
-  // ---- phase 0: start the asynchronous copy of the raw tile + halo (FP32
-  // storage), then stage the salinity/density ring and the axis weights
-  if constexpr (kStageAsync<ST>) {
-    const float *fin32 = reinterpret_cast<const float *>(f_in);
-    const float *gin32 = reinterpret_cast<const float *>(g_in);
-    for (int e = tid; e < NE; e += kThreads) {
-      const int lz = e / EX, lx = e - lz * EX;
-      const int gx = ox + lx, gz = oz + lz;
-      if (gx < 0 || gx >= nx || gz < 0 || gz >= nz) continue;
-      const long long ci = (long long)gz * nx + gx;
-#pragma unroll
-      for (int k = 0; k < 9; k++) cp_async4(sf + k * NE + e, fin32 + k * N + ci);
-#pragma unroll
-      for (int k = 0; k < QS; k++) cp_async4(sg + k * NE + e, gin32 + k * N + ci);
-      cp_async4(sU + e, mac_in + N + ci);
-      cp_async4(sU + NE + e, mac_in + 2 * N + ci);
-    }
-  }
+  // ---- phase 0: stage the salinity/density ring and the axis weights
   for (int e = tid; e < SX * SZ; e += kThreads) {
     const int lz = e / SX, lx = e - lz * SX;
     const int gx = min(max(ox - 1 + lx, 0), nx - 1), gz = min(max(oz - 1 + lz, 0), nz - 1);
@@ -212,8 +175,12 @@ __device__ __forceinline__ void step_tile(const Params &p, int parity, int tile_
       else v = __ldg(p.scout + gA);
       sW[e] = v;
     }
+    constexpr int NQ = G::NS + 1;
+    for (int e = tid; e < 2 * NQ * NWA; e += kThreads) {
+      const int la = e % NWA, r = e / NWA;  // r = s * NQ + q
+      sC[e] = __ldg(p.wC + (long long)r * NA + min(max(oA + la, 0), NA - 1));
+    }
   }
-  if constexpr (kStageAsync<ST>) cp_async_wait_all();
   __syncthreads();
 
   const float c = p.c, c2 = c * c, ic = 1.0f / c, dt = p.dt;
@@ -226,23 +193,13 @@ __device__ __forceinline__ void step_tile(const Params &p, int parity, int tile_
     const int lz = e / EX, lx = e - lz * EX;
     const int gx = ox + lx, gz = oz + lz;
     if (gx < 0 || gx >= nx || gz < 0 || gz >= nz) continue;
-    float f[9], g[QS > 0 ? QS : 1], u, w;
-    if constexpr (kStageAsync<ST>) {
+    float f[9], g[QS > 0 ? QS : 1];
+    const long long ci = (long long)gz * nx + gx;
 #pragma unroll
-      for (int k = 0; k < 9; k++) f[k] = sf[k * NE + e];
+    for (int k = 0; k < 9; k++) f[k] = ld(f_in, k * N + ci, ifs);
 #pragma unroll
-      for (int k = 0; k < QS; k++) g[k] = sg[k * NE + e];
-      u = sU[e];
-      w = sU[NE + e];
-    } else {
-      const long long ci = (long long)gz * nx + gx;
-#pragma unroll
-      for (int k = 0; k < 9; k++) f[k] = ld(f_in, k * N + ci, ifs);
-#pragma unroll
-      for (int k = 0; k < QS; k++) g[k] = ld(g_in, k * N + ci, igs) + wq<QS>(k) * p.s_ref;
-      u = mac_in[N + ci];
-      w = mac_in[2 * N + ci];
-    }
+    for (int k = 0; k < QS; k++) g[k] = ld(g_in, k * N + ci, igs) + wq<QS>(k) * p.s_ref;
+    const float u = mac_in[N + ci], w = mac_in[2 * N + ci];
     const int rs = (lz + 1) * SX + lx + 1;
     const float S = sS[rs], rho = sR[rs];
     // p* (ref: collision.cu:244-246)
@@ -253,55 +210,115 @@ __device__ __forceinline__ void step_tile(const Params &p, int parity, int tile_
     const float pc = pr * c2 / 3.0f;
     const float Fx = -pc * ((sR[rs + 1] - sR[rs - 1]) * __ldg(p.ginvx + gx));
     const float Fz = (float)(-(double)S * p.g_bouss) - pc * ((sR[rs + SX] - sR[rs - SX]) * __ldg(p.ginvz + gz));
-    // equilibrium (ref: collision.cu:3-14) and forcing term (ref: collision.cu:102-110)
     const float uc = u * ic, wc = w * ic;
     const float usq = uc * uc + wc * wc;
-    const float fden = dt * c * 3.0f / (rho * c2);
-    float d[9], fk[9];
-#pragma unroll
-    for (int k = 0; k < 9; k++) {
-      const float eu = (ex(k) ? ex(k) * uc : 0.f) + (ez(k) ? ez(k) * wc : 0.f);
-      const float feq = w9(k) * (pr + 3.0f * eu + 4.5f * eu * eu - 1.5f * usq);
-      const float ef = (ex(k) ? ex(k) * Fx : 0.f) + (ez(k) ? ez(k) * Fz : 0.f);
-      fk[k] = w9(k) * ef * fden;
-      d[k] = f[k] - feq + 0.5f * fk[k];
-    }
+    // forcing term Fk_k = w_k (e_k . F) fden (ref: collision.cu:102-110)
+    const float fden = __fdividef(p.fk3, rho);
     if (p.mrt == 2) {
-      // unit non-shear rates: f* = f - d + (1 - 1/tau) Minv_s M_s d + Fk, with
-      // the Lallemand-Luo shear moments p_xx = d1-d2+d3-d4, p_xz = d5-d6+d7-d8
-      const float m7 = 0.25f * om_shear * ((d[1] - d[2]) + (d[3] - d[4]));
-      const float m8 = 0.25f * om_shear * ((d[5] - d[6]) + (d[7] - d[8]));
-      const float sgn7[9] = {0, 1, -1, 1, -1, 0, 0, 0, 0}, sgn8[9] = {0, 0, 0, 0, 0, 1, -1, 1, -1};
-#pragma unroll
-      for (int a = 0; a < 9; a++) sf[a * NE + e] = f[a] - d[a] + fk[a] + sgn7[a] * m7 + sgn8[a] * m8;
-    } else if (p.mrt == 1) {
-      // f* = f - (MM + Minv_s M_s / tau) d + Fk (ref: collision.cu:115-150)
-      float m7 = 0.f, m8 = 0.f;
-#pragma unroll
-      for (int k = 0; k < 9; k++) {
-        m7 += p.Ms[k] * d[k];
-        m8 += p.Ms[9 + k] * d[k];
+      // MRT with unit non-shear rates (the reference's S file): the
+      // non-shear moments relax to equilibrium in one step, so
+      //   f*_k = feq_k + Fk_k / 2 + (1 - 1/tau) (Minv_s M_s d)_k,
+      //   d = f - feq + Fk/2 (ref: collision.cu:115-150),
+      // whose shear moments reduce to (Lallemand-Luo rows 7, 8)
+      //   p_xx = (f1 + f3 - f2 - f4) - (u^2 - w^2)/c^2, p_xz = (f5 + f7 - f6 - f8) - u w/c^2
+      // (the forcing parts cancel pairwise); feq + Fk/2 is formed per
+      // opposite pair from A = p* - 1.5 u^2 + 4.5 (e.u)^2, B = 3 e.u + e.F fden/2.
+      const float P0 = pr - 1.5f * usq;
+      const float hx = 0.5f * fden * Fx, hz = 0.5f * fden * Fz;
+      const float m7 = 0.25f * om_shear * (((f[1] + f[3]) - (f[2] + f[4])) - (uc * uc - wc * wc));
+      const float m8 = 0.25f * om_shear * (((f[5] + f[7]) - (f[6] + f[8])) - uc * wc);
+      sf[e] = w9(0) * P0;
+      {
+        const float A = fmaf(4.5f * uc, uc, P0), B = fmaf(3.0f, uc, hx);
+        sf[1 * NE + e] = fmaf(w9(1), A + B, m7);
+        sf[3 * NE + e] = fmaf(w9(3), A - B, m7);
       }
-#pragma unroll
-      for (int a = 0; a < 9; a++) {
-        float acc = 0.f;
-#pragma unroll
-        for (int k = 0; k < 9; k++) acc += p.MM[a * 9 + k] * d[k];
-        acc += (p.Mis[a * 2] * m7 + p.Mis[a * 2 + 1] * m8) * itau;
-        sf[a * NE + e] = f[a] - acc + fk[a];
+      {
+        const float A = fmaf(4.5f * wc, wc, P0), B = fmaf(3.0f, wc, hz);
+        sf[2 * NE + e] = fmaf(w9(2), A + B, -m7);
+        sf[4 * NE + e] = fmaf(w9(4), A - B, -m7);
+      }
+      {
+        const float eu = uc + wc;
+        const float A = fmaf(4.5f * eu, eu, P0), B = fmaf(3.0f, eu, hx + hz);
+        sf[5 * NE + e] = fmaf(w9(5), A + B, m8);
+        sf[7 * NE + e] = fmaf(w9(7), A - B, m8);
+      }
+      {
+        const float eu = wc - uc;
+        const float A = fmaf(4.5f * eu, eu, P0), B = fmaf(3.0f, eu, hz - hx);
+        sf[6 * NE + e] = fmaf(w9(6), A + B, -m8);
+        sf[8 * NE + e] = fmaf(w9(8), A - B, -m8);
       }
     } else {
+      // equilibrium (ref: collision.cu:3-14), d = f - feq + Fk/2; d goes to
+      // shared memory (this cell's own slots) so that only the outputs stay
+      // in registers while the 9x9 operator is applied
+      auto feq_of = [&](int k) {
+        const float eu = (ex(k) ? ex(k) * uc : 0.f) + (ez(k) ? ez(k) * wc : 0.f);
+        return w9(k) * (pr + 3.0f * eu + 4.5f * eu * eu - 1.5f * usq);
+      };
+      auto fk_of = [&](int k) {
+        const float ef = (ex(k) ? ex(k) * Fx : 0.f) + (ez(k) ? ez(k) * Fz : 0.f);
+        return w9(k) * ef * fden;
+      };
 #pragma unroll
-      for (int k = 0; k < 9; k++) sf[k * NE + e] = f[k] - d[k] * itau + fk[k];
+      for (int k = 0; k < 9; k++) sf[k * NE + e] = f[k] - feq_of(k) + 0.5f * fk_of(k);
+      if (p.mrt == 1) {
+        // f* = f - (MM + Minv_s M_s / tau) d + Fk (ref: collision.cu:115-150),
+        // with f = d + feq - Fk/2
+        float m7 = 0.f, m8 = 0.f;
+#pragma unroll
+        for (int k = 0; k < 9; k++) {
+          m7 += p.Ms[k] * sf[k * NE + e];
+          m8 += p.Ms[9 + k] * sf[k * NE + e];
+        }
+        // general relaxation rates: the 9x9 product runs as a rolled loop
+        // over d's components so that only the nine outputs stay live
+        float o[9];
+#pragma unroll
+        for (int a = 0; a < 9; a++) o[a] = 0.f;
+#pragma unroll 1
+        for (int k = 0; k < 9; k++) {
+          const float dk = sf[k * NE + e];
+#pragma unroll
+          for (int a = 0; a < 9; a++) o[a] += p.MM[a * 9 + k] * dk;
+        }
+#pragma unroll
+        for (int a = 0; a < 9; a++) {
+          const float acc = o[a] + (p.Mis[a * 2] * m7 + p.Mis[a * 2 + 1] * m8) * itau;
+          o[a] = sf[a * NE + e] + feq_of(a) + 0.5f * fk_of(a) - acc;
+        }
+#pragma unroll
+        for (int a = 0; a < 9; a++) sf[a * NE + e] = o[a];
+      } else {
+        // BGK with forcing (ref: collision.cu:151-165): f* = f - d/tau + Fk
+#pragma unroll
+        for (int k = 0; k < 9; k++) {
+          const float d = sf[k * NE + e];
+          sf[k * NE + e] = d + feq_of(k) + 0.5f * fk_of(k) - d * itau;
+        }
+      }
     }
-    if constexpr (QS > 0) {
-      // regularised scalar collision (ref: collision.cu:167-188)
+    if constexpr (QS == 5) {
+      // regularised D2Q5 collision (ref: collision.cu:167-188 on the D2Q5
+      // lattice, linear equilibrium w S (1 + 3 e.u/c)): the first moment of
+      // g - geq is j = (g1 - g3, g2 - g4) - S u/c, and
+      //   g*_k = w_k (S + 3 e_k . (S u/c + (1 - 1/tau_s) j)).
+      const float jx = (g[1] - g[3]) - S * uc, jz = (g[2] - g[4]) - S * wc;
+      const float ax3 = 3.0f * fmaf(omg, jx, S * uc), az3 = 3.0f * fmaf(omg, jz, S * wc);
+      sg[e] = w5(0) * S;
+      sg[1 * NE + e] = w5(1) * (S + ax3);
+      sg[3 * NE + e] = w5(3) * (S - ax3);
+      sg[2 * NE + e] = w5(2) * (S + az3);
+      sg[4 * NE + e] = w5(4) * (S - az3);
+    } else if constexpr (QS == 9) {
+      // regularised scalar collision on the reference's Q9 scalar lattice (ref: collision.cu:167-188)
       float ge[QS], jx = 0.f, jz = 0.f;
 #pragma unroll
       for (int k = 0; k < QS; k++) {
         const float eu = (ex(k) ? ex(k) * uc : 0.f) + (ez(k) ? ez(k) * wc : 0.f);
-        const float shape = (QS == 9) ? (1.0f + 3.0f * eu + 4.5f * eu * eu - 1.5f * usq) : (1.0f + 3.0f * eu);
-        ge[k] = wq<QS>(k) * S * shape;
+        ge[k] = wq<QS>(k) * S * (1.0f + 3.0f * eu + 4.5f * eu * eu - 1.5f * usq);
         const float ne = g[k] - ge[k];
         if (ex(k)) jx += ex(k) * ne;
         if (ez(k)) jz += ez(k) * ne;
@@ -379,26 +396,33 @@ __device__ __forceinline__ void step_tile(const Params &p, int parity, int tile_
                                   : (gA >= G::H && gA <= NA - 1 - G::H && gB >= 1 && gB <= NB - 2);
     float fv[9], gv[QS > 0 ? QS : 1];
     if (fast) {
-      fv[0] = Fast<GEO, 0, false>::pull(sf, lc, la, sW);
-      fv[1] = Fast<GEO, 1, true>::pull(sf, lc, la, sW);
-      fv[2] = Fast<GEO, 2, true>::pull(sf, lc, la, sW);
-      fv[3] = Fast<GEO, 3, true>::pull(sf, lc, la, sW);
-      fv[4] = Fast<GEO, 4, true>::pull(sf, lc, la, sW);
-      fv[5] = Fast<GEO, 5, true>::pull(sf, lc, la, sW);
-      fv[6] = Fast<GEO, 6, true>::pull(sf, lc, la, sW);
-      fv[7] = Fast<GEO, 7, true>::pull(sf, lc, la, sW);
-      fv[8] = Fast<GEO, 8, true>::pull(sf, lc, la, sW);
+      float W[2][G::NS + 1];
+      if constexpr (G::AX >= 0) {
+#pragma unroll
+        for (int sidx = 0; sidx < 2; sidx++)
+#pragma unroll
+          for (int q = 0; q <= G::NS; q++) W[sidx][q] = sC[(sidx * (G::NS + 1) + q) * NWA + la];
+      }
+      fv[0] = Fast<GEO, 0>::pull(sf, lc, W);
+      fv[1] = Fast<GEO, 1>::pull(sf, lc, W);
+      fv[2] = Fast<GEO, 2>::pull(sf, lc, W);
+      fv[3] = Fast<GEO, 3>::pull(sf, lc, W);
+      fv[4] = Fast<GEO, 4>::pull(sf, lc, W);
+      fv[5] = Fast<GEO, 5>::pull(sf, lc, W);
+      fv[6] = Fast<GEO, 6>::pull(sf, lc, W);
+      fv[7] = Fast<GEO, 7>::pull(sf, lc, W);
+      fv[8] = Fast<GEO, 8>::pull(sf, lc, W);
       if constexpr (QS > 0) {
-        gv[0] = Fast<GEO, 0, false>::pull(sg, lc, la, sW);
-        gv[1] = Fast<GEO, 1, true>::pull(sg, lc, la, sW);
-        gv[2] = Fast<GEO, 2, true>::pull(sg, lc, la, sW);
-        gv[3] = Fast<GEO, 3, true>::pull(sg, lc, la, sW);
-        gv[4] = Fast<GEO, 4, true>::pull(sg, lc, la, sW);
+        gv[0] = Fast<GEO, 0>::pull(sg, lc, W);
+        gv[1] = Fast<GEO, 1>::pull(sg, lc, W);
+        gv[2] = Fast<GEO, 2>::pull(sg, lc, W);
+        gv[3] = Fast<GEO, 3>::pull(sg, lc, W);
+        gv[4] = Fast<GEO, 4>::pull(sg, lc, W);
         if constexpr (QS == 9) {
-          gv[5] = Fast<GEO, 5, true>::pull(sg, lc, la, sW);
-          gv[6] = Fast<GEO, 6, true>::pull(sg, lc, la, sW);
-          gv[7] = Fast<GEO, 7, true>::pull(sg, lc, la, sW);
-          gv[8] = Fast<GEO, 8, true>::pull(sg, lc, la, sW);
+          gv[5] = Fast<GEO, 5>::pull(sg, lc, W);
+          gv[6] = Fast<GEO, 6>::pull(sg, lc, W);
+          gv[7] = Fast<GEO, 7>::pull(sg, lc, W);
+          gv[8] = Fast<GEO, 8>::pull(sg, lc, W);
         }
       }
     } else {
@@ -430,7 +454,7 @@ __device__ __forceinline__ void step_tile(const Params &p, int parity, int tile_
     }
     // moments (ref: collision.cu:244-254)
     const float rho = (float)((double)rho0 + (double)S * p.rho_sal);
-    const float h = dt / (2.0f * rho);
+    const float h = __fdividef(p.hdt, rho);
     const float ux = c * jx + sF[e] * h, uz = c * jz + sF[kTX * kTZ + e] * h;
     mac_out[ci] = S;
     mac_out[N + ci] = ux;

@@ -25,7 +25,7 @@ struct ipcu_sim {
   void *f[2] = {nullptr, nullptr};
   void *g[2] = {nullptr, nullptr};
   float *mac[2] = {nullptr, nullptr};
-  float *wA = nullptr, *scin = nullptr, *scout = nullptr, *ginvx = nullptr, *ginvz = nullptr;
+  float *wA = nullptr, *scin = nullptr, *scout = nullptr, *wC = nullptr, *ginvx = nullptr, *ginvz = nullptr;
   unsigned *status = nullptr;
   double *partials = nullptr;
   int cur = 0;
@@ -58,14 +58,12 @@ inline int geo_ns(int geo) {
 // (ref: function/adv.cu:16-21 set_posl_x; 41-48 Lagrange_interpolation;
 // 76-86 evaluation point and flux scales).
 void axis_tables(const std::vector<double> &X, const std::vector<double> &D, double dz, int ns, std::vector<float> &w,
-                 std::vector<float> &scin, std::vector<float> &scout) {
+                 std::vector<float> &scin, std::vector<float> &scout, std::vector<float> &wc) {
   const int n = (int)X.size();
-  w.assign((size_t)2 * n * ns, 0.f);
-  scin.assign((size_t)2 * n, 0.f);
-  scout.assign(n, 0.f);
+  std::vector<double> wd((size_t)2 * n * ns, 0.0), sid((size_t)2 * n, 0.0), sod(n, 0.0);
   auto cl = [&](int i) { return std::min(std::max(i, 0), n - 1); };
   for (int j = 0; j < n; j++) {
-    scout[j] = (float)(dz / D[j]);
+    sod[j] = dz / D[j];
     for (int s = 0; s < 2; s++) {
       const int sg = s == 0 ? 1 : -1;
       const double xa = X[j] + sg * (D[j] - dz) / 2.0;
@@ -79,11 +77,33 @@ void axis_tables(const std::vector<double> &X, const std::vector<double> &D, dou
         double v = 1.0;
         for (int b = 0; b < ns; b++)
           if (b != a) v *= (xa - pl[b]) / (pl[a] - pl[b]);
-        w[((size_t)s * n + j) * ns + a] = (float)v;
+        wd[((size_t)s * n + j) * ns + a] = v;
       }
-      scin[(size_t)s * n + j] = (float)(dz / D[cl(j + sg)]);
+      sid[(size_t)s * n + j] = dz / D[cl(j + sg)];
     }
   }
+  w.resize(wd.size());
+  scin.resize(sid.size());
+  scout.resize(sod.size());
+  for (size_t i = 0; i < wd.size(); i++) w[i] = (float)wd[i];
+  for (size_t i = 0; i < sid.size(); i++) scin[i] = (float)sid[i];
+  for (size_t i = 0; i < sod.size(); i++) scout[i] = (float)sod[i];
+  // Interior cells (stencils clear of the walls) take the flux form as one
+  // dot product over the NS+1 nodes c'+sg*(q-h-1), q = 0..NS, around the
+  // source cell c' (axis index j): the centre value, plus fin of the
+  // upstream cell j-sg, minus fout of c'. wc layout [2][NS+1][n].
+  const int nq = ns + 1, h = ns / 2;
+  wc.assign((size_t)2 * nq * n, 0.f);
+  for (int j = 0; j < n; j++)
+    for (int s = 0; s < 2; s++) {
+      const int sg = s == 0 ? 1 : -1, ju = cl(j - sg);
+      for (int q = 0; q < nq; q++) {
+        double v = (q == h + 1) ? 1.0 : 0.0;
+        if (q < ns) v += sid[(size_t)s * n + ju] * wd[((size_t)s * n + ju) * ns + q];
+        if (q >= 1) v -= sod[j] * wd[((size_t)s * n + j) * ns + q - 1];
+        wc[((size_t)s * nq + q) * n + j] = (float)v;
+      }
+    }
 }
 
 // 1/(x_{i+1} - x_{i-1} + dz/1000) in float, clamped neighbours
@@ -220,6 +240,7 @@ void free_sim(ipcu_sim *s) {
   cudaFree(s->wA);
   cudaFree(s->scin);
   cudaFree(s->scout);
+  cudaFree(s->wC);
   cudaFree(s->ginvx);
   cudaFree(s->ginvz);
   cudaFree(s->status);
@@ -310,9 +331,11 @@ extern "C" int ipcu_sim_create(const ipcu_sim_config *cfg, const double *s0, ipc
     st = IPCU_ERR_NOMEM;
   if (st == IPCU_OK) cudaMemset(s->status, 0, sizeof(unsigned));
   if (st == IPCU_OK && ax >= 0) {
-    std::vector<float> w, si, so;
-    axis_tables(ax == 0 ? s->X : s->Z, ax == 0 ? s->DX : s->DZ, dz, ns, w, si, so);
-    if ((st = upload(&s->wA, w)) == IPCU_OK && (st = upload(&s->scin, si)) == IPCU_OK) st = upload(&s->scout, so);
+    std::vector<float> w, si, so, wc;
+    axis_tables(ax == 0 ? s->X : s->Z, ax == 0 ? s->DX : s->DZ, dz, ns, w, si, so, wc);
+    if ((st = upload(&s->wA, w)) == IPCU_OK && (st = upload(&s->scin, si)) == IPCU_OK &&
+        (st = upload(&s->scout, so)) == IPCU_OK)
+      st = upload(&s->wC, wc);
   }
   if (st == IPCU_OK) {
     std::vector<float> gx = grad_inv(s->X, dz), gz = grad_inv(s->Z, dz);
@@ -332,10 +355,13 @@ extern "C" int ipcu_sim_create(const ipcu_sim_config *cfg, const double *s0, ipc
   P.wA = s->wA;
   P.scin = s->scin;
   P.scout = s->scout;
+  P.wC = s->wC;
   P.ginvx = s->ginvx;
   P.ginvz = s->ginvz;
   P.c = (float)(dz / c.dt);
   P.dt = (float)c.dt;
+  P.fk3 = (float)(3.0 * c.dt * c.dt / dz);
+  P.hdt = (float)(0.5 * c.dt);
   P.tau = (float)c.tau;
   P.taus = (float)(c.q_scalar ? c.taus : 1.0);
   P.rhoL = (float)c.rhoL;
