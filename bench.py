@@ -100,6 +100,16 @@ class Clocks:
                 "reasons": reasons, "samples": len(samples)}
 
 
+def measured_traffic(args):
+    """DRAM bytes per launch of the default FP32 workload's step kernel from
+    the committed ncu summary (profiles/traffic.json), else None."""
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    if args.storage != "f32" or args.inner != INNER or not os.path.exists(p):
+        return None
+    d = json.load(open(p)).get("step_kernel<float,5,z3,TMA>@1024x256")
+    return d["dram_bytes_per_launch"] if d else None
+
+
 def load_peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -177,7 +187,7 @@ def run_ours(args):
     hdt = torch.float32 if esz == 4 else torch.float16
     hf = torch.empty(9 * N, dtype=hdt, pin_memory=True)
     hg = torch.empty(5 * N, dtype=hdt, pin_memory=True)
-    hm = torch.empty(3 * N, dtype=torch.float32, pin_memory=True)
+    hm = torch.empty(sim.mac_planes() * N, dtype=torch.float32, pin_memory=True)
     sim.download(hf, hg, hm)
     sim.sync()
     e2e_steps = max(3, args.steps)
@@ -203,11 +213,14 @@ def run_ours(args):
                    "parallelism": f"replicas x{world}",
                    "l2": "flushed (256 MiB write) between timed steps; the 36 MB state is L2-resident within a step"},
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                     "frac": round(achieved / peak, 4), "traffic": None,
+                     "frac": round(achieved / peak, 4), "traffic": measured_traffic(args),
                      "bytes_per_cell": bpc, "peak_source": f"{peak_src} (MEASURED_PEAKS.json hbm_gbs)",
-                     "note": "algorithmic bytes (each stored value read once and written once) / mean launch time"},
-        "e2e": {"value": round(e2e, 2), "unit": METRIC, "h2d_bytes_per_step": int(N * (14 * esz + 12)),
-                "d2h_bytes_per_step": int(N * 12)},
+                     "note": "algorithmic bytes (each stored value read once and written once) / mean launch time; "
+                             "traffic = ncu dram read+write bytes of one launch (caches flushed by ncu; the "
+                             "new state stays in L2, so the writes do not reach DRAM)"},
+        "e2e": {"value": round(e2e, 2), "unit": METRIC, "h2d_bytes_per_step": int(hf.numel() * hf.element_size() + hg.numel() * hg.element_size()
+                                                                 + hm.numel() * 4),
+                "d2h_bytes_per_step": int(hm.numel() * 4)},
         "gpu_launches": args.steps * inner,
         "clocks": clk.summary(),
     }
@@ -219,6 +232,80 @@ def run_ours(args):
     if rank == 0:
         print(json.dumps(line), flush=True)
     sim.close()
+    R.close()
+
+
+def run_3d(args):
+    """The 3-D path at the C4 size: 160 x 160 x 640 uniform box (16.4M cells,
+    state 3.8 GB > L2), D3Q19 MRT + D3Q7 salinity with a linear stratification,
+    bounce-back, FP32. A step is --inner LBM steps (default 20) replayed from
+    a CUDA graph; the inputs are far larger than L2, so no flush is needed."""
+    import torch
+
+    from ip_cu_lbm_b200.replicas import Replicas
+    from ip_cu_lbm_b200.sim3d import Sim3D
+
+    R = Replicas("nccl")
+    world, local = R.world, R.local
+    nx, ny, nz = (int(v) for v in args.dims.split(","))
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.current_stream(dev)
+    zz = np.broadcast_to((np.arange(nz) + 0.5)[:, None, None] / nz, (nz, ny, nx))
+    rng = np.random.default_rng(20261203)
+    S0 = 1.0 - zz + 1e-4 * rng.uniform(-1, 1, (nz, ny, nx))  # linear stratification, seeded noise
+    sim = Sim3D(nx, ny, nz, tau=0.55, taus=0.52, rho_sal=1e-3, g_bouss=1e-5, s0=S0.ravel(), stream=stream.cuda_stream)
+    N, inner = sim.N, args.inner if args.inner != INNER else 20
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    with Clocks(local) as clk:
+        time.sleep(0.3)
+        for _ in range(args.warmup):
+            sim.step_graph(inner)
+        R.barrier()
+        t_start = time.perf_counter()
+        for k in range(args.steps):
+            ev[k][0].record(stream)
+            sim.step_graph(inner)
+            ev[k][1].record(stream)
+        R.barrier()
+        clk.window(t_start, time.perf_counter())
+    total_ms = R.max(sum(a.elapsed_time(b) for a, b in ev))
+    assert sim.status() == 0, "non-finite state"
+    value = world * N * inner * args.steps / (total_ms / 1e3) / 1e6
+    launch_ms = total_ms / (args.steps * inner)
+    bpc = sim.bytes_per_cell()
+    peak, peak_src = load_peaks()
+    achieved = N * bpc / (launch_ms / 1e3) / 1e9
+    # end to end: upload the state from pinned host memory, advance, read back the force and salinity planes
+    hf = torch.empty(19 * N, dtype=torch.float32, pin_memory=True)
+    hg = torch.empty(7 * N, dtype=torch.float32, pin_memory=True)
+    hF = torch.empty(3 * N, dtype=torch.float32, pin_memory=True)
+    sim.download(hf, hg, hF)
+    sim.sync()
+    R.barrier()
+    t0 = time.perf_counter()
+    for _ in range(max(3, args.steps)):
+        sim.upload(hf, hg, hF)
+        sim.step_graph(inner)
+        sim.download(None, hg, None)
+        sim.sync()
+    R.barrier()
+    e2e = world * N * inner * max(3, args.steps) / R.max(time.perf_counter() - t0) / 1e6
+    line = {
+        "metric": METRIC, "value": round(value, 2), "unit": METRIC, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(total_ms / args.steps, 4), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded linear stratification)",
+        "config": {"workload": f"3-D uniform box {nx}x{ny}x{nz} D3Q19 MRT + D3Q7, bounce-back",
+                   "lbm_steps_per_step": inner, "cells": N, "storage": "f32", "parallelism": f"replicas x{world}",
+                   "l2": f"inputs ({4 * 29 * N / 1e9:.2f} GB) larger than L2"},
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4), "traffic": None, "bytes_per_cell": bpc,
+                     "peak_source": f"{peak_src} (MEASURED_PEAKS.json hbm_gbs)" if peak_src == "measured" else peak_src},
+        "e2e": {"value": round(e2e, 2), "unit": METRIC,
+                "h2d_bytes_per_step": int(4 * (19 + 7 + 3) * N), "d2h_bytes_per_step": int(4 * 7 * N)},
+        "gpu_launches": args.steps * inner, "clocks": clk.summary(),
+    }
+    if R.rank == 0:
+        print(json.dumps(line), flush=True)
     R.close()
 
 
@@ -312,16 +399,22 @@ def run_reference(args):
 
 
 def run_serving(args):
-    """Continuous-batching serving stream (a scaled-down version of the
-    512-request serving configuration): 2-D lock-exchange requests on
-    log-uniform grids 128x128 .. 1024x512 with U[200, 2000] steps, Poisson
-    arrivals at 80 % of the measured batched capacity, FP16 storage, 150 GB
-    admission budget; reports p50/p99 completion latency and aggregate MLUPS
-    against the same jobs run one at a time in plain FP32."""
+    """Continuous-batching serving stream after the 512-request serving
+    configuration: 2-D requests, alternately lock exchange (salinity) and
+    Rayleigh-Taylor (Allen-Cahn phase field), on log-uniform grids
+    128x128 .. 1024x512 with U[200, 2000] steps (a tenth of the configured
+    2,000-20,000 to keep the run at a few seconds), FP16 storage, 150 GB
+    admission budget.
+      * capacity: every request submitted at t = 0, served by continuous
+        batching -> aggregate MLUPS (the headline value);
+      * latency: Poisson arrivals at 80 % of that capacity -> p50/p99
+        completion latency;
+      * baseline: the same jobs run one at a time in plain FP32.
+    The served velocities are compared with the FP32 runs (rel-L2)."""
     import torch
 
     from ip_cu_lbm_b200 import Sim
-    from ip_cu_lbm_b200.serving import Server, lock_exchange_request
+    from ip_cu_lbm_b200.serving import Server, lock_exchange_request, rayleigh_taylor_request
 
     torch.cuda.set_device(0)
     rng = np.random.default_rng(20261203)
@@ -330,20 +423,28 @@ def run_serving(args):
     nz = np.exp(rng.uniform(np.log(128), np.log(512), n)).astype(int) // 16 * 16
     steps = rng.integers(200, 2001, n)
     work = nx * nz * steps
-    mk = lambda i, t, storage: lock_exchange_request(i, int(nx[i]), int(nz[i]), int(steps[i]), arrival=t,
-                                                     storage=storage, seed=i)
+    def mk(i, t, storage):
+        kind = lock_exchange_request if i % 2 == 0 else rayleigh_taylor_request
+        return kind(i, int(nx[i]), int(nz[i]), int(steps[i]), arrival=t, storage=storage, seed=i)
+    # warm-up: one request through each path (kernel attributes, pools)
+    for storage in ("f16", "f32"):
+        w = Server(budget_bytes=150e9, tick_steps=200)
+        w.run([lock_exchange_request(0, 128, 128, 200, storage=storage),
+               rayleigh_taylor_request(1, 128, 128, 200, storage=storage)])
+        w.close()
     # capacity: everything submitted at once
     srv = Server(budget_bytes=150e9, tick_steps=200)
-    cal = srv.run([mk(i, 0.0, "f16") for i in range(min(n, 16))])
+    cap = srv.run([mk(i, 0.0, "f16") for i in range(n)])
+    served = {r.rid: r.result for r in srv.done}
     srv.close()
-    lam = 0.8 * cal["mlups"] * 1e6 / work.mean()
+    # latency under load: Poisson arrivals at 80 % of the measured capacity
+    lam = 0.8 * cap["mlups"] * 1e6 / work.mean()
     arrivals = np.cumsum(rng.exponential(1 / lam, n))
     arrivals -= arrivals[0]
     srv = Server(budget_bytes=150e9, tick_steps=200)
-    st = srv.run([mk(i, float(arrivals[i]), "f16") for i in range(n)])
-    served = {r.rid: r.result for r in srv.done}
+    lat = srv.run([mk(i, float(arrivals[i]), "f16") for i in range(n)])
     srv.close()
-    # serial plain FP32: the same jobs one at a time
+    # serial plain FP32: the same jobs one at a time through the same API
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     errs = []
@@ -351,22 +452,25 @@ def run_serving(args):
         r = mk(i, 0.0, "f32")
         s = Sim(r.nx, r.nz, s0=r.s0, **r.kwargs)
         s.step_graph(r.steps, chunk=200)
-        s.sync()
+        ux, uz = s.get("ux"), s.get("uz")
         if i < 8:
-            a = np.stack([s.get("ux"), s.get("uz")])
+            a = np.stack([ux, uz])
             b = np.stack([served[i]["ux"], served[i]["uz"]])
             errs.append(float(np.linalg.norm(b - a) / max(np.linalg.norm(a), 1e-30)))
         s.close()
     serial_s = time.perf_counter() - t0
     serial = float(work.sum()) / serial_s / 1e6
     print(json.dumps({
-        "metric": "served-batch MLUPS", "value": round(st["mlups"], 1), "unit": "MLUPS", "n_gpus": 1,
-        "requests": n, "p50_s": round(st["p50_s"], 4), "p99_s": round(st["p99_s"], 4),
-        "serial_fp32_mlups": round(serial, 1), "speedup_vs_serial_fp32": round(st["mlups"] / serial, 3),
-        "max_rel_l2_velocity_vs_fp32": max(errs) if errs else None, "arrival_rate_per_s": round(lam, 2),
-        "config": {"workload": "2-D lock exchange, log-uniform 128x128..1024x512, U[200,2000] steps, "
-                               "Poisson arrivals at 80% of batched capacity", "storage": "f16 served / f32 serial",
-                   "budget_gb": 150, "tick_steps": 200},
+        "metric": "served-batch MLUPS", "value": round(cap["mlups"], 1), "unit": "MLUPS", "n_gpus": 1,
+        "requests": n, "capacity_wall_s": round(cap["wall_s"], 3), "capacity_host_s": cap["host_s"],
+        "p50_s": round(lat["p50_s"], 4), "p99_s": round(lat["p99_s"], 4),
+        "offered_mlups": round(lat["mlups"], 1), "arrival_rate_per_s": round(lam, 2),
+        "serial_fp32_mlups": round(serial, 1), "speedup_vs_serial_fp32": round(cap["mlups"] / serial, 3),
+        "max_rel_l2_velocity_vs_fp32": max(errs) if errs else None,
+        "config": {"workload": "2-D lock exchange (salinity) and Rayleigh-Taylor (Allen-Cahn) requests, alternating, "
+                               "log-uniform 128x128..1024x512, U[200,2000] steps; capacity = all submitted at t=0, "
+                               "latency = Poisson arrivals at 80% of capacity",
+                   "storage": "f16 served / f32 serial", "budget_gb": 150, "tick_steps": 200},
         "higher_is_better": True}), flush=True)
 
 
@@ -380,7 +484,9 @@ def main():
     ap.add_argument("--inner", type=int, default=INNER)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--serving", action="store_true", help="run the continuous-batching serving stream instead")
-    ap.add_argument("--requests", type=int, default=64)
+    ap.add_argument("--requests", type=int, default=512)
+    ap.add_argument("--case", default="2d", choices=["2d", "3d"], help="3d: the C4-sized 3-D box")
+    ap.add_argument("--dims", default="160,160,640", help="3-D box nx,ny,nz (--case 3d)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -388,6 +494,8 @@ def main():
         run_serving(args)
     elif args.impl == "reference":
         run_reference(args)
+    elif args.case == "3d":
+        run_3d(args)
     else:
         run_ours(args)
 

@@ -221,6 +221,7 @@ int ipcu_add_scalar_f32(float *data, int64_t n, float value, ipcu_stream_t strea
  * 2. Structured-grid solver (fused B200 path)
  * ====================================================================== */
 #include "ipcu_sim.h"
+#include "ipcu_sim3d.h"
 
 #ifdef __cplusplus
 }

@@ -2,13 +2,20 @@
  * ipcu_sim.h -- structured-grid solver of libipcu (included by ipcu.h).
  *
  * One simulation = one rectangular box of nx x nz cells (2-D, x-z plane,
- * D2Q9 flow) with a passive salinity lattice (D2Q5 or the reference's Q9
- * scalar), rectilinear coordinates and one interpolated axis. Each step is
- * the reference's LockExchange step (ref: LockExchange/LockExchange.cu:
- * 220-236 without the wall model): equilibrium, force, MRT/SRT collision,
- * conservative interpolated streaming of f, regularised scalar collision
- * and streaming of g, then the moments -- fused into one kernel launch that
- * reads each stored value once and writes it once.
+ * D2Q9 flow) with a scalar lattice (D2Q5 or the reference's Q9 scalar),
+ * rectilinear coordinates and one interpolated axis. The scalar is either
+ *   - salinity (IPCU_SCALAR_SALINITY): each step is the reference's
+ *     LockExchange step (ref: LockExchange/LockExchange.cu:220-236 without
+ *     the wall model): equilibrium, Boussinesq force, MRT/SRT collision,
+ *     conservative interpolated streaming of f, regularised scalar
+ *     collision and streaming of g, then the moments; or
+ *   - the Allen-Cahn phase field (IPCU_SCALAR_PHASE): the reference's
+ *     two-phase step (ref: RTinstability/RTinstability.cu:177-206):
+ *     rho = rhoL + (rhoH - rhoL) phi, surface tension and the mixture's
+ *     weight in the force, the conservative Allen-Cahn collision with its
+ *     d(phi u)/dt term (function/collision.cu:57-113,190-223);
+ * fused into one kernel launch that reads each stored value once and
+ * writes it once.
  *
  * Storage: structure-of-arrays, x fastest, ping-pong buffers resident in
  * HBM; distributions in FP32 or in FP16/BF16 (the pressure-form f is a
@@ -33,6 +40,9 @@
 #define IPCU_WALL_SLIP 0 /* specular reflection, reference set_bound2D tables */
 #define IPCU_WALL_BB 1   /* halfway bounce-back */
 
+#define IPCU_SCALAR_SALINITY 0 /* passive salinity, Boussinesq buoyancy */
+#define IPCU_SCALAR_PHASE 1    /* conservative Allen-Cahn phase field, two-phase density */
+
 typedef struct ipcu_sim_config {
   int32_t nx, nz;       /* cells */
   int32_t q_scalar;     /* 0 none, 5 D2Q5, 9 reference Q9 scalar */
@@ -40,21 +50,26 @@ typedef struct ipcu_sim_config {
   int32_t storage;      /* IPCU_STORE_* */
   int32_t wall;         /* IPCU_WALL_* on all four walls */
   int32_t mrt;          /* 1 MRT (matrices below), 0 SRT */
-  int32_t reserved;
+  int32_t scalar_kind;  /* IPCU_SCALAR_* (phase field needs q_scalar 5 or 9) */
   double dz;            /* lattice spacing; c = dz/dt */
   double dt;
   const double *x;      /* host, nx cell centres (NULL: (i+0.5)*dz) */
   const double *z;      /* host, nz cell centres (NULL: (l+0.5)*dz) */
   const double *wx;     /* host, nx cell widths (NULL: dz) */
   const double *wz;     /* host, nz cell widths (NULL: dz) */
-  double tau, taus;     /* relaxation times of f and g */
-  double rhoL, rhoH, phi; /* rho = rhoL + (rhoH-rhoL)*phi + rho_sal*S */
+  double tau, taus;     /* relaxation times of f and g (phase field: tau_phi; the reference fixes 0.58) */
+  double rhoL, rhoH, phi; /* salinity: rho = rhoL + (rhoH-rhoL)*phi + rho_sal*S; phase field:
+                             rho = rhoL + (rhoH-rhoL)*phi(x) with phi the scalar field */
   double rho_sal;       /* reference: 0.824493 */
   double g_bouss;       /* buoyancy Fz = -g_bouss*S (reference: 0.824493*9.81) */
-  double s_ref;         /* salinity shift for reduced-precision g storage */
+  double s_ref;         /* unused (16-bit storage keeps deviations from the local equilibrium) */
   const double *M;      /* host 9x9 moment matrix (row-major), MRT only */
   const double *Minv;   /* host 9x9 inverse */
   const double *S;      /* host 9 relaxation rates (shear entries 7,8 are replaced by 1/tau) */
+  /* phase field only */
+  double sigma;         /* surface tension */
+  double pf_width;      /* interface thickness W (reference: items PFthick) */
+  double gravity;       /* weight -rho*gravity along z (reference: 9.81) */
 } ipcu_sim_config;
 
 typedef struct ipcu_sim ipcu_sim;
@@ -120,12 +135,24 @@ int ipcu_sim_totals(ipcu_sim *sim, double *sum_p, double *sum_s);
  * serving): each call advances every listed simulation by nsteps with one
  * launch per step per kernel class (storage, scalar lattice, geometry); CTAs
  * walk a device work list of (simulation, tile). A simulation's arithmetic is
- * the same tile by tile as when it runs alone. Synchronous; the simulations'
- * own streams must be idle. */
+ * the same tile by tile as when it runs alone. Synchronous; the batch
+ * stream first waits (on the device) for work already queued on each
+ * simulation's own stream. */
 typedef struct ipcu_batch ipcu_batch;
 int ipcu_batch_create(ipcu_stream_t stream, ipcu_batch **out);
 void ipcu_batch_destroy(ipcu_batch *batch);
 int ipcu_batch_step(ipcu_batch *batch, ipcu_sim *const *sims, int n, int64_t nsteps);
+/* The same steps enqueued without waiting: each listed simulation's own
+ * stream is ordered after them, so its reads, further steps and destruction
+ * see the results; ipcu_batch_sync waits for everything enqueued. A server
+ * admits new requests on the host while the GPU runs the batch. */
+int ipcu_batch_launch(ipcu_batch *batch, ipcu_sim *const *sims, int n, int64_t nsteps);
+int ipcu_batch_sync(ipcu_batch *batch);
+/* Progress marks: ipcu_batch_mark records the point reached by everything
+ * enqueued so far and returns its handle (a ring of 4); ipcu_batch_wait_mark
+ * waits for it. A server keeps the host one tick ahead of the GPU with them. */
+int ipcu_batch_mark(ipcu_batch *batch);
+int ipcu_batch_wait_mark(ipcu_batch *batch, int mark);
 /* Device bytes a simulation holds (state, ping-pong, tables). */
 int64_t ipcu_sim_device_bytes(const ipcu_sim *sim);
 

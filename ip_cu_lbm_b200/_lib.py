@@ -60,13 +60,23 @@ class SimConfig(ctypes.Structure):
     _fields_ = [
         ("nx", ctypes.c_int32), ("nz", ctypes.c_int32), ("q_scalar", ctypes.c_int32),
         ("geometry", ctypes.c_int32), ("storage", ctypes.c_int32), ("wall", ctypes.c_int32),
-        ("mrt", ctypes.c_int32), ("reserved", ctypes.c_int32),
+        ("mrt", ctypes.c_int32), ("scalar_kind", ctypes.c_int32),
         ("dz", ctypes.c_double), ("dt", ctypes.c_double),
         ("x", ctypes.c_void_p), ("z", ctypes.c_void_p), ("wx", ctypes.c_void_p), ("wz", ctypes.c_void_p),
         ("tau", ctypes.c_double), ("taus", ctypes.c_double),
         ("rhoL", ctypes.c_double), ("rhoH", ctypes.c_double), ("phi", ctypes.c_double),
         ("rho_sal", ctypes.c_double), ("g_bouss", ctypes.c_double), ("s_ref", ctypes.c_double),
         ("M", ctypes.c_void_p), ("Minv", ctypes.c_void_p), ("S", ctypes.c_void_p),
+        ("sigma", ctypes.c_double), ("pf_width", ctypes.c_double), ("gravity", ctypes.c_double),
+    ]
+
+
+class Sim3DConfig(ctypes.Structure):
+    """Mirror of ipcu_sim3d_config (include/ipcu_sim3d.h)."""
+    _fields_ = [
+        ("nx", ctypes.c_int32), ("ny", ctypes.c_int32), ("nz", ctypes.c_int32), ("mrt", ctypes.c_int32),
+        ("dz", ctypes.c_double), ("dt", ctypes.c_double), ("tau", ctypes.c_double), ("taus", ctypes.c_double),
+        ("rho0", ctypes.c_double), ("rho_sal", ctypes.c_double), ("g_bouss", ctypes.c_double),
     ]
 
 
@@ -115,7 +125,23 @@ def _declare(L: ctypes.CDLL) -> None:
         "ipcu_batch_create": ([P, ctypes.POINTER(P)], I),
         "ipcu_batch_destroy": ([P], None),
         "ipcu_batch_step": ([P, P, I, I64], I),
+        "ipcu_batch_launch": ([P, P, I, I64], I),
+        "ipcu_batch_sync": ([P], I),
+        "ipcu_batch_mark": ([P], I),
+        "ipcu_batch_wait_mark": ([P, I], I),
         "ipcu_sim_device_bytes": ([P], I64),
+        "ipcu_sim3d_create": ([ctypes.POINTER(Sim3DConfig), P, P, ctypes.POINTER(P)], I),
+        "ipcu_sim3d_destroy": ([P], None),
+        "ipcu_sim3d_step": ([P, I64], I),
+        "ipcu_sim3d_step_graph": ([P, I64], I),
+        "ipcu_sim3d_get": ([P, ctypes.c_char_p, P, I64], I),
+        "ipcu_sim3d_set_state": ([P, P, P, P], I),
+        "ipcu_sim3d_upload": ([P, P, P, P], I),
+        "ipcu_sim3d_download": ([P, P, P, P], I),
+        "ipcu_sim3d_sync": ([P], I),
+        "ipcu_sim3d_status": ([P, ctypes.POINTER(ctypes.c_uint32)], I),
+        "ipcu_sim3d_cells": ([P], I64),
+        "ipcu_sim3d_bytes_per_cell": ([P], I64),
         "ipcu_build_box_device_f32": ([I, I, I, I, D, D, D, P, P, P, P, P, P, P, P, P, I64, P,
                                        ctypes.POINTER(I64), ctypes.POINTER(I64), P], I),
         "ipcu_build_box_device_f64": ([I, I, I, I, D, D, D, P, P, P, P, P, P, P, P, P, I64, P,

@@ -1,5 +1,6 @@
 // Parameters of the fused 2-D step kernel (fused2d.cu).
 #pragma once
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -12,14 +13,23 @@ constexpr int kTX = 32;  // tile width along x (one warp per row)
 constexpr int kTZ = 16;  // tile height along z
 constexpr int kThreads = 256;
 constexpr int kMinBlocks = 4;  // resident CTAs per SM the register budget is sized for
+constexpr int kTmaBoxX = kTX + 8;  // TMA box width: [x0-4, x0+kTX+4), 16-byte aligned start
 
-struct Params {
+// halo rows of the streaming stencil along z (1 unless z is the interpolated axis)
+inline int halo_z(int geo) { return geo == IPCU_GEO_Z5 ? 3 : (geo == IPCU_GEO_Z3 ? 2 : 1); }
+
+struct alignas(64) Params {
+  // TMA descriptors of the ping-pong buffers (FP32 storage, nx % 4 == 0):
+  // f [9][nz][nx], g [q][nz][nx], macroscopic [3][nz][nx]; boxes sized for
+  // the tile + halo (f, g) and the salinity ring rows (macroscopic)
+  CUtensorMap tm_f[2], tm_g[2], tm_m[2];
+  int tma;  // 1: the single-simulation kernel stages with the maps above
   int nx, nz;
   int mrt, wall;  // mrt: 0 BGK, 1 general MRT, 2 MRT with unit non-shear rates (two-moment form)
   // ping-pong state; a step reads buffer (cur ^ parity) and writes the other
   void *fbuf[2];
   void *gbuf[2];
-  float *mbuf[2];  // [3][N]: S, ux, uz
+  float *mbuf[2];  // [3][N]: S, ux, uz; 16-bit storage adds p* as a 4th plane
   int cur;
   // interpolated axis: weights [2][NA][NS], fin scale [2][NA], fout scale [NA],
   // and the interior cells' combined flux weights [2][NS+1][NA]
@@ -28,9 +38,23 @@ struct Params {
   const float *ginvx, *ginvz;
   float c, dt, tau, taus;
   float fk3, hdt;  // 3 dt / c (forcing term per unit density) and dt / 2
+  // rho = rho_base + rho_sal_f * S: salinity (base rhoL + (rhoH - rhoL) phi)
+  // or the phase field phi (base rhoL, slope rhoH - rhoL)
+  float rho_base;
+  // phase field: obuf[2] = [2][N] phi u, phi w of the previous step;
+  // ilx2, ilz2 = 1/dx^2, 1/dz^2 per column / row (Laplacian of phi);
+  // 4 beta = 48 sigma / W, kappa = 1.5 sigma W, 1/W,
+  // (tau_phi - 1/2)/tau_phi, gravity
+  float *obuf[2];
+  const float *ilx2, *ilz2;
+  float pf_beta4, pf_kap, pf_invw, pf_lam, grav;
+  int pf;
   float rhoL, rhoH, phi;
   double rho_sal, g_bouss;
-  float fscale, inv_fscale, gscale, inv_gscale, s_ref;
+  float rho_sal_f, g_bouss_f;
+  // 16-bit storage: stored = (value - equilibrium) * scale; store_max is the
+  // largest finite stored magnitude (FP16 65504)
+  float fscale, inv_fscale, gscale, inv_gscale, store_max;
   float MM[81];   // Minv diag(S) M with the shear rates zeroed
   float Ms[18];   // shear rows 7, 8 of M
   float Mis[18];  // shear columns 7, 8 of Minv, [a][2]
@@ -39,7 +63,8 @@ struct Params {
   unsigned *status;
 };
 
-// prepare_only: set the kernel's shared-memory attribute (call once before any capture)
+// prepare_only: set the kernel's shared-memory attribute (call once before any capture);
+// p.pf selects the phase-field kernels
 int launch_step(const Params &p, int storage, int qs, int geo, cudaStream_t s, bool prepare_only = false);
 
 // One work item of a batched step: simulation index and tile coordinates.
@@ -51,7 +76,7 @@ struct WorkItem {
 // arrays; `parity` flips the ping-pong buffers of all of them. `grid` CTAs
 // loop over the work list.
 int launch_batched(const Params *params, const WorkItem *work, int nwork, int parity, int storage, int qs, int geo,
-                   int grid, cudaStream_t s, bool prepare_only = false);
+                   int pf, int grid, cudaStream_t s, bool prepare_only = false);
 
 }  // namespace f2d
 }  // namespace ipcu

@@ -1,27 +1,8 @@
-// Instantiations of the fused 2-D step for __half distribution storage.
+// Instantiations of the fused 2-D step for FP16 distribution storage, salinity scalar.
 #include "fused2d_impl.cuh"
 
 namespace ipcu {
 namespace f2d {
-
-int launch_f16(const Params &p, int qs, int geo, cudaStream_t s, bool prep) {
-  switch (qs) {
-    case 0: return launch_g<__half, 0>(p, geo, s, prep);
-    case 5: return launch_g<__half, 5>(p, geo, s, prep);
-    case 9: return launch_g<__half, 9>(p, geo, s, prep);
-  }
-  return IPCU_ERR_UNSUPPORTED;
-}
-
-int launch_batched_f16(const Params *ps, const WorkItem *work, int nwork, int parity, int qs, int geo, int grid,
-                        cudaStream_t s, bool prep) {
-  switch (qs) {
-    case 0: return launch_bg<__half, 0>(ps, work, nwork, parity, geo, grid, s, prep);
-    case 5: return launch_bg<__half, 5>(ps, work, nwork, parity, geo, grid, s, prep);
-    case 9: return launch_bg<__half, 9>(ps, work, nwork, parity, geo, grid, s, prep);
-  }
-  return IPCU_ERR_UNSUPPORTED;
-}
-
+IPCU_F2D_INSTANTIATE(__half, f16, 0)
 }  // namespace f2d
 }  // namespace ipcu

@@ -1,27 +1,8 @@
-// Instantiations of the fused 2-D step for float distribution storage.
+// Instantiations of the fused 2-D step for float distribution storage, salinity scalar.
 #include "fused2d_impl.cuh"
 
 namespace ipcu {
 namespace f2d {
-
-int launch_f32(const Params &p, int qs, int geo, cudaStream_t s, bool prep) {
-  switch (qs) {
-    case 0: return launch_g<float, 0>(p, geo, s, prep);
-    case 5: return launch_g<float, 5>(p, geo, s, prep);
-    case 9: return launch_g<float, 9>(p, geo, s, prep);
-  }
-  return IPCU_ERR_UNSUPPORTED;
-}
-
-int launch_batched_f32(const Params *ps, const WorkItem *work, int nwork, int parity, int qs, int geo, int grid,
-                        cudaStream_t s, bool prep) {
-  switch (qs) {
-    case 0: return launch_bg<float, 0>(ps, work, nwork, parity, geo, grid, s, prep);
-    case 5: return launch_bg<float, 5>(ps, work, nwork, parity, geo, grid, s, prep);
-    case 9: return launch_bg<float, 9>(ps, work, nwork, parity, geo, grid, s, prep);
-  }
-  return IPCU_ERR_UNSUPPORTED;
-}
-
+IPCU_F2D_INSTANTIATE(float, f32, 0)
 }  // namespace f2d
 }  // namespace ipcu

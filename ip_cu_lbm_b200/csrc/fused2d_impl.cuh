@@ -5,14 +5,18 @@
 // (ref: LockExchange/LockExchange.cu:220-236; kernels in function/collision.cu,
 // function/adv.cu, function/set_bound.cu, function/propagation.cu).
 //
-// One launch per time step. A CTA owns a kTX x kTZ tile; phase 0 stages the
-// salinity/density ring and the tile's axis weights, phase 1 collides the
-// tile plus its streaming halo (HX cells along x, HZ along z) straight from
-// HBM into shared memory, phase 2 evaluates the reference's conservative
-// interpolated streaming for the interior from shared memory, forms the
-// moments and writes the new state. Every stored value is read from HBM once
-// and written once per step (halo re-reads hit L2). Storage is
-// structure-of-arrays, x fastest, so each warp touches 128-byte lines.
+// One launch per time step. A CTA owns a kTX x kTZ tile. Phase 0 stages the
+// tile, its streaming halo (HX cells along x, HZ along z) and the salinity
+// ring one cell wider: with FP32 storage and nx a multiple of 4 as three TMA
+// box loads (f, g and the S/u_x/u_z planes, cp.async.bulk.tensor completing
+// on one mbarrier), otherwise the ring through registers while phase 1 loads
+// f, g, u itself. Phase 1 collides tile + halo into shared memory, phase 2
+// evaluates the reference's conservative interpolated streaming for the
+// interior from shared memory, forms the moments and writes the new state.
+// Every stored value is read from HBM once and written once per step (halo
+// re-reads hit L2). Storage is structure-of-arrays, x fastest. With 16-bit
+// storage the populations are kept as deviations from the local
+// equilibrium (storage.cuh).
 //
 // The streaming reproduces IP_process on a rectilinear box exactly:
 //   ftmp(j,k) = f*(j+a,k) + (fin(j,k) - fout(j+a,k))        (adv.cu:234-244)
@@ -32,10 +36,12 @@
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 
+#include <cstddef>
 #include <type_traits>
 
 #include "fused2d.cuh"
 #include "ipcu_common.cuh"
+#include "storage.cuh"
 
 namespace ipcu {
 namespace f2d {
@@ -56,25 +62,82 @@ __host__ __device__ constexpr float w5(int k) { return k == 0 ? 1.0f / 3.0f : 1.
 template <int Q>
 __host__ __device__ constexpr float wq(int k) { return Q == 5 ? w5(k) : w9(k); }
 
-template <int GEO>
+// Tile geometry. TMA staging needs the smem box to start on a 16-byte
+// boundary in x, so its rows span [x0-4, x0+kTX+4) (40 floats); register
+// staging keeps just the halo columns.
+template <int GEO, bool TMA>
 struct Geo {
   static constexpr int AX = (GEO == IPCU_GEO_X5 || GEO == IPCU_GEO_X3) ? 0 : ((GEO == IPCU_GEO_Z5 || GEO == IPCU_GEO_Z3) ? 1 : -1);
   static constexpr int NS = (GEO == IPCU_GEO_X5 || GEO == IPCU_GEO_Z5) ? 5 : ((GEO == IPCU_GEO_X3 || GEO == IPCU_GEO_Z3) ? 3 : 1);
   static constexpr int H = NS == 5 ? 3 : (NS == 3 ? 2 : 1);
   static constexpr int HX = AX == 0 ? H : 1;
   static constexpr int HZ = AX == 1 ? H : 1;
-  static constexpr int EX = kTX + 2 * HX, EZ = kTZ + 2 * HZ, NE = EX * EZ;
-  static constexpr int SX = EX + 2, SZ = EZ + 2;  // density ring for the gradient
+  static constexpr int XO = TMA ? 4 : HX;               // smem column of the tile's first cell
+  static constexpr int EX = TMA ? kTX + 8 : kTX + 2 * HX;
+  static constexpr int EZ = kTZ + 2 * HZ, NE = EX * EZ;
+  static constexpr int CX0 = XO - HX, CW = kTX + 2 * HX;  // columns that are collided
+  static constexpr int NC = CW * EZ;
+  // salinity ring (rows z0-HZ-1 .. z0+kTZ+HZ): TMA shares the tile's columns,
+  // register staging keeps one extra column on each side
+  static constexpr int RX = TMA ? EX : EX + 2, RO = TMA ? 0 : 1, SZ = EZ + 2;
   static constexpr int NWA = AX == 0 ? EX : (AX == 1 ? EZ : 0);
-  static constexpr int WREC = NS + 2;             // NS weights, fin scale, fout scale
+  static constexpr int WREC = NS + 2;                     // NS weights, fin scale, fout scale
+  static_assert(!TMA || EX == kTmaBoxX, "tensor-map box width");
 };
 
-template <class ST, int QS, int GEO>
-constexpr size_t smem_bytes() {
-  using G = Geo<GEO>;
-  return sizeof(float) * ((9 + QS) * G::NE + 2 * G::SX * G::SZ + 2 * kTX * kTZ + 2 * G::NWA * G::WREC +
-                          2 * G::NWA * (G::NS + 1));
+// Cells next to a wall are queued in shared memory and processed after the
+// interior cells by a compacted set of threads (up to kQueue per tile; more
+// are processed in place). At the C2 size a tile has at most ~80 of them.
+constexpr int kQueue = 127;
+
+// Shared-memory layout in floats; TMA destinations start on 128-byte boundaries.
+template <int QS, int GEO, bool TMA>
+struct Smem {
+  using G = Geo<GEO, TMA>;
+  static constexpr int al(int v, int a) { return (v + a - 1) / a * a; }
+  static constexpr int G0 = al(9 * G::NE, 32);                   // g tile
+  static constexpr int S0 = al(G0 + QS * G::NE, 32);             // ring (TMA: S, u_x, u_z planes)
+  static constexpr int F0 = S0 + (TMA ? 3 : 1) * G::SZ * G::RX;  // registers: interior force
+  static constexpr int W0 = F0 + (TMA ? 0 : 2 * kTX * kTZ);      // axis weights
+  static constexpr int C0 = W0 + 2 * G::WREC * G::NWA;            // combined interior weights
+  static constexpr int B0 = al(C0 + 2 * (G::NS + 1) * G::NWA, 2);  // mbarrier
+  static constexpr int Q0 = B0 + 4;                                // wall-cell queue: count + kQueue slots
+  static constexpr size_t bytes = sizeof(float) * (size_t)(Q0 + 1 + kQueue);
+};
+template <int QS, int GEO, bool TMA>
+constexpr size_t smem_bytes() { return Smem<QS, GEO, TMA>::bytes; }
+
+__device__ __forceinline__ unsigned smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(unsigned bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
+__device__ __forceinline__ void mbar_expect_tx(unsigned bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+// 3-D tiled TMA load (no multicast) into this CTA's shared memory
+__device__ __forceinline__ void tma_load_3d(unsigned dst, const CUtensorMap *map, int x, int y, int z, unsigned bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];"
+      ::"r"(dst), "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(bar)
+      : "memory");
+}
+// Waits for phase `phase` of the barrier, giving up after `limit` clock cycles.
+__device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned phase, long long limit) {
+  const long long t0 = clock64();
+  while (true) {
+    unsigned done;
+    asm volatile(
+        "{\n .reg .pred P;\n mbarrier.try_wait.parity.shared::cta.b64 P, [%1], %2;\n selp.u32 %0, 1, 0, P;\n}"
+        : "=r"(done)
+        : "r"(bar), "r"(phase)
+        : "memory");
+    if (done) return true;
+    if (clock64() - t0 > limit) return false;
+  }
+}
+constexpr long long kWaitLimit = 2000000000LL;  // ~1 s at the B200 boost clock
 
 // storage conversion: value = stored*inv_scale
 template <class ST>
@@ -102,9 +165,9 @@ __device__ __forceinline__ void st(ST *p, long long i, float v, float scale) {
 // holds the combined flux weights of its axis position for both signs of
 // the axis velocity (see axis_tables on the host), so the flux form is one
 // dot product over the NS+1 nodes around the source cell.
-template <int GEO, int K>
+template <int GEO, bool TMA, int K>
 struct Fast {
-  using G = Geo<GEO>;
+  using G = Geo<GEO, TMA>;
   static constexpr int DA = G::AX == 0 ? 1 : G::EX;   // one cell along the interpolated axis
   static constexpr int A = G::AX == 0 ? ex(K) : (G::AX == 1 ? ez(K) : 0);
   static constexpr int BX = G::AX == 0 ? 0 : ex(K);   // shift-axis part of e_K
@@ -125,24 +188,32 @@ struct Fast {
 };
 
 // One tile of one step; shared by the single-simulation kernel (parameters in
-// the kernel's constant bank) and the batched kernel (parameters in global memory).
-template <class ST, int QS, int GEO>
+// the kernel's constant bank) and the batched kernel (parameters in global
+// memory). TMA: stage with tensor-map box loads (single-simulation FP32
+// kernel; the tensor maps live in the __grid_constant__ parameters).
+template <class ST, int QS, int GEO, bool TMA, int PHYS>
 __device__ __forceinline__ void step_tile(const Params &p, int parity, int tile_x, int tile_z, float *smem) {
-  using G = Geo<GEO>;
-  constexpr int HX = G::HX, HZ = G::HZ, EX = G::EX, NE = G::NE, SX = G::SX, SZ = G::SZ;
-  constexpr int NWA = G::NWA, WREC = G::WREC;
-  float *sf = smem;                       // [9][EZ][EX] post-collision f
-  float *sg = sf + 9 * NE;                // [QS][EZ][EX] post-collision g
-  float *sS = sg + QS * NE;               // [SZ][SX] salinity
-  float *sR = sS + SZ * SX;               // [SZ][SX] density
-  float *sF = sR + SZ * SX;               // [2][kTZ][kTX] interior force
-  float *sW = sF + 2 * kTX * kTZ;         // [2][WREC][NWA] axis weights
-  float *sC = sW + 2 * WREC * NWA;        // [2][NS+1][NWA] combined interior weights
+  using G = Geo<GEO, TMA>;
+  using SL = Smem<QS, GEO, TMA>;
+  constexpr int HZ = G::HZ, EX = G::EX, NE = G::NE, SZ = G::SZ, RX = G::RX, RO = G::RO;
+  constexpr int XO = G::XO, NWA = G::NWA, WREC = G::WREC;
+  // RES (16-bit storage): f and g hold deviations from the local
+  // equilibrium, p* comes from its own FP32 plane
+  constexpr bool RES = sizeof(ST) == 2;
+  static_assert(!TMA || sizeof(ST) == 4, "TMA staging is for FP32 storage");
+  float *sf = smem;            // [9][EZ][EX] f, collided in place
+  float *sg = smem + SL::G0;   // [QS][EZ][EX] g
+  float *sS = smem + SL::S0;   // [SZ][RX] salinity ring (TMA: then the u_x, u_z planes)
+  float *sF = smem + SL::F0;   // registers: [2][kTZ][kTX] interior force
+  float *sW = smem + SL::W0;   // [2][WREC][NWA] axis weights
+  float *sC = smem + SL::C0;   // [2][NS+1][NWA] combined interior weights
+  uint64_t *bar = reinterpret_cast<uint64_t *>(smem + SL::B0);
+  int *qcount = reinterpret_cast<int *>(smem + SL::Q0), *queue = qcount + 1;
 
   const int nx = p.nx, nz = p.nz;
   const long long N = (long long)nx * nz;
   const int x0 = tile_x * kTX, z0 = tile_z * kTZ;
-  const int ox = x0 - HX, oz = z0 - HZ;  // global coords of local (0,0)
+  const int ox = x0 - XO, oz = z0 - HZ;  // global coords of smem (0,0)
   const int tid = threadIdx.x;
   const int bi = p.cur ^ parity, bo = bi ^ 1;
   const ST *__restrict__ f_in = static_cast<const ST *>(p.fbuf[bi]);
@@ -152,17 +223,33 @@ __device__ __forceinline__ void step_tile(const Params &p, int parity, int tile_
   const float *__restrict__ mac_in = p.mbuf[bi];
   float *__restrict__ mac_out = p.mbuf[bo];
 
-  // density as the reference forms it: float base plus a double salinity
-  // term, rounded once (ref: collision.cu:251)
-  const float rho0 = p.rhoL + (p.rhoH - p.rhoL) * p.phi;
+  // density from the scalar, in FP32 (ref: collision.cu:251): salinity
+  // rhoL + (rhoH - rhoL) phi + rho_sal S, or the phase-field mixture
+  // rhoL + (rhoH - rhoL) phi(x) (PHYS 1: the scalar is phi)
+  static_assert(PHYS == 0 || QS > 0, "the phase field lives on the scalar lattice");
+  const float rho0 = p.rho_base, rsal = p.rho_sal_f;
+  auto rho_of = [&](float S) { return fmaf(S, rsal, rho0); };
 
-  // ---- phase 0: stage the salinity/density ring and the axis weights
-  for (int e = tid; e < SX * SZ; e += kThreads) {
-    const int lz = e / SX, lx = e - lz * SX;
-    const int gx = min(max(ox - 1 + lx, 0), nx - 1), gz = min(max(oz - 1 + lz, 0), nz - 1);
-    const float S = mac_in[(long long)gz * nx + gx];
-    sS[e] = S;
-    sR[e] = (float)((double)rho0 + (double)S * p.rho_sal);
+  // ---- phase 0: stage the tile (TMA) or the salinity ring, and the axis weights
+  if (tid == 0) *qcount = 0;
+  unsigned bar_a = 0;
+  if constexpr (TMA) {
+    bar_a = smem_u32(bar);
+    if (tid == 0) mbar_init(bar_a, 1);
+    __syncthreads();
+    if (tid == 0) {
+      constexpr unsigned bytes = 4u * (unsigned)((9 + QS) * NE + 3 * SZ * RX);
+      mbar_expect_tx(bar_a, bytes);
+      tma_load_3d(smem_u32(sf), &p.tm_f[bi], ox, oz, 0, bar_a);
+      if constexpr (QS > 0) tma_load_3d(smem_u32(sg), &p.tm_g[bi], ox, oz, 0, bar_a);
+      tma_load_3d(smem_u32(sS), &p.tm_m[bi], ox, oz - 1, 0, bar_a);
+    }
+  } else {
+    for (int e = tid; e < SZ * RX; e += kThreads) {
+      const int lz = e / RX, lx = e - lz * RX;
+      const int gx = min(max(ox - RO + lx, 0), nx - 1), gz = min(max(oz - 1 + lz, 0), nz - 1);
+      sS[e] = mac_in[(long long)gz * nx + gx];
+    }
   }
   if constexpr (G::AX >= 0) {
     const int NA = (G::AX == 0) ? nx : nz, oA = (G::AX == 0) ? ox : oz;
@@ -181,35 +268,86 @@ __device__ __forceinline__ void step_tile(const Params &p, int parity, int tile_
       sC[e] = __ldg(p.wC + (long long)r * NA + min(max(oA + la, 0), NA - 1));
     }
   }
+  if constexpr (TMA) {
+    // every thread observes the barrier phase itself; the decision to go on
+    // is made block-wide so that all threads leave together on a timeout
+    const bool ok = __syncthreads_and(mbar_wait(bar_a, 0, kWaitLimit));
+    if (!ok) {
+      if (tid == 0) atomicOr(p.status, 4u);
+      mbar_wait(bar_a, 0, kWaitLimit);  // let copies still in flight land before the CTA exits
+      return;
+    }
+    // the box reads zeros outside the domain: give the ring's outside cells
+    // their clamped (owner) salinity, as the ghosts carry it
+    if (ox < 0 || ox + EX > nx || oz - 1 < 0 || oz - 1 + SZ > nz) {
+      for (int e = tid; e < SZ * RX; e += kThreads) {
+        const int lz = e / RX, lx = e - lz * RX;
+        const int gx = ox + lx, gz = oz - 1 + lz;
+        if (gx >= 0 && gx < nx && gz >= 0 && gz < nz) continue;
+        const int cx = min(max(gx, 0), nx - 1) - ox, cz = min(max(gz, 0), nz - 1) - (oz - 1);
+        sS[e] = sS[cz * RX + cx];
+      }
+    }
+  }
   __syncthreads();
 
-  const float c = p.c, c2 = c * c, ic = 1.0f / c, dt = p.dt;
+  const float c = p.c, c2 = c * c, ic = 1.0f / c;
   const float itau = 1.0f / p.tau, omg = 1.0f - 1.0f / p.taus;
   const float ifs = p.inv_fscale, igs = p.inv_gscale;
   const float om_shear = 1.0f - itau;
 
-  // ---- phase 1: collide tile + halo into shared memory
-  for (int e = tid; e < NE; e += kThreads) {
-    const int lz = e / EX, lx = e - lz * EX;
+  // ---- phase 1: collide tile + halo in shared memory
+  for (int i = tid; i < G::NC; i += kThreads) {
+    const int lz = i / G::CW, lx = G::CX0 + (i - lz * G::CW);
     const int gx = ox + lx, gz = oz + lz;
     if (gx < 0 || gx >= nx || gz < 0 || gz >= nz) continue;
-    float f[9], g[QS > 0 ? QS : 1];
-    const long long ci = (long long)gz * nx + gx;
+    const int e = lz * EX + lx;              // tile slot
+    const int rs = (lz + 1) * RX + lx + RO;  // ring slot
+    float f[9], g[QS > 0 ? QS : 1], u, w, pr = 0.f;
+    if constexpr (TMA) {
 #pragma unroll
-    for (int k = 0; k < 9; k++) f[k] = ld(f_in, k * N + ci, ifs);
+      for (int k = 0; k < 9; k++) f[k] = sf[k * NE + e];
 #pragma unroll
-    for (int k = 0; k < QS; k++) g[k] = ld(g_in, k * N + ci, igs) + wq<QS>(k) * p.s_ref;
-    const float u = mac_in[N + ci], w = mac_in[2 * N + ci];
-    const int rs = (lz + 1) * SX + lx + 1;
-    const float S = sS[rs], rho = sR[rs];
+      for (int k = 0; k < QS; k++) g[k] = sg[k * NE + e];
+      u = sS[SZ * RX + rs];
+      w = sS[2 * SZ * RX + rs];
+    } else {
+      const long long ci = (long long)gz * nx + gx;
+#pragma unroll
+      for (int k = 0; k < 9; k++) f[k] = ld(f_in, k * N + ci, ifs);
+#pragma unroll
+      for (int k = 0; k < QS; k++) g[k] = ld(g_in, k * N + ci, igs);
+      u = mac_in[N + ci];
+      w = mac_in[2 * N + ci];
+      if constexpr (RES) pr = mac_in[3 * N + ci];
+    }
+    const float S = sS[rs], rho = rho_of(S);
     // p* (ref: collision.cu:244-246)
-    float pr = 0.f;
+    if constexpr (!RES) {
 #pragma unroll
-    for (int k = 0; k < 9; k++) pr += f[k];
-    // force: buoyancy + pressure gradient on the density (ref: collision.cu:77-88)
+      for (int k = 0; k < 9; k++) pr += f[k];
+    }
+    // force: buoyancy (salinity) or surface tension + weight (phase field),
+    // plus the pressure gradient on the density (ref: collision.cu:57-112)
     const float pc = pr * c2 / 3.0f;
-    const float Fx = -pc * ((sR[rs + 1] - sR[rs - 1]) * __ldg(p.ginvx + gx));
-    const float Fz = (float)(-(double)S * p.g_bouss) - pc * ((sR[rs + SX] - sR[rs - SX]) * __ldg(p.ginvz + gz));
+    const float gix = __ldg(p.ginvx + gx), giz = __ldg(p.ginvz + gz);
+    float Fx = -pc * ((rho_of(sS[rs + 1]) - rho_of(sS[rs - 1])) * gix);
+    float Fz = -pc * ((rho_of(sS[rs + RX]) - rho_of(sS[rs - RX])) * giz);
+    float dpx = 0.f, dpz = 0.f;  // grad(phi) (phase field)
+    if constexpr (PHYS == 1) {
+      // chemical potential of the double well, mu = 4 beta phi (phi - 1)(phi - 1/2)
+      // - kappa lap(phi), beta = 12 sigma / W, kappa = 3 sigma W / 2; the
+      // Laplacian divides by the cell's own dx^2 and dz^2 (ref: collision.cu:65-76)
+      const float Sxp = sS[rs + 1], Sxm = sS[rs - 1], Szp = sS[rs + RX], Szm = sS[rs - RX];
+      dpx = (Sxp - Sxm) * gix;
+      dpz = (Szp - Szm) * giz;
+      const float lap = (Sxp - 2.0f * S + Sxm) * __ldg(p.ilx2 + gx) + (Szp - 2.0f * S + Szm) * __ldg(p.ilz2 + gz);
+      const float mu = p.pf_beta4 * S * (S - 1.0f) * (S - 0.5f) - p.pf_kap * lap;
+      Fx += mu * dpx;
+      Fz += mu * dpz - rho * p.grav;  // the mixture's weight (Boussi_flag off)
+    } else {
+      Fz -= S * p.g_bouss_f;  // Boussinesq buoyancy of the salinity
+    }
     const float uc = u * ic, wc = w * ic;
     const float usq = uc * uc + wc * wc;
     // forcing term Fk_k = w_k (e_k . F) fden (ref: collision.cu:102-110)
@@ -225,8 +363,11 @@ __device__ __forceinline__ void step_tile(const Params &p, int parity, int tile_
       // opposite pair from A = p* - 1.5 u^2 + 4.5 (e.u)^2, B = 3 e.u + e.F fden/2.
       const float P0 = pr - 1.5f * usq;
       const float hx = 0.5f * fden * Fx, hz = 0.5f * fden * Fz;
-      const float m7 = 0.25f * om_shear * (((f[1] + f[3]) - (f[2] + f[4])) - (uc * uc - wc * wc));
-      const float m8 = 0.25f * om_shear * (((f[5] + f[7]) - (f[6] + f[8])) - uc * wc);
+      // (16-bit storage holds f - feq already, whose shear sums are these)
+      const float m7 = 0.25f * om_shear * (RES ? (f[1] + f[3]) - (f[2] + f[4])
+                                               : ((f[1] + f[3]) - (f[2] + f[4])) - (uc * uc - wc * wc));
+      const float m8 = 0.25f * om_shear * (RES ? (f[5] + f[7]) - (f[6] + f[8])
+                                               : ((f[5] + f[7]) - (f[6] + f[8])) - uc * wc);
       sf[e] = w9(0) * P0;
       {
         const float A = fmaf(4.5f * uc, uc, P0), B = fmaf(3.0f, uc, hx);
@@ -258,6 +399,11 @@ __device__ __forceinline__ void step_tile(const Params &p, int parity, int tile_
         const float eu = (ex(k) ? ex(k) * uc : 0.f) + (ez(k) ? ez(k) * wc : 0.f);
         return w9(k) * (pr + 3.0f * eu + 4.5f * eu * eu - 1.5f * usq);
       };
+      if constexpr (RES) {
+        const float u2 = rstore::usq(uc, wc);
+#pragma unroll
+        for (int k = 0; k < 9; k++) f[k] += rstore::feq(k, pr, uc, wc, u2);
+      }
       auto fk_of = [&](int k) {
         const float ef = (ex(k) ? ex(k) * Fx : 0.f) + (ez(k) ? ez(k) * Fz : 0.f);
         return w9(k) * ef * fden;
@@ -300,12 +446,39 @@ __device__ __forceinline__ void step_tile(const Params &p, int parity, int tile_
         }
       }
     }
-    if constexpr (QS == 5) {
+    if constexpr (PHYS == 1) {
+      // conservative Allen-Cahn collision (ref: collision.cu:190-223):
+      //   g*_k = g_k - (g_k - geq_k)/tau_phi + (tau_phi - 1/2)/tau_phi Fp_k,
+      //   Fp_k = dt w_k [(1 - 4 (phi - 1/2)^2)/W c e_k.grad(phi)/|grad(phi)|
+      //                  + 3 e_k.d(phi u)/dt / c] = w_k e_k.V
+      // with d(phi u)/dt against the previous step's phi u kept in obuf.
+      const float *__restrict__ old_in = p.obuf[bi];
+      const long long ci = (long long)gz * nx + gx;
+      const float nbx = (S * u - old_in[ci]) / p.dt, nbz = (S * w - old_in[N + ci]) / p.dt;
+      const float nrm = sqrtf(dpx * dpx + dpz * dpz + 1e-8f);
+      const float sh = S - 0.5f, A = p.dt * (1.0f - 4.0f * sh * sh) * p.pf_invw * c / nrm, B = 3.0f * p.dt * ic;
+      const float Vx = A * dpx + B * nbx, Vz = A * dpz + B * nbz;
+      const float u2 = rstore::usq(uc, wc);
+#pragma unroll
+      for (int k = 0; k < QS; k++) {
+        const float geq = QS == 5 ? rstore::geq5(k, S, uc, wc) : rstore::geq9(k, S, uc, wc, u2);
+        const float r = RES ? g[k] : g[k] - geq;  // 16-bit storage holds g - geq already
+        const float ev = (ex(k) ? ex(k) * Vx : 0.f) + (ez(k) ? ez(k) * Vz : 0.f);
+        sg[k * NE + e] = geq + omg * r + p.pf_lam * wq<QS>(k) * ev;
+      }
+      // this step's phi u for the next one (each interior cell by its own tile)
+      if (lx >= XO && lx < XO + kTX && lz >= HZ && lz < HZ + kTZ) {
+        float *__restrict__ old_out = p.obuf[bo];
+        old_out[ci] = S * u;
+        old_out[N + ci] = S * w;
+      }
+    } else if constexpr (QS == 5) {
       // regularised D2Q5 collision (ref: collision.cu:167-188 on the D2Q5
       // lattice, linear equilibrium w S (1 + 3 e.u/c)): the first moment of
       // g - geq is j = (g1 - g3, g2 - g4) - S u/c, and
       //   g*_k = w_k (S + 3 e_k . (S u/c + (1 - 1/tau_s) j)).
-      const float jx = (g[1] - g[3]) - S * uc, jz = (g[2] - g[4]) - S * wc;
+      const float jx = RES ? g[1] - g[3] : (g[1] - g[3]) - S * uc;
+      const float jz = RES ? g[2] - g[4] : (g[2] - g[4]) - S * wc;
       const float ax3 = 3.0f * fmaf(omg, jx, S * uc), az3 = 3.0f * fmaf(omg, jz, S * wc);
       sg[e] = w5(0) * S;
       sg[1 * NE + e] = w5(1) * (S + ax3);
@@ -314,6 +487,11 @@ __device__ __forceinline__ void step_tile(const Params &p, int parity, int tile_
       sg[4 * NE + e] = w5(4) * (S - az3);
     } else if constexpr (QS == 9) {
       // regularised scalar collision on the reference's Q9 scalar lattice (ref: collision.cu:167-188)
+      if constexpr (RES) {
+        const float u2 = rstore::usq(uc, wc);
+#pragma unroll
+        for (int k = 0; k < QS; k++) g[k] += rstore::geq9(k, S, uc, wc, u2);
+      }
       float ge[QS], jx = 0.f, jz = 0.f;
 #pragma unroll
       for (int k = 0; k < QS; k++) {
@@ -329,8 +507,12 @@ __device__ __forceinline__ void step_tile(const Params &p, int parity, int tile_
         sg[k * NE + e] = ge[k] + omg * (wq<QS>(k) * 3.0f * ej);
       }
     }
-    if (lx >= HX && lx < HX + kTX && lz >= HZ && lz < HZ + kTZ) {
-      const int ii = (lz - HZ) * kTX + (lx - HX);
+    if constexpr (TMA) {
+      // u, w of this slot have been read; the slot keeps the force for phase 2
+      sS[SZ * RX + rs] = Fx;
+      sS[2 * SZ * RX + rs] = Fz;
+    } else if (lx >= XO && lx < XO + kTX && lz >= HZ && lz < HZ + kTZ) {
+      const int ii = (lz - HZ) * kTX + (lx - XO);
       sF[ii] = Fx;
       sF[kTX * kTZ + ii] = Fz;
     }
@@ -383,56 +565,8 @@ __device__ __forceinline__ void step_tile(const Params &p, int parity, int tile_
     return ftmp(arr, kk, gx + ex(nb), gz + ez(nb));
   };
 
-  for (int e = tid; e < kTX * kTZ; e += kThreads) {
-    const int iz = e / kTX, ix = e - iz * kTX;
-    const int gx = x0 + ix, gz = z0 + iz;
-    if (gx >= nx || gz >= nz) continue;
-    const long long ci = (long long)gz * nx + gx;
-    const int lc = (iz + HZ) * EX + ix + HX;
-    const int gA = G::AX == 0 ? gx : gz, gB = G::AX == 0 ? gz : gx, NB = G::AX == 0 ? nz : nx;
-    const int la = G::AX == 0 ? ix + HX : iz + HZ;
-    // interior: every source and stencil node inside the box
-    const bool fast = (G::AX < 0) ? (gx >= 1 && gx <= nx - 2 && gz >= 1 && gz <= nz - 2)
-                                  : (gA >= G::H && gA <= NA - 1 - G::H && gB >= 1 && gB <= NB - 2);
-    float fv[9], gv[QS > 0 ? QS : 1];
-    if (fast) {
-      float W[2][G::NS + 1];
-      if constexpr (G::AX >= 0) {
-#pragma unroll
-        for (int sidx = 0; sidx < 2; sidx++)
-#pragma unroll
-          for (int q = 0; q <= G::NS; q++) W[sidx][q] = sC[(sidx * (G::NS + 1) + q) * NWA + la];
-      }
-      fv[0] = Fast<GEO, 0>::pull(sf, lc, W);
-      fv[1] = Fast<GEO, 1>::pull(sf, lc, W);
-      fv[2] = Fast<GEO, 2>::pull(sf, lc, W);
-      fv[3] = Fast<GEO, 3>::pull(sf, lc, W);
-      fv[4] = Fast<GEO, 4>::pull(sf, lc, W);
-      fv[5] = Fast<GEO, 5>::pull(sf, lc, W);
-      fv[6] = Fast<GEO, 6>::pull(sf, lc, W);
-      fv[7] = Fast<GEO, 7>::pull(sf, lc, W);
-      fv[8] = Fast<GEO, 8>::pull(sf, lc, W);
-      if constexpr (QS > 0) {
-        gv[0] = Fast<GEO, 0>::pull(sg, lc, W);
-        gv[1] = Fast<GEO, 1>::pull(sg, lc, W);
-        gv[2] = Fast<GEO, 2>::pull(sg, lc, W);
-        gv[3] = Fast<GEO, 3>::pull(sg, lc, W);
-        gv[4] = Fast<GEO, 4>::pull(sg, lc, W);
-        if constexpr (QS == 9) {
-          gv[5] = Fast<GEO, 5>::pull(sg, lc, W);
-          gv[6] = Fast<GEO, 6>::pull(sg, lc, W);
-          gv[7] = Fast<GEO, 7>::pull(sg, lc, W);
-          gv[8] = Fast<GEO, 8>::pull(sg, lc, W);
-        }
-      }
-    } else {
-      const int cls = (gx == 0 ? 1 : 0) | (gx == nx - 1 ? 2 : 0) | (gz == 0 ? 4 : 0) | (gz == nz - 1 ? 8 : 0);
-#pragma unroll
-      for (int k = 0; k < 9; k++) fv[k] = pull(sf, k, gx, gz, cls, p.slipB9, p.slipK9);
-#pragma unroll
-      for (int k = 0; k < QS; k++)
-        gv[k] = pull(sg, k, gx, gz, cls, QS == 9 ? p.slipB9 : p.slipB5, QS == 9 ? p.slipK9 : p.slipK5);
-    }
+  // moments and store of one cell from its streamed populations
+  auto finish = [&](int e, long long ci, int rc, const float (&fv)[9], const float (&gv)[QS > 0 ? QS : 1]) {
     float pr = 0.f, jx = 0.f, jz = 0.f;
 #pragma unroll
     for (int k = 0; k < 9; k++) {
@@ -440,93 +574,237 @@ __device__ __forceinline__ void step_tile(const Params &p, int parity, int tile_
       pr += v;
       if (ex(k)) jx += ex(k) * v;
       if (ez(k)) jz += ez(k) * v;
-      st(f_out, k * N + ci, v, p.fscale);
     }
     float S = 0.f;
     if constexpr (QS > 0) {
 #pragma unroll
-      for (int k = 0; k < QS; k++) {
-        S += gv[k];
-        st(g_out, k * N + ci, gv[k] - wq<QS>(k) * p.s_ref, p.gscale);
-      }
+      for (int k = 0; k < QS; k++) S += gv[k];
     } else {
-      S = sS[(iz + HZ + 1) * SX + (ix + HX + 1)];
+      S = sS[rc];
     }
     // moments (ref: collision.cu:244-254)
-    const float rho = (float)((double)rho0 + (double)S * p.rho_sal);
-    const float h = __fdividef(p.hdt, rho);
-    const float ux = c * jx + sF[e] * h, uz = c * jz + sF[kTX * kTZ + e] * h;
+    const float h = __fdividef(p.hdt, rho_of(S));
+    const float Fx = TMA ? sS[SZ * RX + rc] : sF[e], Fz = TMA ? sS[2 * SZ * RX + rc] : sF[kTX * kTZ + e];
+    const float ux = c * jx + Fx * h, uz = c * jz + Fz * h;
+    if constexpr (RES) {
+      // deviations from the equilibrium of the moments stored beside them
+      const float ucn = ux * ic, wcn = uz * ic, u2 = rstore::usq(ucn, wcn);
+      float amax = 0.f;
+#pragma unroll
+      for (int k = 0; k < 9; k++) {
+        const float r = fv[k] - rstore::feq(k, pr, ucn, wcn, u2);
+        amax = fmaxf(amax, fabsf(r) * p.fscale);
+        st(f_out, k * N + ci, r, p.fscale);
+      }
+#pragma unroll
+      for (int k = 0; k < QS; k++) {
+        const float r = gv[k] - (QS == 5 ? rstore::geq5(k, S, ucn, wcn) : rstore::geq9(k, S, ucn, wcn, u2));
+        amax = fmaxf(amax, fabsf(r) * p.gscale);
+        st(g_out, k * N + ci, r, p.gscale);
+      }
+      mac_out[3 * N + ci] = pr;
+      if (amax > p.store_max) atomicOr(p.status, 2u);  // beyond the 16-bit range
+    } else {
+#pragma unroll
+      for (int k = 0; k < 9; k++) st(f_out, k * N + ci, fv[k], 1.0f);
+#pragma unroll
+      for (int k = 0; k < QS; k++) st(g_out, k * N + ci, gv[k], 1.0f);
+    }
     mac_out[ci] = S;
     mac_out[N + ci] = ux;
     mac_out[2 * N + ci] = uz;
     if (!(isfinite(ux) && isfinite(uz) && isfinite(S) && isfinite(pr))) atomicOr(p.status, 1u);
+  };
+  // general path: clamped stencils, ghost rules (cells next to a wall)
+  auto general = [&](int e) {
+    const int iz = e / kTX, ix = e - iz * kTX;
+    const int gx = x0 + ix, gz = z0 + iz;
+    const long long ci = (long long)gz * nx + gx;
+    const int rc = (iz + HZ + 1) * RX + ix + XO + RO;
+    float fv[9], gv[QS > 0 ? QS : 1];
+    const int cls = (gx == 0 ? 1 : 0) | (gx == nx - 1 ? 2 : 0) | (gz == 0 ? 4 : 0) | (gz == nz - 1 ? 8 : 0);
+#pragma unroll
+    for (int k = 0; k < 9; k++) fv[k] = pull(sf, k, gx, gz, cls, p.slipB9, p.slipK9);
+#pragma unroll
+    for (int k = 0; k < QS; k++)
+      gv[k] = pull(sg, k, gx, gz, cls, QS == 9 ? p.slipB9 : p.slipB5, QS == 9 ? p.slipK9 : p.slipK5);
+    finish(e, ci, rc, fv, gv);
+  };
+
+  for (int e = tid; e < kTX * kTZ; e += kThreads) {
+    const int iz = e / kTX, ix = e - iz * kTX;
+    const int gx = x0 + ix, gz = z0 + iz;
+    if (gx >= nx || gz >= nz) continue;
+    const int gA = G::AX == 0 ? gx : gz, gB = G::AX == 0 ? gz : gx, NB = G::AX == 0 ? nz : nx;
+    // interior: every source and stencil node inside the box
+    const bool fast = (G::AX < 0) ? (gx >= 1 && gx <= nx - 2 && gz >= 1 && gz <= nz - 2)
+                                  : (gA >= G::H && gA <= NA - 1 - G::H && gB >= 1 && gB <= NB - 2);
+    if (!fast) {
+      const int slot = atomicAdd(qcount, 1);
+      if (slot < kQueue) queue[slot] = e;
+      else general(e);  // queue full (tiles of very small boxes)
+      continue;
+    }
+    const long long ci = (long long)gz * nx + gx;
+    const int lc = (iz + HZ) * EX + ix + XO;
+    const int rc = (iz + HZ + 1) * RX + ix + XO + RO;  // ring slot of the cell
+    const int la = G::AX == 0 ? ix + XO : iz + HZ;
+    float fv[9], gv[QS > 0 ? QS : 1];
+    float W[2][G::NS + 1];
+    if constexpr (G::AX >= 0) {
+#pragma unroll
+      for (int sidx = 0; sidx < 2; sidx++)
+#pragma unroll
+        for (int q = 0; q <= G::NS; q++) W[sidx][q] = sC[(sidx * (G::NS + 1) + q) * NWA + la];
+    }
+    fv[0] = Fast<GEO, TMA, 0>::pull(sf, lc, W);
+    fv[1] = Fast<GEO, TMA, 1>::pull(sf, lc, W);
+    fv[2] = Fast<GEO, TMA, 2>::pull(sf, lc, W);
+    fv[3] = Fast<GEO, TMA, 3>::pull(sf, lc, W);
+    fv[4] = Fast<GEO, TMA, 4>::pull(sf, lc, W);
+    fv[5] = Fast<GEO, TMA, 5>::pull(sf, lc, W);
+    fv[6] = Fast<GEO, TMA, 6>::pull(sf, lc, W);
+    fv[7] = Fast<GEO, TMA, 7>::pull(sf, lc, W);
+    fv[8] = Fast<GEO, TMA, 8>::pull(sf, lc, W);
+    if constexpr (QS > 0) {
+      gv[0] = Fast<GEO, TMA, 0>::pull(sg, lc, W);
+      gv[1] = Fast<GEO, TMA, 1>::pull(sg, lc, W);
+      gv[2] = Fast<GEO, TMA, 2>::pull(sg, lc, W);
+      gv[3] = Fast<GEO, TMA, 3>::pull(sg, lc, W);
+      gv[4] = Fast<GEO, TMA, 4>::pull(sg, lc, W);
+      if constexpr (QS == 9) {
+        gv[5] = Fast<GEO, TMA, 5>::pull(sg, lc, W);
+        gv[6] = Fast<GEO, TMA, 6>::pull(sg, lc, W);
+        gv[7] = Fast<GEO, TMA, 7>::pull(sg, lc, W);
+        gv[8] = Fast<GEO, TMA, 8>::pull(sg, lc, W);
+      }
+    }
+    finish(e, ci, rc, fv, gv);
   }
+  // the queued wall cells, spread over the CTA's threads
+  __syncthreads();
+  const int nq = min(*qcount, kQueue);
+  for (int j = tid; j < nq; j += kThreads) general(queue[j]);
 }
 
-template <class ST, int QS, int GEO>
+template <class ST, int QS, int GEO, bool TMA, int PHYS>
 __global__ void __launch_bounds__(kThreads, kMinBlocks) step_kernel(const __grid_constant__ Params p) {
-  extern __shared__ float smem[];
-  step_tile<ST, QS, GEO>(p, 0, blockIdx.x, blockIdx.y, smem);
+  extern __shared__ __align__(128) float smem[];
+  step_tile<ST, QS, GEO, TMA, PHYS>(p, 0, blockIdx.x, blockIdx.y, smem);
 }
 
-template <class ST, int QS, int GEO>
+// The batched kernel copies each work item's parameters (past the tensor
+// maps, which register staging does not use) into shared memory, so that
+// the tile reads them as shared loads rather than global ones.
+template <class ST, int QS, int GEO, int PHYS>
 __global__ void __launch_bounds__(kThreads, kMinBlocks)
     step_kernel_batched(const Params *__restrict__ ps, const WorkItem *__restrict__ work, int nwork, int parity) {
-  extern __shared__ float smem[];
+  extern __shared__ __align__(128) float smem[];
+  __shared__ Params sp;
+  constexpr int kSkip = offsetof(Params, tma) / 4, kWords = sizeof(Params) / 4;
+  int cur_sim = -1;
   for (int i = blockIdx.x; i < nwork; i += gridDim.x) {
     const WorkItem w = work[i];
-    step_tile<ST, QS, GEO>(ps[w.sim], parity, w.tx, w.tz, smem);
+    if (w.sim != cur_sim) {  // consecutive items of one simulation share the copy
+      const uint32_t *src = reinterpret_cast<const uint32_t *>(ps + w.sim);
+      uint32_t *dst = reinterpret_cast<uint32_t *>(&sp);
+      for (int j = kSkip + threadIdx.x; j < kWords; j += kThreads) dst[j] = src[j];
+      cur_sim = w.sim;
+      __syncthreads();
+    }
+    step_tile<ST, QS, GEO, false, PHYS>(sp, parity, w.tx, w.tz, smem);
     __syncthreads();  // the next item reuses shared memory
   }
 }
 
-template <class ST, int QS, int GEO>
+template <class ST, int QS, int GEO, int PHYS>
 int launch_b(const Params *ps, const WorkItem *work, int nwork, int parity, int grid, cudaStream_t s, bool prep) {
-  constexpr size_t sm = smem_bytes<ST, QS, GEO>();
+  constexpr size_t sm = smem_bytes<QS, GEO, false>();
   if (prep)
-    return status_from_cuda(cudaFuncSetAttribute(step_kernel_batched<ST, QS, GEO>,
+    return status_from_cuda(cudaFuncSetAttribute(step_kernel_batched<ST, QS, GEO, PHYS>,
                                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
   if (nwork <= 0) return IPCU_OK;
-  step_kernel_batched<ST, QS, GEO><<<grid, kThreads, sm, s>>>(ps, work, nwork, parity);
+  step_kernel_batched<ST, QS, GEO, PHYS><<<grid, kThreads, sm, s>>>(ps, work, nwork, parity);
   return status_from_cuda(cudaGetLastError());
 }
 
-template <class ST, int QS>
+template <class ST, int QS, int PHYS>
 int launch_bg(const Params *ps, const WorkItem *work, int nwork, int parity, int geo, int grid, cudaStream_t s,
               bool prep) {
   switch (geo) {
-    case IPCU_GEO_UNIFORM: return launch_b<ST, QS, IPCU_GEO_UNIFORM>(ps, work, nwork, parity, grid, s, prep);
-    case IPCU_GEO_X5: return launch_b<ST, QS, IPCU_GEO_X5>(ps, work, nwork, parity, grid, s, prep);
-    case IPCU_GEO_X3: return launch_b<ST, QS, IPCU_GEO_X3>(ps, work, nwork, parity, grid, s, prep);
-    case IPCU_GEO_Z5: return launch_b<ST, QS, IPCU_GEO_Z5>(ps, work, nwork, parity, grid, s, prep);
-    case IPCU_GEO_Z3: return launch_b<ST, QS, IPCU_GEO_Z3>(ps, work, nwork, parity, grid, s, prep);
+    case IPCU_GEO_UNIFORM: return launch_b<ST, QS, IPCU_GEO_UNIFORM, PHYS>(ps, work, nwork, parity, grid, s, prep);
+    case IPCU_GEO_X5: return launch_b<ST, QS, IPCU_GEO_X5, PHYS>(ps, work, nwork, parity, grid, s, prep);
+    case IPCU_GEO_X3: return launch_b<ST, QS, IPCU_GEO_X3, PHYS>(ps, work, nwork, parity, grid, s, prep);
+    case IPCU_GEO_Z5: return launch_b<ST, QS, IPCU_GEO_Z5, PHYS>(ps, work, nwork, parity, grid, s, prep);
+    case IPCU_GEO_Z3: return launch_b<ST, QS, IPCU_GEO_Z3, PHYS>(ps, work, nwork, parity, grid, s, prep);
   }
   return IPCU_ERR_UNSUPPORTED;
 }
 
-template <class ST, int QS, int GEO>
-int launch_t(const Params &p, cudaStream_t s, bool prepare_only) {
-  constexpr size_t sm = smem_bytes<ST, QS, GEO>();
+template <class ST, int QS, int GEO, bool TMA, int PHYS>
+int launch_t1(const Params &p, cudaStream_t s, bool prepare_only) {
+  constexpr size_t sm = smem_bytes<QS, GEO, TMA>();
   if (prepare_only) {  // once per sim, outside any stream capture
-    return status_from_cuda(
-        cudaFuncSetAttribute(step_kernel<ST, QS, GEO>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    return status_from_cuda(cudaFuncSetAttribute(step_kernel<ST, QS, GEO, TMA, PHYS>,
+                                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
   }
   dim3 grid((p.nx + kTX - 1) / kTX, (p.nz + kTZ - 1) / kTZ);
-  step_kernel<ST, QS, GEO><<<grid, kThreads, sm, s>>>(p);
+  step_kernel<ST, QS, GEO, TMA, PHYS><<<grid, kThreads, sm, s>>>(p);
   return status_from_cuda(cudaGetLastError());
 }
 
-template <class ST, int QS>
+// TMA staging for FP32 storage when the host built the tensor maps (p.tma)
+template <class ST, int QS, int GEO, int PHYS>
+int launch_t(const Params &p, cudaStream_t s, bool prepare_only) {
+  if constexpr (sizeof(ST) == 4) {
+    if (p.tma) return launch_t1<ST, QS, GEO, true, PHYS>(p, s, prepare_only);
+  }
+  return launch_t1<ST, QS, GEO, false, PHYS>(p, s, prepare_only);
+}
+
+template <class ST, int QS, int PHYS>
 int launch_g(const Params &p, int geo, cudaStream_t s, bool prep) {
   switch (geo) {
-    case IPCU_GEO_UNIFORM: return launch_t<ST, QS, IPCU_GEO_UNIFORM>(p, s, prep);
-    case IPCU_GEO_X5: return launch_t<ST, QS, IPCU_GEO_X5>(p, s, prep);
-    case IPCU_GEO_X3: return launch_t<ST, QS, IPCU_GEO_X3>(p, s, prep);
-    case IPCU_GEO_Z5: return launch_t<ST, QS, IPCU_GEO_Z5>(p, s, prep);
-    case IPCU_GEO_Z3: return launch_t<ST, QS, IPCU_GEO_Z3>(p, s, prep);
+    case IPCU_GEO_UNIFORM: return launch_t<ST, QS, IPCU_GEO_UNIFORM, PHYS>(p, s, prep);
+    case IPCU_GEO_X5: return launch_t<ST, QS, IPCU_GEO_X5, PHYS>(p, s, prep);
+    case IPCU_GEO_X3: return launch_t<ST, QS, IPCU_GEO_X3, PHYS>(p, s, prep);
+    case IPCU_GEO_Z5: return launch_t<ST, QS, IPCU_GEO_Z5, PHYS>(p, s, prep);
+    case IPCU_GEO_Z3: return launch_t<ST, QS, IPCU_GEO_Z3, PHYS>(p, s, prep);
   }
   return IPCU_ERR_UNSUPPORTED;
 }
+
+// Entry points of one instantiation unit: storage ST, scalar physics PHYS
+// (the phase field needs a scalar lattice, q = 5 or 9).
+template <class ST, int PHYS>
+int launch_q(const Params &p, int qs, int geo, cudaStream_t s, bool prep) {
+  if (qs == 0) {
+    if constexpr (PHYS == 0) return launch_g<ST, 0, 0>(p, geo, s, prep);
+    return IPCU_ERR_UNSUPPORTED;
+  }
+  if (qs == 5) return launch_g<ST, 5, PHYS>(p, geo, s, prep);
+  if (qs == 9) return launch_g<ST, 9, PHYS>(p, geo, s, prep);
+  return IPCU_ERR_UNSUPPORTED;
+}
+template <class ST, int PHYS>
+int launch_bq(const Params *ps, const WorkItem *work, int nwork, int parity, int qs, int geo, int grid,
+              cudaStream_t s, bool prep) {
+  if (qs == 0) {
+    if constexpr (PHYS == 0) return launch_bg<ST, 0, 0>(ps, work, nwork, parity, geo, grid, s, prep);
+    return IPCU_ERR_UNSUPPORTED;
+  }
+  if (qs == 5) return launch_bg<ST, 5, PHYS>(ps, work, nwork, parity, geo, grid, s, prep);
+  if (qs == 9) return launch_bg<ST, 9, PHYS>(ps, work, nwork, parity, geo, grid, s, prep);
+  return IPCU_ERR_UNSUPPORTED;
+}
+#define IPCU_F2D_INSTANTIATE(ST, NAME, PHYS)                                                              \
+  int launch_##NAME(const Params &p, int qs, int geo, cudaStream_t s, bool prep) {                        \
+    return launch_q<ST, PHYS>(p, qs, geo, s, prep);                                                       \
+  }                                                                                                       \
+  int launch_batched_##NAME(const Params *ps, const WorkItem *work, int nwork, int parity, int qs, int geo, \
+                            int grid, cudaStream_t s, bool prep) {                                        \
+    return launch_bq<ST, PHYS>(ps, work, nwork, parity, qs, geo, grid, s, prep);                          \
+  }
 
 }  // namespace f2d
 }  // namespace ipcu

@@ -11,8 +11,11 @@
 #include <string>
 #include <vector>
 
+#include <cudaTypedefs.h>
+
 #include "fused2d.cuh"
 #include "ipcu_common.cuh"
+#include "storage.cuh"
 
 using namespace ipcu;
 
@@ -26,8 +29,11 @@ struct ipcu_sim {
   void *g[2] = {nullptr, nullptr};
   float *mac[2] = {nullptr, nullptr};
   float *wA = nullptr, *scin = nullptr, *scout = nullptr, *wC = nullptr, *ginvx = nullptr, *ginvz = nullptr;
+  float *obuf[2] = {nullptr, nullptr};     // phase field: previous step's phi u, phi w
+  float *ilx2 = nullptr, *ilz2 = nullptr;  // phase field: 1/dx^2, 1/dz^2
   unsigned *status = nullptr;
   double *partials = nullptr;
+  cudaEvent_t ready = nullptr;  // recorded on the stream before a batch takes the simulation
   int cur = 0;
   f2d::Params P;
   cudaGraphExec_t graph[2] = {nullptr, nullptr};  // per starting parity
@@ -37,13 +43,14 @@ struct ipcu_sim {
   long long steps = 0;                  // time steps taken since creation / restore
 };
 
+// Macroscopic planes: S, u_x, u_z (+ p* with 16-bit storage)
+static int nmac(const ipcu_sim *s) { return s->cfg.storage == IPCU_STORE_F32 ? 3 : 4; }
+
 namespace {
 
 constexpr int ex9[9] = {0, 1, 0, -1, 0, 1, -1, -1, 1};
 constexpr int ez9[9] = {0, 0, 1, 0, -1, 1, 1, -1, -1};
 constexpr int kinv9[9] = {0, 3, 4, 1, 2, 7, 8, 5, 6};
-constexpr double w9d[9] = {4.0 / 9, 1.0 / 9, 1.0 / 9, 1.0 / 9, 1.0 / 9, 1.0 / 36, 1.0 / 36, 1.0 / 36, 1.0 / 36};
-constexpr double w5d[5] = {1.0 / 3, 1.0 / 6, 1.0 / 6, 1.0 / 6, 1.0 / 6};
 
 inline int geo_axis(int geo) {
   return (geo == IPCU_GEO_X5 || geo == IPCU_GEO_X3) ? 0 : ((geo == IPCU_GEO_Z5 || geo == IPCU_GEO_Z3) ? 1 : -1);
@@ -106,6 +113,36 @@ void axis_tables(const std::vector<double> &X, const std::vector<double> &D, dou
     }
 }
 
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link
+// against the driver library); null when the driver does not provide it
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static bool tried = false;
+  if (!tried) {
+    tried = true;
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  }
+  return fn;
+}
+
+// FP32 planes [planes][nz][nx] read as boxes of [planes][rows][kTmaBoxX];
+// cells outside the array read as zero
+bool encode_planes(CUtensorMap *map, void *base, int nx, int nz, int planes, int rows) {
+  PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+  if (!enc || nx % 4 != 0) return false;
+  const cuuint64_t dims[3] = {(cuuint64_t)nx, (cuuint64_t)nz, (cuuint64_t)planes};
+  const cuuint64_t strides[2] = {(cuuint64_t)nx * 4, (cuuint64_t)nx * nz * 4};
+  const cuuint32_t box[3] = {(cuuint32_t)f2d::kTmaBoxX, (cuuint32_t)rows, (cuuint32_t)planes};
+  const cuuint32_t es[3] = {1, 1, 1};
+  return enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, base, dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+             CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 // 1/(x_{i+1} - x_{i-1} + dz/1000) in float, clamped neighbours
 // (ref: function/collision.cu:82-85; ghosts carry their owner's position)
 std::vector<float> grad_inv(const std::vector<double> &X, double dz) {
@@ -153,48 +190,52 @@ void slip_tables(int q, int8_t *B, int8_t *K) {
   }
 }
 
+// FP32 <-> stored value (16-bit storage multiplies by `scale` first)
 template <class ST>
-void to_store(const double *src, void *dst_host, long long n, double scale, double shift_w, const double *wk, int q,
-              long long N) {
-  ST *d = (ST *)dst_host;
+inline void enc(const float *src, void *dst, long long n, float scale) {
+  ST *d = (ST *)dst;
   for (long long i = 0; i < n; i++) {
-    double v = src[i];
-    if (wk) v -= wk[i / N] * shift_w;
-    if constexpr (sizeof(ST) == 4) d[i] = (float)v;
-    else if constexpr (std::is_same<ST, __half>::value) d[i] = __float2half_rn((float)(v * scale));
-    else d[i] = __float2bfloat16_rn((float)(v * scale));
+    if constexpr (sizeof(ST) == 4) d[i] = src[i];
+    else if constexpr (std::is_same<ST, __half>::value) d[i] = __float2half_rn(src[i] * scale);
+    else d[i] = __float2bfloat16_rn(src[i] * scale);
   }
-  (void)q;
 }
 template <class ST>
-void from_store(const void *src_host, double *dst, long long n, double inv_scale, double shift_w, const double *wk,
-                long long N) {
-  const ST *s = (const ST *)src_host;
+inline void dec(const void *src, float *dst, long long n, float inv_scale) {
+  const ST *d = (const ST *)src;
   for (long long i = 0; i < n; i++) {
-    double v;
-    if constexpr (sizeof(ST) == 4) v = (double)((const float *)s)[i];
-    else if constexpr (std::is_same<ST, __half>::value) v = (double)__half2float(s[i]) * inv_scale;
-    else v = (double)__bfloat162float(s[i]) * inv_scale;
-    if (wk) v += wk[i / N] * shift_w;
-    dst[i] = v;
+    if constexpr (sizeof(ST) == 4) dst[i] = ((const float *)d)[i];
+    else if constexpr (std::is_same<ST, __half>::value) dst[i] = __half2float(d[i]) * inv_scale;
+    else dst[i] = __bfloat162float(d[i]) * inv_scale;
+  }
+}
+
+// FP32 scalar lattice at rest: g_k = w_k S (the product in double, rounded once)
+__global__ void k_init_g(const float *S, int q, float *g, long long N) {
+  IPCU_FOR(i, 0, N) {
+    const double v = S[i];
+    for (int k = 0; k < q; k++) {
+      const double w = q == 5 ? (k == 0 ? 1.0 / 3 : 1.0 / 6) : (k == 0 ? 4.0 / 9 : (k <= 4 ? 1.0 / 9 : 1.0 / 36));
+      g[k * N + i] = (float)(w * v);
+    }
   }
 }
 
 // FP64 area-weighted sums of p* (sum of f) and S, two-pass deterministic
 // (per-block partials, then one block in fixed order).
-template <class ST>
-__global__ void k_totals(const ST *f, const float *mac, const float *wx, const float *wz, int nx, int nz,
-                         float inv_fs, double *part) {
+// (16-bit storage keeps p* in the 4th macroscopic plane; pass f = nullptr)
+__global__ void k_totals(const float *f, const float *mac, const float *wx, const float *wz, int nx, int nz,
+                         double *part) {
   const long long N = (long long)nx * nz;
   double sp = 0, ss = 0;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < N; i += (long long)gridDim.x * blockDim.x) {
     const int x = (int)(i % nx), z = (int)(i / nx);
     const double a = (double)wx[x] * (double)wz[z];
     double p = 0;
-    for (int k = 0; k < 9; k++) {
-      if constexpr (sizeof(ST) == 4) p += (double)((const float *)f)[k * N + i];
-      else if constexpr (std::is_same<ST, __half>::value) p += (double)__half2float(f[k * N + i]) * inv_fs;
-      else p += (double)__bfloat162float(f[k * N + i]) * inv_fs;
+    if (f) {
+      for (int k = 0; k < 9; k++) p += (double)f[k * N + i];
+    } else {
+      p = (double)mac[3 * N + i];
     }
     sp += p * a;
     ss += (double)mac[i] * a;
@@ -229,22 +270,60 @@ __global__ void k_totals_final(const double *part, int nb, double *out) {
 
 constexpr int kTotBlocks = 296;
 
+// A simulation's device memory comes from the device's stream-ordered pool
+// (cudaMallocAsync on the simulation's stream): creating and retiring many
+// simulations, as a server does, then neither synchronises the device nor
+// returns memory to the driver in between. The pool keeps freed memory
+// for reuse (release threshold raised once per device, for this process).
+void retain_pool() {
+  static bool done[64] = {false};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64 || done[dev]) return;
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+    uint64_t keep = UINT64_MAX;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  }
+  done[dev] = true;
+}
+template <class V>
+bool salloc(ipcu_sim *s, V **p, size_t bytes) {
+  return cudaMallocAsync((void **)p, bytes, s->stream) == cudaSuccess;
+}
+template <class V>
+int supload(ipcu_sim *s, V **dst, const std::vector<V> &src) {
+  if (src.empty()) return IPCU_OK;
+  if (!salloc(s, dst, sizeof(V) * src.size())) return IPCU_ERR_NOMEM;
+  // pageable source: the call returns once the source has been staged
+  return cudaMemcpyAsync(*dst, src.data(), sizeof(V) * src.size(), cudaMemcpyHostToDevice, s->stream) == cudaSuccess
+             ? IPCU_OK
+             : IPCU_ERR_CUDA;
+}
+
 void free_sim(ipcu_sim *s) {
   if (!s) return;
+  auto fr = [&](void *p) {
+    if (p) cudaFreeAsync(p, s->stream);
+  };
   for (int i = 0; i < 2; i++) {
     if (s->graph[i]) cudaGraphExecDestroy(s->graph[i]);
-    cudaFree(s->f[i]);
-    cudaFree(s->g[i]);
-    cudaFree(s->mac[i]);
+    fr(s->f[i]);
+    fr(s->g[i]);
+    fr(s->mac[i]);
   }
-  cudaFree(s->wA);
-  cudaFree(s->scin);
-  cudaFree(s->scout);
-  cudaFree(s->wC);
-  cudaFree(s->ginvx);
-  cudaFree(s->ginvz);
-  cudaFree(s->status);
-  cudaFree(s->partials);
+  fr(s->wA);
+  fr(s->scin);
+  fr(s->scout);
+  fr(s->wC);
+  fr(s->ginvx);
+  fr(s->ginvz);
+  fr(s->status);
+  fr(s->partials);
+  fr(s->obuf[0]);
+  fr(s->obuf[1]);
+  fr(s->ilx2);
+  fr(s->ilz2);
+  if (s->ready) cudaEventDestroy(s->ready);
   delete s;
 }
 
@@ -267,6 +346,8 @@ extern "C" int ipcu_sim_create(const ipcu_sim_config *cfg, const double *s0, ipc
   if (c.nx < 1 || c.nz < 1 || c.dz <= 0 || c.dt <= 0 || c.tau <= 0.5) return IPCU_ERR_ARG;
   if (c.q_scalar != 0 && c.q_scalar != 5 && c.q_scalar != 9) return IPCU_ERR_ARG;
   if (c.q_scalar != 0 && c.taus <= 0.5) return IPCU_ERR_ARG;
+  if (c.scalar_kind != IPCU_SCALAR_SALINITY && c.scalar_kind != IPCU_SCALAR_PHASE) return IPCU_ERR_ARG;
+  if (c.scalar_kind == IPCU_SCALAR_PHASE && (c.q_scalar == 0 || !(c.pf_width > 0))) return IPCU_ERR_ARG;
   if (c.geometry < IPCU_GEO_UNIFORM || c.geometry > IPCU_GEO_Z3) return IPCU_ERR_ARG;
   if (c.storage < IPCU_STORE_F32 || c.storage > IPCU_STORE_BF16) return IPCU_ERR_ARG;
   if (c.wall != IPCU_WALL_BB && c.wall != IPCU_WALL_SLIP) return IPCU_ERR_ARG;
@@ -319,27 +400,37 @@ extern "C" int ipcu_sim_create(const ipcu_sim_config *cfg, const double *s0, ipc
       return IPCU_ERR_ARG;
     }
   ensure_tables();
-  int st = IPCU_OK;
-  const size_t fb = s->esz * 9 * s->N, gb = s->esz * std::max(c.q_scalar, 1) * s->N, mb = sizeof(float) * 3 * s->N;
+  retain_pool();
+  int st = cudaEventCreateWithFlags(&s->ready, cudaEventDisableTiming) == cudaSuccess ? IPCU_OK : IPCU_ERR_CUDA;
+  const size_t fb = s->esz * 9 * s->N, gb = s->esz * std::max(c.q_scalar, 1) * s->N, mb = sizeof(float) * nmac(s) * s->N;
   for (int i = 0; i < 2 && st == IPCU_OK; i++) {
-    if (cudaMalloc(&s->f[i], fb) != cudaSuccess || cudaMalloc(&s->g[i], gb) != cudaSuccess ||
-        cudaMalloc((void **)&s->mac[i], mb) != cudaSuccess)
-      st = IPCU_ERR_NOMEM;
+    if (!salloc(s, &s->f[i], fb) || !salloc(s, &s->g[i], gb) || !salloc(s, &s->mac[i], mb)) st = IPCU_ERR_NOMEM;
   }
-  if (st == IPCU_OK && (cudaMalloc((void **)&s->status, sizeof(unsigned)) != cudaSuccess ||
-                        cudaMalloc((void **)&s->partials, sizeof(double) * (2 * kTotBlocks + 2)) != cudaSuccess))
+  if (st == IPCU_OK &&
+      (!salloc(s, &s->status, sizeof(unsigned)) || !salloc(s, &s->partials, sizeof(double) * (2 * kTotBlocks + 2))))
     st = IPCU_ERR_NOMEM;
-  if (st == IPCU_OK) cudaMemset(s->status, 0, sizeof(unsigned));
+  if (st == IPCU_OK) cudaMemsetAsync(s->status, 0, sizeof(unsigned), s->stream);
+  const bool pf = c.scalar_kind == IPCU_SCALAR_PHASE;
+  for (int i = 0; i < 2 && st == IPCU_OK && pf; i++) {
+    if (!salloc(s, &s->obuf[i], sizeof(float) * 2 * s->N)) st = IPCU_ERR_NOMEM;
+    else cudaMemsetAsync(s->obuf[i], 0, sizeof(float) * 2 * s->N, s->stream);  // u = 0 at rest
+  }
+  if (st == IPCU_OK && pf) {
+    std::vector<float> lx(c.nx), lz(c.nz);
+    for (int i = 0; i < c.nx; i++) lx[i] = (float)(1.0 / (s->DX[i] * s->DX[i]));
+    for (int l = 0; l < c.nz; l++) lz[l] = (float)(1.0 / (s->DZ[l] * s->DZ[l]));
+    if ((st = supload(s, &s->ilx2, lx)) == IPCU_OK) st = supload(s, &s->ilz2, lz);
+  }
   if (st == IPCU_OK && ax >= 0) {
     std::vector<float> w, si, so, wc;
     axis_tables(ax == 0 ? s->X : s->Z, ax == 0 ? s->DX : s->DZ, dz, ns, w, si, so, wc);
-    if ((st = upload(&s->wA, w)) == IPCU_OK && (st = upload(&s->scin, si)) == IPCU_OK &&
-        (st = upload(&s->scout, so)) == IPCU_OK)
-      st = upload(&s->wC, wc);
+    if ((st = supload(s, &s->wA, w)) == IPCU_OK && (st = supload(s, &s->scin, si)) == IPCU_OK &&
+        (st = supload(s, &s->scout, so)) == IPCU_OK)
+      st = supload(s, &s->wC, wc);
   }
   if (st == IPCU_OK) {
     std::vector<float> gx = grad_inv(s->X, dz), gz = grad_inv(s->Z, dz);
-    if ((st = upload(&s->ginvx, gx)) == IPCU_OK) st = upload(&s->ginvz, gz);
+    if ((st = supload(s, &s->ginvx, gx)) == IPCU_OK) st = supload(s, &s->ginvz, gz);
   }
   if (st != IPCU_OK) {
     free_sim(s);
@@ -369,16 +460,31 @@ extern "C" int ipcu_sim_create(const ipcu_sim_config *cfg, const double *s0, ipc
   P.phi = (float)c.phi;
   P.rho_sal = c.rho_sal;
   P.g_bouss = c.g_bouss;
-  const bool lowp = c.storage != IPCU_STORE_F32;
-  // reduced-precision storage: f is a pressure deviation, scaled into the
-  // normal FP16 range; g is stored as the deviation from w_k * s_ref
-  const double fscale = lowp ? (c.storage == IPCU_STORE_F16 ? 1024.0 : 1.0) : 1.0;
-  const double gscale = lowp ? (c.storage == IPCU_STORE_F16 ? 64.0 : 1.0) : 1.0;
-  P.fscale = (float)fscale;
-  P.inv_fscale = (float)(1.0 / fscale);
-  P.gscale = (float)gscale;
-  P.inv_gscale = (float)(1.0 / gscale);
-  P.s_ref = lowp ? (float)c.s_ref : 0.0f;
+  P.rho_sal_f = (float)c.rho_sal;
+  P.g_bouss_f = (float)c.g_bouss;
+  P.rho_base = std::fmaf(P.rhoH - P.rhoL, P.phi, P.rhoL);
+  P.pf = pf ? 1 : 0;
+  if (pf) {
+    // the scalar is phi: rho = rhoL + (rhoH - rhoL) phi; surface tension
+    // beta = 12 sigma / W, kappa = 3 sigma W / 2 (ref: collision.cu:71)
+    P.rho_base = P.rhoL;
+    P.rho_sal_f = P.rhoH - P.rhoL;
+    P.pf_beta4 = (float)(48.0 * c.sigma / c.pf_width);
+    P.pf_kap = (float)(1.5 * c.sigma * c.pf_width);
+    P.pf_invw = (float)(1.0 / c.pf_width);
+    P.pf_lam = (float)((c.taus - 0.5) / c.taus);
+    P.grav = (float)c.gravity;
+    P.ilx2 = s->ilx2;
+    P.ilz2 = s->ilz2;
+    for (int i = 0; i < 2; i++) P.obuf[i] = s->obuf[i];
+  }
+  // 16-bit storage holds deviations from the local equilibrium (mostly
+  // 1e-8 .. 1e-1 in lattice units); FP16 scales them by 2^12 so that they sit
+  // in its normal range with room up to 16 before the 65504 limit
+  const double scale = c.storage == IPCU_STORE_F16 ? 4096.0 : 1.0;
+  P.fscale = P.gscale = (float)scale;
+  P.inv_fscale = P.inv_gscale = (float)(1.0 / scale);
+  P.store_max = c.storage == IPCU_STORE_F16 ? 65504.0f : 3.0e38f;
   if (c.mrt) {
     double Sv[9], MM[81];
     for (int i = 0; i < 9; i++) Sv[i] = c.S[i];
@@ -420,29 +526,57 @@ extern "C" int ipcu_sim_create(const ipcu_sim_config *cfg, const double *s0, ipc
     P.gbuf[i] = s->g[i];
     P.mbuf[i] = s->mac[i];
   }
+  // TMA staging for FP32 storage: tile + halo rows for f and g, ring rows
+  // (one more on each side) for the S, u_x, u_z planes
+  P.tma = 0;
+  if (c.storage == IPCU_STORE_F32 && c.nx % 4 == 0) {
+    const int rows = f2d::kTZ + 2 * f2d::halo_z(c.geometry);
+    bool ok = true;
+    for (int i = 0; i < 2 && ok; i++) {
+      ok = encode_planes(&P.tm_f[i], s->f[i], c.nx, c.nz, 9, rows) &&
+           encode_planes(&P.tm_m[i], s->mac[i], c.nx, c.nz, 3, rows + 2) &&
+           (c.q_scalar == 0 || encode_planes(&P.tm_g[i], s->g[i], c.nx, c.nz, c.q_scalar, rows));
+    }
+    P.tma = ok ? 1 : 0;
+  }
   st = f2d::launch_step(P, c.storage, c.q_scalar, c.geometry, s->stream, true);
   if (st != IPCU_OK) {
     free_sim(s);
     return st;
   }
-  // initial state: f = 0 (p* = 0, u = 0), g = w_k S, u = 0
-  std::vector<double> S0(s->N, 0.0);
-  if (s0) std::copy(s0, s0 + s->N, S0.begin());
-  std::vector<double> g0((size_t)std::max(c.q_scalar, 1) * s->N, 0.0), f0((size_t)9 * s->N, 0.0), z0(s->N, 0.0);
-  if (c.q_scalar)
-    for (int k = 0; k < c.q_scalar; k++)
-      for (long long i = 0; i < s->N; i++) g0[k * s->N + i] = (c.q_scalar == 5 ? w5d[k] : w9d[k]) * S0[i];
-  *out = s;
-  st = ipcu_sim_set_state(s, f0.data(), c.q_scalar ? g0.data() : nullptr, S0.data(), z0.data(), z0.data());
+  // initial state, built on the device: f = 0 (p* = 0, u = 0), g = w_k S,
+  // u = 0; with 16-bit storage the stored deviations are all zero
+  {
+    const long long N = s->N;
+    std::vector<float> S0f(N, 0.f);
+    if (s0)
+      for (long long i = 0; i < N; i++) S0f[i] = (float)s0[i];
+    const int cb = s->cur;
+    cudaError_t e = cudaMemsetAsync(s->f[cb], 0, s->esz * 9 * N, s->stream);
+    if (e == cudaSuccess && c.q_scalar) e = cudaMemsetAsync(s->g[cb], 0, s->esz * c.q_scalar * N, s->stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(s->mac[cb], 0, sizeof(float) * nmac(s) * N, s->stream);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(s->mac[cb], S0f.data(), sizeof(float) * N, cudaMemcpyHostToDevice, s->stream);
+    if (e == cudaSuccess && c.q_scalar && c.storage == IPCU_STORE_F32) {
+      Launch L = launch_for(N);
+      k_init_g<<<L.grid, L.block, 0, s->stream>>>(s->mac[cb], c.q_scalar, (float *)s->g[cb], N);
+      e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);  // S0f is released on return
+    st = e == cudaSuccess ? IPCU_OK : IPCU_ERR_CUDA;
+  }
   if (st != IPCU_OK) {
     free_sim(s);
-    *out = nullptr;
+    return st;
   }
-  return st;
+  *out = s;
+  return IPCU_OK;
 }
 
+// Memory is returned in stream order; only a simulation that recorded CUDA
+// graphs waits for its stream before the graphs are destroyed.
 extern "C" void ipcu_sim_destroy(ipcu_sim *sim) {
-  if (sim) cudaStreamSynchronize(sim->stream);
+  if (sim && (sim->graph[0] || sim->graph[1])) cudaStreamSynchronize(sim->stream);
   free_sim(sim);
 }
 
@@ -514,8 +648,10 @@ extern "C" int64_t ipcu_sim_cells(const ipcu_sim *sim) { return sim ? sim->N : 0
 
 extern "C" int64_t ipcu_sim_bytes_per_cell(const ipcu_sim *sim) {
   if (!sim) return 0;
-  // every stored distribution and the three macroscopic fields are read once and written once
-  return 2 * ((int64_t)sim->esz * (9 + sim->cfg.q_scalar) + 4 * 3);
+  // every stored distribution and the macroscopic planes are read once and written once
+  // (the phase field also reads and writes the previous step's phi u, phi w)
+  const int old = sim->cfg.scalar_kind == IPCU_SCALAR_PHASE ? 2 : 0;
+  return 2 * ((int64_t)sim->esz * (9 + sim->cfg.q_scalar) + 4 * (nmac(sim) + old));
 }
 
 extern "C" int ipcu_sim_device_state(ipcu_sim *sim, void **f, void **g, float **mac) {
@@ -526,85 +662,153 @@ extern "C" int ipcu_sim_device_state(ipcu_sim *sim, void **f, void **g, float **
   return IPCU_OK;
 }
 
-static const double *wk_of(int q) { return q == 5 ? w5d : w9d; }
+// The physical state in FP32 on the host: f [9][N], g [q][N], mac [4][N]
+// (S, u_x, u_z, p*), converted from / to the storage layout.
+struct HostState {
+  std::vector<float> f, g, mac;
+};
+
+static int state_download(ipcu_sim *s, HostState &h) {
+  const long long N = s->N;
+  const int q = s->cfg.q_scalar, nm = nmac(s);
+  std::vector<unsigned char> fb(s->esz * 9 * N), gb(s->esz * (size_t)q * N);
+  h.f.resize(9 * N);
+  h.g.resize((size_t)q * N);
+  h.mac.assign(4 * N, 0.f);
+  if (cudaStreamSynchronize(s->stream) != cudaSuccess ||
+      cudaMemcpy(fb.data(), s->f[s->cur], fb.size(), cudaMemcpyDeviceToHost) != cudaSuccess ||
+      (q && cudaMemcpy(gb.data(), s->g[s->cur], gb.size(), cudaMemcpyDeviceToHost) != cudaSuccess) ||
+      cudaMemcpy(h.mac.data(), s->mac[s->cur], sizeof(float) * nm * N, cudaMemcpyDeviceToHost) != cudaSuccess)
+    return IPCU_ERR_CUDA;
+  const float ifs = s->P.inv_fscale, igs = s->P.inv_gscale;
+  switch (s->cfg.storage) {
+    case IPCU_STORE_F32: dec<float>(fb.data(), h.f.data(), 9 * N, 1.f), dec<float>(gb.data(), h.g.data(), q * N, 1.f); break;
+    case IPCU_STORE_F16: dec<__half>(fb.data(), h.f.data(), 9 * N, ifs), dec<__half>(gb.data(), h.g.data(), q * N, igs); break;
+    default: dec<__nv_bfloat16>(fb.data(), h.f.data(), 9 * N, ifs), dec<__nv_bfloat16>(gb.data(), h.g.data(), q * N, igs);
+  }
+  const float ic = 1.0f / s->P.c;
+  for (long long i = 0; i < N; i++) {
+    if (nm == 3) {  // p* in the kernel's float order
+      float a = 0.f;
+      for (int k = 0; k < 9; k++) a += h.f[k * N + i];
+      h.mac[3 * N + i] = a;
+      continue;
+    }
+    // 16-bit storage: deviations plus the equilibrium of the stored moments
+    const float S = h.mac[i], uc = h.mac[N + i] * ic, wc = h.mac[2 * N + i] * ic, pr = h.mac[3 * N + i];
+    const float u2 = rstore::usq(uc, wc);
+    for (int k = 0; k < 9; k++) h.f[k * N + i] += rstore::feq(k, pr, uc, wc, u2);
+    for (int k = 0; k < q; k++)
+      h.g[k * N + i] += q == 5 ? rstore::geq5(k, S, uc, wc) : rstore::geq9(k, S, uc, wc, u2);
+  }
+  return IPCU_OK;
+}
+
+static int state_upload(ipcu_sim *s, const HostState &h) {
+  const long long N = s->N;
+  const int q = s->cfg.q_scalar, nm = nmac(s);
+  std::vector<float> f = h.f, g = h.g;
+  if (nm == 4) {
+    const float ic = 1.0f / s->P.c;
+    for (long long i = 0; i < N; i++) {
+      const float S = h.mac[i], uc = h.mac[N + i] * ic, wc = h.mac[2 * N + i] * ic, pr = h.mac[3 * N + i];
+      const float u2 = rstore::usq(uc, wc);
+      for (int k = 0; k < 9; k++) f[k * N + i] -= rstore::feq(k, pr, uc, wc, u2);
+      for (int k = 0; k < q; k++)
+        g[k * N + i] -= q == 5 ? rstore::geq5(k, S, uc, wc) : rstore::geq9(k, S, uc, wc, u2);
+    }
+  }
+  std::vector<unsigned char> fb(s->esz * 9 * N), gb(s->esz * (size_t)q * N);
+  const float fs = s->P.fscale, gs = s->P.gscale;
+  switch (s->cfg.storage) {
+    case IPCU_STORE_F32: enc<float>(f.data(), fb.data(), 9 * N, 1.f), enc<float>(g.data(), gb.data(), q * N, 1.f); break;
+    case IPCU_STORE_F16: enc<__half>(f.data(), fb.data(), 9 * N, fs), enc<__half>(g.data(), gb.data(), q * N, gs); break;
+    default: enc<__nv_bfloat16>(f.data(), fb.data(), 9 * N, fs), enc<__nv_bfloat16>(g.data(), gb.data(), q * N, gs);
+  }
+  if (cudaStreamSynchronize(s->stream) != cudaSuccess ||
+      cudaMemcpy(s->f[s->cur], fb.data(), fb.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
+      (q && cudaMemcpy(s->g[s->cur], gb.data(), gb.size(), cudaMemcpyHostToDevice) != cudaSuccess) ||
+      cudaMemcpy(s->mac[s->cur], h.mac.data(), sizeof(float) * nm * N, cudaMemcpyHostToDevice) != cudaSuccess)
+    return IPCU_ERR_CUDA;
+  if (s->obuf[s->cur]) {
+    // phase field: the previous step's phi u is taken equal to this state's,
+    // so the d(phi u)/dt term starts at zero (the reference driver's
+    // phi_old = phi, u_old = u at start-up)
+    std::vector<float> o(2 * N);
+    for (long long i = 0; i < N; i++) {
+      o[i] = h.mac[i] * h.mac[N + i];
+      o[N + i] = h.mac[i] * h.mac[2 * N + i];
+    }
+    if (cudaMemcpy(s->obuf[s->cur], o.data(), sizeof(float) * 2 * N, cudaMemcpyHostToDevice) != cudaSuccess)
+      return IPCU_ERR_CUDA;
+  }
+  return IPCU_OK;
+}
 
 extern "C" int ipcu_sim_set_state(ipcu_sim *s, const double *f, const double *g, const double *S, const double *ux,
                                   const double *uz) {
   if (!s) return IPCU_ERR_ARG;
   const long long N = s->N;
   const int q = s->cfg.q_scalar;
-  const double fs = s->P.fscale, gs = s->P.gscale, sref = s->P.s_ref;
-  std::vector<unsigned char> buf;
-  if (f) {
-    buf.resize(s->esz * 9 * N);
-    if (s->cfg.storage == IPCU_STORE_F32) to_store<float>(f, buf.data(), 9 * N, fs, 0, nullptr, 9, N);
-    else if (s->cfg.storage == IPCU_STORE_F16) to_store<__half>(f, buf.data(), 9 * N, fs, 0, nullptr, 9, N);
-    else to_store<__nv_bfloat16>(f, buf.data(), 9 * N, fs, 0, nullptr, 9, N);
-    if (cudaMemcpy(s->f[s->cur], buf.data(), buf.size(), cudaMemcpyHostToDevice) != cudaSuccess) return IPCU_ERR_CUDA;
+  HostState h;
+  // fields not given keep their current physical values
+  if (!(f && (g || !q) && S && ux && uz)) {
+    int st = state_download(s, h);
+    if (st) return st;
+  } else {
+    h.f.resize(9 * N);
+    h.g.resize((size_t)q * N);
+    h.mac.assign(4 * N, 0.f);
   }
-  if (g && q) {
-    buf.resize(s->esz * q * N);
-    if (s->cfg.storage == IPCU_STORE_F32) to_store<float>(g, buf.data(), q * N, gs, sref, wk_of(q), q, N);
-    else if (s->cfg.storage == IPCU_STORE_F16) to_store<__half>(g, buf.data(), q * N, gs, sref, wk_of(q), q, N);
-    else to_store<__nv_bfloat16>(g, buf.data(), q * N, gs, sref, wk_of(q), q, N);
-    if (cudaMemcpy(s->g[s->cur], buf.data(), buf.size(), cudaMemcpyHostToDevice) != cudaSuccess) return IPCU_ERR_CUDA;
-  }
+  if (f)
+    for (long long i = 0; i < 9 * N; i++) h.f[i] = (float)f[i];
+  if (g && q)
+    for (long long i = 0; i < q * N; i++) h.g[i] = (float)g[i];
   const double *src[3] = {S, ux, uz};
-  std::vector<float> m(N);
-  for (int a = 0; a < 3; a++) {
-    if (!src[a]) continue;
-    for (long long i = 0; i < N; i++) m[i] = (float)src[a][i];
-    if (cudaMemcpy(s->mac[s->cur] + a * N, m.data(), sizeof(float) * N, cudaMemcpyHostToDevice) != cudaSuccess)
-      return IPCU_ERR_CUDA;
+  for (int a = 0; a < 3; a++)
+    if (src[a])
+      for (long long i = 0; i < N; i++) h.mac[a * N + i] = (float)src[a][i];
+  for (long long i = 0; i < N; i++) {  // p* in the kernel's float order
+    float a = 0.f;
+    for (int k = 0; k < 9; k++) a += h.f[k * N + i];
+    h.mac[3 * N + i] = a;
   }
-  return IPCU_OK;
+  return state_upload(s, h);
 }
 
 extern "C" int ipcu_sim_get(ipcu_sim *s, const char *field, double *out, int64_t n) {
   if (!s || !field || !out) return IPCU_ERR_ARG;
-  if (cudaStreamSynchronize(s->stream) != cudaSuccess) return IPCU_ERR_CUDA;
   const long long N = s->N;
   const int q = s->cfg.q_scalar;
-  std::string fd(field);
-  auto get_dist = [&](void *dev, int qq, double scale, double shift, const double *wk, double *dst) -> int {
-    std::vector<unsigned char> buf(s->esz * qq * N);
-    if (cudaMemcpy(buf.data(), dev, buf.size(), cudaMemcpyDeviceToHost) != cudaSuccess) return IPCU_ERR_CUDA;
-    if (s->cfg.storage == IPCU_STORE_F32) from_store<float>(buf.data(), dst, qq * N, 1.0 / scale, shift, wk, N);
-    else if (s->cfg.storage == IPCU_STORE_F16) from_store<__half>(buf.data(), dst, qq * N, 1.0 / scale, shift, wk, N);
-    else from_store<__nv_bfloat16>(buf.data(), dst, qq * N, 1.0 / scale, shift, wk, N);
-    return IPCU_OK;
-  };
-  if (fd == "f") {
-    if (n < 9 * N) return IPCU_ERR_CAPACITY;
-    return get_dist(s->f[s->cur], 9, s->P.fscale, 0, nullptr, out);
-  }
-  if (fd == "g") {
-    if (!q) return IPCU_ERR_ARG;
-    if (n < q * N) return IPCU_ERR_CAPACITY;
-    return get_dist(s->g[s->cur], q, s->P.gscale, s->P.s_ref, wk_of(q), out);
-  }
-  if (n < N) return IPCU_ERR_CAPACITY;
-  if (fd == "p") {
-    std::vector<double> f(9 * N);
-    int st = get_dist(s->f[s->cur], 9, s->P.fscale, 0, nullptr, f.data());
-    if (st) return st;
-    for (long long i = 0; i < N; i++) {
-      float a = 0.f;  // p* in the kernel's float order
-      for (int k = 0; k < 9; k++) a += (float)f[k * N + i];
-      out[i] = a;
+  const std::string fd(field);
+  const long long need = fd == "f" ? 9 * N : (fd == "g" ? (long long)q * N : N);
+  if (fd == "g" && !q) return IPCU_ERR_ARG;
+  const int slot = fd == "S" ? 0 : (fd == "ux" ? 1 : (fd == "uz" ? 2 : (fd == "rho" ? 0 : (fd == "p" ? 3 : -1))));
+  if (slot < 0 && fd != "f" && fd != "g") return IPCU_ERR_ARG;
+  if (n < need) return IPCU_ERR_CAPACITY;
+  // macroscopic planes straight from the device; p* with FP32 storage and
+  // the populations need the whole state
+  if (slot >= 0 && (slot < 3 || nmac(s) == 4)) {
+    std::vector<float> m(N);
+    if (cudaStreamSynchronize(s->stream) != cudaSuccess ||
+        cudaMemcpy(m.data(), s->mac[s->cur] + (long long)slot * N, sizeof(float) * N, cudaMemcpyDeviceToHost) !=
+            cudaSuccess)
+      return IPCU_ERR_CUDA;
+    if (fd == "rho") {
+      for (long long i = 0; i < N; i++) out[i] = std::fmaf(m[i], s->P.rho_sal_f, s->P.rho_base);
+    } else {
+      for (long long i = 0; i < N; i++) out[i] = m[i];
     }
     return IPCU_OK;
   }
-  int slot = fd == "S" ? 0 : (fd == "ux" ? 1 : (fd == "uz" ? 2 : (fd == "rho" ? 0 : -1)));
-  if (slot < 0) return IPCU_ERR_ARG;
-  std::vector<float> m(N);
-  if (cudaMemcpy(m.data(), s->mac[s->cur] + slot * N, sizeof(float) * N, cudaMemcpyDeviceToHost) != cudaSuccess)
-    return IPCU_ERR_CUDA;
-  if (fd == "rho") {
-    const float rho0 = s->P.rhoL + (s->P.rhoH - s->P.rhoL) * s->P.phi;
-    for (long long i = 0; i < N; i++) out[i] = (float)((double)rho0 + (double)m[i] * s->P.rho_sal);
+  HostState h;
+  int st = state_download(s, h);
+  if (st) return st;
+  if (fd == "f" || fd == "g") {
+    const std::vector<float> &v = fd == "f" ? h.f : h.g;
+    for (long long i = 0; i < need; i++) out[i] = v[i];
   } else {
-    for (long long i = 0; i < N; i++) out[i] = m[i];
+    for (long long i = 0; i < N; i++) out[i] = h.mac[slot * N + i];
   }
   return IPCU_OK;
 }
@@ -630,13 +834,8 @@ extern "C" int ipcu_sim_totals(ipcu_sim *s, double *sum_p, double *sum_s) {
     cudaFree(dwz);
     return IPCU_ERR_NOMEM;
   }
-  const float ifs = s->P.inv_fscale;
-  if (s->cfg.storage == IPCU_STORE_F32)
-    k_totals<float><<<kTotBlocks, 256, 0, s->stream>>>((const float *)s->f[s->cur], s->mac[s->cur], dwx, dwz, s->nx, s->nz, ifs, s->partials);
-  else if (s->cfg.storage == IPCU_STORE_F16)
-    k_totals<__half><<<kTotBlocks, 256, 0, s->stream>>>((const __half *)s->f[s->cur], s->mac[s->cur], dwx, dwz, s->nx, s->nz, ifs, s->partials);
-  else
-    k_totals<__nv_bfloat16><<<kTotBlocks, 256, 0, s->stream>>>((const __nv_bfloat16 *)s->f[s->cur], s->mac[s->cur], dwx, dwz, s->nx, s->nz, ifs, s->partials);
+  const float *f32 = s->cfg.storage == IPCU_STORE_F32 ? (const float *)s->f[s->cur] : nullptr;
+  k_totals<<<kTotBlocks, 256, 0, s->stream>>>(f32, s->mac[s->cur], dwx, dwz, s->nx, s->nz, s->partials);
   k_totals_final<<<1, 32, 0, s->stream>>>(s->partials, kTotBlocks, s->partials + 2 * kTotBlocks);
   double h[2] = {0, 0};
   cudaError_t e = cudaMemcpyAsync(h, s->partials + 2 * kTotBlocks, sizeof h, cudaMemcpyDeviceToHost, s->stream);
@@ -656,7 +855,7 @@ extern "C" int ipcu_sim_upload(ipcu_sim *s, const void *f, const void *g, const 
   if (f) e = cudaMemcpyAsync(s->f[s->cur], f, s->esz * 9 * N, cudaMemcpyHostToDevice, s->stream);
   if (e == cudaSuccess && g && s->cfg.q_scalar)
     e = cudaMemcpyAsync(s->g[s->cur], g, s->esz * s->cfg.q_scalar * N, cudaMemcpyHostToDevice, s->stream);
-  if (e == cudaSuccess && mac) e = cudaMemcpyAsync(s->mac[s->cur], mac, sizeof(float) * 3 * N, cudaMemcpyHostToDevice, s->stream);
+  if (e == cudaSuccess && mac) e = cudaMemcpyAsync(s->mac[s->cur], mac, sizeof(float) * nmac(s) * N, cudaMemcpyHostToDevice, s->stream);
   return e == cudaSuccess ? IPCU_OK : IPCU_ERR_CUDA;
 }
 
@@ -667,7 +866,7 @@ extern "C" int ipcu_sim_download(ipcu_sim *s, void *f, void *g, float *mac) {
   if (f) e = cudaMemcpyAsync(f, s->f[s->cur], s->esz * 9 * N, cudaMemcpyDeviceToHost, s->stream);
   if (e == cudaSuccess && g && s->cfg.q_scalar)
     e = cudaMemcpyAsync(g, s->g[s->cur], s->esz * s->cfg.q_scalar * N, cudaMemcpyDeviceToHost, s->stream);
-  if (e == cudaSuccess && mac) e = cudaMemcpyAsync(mac, s->mac[s->cur], sizeof(float) * 3 * N, cudaMemcpyDeviceToHost, s->stream);
+  if (e == cudaSuccess && mac) e = cudaMemcpyAsync(mac, s->mac[s->cur], sizeof(float) * nmac(s) * N, cudaMemcpyDeviceToHost, s->stream);
   return e == cudaSuccess ? IPCU_OK : IPCU_ERR_CUDA;
 }
 
@@ -716,7 +915,7 @@ extern "C" int ipcu_totals_noalloc_f32(const float *f, const float *mac, const f
     dev_ptr[dev] = static_cast<double *>(ptr);
   }
   const int nb = (int)((N + kNoAllocCells - 1) / kNoAllocCells);
-  k_totals<float><<<nb, 256, 0, (cudaStream_t)stream>>>(f, mac, wx, wz, nx, nz, 1.0f, dev_ptr[dev]);
+  k_totals<<<nb, 256, 0, (cudaStream_t)stream>>>(f, mac, wx, wz, nx, nz, dev_ptr[dev]);
   k_totals_final<<<1, 32, 0, (cudaStream_t)stream>>>(dev_ptr[dev], nb, out);
   return status_from_cuda(cudaGetLastError());
 }
@@ -728,7 +927,9 @@ extern "C" int ipcu_totals_noalloc_f32(const float *f, const float *mac, const f
 // ref: function/basic.cu:31-56, which had no reader).
 namespace {
 constexpr char kMagic[8] = {'I', 'P', 'C', 'U', 'S', 'I', 'M', '1'};
-constexpr int32_t kSnapVersion = 1;
+// 2: 16-bit storage as equilibrium deviations + p* plane; 3: scalar kind and
+// phase-field parameters in the configuration, previous-step phi u planes
+constexpr int32_t kSnapVersion = 3;
 template <class T>
 bool wr(FILE *f, const T *p, size_t n) { return fwrite(p, sizeof(T), n, f) == n; }
 template <class T>
@@ -743,10 +944,14 @@ extern "C" int ipcu_sim_save(ipcu_sim *s, const char *path) {
   const long long N = s->N;
   const int q = s->cfg.q_scalar;
   std::vector<unsigned char> fb(s->esz * 9 * N), gb(s->esz * (size_t)q * N);
-  std::vector<float> mb(3 * N);
+  std::vector<float> mb((size_t)nmac(s) * N);
   if (cudaMemcpy(fb.data(), s->f[s->cur], fb.size(), cudaMemcpyDeviceToHost) != cudaSuccess) return IPCU_ERR_CUDA;
   if (q && cudaMemcpy(gb.data(), s->g[s->cur], gb.size(), cudaMemcpyDeviceToHost) != cudaSuccess) return IPCU_ERR_CUDA;
-  if (cudaMemcpy(mb.data(), s->mac[s->cur], sizeof(float) * 3 * N, cudaMemcpyDeviceToHost) != cudaSuccess)
+  if (cudaMemcpy(mb.data(), s->mac[s->cur], sizeof(float) * mb.size(), cudaMemcpyDeviceToHost) != cudaSuccess)
+    return IPCU_ERR_CUDA;
+  std::vector<float> ob(s->obuf[s->cur] ? 2 * N : 0);
+  if (!ob.empty() &&
+      cudaMemcpy(ob.data(), s->obuf[s->cur], sizeof(float) * ob.size(), cudaMemcpyDeviceToHost) != cudaSuccess)
     return IPCU_ERR_CUDA;
   FILE *f = fopen(path, "wb");
   if (!f) return IPCU_ERR_IO;
@@ -756,7 +961,8 @@ extern "C" int ipcu_sim_save(ipcu_sim *s, const char *path) {
             wr(f, s->X.data(), s->X.size()) && wr(f, s->Z.data(), s->Z.size()) && wr(f, s->DX.data(), s->DX.size()) &&
             wr(f, s->DZ.data(), s->DZ.size());
   if (ok && c.mrt) ok = wr(f, s->M.data(), 81) && wr(f, s->Minv.data(), 81) && wr(f, s->Srates.data(), 9);
-  ok = ok && wr(f, fb.data(), fb.size()) && wr(f, gb.data(), gb.size()) && wr(f, mb.data(), mb.size());
+  ok = ok && wr(f, fb.data(), fb.size()) && wr(f, gb.data(), gb.size()) && wr(f, mb.data(), mb.size()) &&
+       wr(f, ob.data(), ob.size());
   ok = (fclose(f) == 0) && ok;
   return ok ? IPCU_OK : IPCU_ERR_IO;
 }
@@ -796,8 +1002,9 @@ extern "C" int ipcu_sim_load(const char *path, ipcu_stream_t stream, ipcu_sim **
   const long long N = s->N;
   const int q = c.q_scalar;
   std::vector<unsigned char> fb(s->esz * 9 * N), gb(s->esz * (size_t)q * N);
-  std::vector<float> mb(3 * N);
-  ok = rd(f, fb.data(), fb.size()) && rd(f, gb.data(), gb.size()) && rd(f, mb.data(), mb.size());
+  std::vector<float> mb((size_t)nmac(s) * N), ob(s->obuf[s->cur] ? 2 * N : 0);
+  ok = rd(f, fb.data(), fb.size()) && rd(f, gb.data(), gb.size()) && rd(f, mb.data(), mb.size()) &&
+       rd(f, ob.data(), ob.size());
   fclose(f);
   if (!ok) {
     ipcu_sim_destroy(s);
@@ -805,7 +1012,9 @@ extern "C" int ipcu_sim_load(const char *path, ipcu_stream_t stream, ipcu_sim **
   }
   if (cudaMemcpy(s->f[s->cur], fb.data(), fb.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
       (q && cudaMemcpy(s->g[s->cur], gb.data(), gb.size(), cudaMemcpyHostToDevice) != cudaSuccess) ||
-      cudaMemcpy(s->mac[s->cur], mb.data(), sizeof(float) * 3 * N, cudaMemcpyHostToDevice) != cudaSuccess) {
+      cudaMemcpy(s->mac[s->cur], mb.data(), sizeof(float) * mb.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
+      (!ob.empty() &&
+       cudaMemcpy(s->obuf[s->cur], ob.data(), sizeof(float) * ob.size(), cudaMemcpyHostToDevice) != cudaSuccess)) {
     ipcu_sim_destroy(s);
     return IPCU_ERR_CUDA;
   }
@@ -856,6 +1065,9 @@ extern "C" int ipcu_sim_write_csv(ipcu_sim *s, const char *path) {
 // depend on what it is batched with.
 struct ipcu_batch {
   cudaStream_t stream;
+  cudaEvent_t done = nullptr;  // recorded after each enqueue; the simulations' streams wait on it
+  cudaEvent_t mark[4] = {nullptr, nullptr, nullptr, nullptr};  // ring of progress marks
+  int next_mark = 0;
   f2d::Params *d_params = nullptr;
   f2d::WorkItem *d_work = nullptr;
   size_t cap_params = 0, cap_work = 0;
@@ -870,6 +1082,12 @@ extern "C" int ipcu_batch_create(ipcu_stream_t stream, ipcu_batch **out) {
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   b->grid_cap = sms * f2d::kMinBlocks;
+  bool ok = cudaEventCreateWithFlags(&b->done, cudaEventDisableTiming) == cudaSuccess;
+  for (int i = 0; i < 4 && ok; i++) ok = cudaEventCreateWithFlags(&b->mark[i], cudaEventDisableTiming) == cudaSuccess;
+  if (!ok) {
+    ipcu_batch_destroy(b);
+    return IPCU_ERR_CUDA;
+  }
   *out = b;
   return IPCU_OK;
 }
@@ -879,27 +1097,36 @@ extern "C" void ipcu_batch_destroy(ipcu_batch *b) {
   cudaStreamSynchronize(b->stream);
   cudaFree(b->d_params);
   cudaFree(b->d_work);
+  if (b->done) cudaEventDestroy(b->done);
+  for (int i = 0; i < 4; i++)
+    if (b->mark[i]) cudaEventDestroy(b->mark[i]);
   delete b;
 }
 
-extern "C" int ipcu_batch_step(ipcu_batch *b, ipcu_sim *const *sims, int n, int64_t nsteps) {
+// Enqueues nsteps batched steps on the batch stream and orders every listed
+// simulation's own stream after them (event wait), so that later work on a
+// simulation -- reads, more steps, destruction -- sees the results.
+static int batch_enqueue(ipcu_batch *b, ipcu_sim *const *sims, int n, int64_t nsteps) {
   if (!b || (n > 0 && !sims) || nsteps < 0) return IPCU_ERR_ARG;
   if (n == 0 || nsteps == 0) return IPCU_OK;
   for (int i = 0; i < n; i++) {
     if (!sims[i]) return IPCU_ERR_ARG;
-    // the batch stream takes over: the simulation's own work must be finished
-    if (cudaStreamSynchronize(sims[i]->stream) != cudaSuccess) return IPCU_ERR_CUDA;
+    // the batch stream waits (on the device) for the simulation's own work
+    if (cudaEventRecord(sims[i]->ready, sims[i]->stream) != cudaSuccess ||
+        cudaStreamWaitEvent(b->stream, sims[i]->ready, 0) != cudaSuccess)
+      return IPCU_ERR_CUDA;
   }
   // group by kernel class, keeping order
   std::vector<int> order(n);
   for (int i = 0; i < n; i++) order[i] = i;
   std::stable_sort(order.begin(), order.end(), [&](int a, int c) {
     const ipcu_sim_config &A = sims[a]->cfg, &C = sims[c]->cfg;
-    return std::make_tuple(A.storage, A.q_scalar, A.geometry) < std::make_tuple(C.storage, C.q_scalar, C.geometry);
+    return std::make_tuple(A.storage, A.q_scalar, A.geometry, A.scalar_kind) <
+           std::make_tuple(C.storage, C.q_scalar, C.geometry, C.scalar_kind);
   });
   std::vector<f2d::Params> hp(n);
   std::vector<f2d::WorkItem> hw;
-  struct Group { int storage, qs, geo, w0, w1; };
+  struct Group { int storage, qs, geo, pf, w0, w1; };
   std::vector<Group> groups;
   for (int oi = 0; oi < n; oi++) {
     ipcu_sim *s = sims[order[oi]];
@@ -907,8 +1134,8 @@ extern "C" int ipcu_batch_step(ipcu_batch *b, ipcu_sim *const *sims, int n, int6
     hp[oi].cur = s->cur;
     const ipcu_sim_config &c = s->cfg;
     if (groups.empty() || groups.back().storage != c.storage || groups.back().qs != c.q_scalar ||
-        groups.back().geo != c.geometry)
-      groups.push_back({c.storage, c.q_scalar, c.geometry, (int)hw.size(), (int)hw.size()});
+        groups.back().geo != c.geometry || groups.back().pf != c.scalar_kind)
+      groups.push_back({c.storage, c.q_scalar, c.geometry, c.scalar_kind, (int)hw.size(), (int)hw.size()});
     const int tx = (s->nx + f2d::kTX - 1) / f2d::kTX, tz = (s->nz + f2d::kTZ - 1) / f2d::kTZ;
     for (int z = 0; z < tz; z++)
       for (int x = 0; x < tx; x++) hw.push_back({oi, x, z, 0});
@@ -930,29 +1157,59 @@ extern "C" int ipcu_batch_step(ipcu_batch *b, ipcu_sim *const *sims, int n, int6
           cudaSuccess)
     return IPCU_ERR_CUDA;
   for (const Group &g : groups) {
-    int st = f2d::launch_batched(nullptr, nullptr, 0, 0, g.storage, g.qs, g.geo, 0, b->stream, true);
+    int st = f2d::launch_batched(nullptr, nullptr, 0, 0, g.storage, g.qs, g.geo, g.pf, 0, b->stream, true);
     if (st) return st;
   }
   for (int64_t k = 0; k < nsteps; k++) {
     for (const Group &g : groups) {
       const int nw = g.w1 - g.w0;
       const int grid = std::min(nw, b->grid_cap);
-      int st = f2d::launch_batched(b->d_params, b->d_work + g.w0, nw, (int)(k & 1), g.storage, g.qs, g.geo, grid,
+      int st = f2d::launch_batched(b->d_params, b->d_work + g.w0, nw, (int)(k & 1), g.storage, g.qs, g.geo, g.pf, grid,
                                    b->stream, false);
       if (st) return st;
     }
   }
-  if (cudaStreamSynchronize(b->stream) != cudaSuccess) return IPCU_ERR_CUDA;
+  if (cudaEventRecord(b->done, b->stream) != cudaSuccess) return IPCU_ERR_CUDA;
   for (int i = 0; i < n; i++) {
+    if (cudaStreamWaitEvent(sims[i]->stream, b->done, 0) != cudaSuccess) return IPCU_ERR_CUDA;
     sims[i]->cur ^= (int)(nsteps & 1);
     sims[i]->steps += nsteps;
   }
   return IPCU_OK;
 }
 
+extern "C" int ipcu_batch_step(ipcu_batch *b, ipcu_sim *const *sims, int n, int64_t nsteps) {
+  const int st = batch_enqueue(b, sims, n, nsteps);
+  if (st != IPCU_OK || n == 0 || nsteps == 0) return st;
+  return cudaStreamSynchronize(b->stream) == cudaSuccess ? IPCU_OK : IPCU_ERR_CUDA;
+}
+
+extern "C" int ipcu_batch_launch(ipcu_batch *b, ipcu_sim *const *sims, int n, int64_t nsteps) {
+  return batch_enqueue(b, sims, n, nsteps);
+}
+
+extern "C" int ipcu_batch_mark(ipcu_batch *b) {
+  if (!b) return IPCU_ERR_ARG;
+  const int m = b->next_mark;
+  if (cudaEventRecord(b->mark[m], b->stream) != cudaSuccess) return IPCU_ERR_CUDA;
+  b->next_mark = (m + 1) % 4;
+  return m;
+}
+
+extern "C" int ipcu_batch_wait_mark(ipcu_batch *b, int mark) {
+  if (!b || mark < 0 || mark >= 4) return IPCU_ERR_ARG;
+  return cudaEventSynchronize(b->mark[mark]) == cudaSuccess ? IPCU_OK : IPCU_ERR_CUDA;
+}
+
+extern "C" int ipcu_batch_sync(ipcu_batch *b) {
+  if (!b) return IPCU_ERR_ARG;
+  return cudaStreamSynchronize(b->stream) == cudaSuccess ? IPCU_OK : IPCU_ERR_CUDA;
+}
+
 extern "C" int64_t ipcu_sim_device_bytes(const ipcu_sim *s) {
   if (!s) return 0;
   const long long N = s->N;
-  return 2 * ((long long)s->esz * (9 + std::max(s->cfg.q_scalar, 1)) * N + 4LL * 3 * N) +
-         4LL * (3 * (s->nx + s->nz) + 2 * 5 * std::max(s->nx, s->nz)) + 2048;
+  return 2 * ((long long)s->esz * (9 + std::max(s->cfg.q_scalar, 1)) * N + 4LL * (nmac(s) + (s->cfg.scalar_kind == IPCU_SCALAR_PHASE ? 2 : 0)) * N) +
+         4LL * (3 * (s->nx + s->nz) + 2 * 5 * std::max(s->nx, s->nz)) + 2048 +
+         (s->cfg.scalar_kind == IPCU_SCALAR_PHASE ? 4LL * (s->nx + s->nz) : 0);  // 1/dx^2, 1/dz^2
 }

@@ -1,0 +1,265 @@
+// 3-D structured solver object (ipcu_sim3d_*): device-resident FP32 state,
+// stepping (direct or CUDA-graph replay), field I/O.
+#include <algorithm>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "fused3d.cuh"
+#include "ipcu_common.cuh"
+
+using namespace ipcu;
+
+struct ipcu_sim3d {
+  ipcu_sim3d_config cfg;
+  long long N;
+  cudaStream_t stream;
+  float *f[2] = {nullptr, nullptr}, *g[2] = {nullptr, nullptr}, *F[2] = {nullptr, nullptr};
+  unsigned *status = nullptr;
+  int cur = 0;
+  f3d::Params3 P;
+  cudaGraphExec_t graph[2] = {nullptr, nullptr};  // two steps, per starting buffer
+  long long steps = 0;
+};
+
+namespace {
+
+constexpr double w7d(int k) { return k == 0 ? 0.25 : 0.125; }
+constexpr int E19[19][3] = {{0, 0, 0}, {1, 0, 0}, {0, 1, 0}, {-1, 0, 0}, {0, -1, 0}, {0, 0, 1}, {0, 0, -1},
+                            {1, 1, 0}, {1, -1, 0}, {-1, 1, 0}, {-1, -1, 0}, {1, 0, 1}, {1, 0, -1}, {-1, 0, 1},
+                            {-1, 0, -1}, {0, 1, 1}, {0, 1, -1}, {0, -1, 1}, {0, -1, -1}};
+
+void free3(ipcu_sim3d *s) {
+  if (!s) return;
+  for (int i = 0; i < 2; i++) {
+    if (s->graph[i]) cudaGraphExecDestroy(s->graph[i]);
+    cudaFree(s->f[i]);
+    cudaFree(s->g[i]);
+    cudaFree(s->F[i]);
+  }
+  cudaFree(s->status);
+  delete s;
+}
+
+f3d::Params3 params_for(const ipcu_sim3d *s, int cur) {
+  f3d::Params3 P = s->P;
+  P.f_in = s->f[cur];
+  P.g_in = s->g[cur];
+  P.F_in = s->F[cur];
+  P.f_out = s->f[cur ^ 1];
+  P.g_out = s->g[cur ^ 1];
+  P.F_out = s->F[cur ^ 1];
+  return P;
+}
+
+}  // namespace
+
+extern "C" int ipcu_sim3d_create(const ipcu_sim3d_config *cfg, const double *s0, ipcu_stream_t stream,
+                                 ipcu_sim3d **out) {
+  if (!cfg || !out) return IPCU_ERR_ARG;
+  *out = nullptr;
+  const ipcu_sim3d_config &c = *cfg;
+  if (c.nx < 1 || c.ny < 1 || c.nz < 1 || !(c.dz > 0) || !(c.dt > 0) || c.tau <= 0.5 || c.taus <= 0.5)
+    return IPCU_ERR_ARG;
+  ipcu_sim3d *s = new ipcu_sim3d();
+  s->cfg = c;
+  s->N = (long long)c.nx * c.ny * c.nz;
+  s->stream = (cudaStream_t)stream;
+  ensure_tables();
+  const long long N = s->N;
+  for (int i = 0; i < 2; i++)
+    if (cudaMalloc((void **)&s->f[i], sizeof(float) * 19 * N) != cudaSuccess ||
+        cudaMalloc((void **)&s->g[i], sizeof(float) * 7 * N) != cudaSuccess ||
+        cudaMalloc((void **)&s->F[i], sizeof(float) * 3 * N) != cudaSuccess) {
+      free3(s);
+      return IPCU_ERR_NOMEM;
+    }
+  if (cudaMalloc((void **)&s->status, sizeof(unsigned)) != cudaSuccess) {
+    free3(s);
+    return IPCU_ERR_NOMEM;
+  }
+  f3d::Params3 &P = s->P;
+  std::memset(&P, 0, sizeof P);
+  P.nx = c.nx;
+  P.ny = c.ny;
+  P.nz = c.nz;
+  // z cells per CTA: enough CTAs for several waves of 3 per SM on 148 SMs
+  const long long cols = (long long)((c.nx + 31) / 32) * ((c.ny + 7) / 8);
+  P.zchunk = (int)std::max(4LL, std::min<long long>(64, (long long)c.nz * cols / (148LL * 3 * 6)));
+  const double cl = c.dz / c.dt;
+  P.c = (float)cl;
+  P.dt = (float)c.dt;
+  P.itau = (float)(1.0 / c.tau);
+  P.omg_s = (float)(1.0 - 1.0 / c.taus);
+  P.fk3 = (float)(3.0 * c.dt / cl);
+  P.hdt = (float)(0.5 * c.dt);
+  P.rho0 = (float)c.rho0;
+  P.rsal = (float)c.rho_sal;
+  P.gb = (float)c.g_bouss;
+  // clamped central differences: 1/(x_{i+1} - x_{i-1} + dz/1000), the ghost
+  // carrying its owner's position at a wall (ref: function/collision.cu:82-85)
+  const float reg = (float)c.dz / 1000.0f;
+  P.gi_in = 1.0f / (2.0f * (float)c.dz + reg);
+  P.gi_wall = 1.0f / ((float)c.dz + reg);
+  P.mrt = c.mrt ? 1 : 0;
+  P.status = s->status;
+  // state at rest: f = 0, g = w_k S0, F = 0
+  std::vector<float> g0(7 * N);
+  for (long long i = 0; i < N; i++) {
+    const double S = s0 ? s0[i] : 0.0;
+    for (int k = 0; k < 7; k++) g0[k * N + i] = (float)(w7d(k) * S);
+  }
+  if (cudaMemsetAsync(s->status, 0, sizeof(unsigned), s->stream) != cudaSuccess ||
+      cudaMemsetAsync(s->f[0], 0, sizeof(float) * 19 * N, s->stream) != cudaSuccess ||
+      cudaMemsetAsync(s->F[0], 0, sizeof(float) * 3 * N, s->stream) != cudaSuccess ||
+      cudaMemcpyAsync(s->g[0], g0.data(), sizeof(float) * 7 * N, cudaMemcpyHostToDevice, s->stream) != cudaSuccess ||
+      cudaStreamSynchronize(s->stream) != cudaSuccess) {
+    free3(s);
+    return IPCU_ERR_CUDA;
+  }
+  *out = s;
+  return IPCU_OK;
+}
+
+extern "C" void ipcu_sim3d_destroy(ipcu_sim3d *s) {
+  if (s) cudaStreamSynchronize(s->stream);
+  free3(s);
+}
+
+extern "C" int ipcu_sim3d_step(ipcu_sim3d *s, int64_t nsteps) {
+  if (!s || nsteps < 0) return IPCU_ERR_ARG;
+  for (int64_t k = 0; k < nsteps; k++) {
+    const int st = f3d::launch3d(params_for(s, s->cur), s->stream);
+    if (st != IPCU_OK) return st;
+    s->cur ^= 1;
+    s->steps++;
+  }
+  return IPCU_OK;
+}
+
+extern "C" int ipcu_sim3d_step_graph(ipcu_sim3d *s, int64_t nsteps) {
+  if (!s || nsteps < 0) return IPCU_ERR_ARG;
+  const int64_t pairs = nsteps / 2;
+  if (pairs > 0) {
+    cudaGraphExec_t &ge = s->graph[s->cur];
+    if (!ge) {
+      // record on a private stream (the simulation's may be the legacy
+      // default stream, which cannot be captured), replay on the simulation's
+      cudaStream_t cs;
+      if (cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking) != cudaSuccess) return IPCU_ERR_CUDA;
+      cudaGraph_t gr;
+      if (cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+        cudaStreamDestroy(cs);
+        return IPCU_ERR_CUDA;
+      }
+      int st = f3d::launch3d(params_for(s, s->cur), cs);
+      if (st == IPCU_OK) st = f3d::launch3d(params_for(s, s->cur ^ 1), cs);
+      const cudaError_t e = cudaStreamEndCapture(cs, &gr);
+      cudaStreamDestroy(cs);
+      if (st != IPCU_OK || e != cudaSuccess) return st != IPCU_OK ? st : IPCU_ERR_CUDA;
+      const cudaError_t ei = cudaGraphInstantiate(&ge, gr, 0);
+      cudaGraphDestroy(gr);
+      if (ei != cudaSuccess) return IPCU_ERR_CUDA;
+    }
+    for (int64_t k = 0; k < pairs; k++)
+      if (cudaGraphLaunch(ge, s->stream) != cudaSuccess) return IPCU_ERR_CUDA;
+    s->steps += 2 * pairs;  // two steps return to the same buffer
+  }
+  return ipcu_sim3d_step(s, nsteps % 2);
+}
+
+extern "C" int ipcu_sim3d_get(ipcu_sim3d *s, const char *field, double *out, int64_t n) {
+  if (!s || !field || !out) return IPCU_ERR_ARG;
+  const long long N = s->N;
+  const std::string fd(field);
+  const long long need = fd == "f" ? 19 * N : (fd == "g" ? 7 * N : (fd == "F" ? 3 * N : N));
+  if (fd != "f" && fd != "g" && fd != "F" && fd != "S" && fd != "p" && fd != "ux" && fd != "uy" && fd != "uz")
+    return IPCU_ERR_ARG;
+  if (n < need) return IPCU_ERR_CAPACITY;
+  std::vector<float> f(19 * N), g(7 * N), F(3 * N);
+  if (cudaStreamSynchronize(s->stream) != cudaSuccess ||
+      cudaMemcpy(f.data(), s->f[s->cur], sizeof(float) * f.size(), cudaMemcpyDeviceToHost) != cudaSuccess ||
+      cudaMemcpy(g.data(), s->g[s->cur], sizeof(float) * g.size(), cudaMemcpyDeviceToHost) != cudaSuccess ||
+      cudaMemcpy(F.data(), s->F[s->cur], sizeof(float) * F.size(), cudaMemcpyDeviceToHost) != cudaSuccess)
+    return IPCU_ERR_CUDA;
+  const std::vector<float> *raw = fd == "f" ? &f : (fd == "g" ? &g : (fd == "F" ? &F : nullptr));
+  if (raw) {
+    for (long long i = 0; i < need; i++) out[i] = (*raw)[i];
+    return IPCU_OK;
+  }
+  // moments in the kernel's float order
+  const float c = s->P.c;
+  for (long long i = 0; i < N; i++) {
+    float pr = 0.f, j[3] = {0.f, 0.f, 0.f}, S = 0.f;
+    for (int k = 0; k < 19; k++) {
+      const float v = f[k * N + i];
+      pr += v;
+      for (int a = 0; a < 3; a++)
+        if (E19[k][a]) j[a] += E19[k][a] * v;
+    }
+    for (int k = 0; k < 7; k++) S += g[k * N + i];
+    const float rho = std::fmaf(S, s->P.rsal, s->P.rho0), h = s->P.hdt / rho;
+    if (fd == "p") out[i] = pr;
+    else if (fd == "S") out[i] = S;
+    else {
+      const int a = fd == "ux" ? 0 : (fd == "uy" ? 1 : 2);
+      out[i] = c * j[a] + F[a * N + i] * h;
+    }
+  }
+  return IPCU_OK;
+}
+
+extern "C" int ipcu_sim3d_set_state(ipcu_sim3d *s, const double *f, const double *g, const double *F) {
+  if (!s) return IPCU_ERR_ARG;
+  const long long N = s->N;
+  auto put = [&](const double *src, float *dst, long long n) -> bool {
+    if (!src) return true;
+    std::vector<float> v(n);
+    for (long long i = 0; i < n; i++) v[i] = (float)src[i];
+    return cudaMemcpy(dst, v.data(), sizeof(float) * n, cudaMemcpyHostToDevice) == cudaSuccess;
+  };
+  if (cudaStreamSynchronize(s->stream) != cudaSuccess) return IPCU_ERR_CUDA;
+  return put(f, s->f[s->cur], 19 * N) && put(g, s->g[s->cur], 7 * N) && put(F, s->F[s->cur], 3 * N) ? IPCU_OK
+                                                                                                      : IPCU_ERR_CUDA;
+}
+
+extern "C" int ipcu_sim3d_upload(ipcu_sim3d *s, const float *f, const float *g, const float *F) {
+  if (!s) return IPCU_ERR_ARG;
+  const long long N = s->N;
+  cudaError_t e = cudaSuccess;
+  if (f) e = cudaMemcpyAsync(s->f[s->cur], f, sizeof(float) * 19 * N, cudaMemcpyHostToDevice, s->stream);
+  if (e == cudaSuccess && g) e = cudaMemcpyAsync(s->g[s->cur], g, sizeof(float) * 7 * N, cudaMemcpyHostToDevice, s->stream);
+  if (e == cudaSuccess && F) e = cudaMemcpyAsync(s->F[s->cur], F, sizeof(float) * 3 * N, cudaMemcpyHostToDevice, s->stream);
+  return e == cudaSuccess ? IPCU_OK : IPCU_ERR_CUDA;
+}
+
+extern "C" int ipcu_sim3d_download(ipcu_sim3d *s, float *f, float *g, float *F) {
+  if (!s) return IPCU_ERR_ARG;
+  const long long N = s->N;
+  cudaError_t e = cudaSuccess;
+  if (f) e = cudaMemcpyAsync(f, s->f[s->cur], sizeof(float) * 19 * N, cudaMemcpyDeviceToHost, s->stream);
+  if (e == cudaSuccess && g) e = cudaMemcpyAsync(g, s->g[s->cur], sizeof(float) * 7 * N, cudaMemcpyDeviceToHost, s->stream);
+  if (e == cudaSuccess && F) e = cudaMemcpyAsync(F, s->F[s->cur], sizeof(float) * 3 * N, cudaMemcpyDeviceToHost, s->stream);
+  return e == cudaSuccess ? IPCU_OK : IPCU_ERR_CUDA;
+}
+
+extern "C" int ipcu_sim3d_sync(ipcu_sim3d *s) {
+  if (!s) return IPCU_ERR_ARG;
+  return cudaStreamSynchronize(s->stream) == cudaSuccess ? IPCU_OK : IPCU_ERR_CUDA;
+}
+
+extern "C" int ipcu_sim3d_status(ipcu_sim3d *s, uint32_t *flags) {
+  if (!s || !flags) return IPCU_ERR_ARG;
+  unsigned v = 0;
+  if (cudaMemcpyAsync(&v, s->status, sizeof v, cudaMemcpyDeviceToHost, s->stream) != cudaSuccess ||
+      cudaStreamSynchronize(s->stream) != cudaSuccess)
+    return IPCU_ERR_CUDA;
+  *flags = v;
+  return v ? IPCU_ERR_NONFINITE : IPCU_OK;
+}
+
+extern "C" int64_t ipcu_sim3d_cells(const ipcu_sim3d *s) { return s ? s->N : 0; }
+
+extern "C" int64_t ipcu_sim3d_bytes_per_cell(const ipcu_sim3d *s) {
+  return s ? 2 * 4 * (19 + 7 + 3) : 0;
+}

@@ -47,6 +47,30 @@ def le_step(call, ip, B, *, mrt=True, scalar=True, wall_function=False, boussi=1
     call("resetF", B.items, B.Fx, B.Fy, B.Fz, int(num_F))
 
 
+def pf_step(call, ip, B, *, mrt=True, rhoL=1.0, rhoH=3.0, num_F=None):
+    """One step of the reference's two-phase driver order (ref:
+    RTinstability/RTinstability.cu:177-206): equilibrium, force with surface
+    tension and the mixture's weight (Boussi_flag off), MRT collision and
+    interpolated streaming of f, conservative Allen-Cahn collision and
+    streaming of the phase field g, phi = sum g, moments, ghost rho and phi."""
+    call("equ_f", B.items, B.feq, B.p, B.u, B.v, B.w)
+    call("Force", B.items, 0, B.neib, B.f, B.feq, B.tau, B.Fk, B.Fx, B.Fy, B.Fz, B.p, B.rho, B.sal, B.phi,
+         B.u, B.v, B.w, B.delX, B.delY, B.posx, B.posy, B.posz)
+    if mrt:
+        call("col_f_MRT", B.items, B.tau, B.f, B.ftmp, B.feq, B.Fk, B.M, B.Minv, B.S, B.MM)
+    else:
+        call("col_f_SRT", B.items, B.tau, B.f, B.ftmp, B.feq, B.Fk)
+    ip(B.f, B.feq, B.ftmp, B.fout)
+    call("col_PF", B.items, B.neib, B.taus, B.g, B.ftmp, B.feq, B.phi, B.u, B.v, B.w, B.phiold, B.uold, B.vold,
+         B.wold, B.posx, B.posy, B.posz)
+    ip(B.g, B.feq, B.ftmp, B.fout)
+    call("update_scalar", B.items, B.g, B.phi)
+    call("update_rho", B.items, rhoL, rhoH, B.f, B.Fx, B.Fy, B.Fz, B.p, B.sal, B.phi, B.rho, B.u, B.v, B.w)
+    call("set_wall_rho", B.items, B.neib, B.rho)
+    call("set_wall_rho", B.items, B.neib, B.phi)
+    call("resetF", B.items, B.Fx, B.Fy, B.Fz, int(num_F))
+
+
 def ibm_step(call, ip, B, *, mrt=False, boussi=1, rhoL=1.0, rhoH=1000.0, num_F=None, num_Gw=None):
     call("equ_f", B.items, B.feq, B.p, B.u, B.v, B.w)
     call("Force", B.items, int(boussi), B.neib, B.f, B.feq, B.tau, B.Fk, B.Fx, B.Fy, B.Fz, B.p, B.rho, B.sal, B.phi,

@@ -20,6 +20,7 @@ import time
 from dataclasses import dataclass, field
 
 import numpy as np
+import torch
 
 from . import _lib
 from .sim import Sim
@@ -34,10 +35,32 @@ class Batch:
         self._h = h
 
     def step(self, sims, n):
+        """Advances `sims` by n steps and waits."""
         if not sims or n <= 0:
             return
         arr = (ctypes.c_void_p * len(sims))(*[s._h.value for s in sims])
         _lib.check(_lib.lib().ipcu_batch_step(self._h, arr, len(sims), int(n)), "ipcu_batch_step")
+
+    def launch(self, sims, n):
+        """Enqueues n steps of `sims` without waiting (each simulation's own
+        stream is ordered after them)."""
+        if not sims or n <= 0:
+            return
+        arr = (ctypes.c_void_p * len(sims))(*[s._h.value for s in sims])
+        _lib.check(_lib.lib().ipcu_batch_launch(self._h, arr, len(sims), int(n)), "ipcu_batch_launch")
+
+    def sync(self):
+        _lib.check(_lib.lib().ipcu_batch_sync(self._h), "ipcu_batch_sync")
+
+    def mark(self):
+        """Handle of the point reached by everything enqueued so far."""
+        m = _lib.lib().ipcu_batch_mark(self._h)
+        if m < 0:
+            _lib.check(m, "ipcu_batch_mark")
+        return m
+
+    def wait_mark(self, m):
+        _lib.check(_lib.lib().ipcu_batch_wait_mark(self._h, int(m)), "ipcu_batch_wait_mark")
 
     def close(self):
         if getattr(self, "_h", None):
@@ -74,14 +97,21 @@ class Request:
 
 def request_bytes(req: Request) -> int:
     """Device bytes a request needs once admitted (same formula as ipcu_sim_device_bytes)."""
-    esz = 4 if req.kwargs.get("storage", "f32") == "f32" else 2
+    f32 = req.kwargs.get("storage", "f32") == "f32"
+    esz, nmac = (4, 3) if f32 else (2, 4)  # 16-bit storage keeps p* in a 4th FP32 plane
+    pf = req.kwargs.get("scalar", "salinity") == "phase"
+    if pf:
+        nmac += 2  # previous step's phi u, phi w
     q = max(req.kwargs.get("q_scalar", 5), 1)
     N = req.cells
-    return 2 * (esz * (9 + q) * N + 12 * N) + 4 * (3 * (req.nx + req.nz) + 10 * max(req.nx, req.nz)) + 2048
+    return (2 * (esz * (9 + q) * N + 4 * nmac * N) + 4 * (3 * (req.nx + req.nz) + 10 * max(req.nx, req.nz)) + 2048
+            + (4 * (req.nx + req.nz) if pf else 0))
 
 
 class Server:
     def __init__(self, budget_bytes=150e9, tick_steps=200, keep_results=("S", "ux", "uz"), stream=None):
+        """keep_results: macroscopic planes copied back per finished request
+        ("S", "ux", "uz"; "p" too with 16-bit storage)."""
         self.budget = float(budget_bytes)
         self.tick_steps = int(tick_steps)
         self.keep = keep_results
@@ -92,46 +122,89 @@ class Server:
         self.done: list[Request] = []
         self.in_use = 0
         self.cell_updates = 0
+        self.t_admit = self.t_step = self.t_retire = 0.0  # host seconds per phase
+        self.retiring = []      # finished requests whose results are being copied back
+        self.prev_mark = None   # progress mark of the previous tick's batch
 
     def submit(self, req: Request, now: float):
         req.remaining = req.steps
         heapq.heappush(self.waiting, req)
 
     def _admit(self, now):
+        t0 = time.perf_counter()
         while self.waiting and self.in_use + request_bytes(self.waiting[0]) <= self.budget:
             r = heapq.heappop(self.waiting)
             r.sim = Sim(r.nx, r.nz, s0=r.s0, stream=self.stream, **r.kwargs)
             r.admitted = now
             self.in_use += r.sim.device_bytes()
             self.active.append(r)
+        self.t_admit += time.perf_counter() - t0
 
     def tick(self, clock):
-        """Admit, advance every active simulation by up to tick_steps, retire."""
-        self._admit(clock())
-        if not self.active:
-            return 0
+        """One pipelined tick: enqueue up to tick_steps for every active
+        simulation, enqueue the result copies of those that finish with it,
+        then -- while the GPU runs -- hand out the results of the previous
+        tick's finishers, admit waiting requests, and wait for the previous
+        tick's batch, so the host stays one tick ahead of the GPU."""
+        if not self.active and not self.retiring:
+            self._admit(clock())
+            if not self.active:
+                return 0
+        t0 = time.perf_counter()
         groups = {}
         for r in self.active:
             groups.setdefault(min(self.tick_steps, r.remaining), []).append(r)
         for n, rs in sorted(groups.items(), reverse=True):
-            self.batch.step([r.sim for r in rs], n)
+            self.batch.launch([r.sim for r in rs], n)
             for r in rs:
                 r.remaining -= n
                 self.cell_updates += r.cells * n
-        now = clock()
-        still = []
+        mark = self.batch.mark()
+        # finishers: copy the macroscopic planes back on their own streams,
+        # which the batch launch ordered after their last steps
+        still, new_retiring = [], []
         for r in self.active:
             if r.remaining == 0:
-                r.finished = now
-                r.result = {k: r.sim.get(k) for k in self.keep}
-                self.in_use -= r.sim.device_bytes()
-                r.sim.close()
-                r.sim = None
-                self.done.append(r)
+                buf = torch.empty(r.sim.mac_planes() * r.cells, dtype=torch.float32, pin_memory=True)
+                r.sim.download(None, None, buf)
+                new_retiring.append((r, buf))
             else:
                 still.append(r)
         self.active = still
-        return len(self.active)
+        t1 = time.perf_counter()
+        self._finish(self.retiring, clock)
+        self.retiring = new_retiring
+        t2 = time.perf_counter()
+        a0 = self.t_admit
+        self._admit(clock())
+        if self.prev_mark is not None:
+            self.batch.wait_mark(self.prev_mark)
+        self.prev_mark = mark
+        t3 = time.perf_counter()
+        self.t_retire += t2 - t1
+        self.t_step += (t1 - t0) + (t3 - t2) - (self.t_admit - a0)
+        if not self.active and not self.waiting:
+            # drain: the last batch and its finishers
+            self.batch.wait_mark(mark)
+            self._finish(self.retiring, clock)
+            self.retiring = []
+            self.prev_mark = None
+        return len(self.active) + len(self.retiring)
+
+    def _finish(self, retiring, clock):
+        """Results of requests whose copies were enqueued a tick ago: wait
+        for each copy, keep the planes, free the simulation (stream-ordered)."""
+        planes = {"S": 0, "ux": 1, "uz": 2, "p": 3}
+        for r, buf in retiring:
+            r.sim.sync()
+            a = buf.numpy()
+            r.result = {k: a[planes[k] * r.cells:(planes[k] + 1) * r.cells].astype(np.float64).reshape(r.nz, r.nx)
+                        for k in self.keep}
+            r.finished = clock()
+            self.in_use -= r.sim.device_bytes()
+            r.sim.close()
+            r.sim = None
+            self.done.append(r)
 
     def run(self, requests, clock=time.perf_counter):
         """Serve `requests` (arrival times relative to the start); returns stats."""
@@ -139,24 +212,27 @@ class Server:
         t0 = clock()
         rel = lambda: clock() - t0
         i = 0
-        while i < len(pending) or self.waiting or self.active:
+        while i < len(pending) or self.waiting or self.active or self.retiring:
             now = rel()
             while i < len(pending) and pending[i].arrival <= now:
                 self.submit(pending[i], now)
                 i += 1
-            if not self.waiting and not self.active and i < len(pending):
+            if not self.waiting and not self.active and not self.retiring and i < len(pending):
                 time.sleep(max(0.0, min(pending[i].arrival - now, 0.05)))
                 continue
             self.tick(rel)
         wall = rel()
         lat = np.array([r.finished - r.arrival for r in self.done])
         return {"requests": len(self.done), "wall_s": wall, "cell_updates": self.cell_updates,
-                "mlups": self.cell_updates / wall / 1e6,
+                "mlups": self.cell_updates / wall / 1e6, "host_s": {"admit": round(self.t_admit, 4),
+                                                                  "step": round(self.t_step, 4),
+                                                                  "retire": round(self.t_retire, 4)},
                 "p50_s": float(np.percentile(lat, 50)) if len(lat) else None,
                 "p99_s": float(np.percentile(lat, 99)) if len(lat) else None}
 
     def close(self):
-        for r in self.active:
+        self.batch.sync()
+        for r in self.active + [r for r, _ in self.retiring]:
             if r.sim is not None:
                 r.sim.close()
         self.batch.close()
@@ -164,10 +240,30 @@ class Server:
 
 def lock_exchange_request(rid, nx, nz, steps, arrival=0.0, storage="f16", seed=0):
     """A 2-D lock-exchange request: S = 1 on the left half (seeded interface
-    noise), D2Q9 MRT + D2Q5, uniform grid, bounce-back, lattice units."""
+    noise), D2Q9 MRT + D2Q5, uniform grid, bounce-back, lattice units. The
+    reduced gravity g' = 1e-4 (64 / nz) keeps the front speed, about
+    sqrt(g' nz) / 2, at 0.04 lattice units on every grid height."""
     rng = np.random.default_rng(seed)
     S0 = np.where(np.arange(nx)[None, :] < nx // 2, 1.0, 0.0) * np.ones((nz, 1))
     S0[:, nx // 2 - 1: nx // 2 + 1] += rng.uniform(-1e-4, 1e-4, (nz, 2))
+    gp = 1e-4 * 64.0 / nz
     kw = dict(q_scalar=5, geometry="uniform", storage=storage, wall="bb", mrt=True, tau=0.53, taus=0.503,
-              rho_sal=1e-4, g_bouss=1e-4, s_ref=0.5)
+              rho_sal=gp, g_bouss=gp)
     return Request(arrival=arrival, rid=rid, nx=nx, nz=nz, steps=steps, kwargs=kw, s0=S0.ravel())
+
+
+def rayleigh_taylor_request(rid, nx, nz, steps, arrival=0.0, storage="f16", seed=0):
+    """A 2-D Rayleigh-Taylor request on the conservative Allen-Cahn phase
+    field: heavy fluid (phi = 1, density 3) over light (phi = 0, density 1),
+    interface width W = 4, mobility (tau_phi - 1/2)/3 = 0.02, a seeded
+    single-mode perturbation of amplitude 0.05 nx, slip walls, D2Q9 MRT with
+    a D2Q9 phase lattice, lattice units. Gravity g = 1e-5 (256 / nx) keeps
+    the growth speed sqrt(At g nx) near 0.04 on every grid width."""
+    rng = np.random.default_rng(seed)
+    xx, zz = np.meshgrid(np.arange(nx) + 0.5, np.arange(nz) + 0.5)
+    amp = 0.05 * nx * (1.0 + rng.uniform(-0.02, 0.02))
+    zi = nz / 2 + amp * np.cos(2 * np.pi * xx / nx + rng.uniform(0, 2 * np.pi))
+    phi0 = 0.5 * (1.0 + np.tanh(2.0 * (zz - zi) / 4.0))
+    kw = dict(q_scalar=9, geometry="uniform", storage=storage, wall="slip", mrt=True, tau=0.56, taus=0.56,
+              scalar="phase", rhoL=1.0, rhoH=3.0, sigma=5e-5, pf_width=4.0, gravity=1e-5 * 256.0 / nx)
+    return Request(arrival=arrival, rid=rid, nx=nx, nz=nz, steps=steps, kwargs=kw, s0=phi0.ravel())

@@ -11,6 +11,7 @@ from .cases import d2q9_mrt
 GEOMETRY = {"uniform": 0, "x5": 1, "x3": 2, "z5": 3, "z3": 4}
 STORAGE = {"f32": 0, "f16": 1, "bf16": 2}
 WALL = {"slip": 0, "bb": 1}
+SCALAR = {"salinity": 0, "phase": 1}
 
 # the reference's constants (ref: function/collision.cu:78,251)
 REF_RHO_SAL = 0.824493
@@ -27,7 +28,8 @@ class Sim:
     def __init__(self, nx, nz, *, q_scalar=5, geometry="uniform", storage="f32", wall="bb", mrt=True,
                  dz=1.0, dt=1.0, x=None, z=None, wx=None, wz=None, tau=0.53, taus=0.503,
                  rhoL=1.0, rhoH=1.0, phi=1.0, rho_sal=0.0, g_bouss=1e-4, s_ref=0.5,
-                 M=None, Minv=None, S=None, s0=None, stream=None):
+                 M=None, Minv=None, S=None, s0=None, stream=None, scalar="salinity", sigma=0.0, pf_width=4.0,
+                 gravity=0.0):
         L = _lib.lib()
         self.nx, self.nz, self.q_scalar = int(nx), int(nz), int(q_scalar)
         self._keep = []
@@ -54,6 +56,8 @@ class Sim:
         cfg.tau, cfg.taus = tau, taus
         cfg.rhoL, cfg.rhoH, cfg.phi = rhoL, rhoH, phi
         cfg.rho_sal, cfg.g_bouss, cfg.s_ref = rho_sal, g_bouss, s_ref
+        cfg.scalar_kind = SCALAR[scalar] if isinstance(scalar, str) else int(scalar)
+        cfg.sigma, cfg.pf_width, cfg.gravity = sigma, pf_width, gravity
         if mrt:
             cfg.M, cfg.Minv, cfg.S = arr(M, 81), arr(Minv, 81), arr(S, 9)
         s0p = arr(s0, nx * nz)
@@ -108,6 +112,10 @@ class Sim:
 
     def bytes_per_cell(self):
         return int(_lib.lib().ipcu_sim_bytes_per_cell(self._h))
+
+    def mac_planes(self):
+        """FP32 macroscopic planes of the raw state: S, u_x, u_z (+ p* with 16-bit storage)."""
+        return 3 if self.storage_bytes() == 4 else 4
 
     def upload(self, f=None, g=None, mac=None):
         """Asynchronous raw upload from (ideally pinned) host buffers in the storage layout."""

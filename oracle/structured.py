@@ -10,6 +10,14 @@ Step (ref: LockExchange/LockExchange.cu:220-236):
                                                         set_bound.cu:164-183, propagation.cu)
   S = sum g, p* = sum f, u = sum e f + F dt / 2 rho    (collision.cu:225-257)
 
+Phase-field mode (phase_field=True): the scalar lattice carries the
+Allen-Cahn order parameter phi instead of salinity, in the reference's
+two-phase step order (RTinstability/RTinstability.cu:177-206):
+  rho = rhoL + (rhoH - rhoL) phi; F = mu grad(phi) - rho g e_z - p* c^2/3 grad(rho)
+  with mu = 4 beta phi (phi - 1)(phi - 1/2) - kappa lap(phi)  (collision.cu:57-112, Boussi_flag off)
+  conservative Allen-Cahn collision of g with the d(phi u)/dt term (collision.cu:190-223)
+  phi = sum g                                                   (collision.cu:225-236)
+
 On the reference's own layouts it is pinned against the oracle's kernel
 chain (tests/test_structured_oracle.py); it extends the same rules to an
 interpolated z axis, the 3-point upwind-biased quadratic stencil and the
@@ -89,8 +97,11 @@ def slip_partner(k, L, R, B, T):
 class Box:
     def __init__(self, nx, nz, *, q_scalar=5, geometry="uniform", wall="bb", mrt=True, dz=1.0, dt=1.0, x=None,
                  z=None, wx=None, wz=None, tau=0.53, taus=0.503, rhoL=1.0, rhoH=1.0, phi=1.0, rho_sal=0.0,
-                 g_bouss=1e-4, M=None, Minv=None, S=None):
+                 g_bouss=1e-4, M=None, Minv=None, S=None, phase_field=False, sigma=0.0, pf_width=4.0,
+                 gravity=0.0):
         self.nx, self.nz, self.qs = nx, nz, q_scalar
+        self.pf, self.sigma, self.pfw, self.grav = phase_field, sigma, pf_width, gravity
+        self.rhoL, self.rhoH = rhoL, rhoH
         self.axis, self.ns = GEOS[geometry]
         self.wall, self.mrt = wall, mrt
         self.dz, self.dt, self.c = dz, dt, dz / dt
@@ -118,6 +129,7 @@ class Box:
         self.S = np.zeros((nz, nx))
         self.ux = np.zeros((nz, nx))
         self.uz = np.zeros((nz, nx))
+        self.old = np.zeros((2, nz, nx))  # phase field: phi u, phi w of the previous step
 
     # ------------------------------------------------------------------ pieces
     def _interp(self, fs, s):
@@ -192,6 +204,13 @@ class Box:
             new[k] = v
         return new
 
+    def rho_of(self, S):
+        """Density from the scalar field: the mixture rhoL + (rhoH - rhoL) phi
+        (phase field) or rho0 + rho_sal S (salinity) (ref: collision.cu:251)."""
+        if self.pf:
+            return self.rhoL + (self.rhoH - self.rhoL) * S
+        return self.rho0 + self.rho_sal * S
+
     # ------------------------------------------------------------------ step
     def step(self, n=1):
         for _ in range(n):
@@ -201,7 +220,7 @@ class Box:
         c, c2, dt = self.c, self.c ** 2, self.dt
         f, S, u, w = self.f, self.S, self.ux, self.uz
         p = f.sum(0)
-        rho = self.rho0 + self.rho_sal * S
+        rho = self.rho_of(S)
         xi = np.arange(self.nx)
         zi = np.arange(self.nz)
         rxp = rho[:, np.minimum(xi + 1, self.nx - 1)]
@@ -210,7 +229,23 @@ class Box:
         rzm = rho[np.maximum(zi - 1, 0), :]
         pc = p * c2 / 3
         Fx = -pc * (rxp - rxm) * self.gix[None, :]
-        Fz = -S * self.g_bouss - pc * (rzp - rzm) * self.giz[:, None]
+        Fz = -pc * (rzp - rzm) * self.giz[:, None]
+        if self.pf:
+            # surface tension mu grad(phi) (chemical potential of the double
+            # well) and the weight of the mixture (ref: collision.cu:65-78)
+            sxp = S[:, np.minimum(xi + 1, self.nx - 1)]
+            sxm = S[:, np.maximum(xi - 1, 0)]
+            szp = S[np.minimum(zi + 1, self.nz - 1), :]
+            szm = S[np.maximum(zi - 1, 0), :]
+            dpx = (sxp - sxm) * self.gix[None, :]
+            dpz = (szp - szm) * self.giz[:, None]
+            lap = (sxp - 2 * S + sxm) / self.DX[None, :] ** 2 + (szp - 2 * S + szm) / self.DZ[:, None] ** 2
+            beta, kap = 12 * self.sigma / self.pfw, 1.5 * self.sigma * self.pfw
+            mu = 4 * beta * S * (S - 1) * (S - 0.5) - kap * lap
+            Fx = Fx + mu * dpx
+            Fz = Fz + mu * dpz - rho * self.grav
+        else:
+            Fz = Fz - S * self.g_bouss
         eu = c * (EX9[:, None, None] * u[None] + EZ9[:, None, None] * w[None]) / c2
         us = (u * u + w * w) / c2
         feq = W9[:, None, None] * (p[None] + 3 * eu + 4.5 * eu ** 2 - 1.5 * us[None])
@@ -228,16 +263,31 @@ class Box:
             eq = c * (EX9[:qs, None, None] * u[None] + EZ9[:qs, None, None] * w[None]) / c2
             shape = 1 + 3 * eq if qs == 5 else 1 + 3 * eq + 4.5 * eq ** 2 - 1.5 * us[None]
             geq = w_[:, None, None] * S[None] * shape
-            ne = self.g - geq
-            jx = (ne * (c * EX9[:qs, None, None])).sum(0)
-            jz = (ne * (c * EZ9[:qs, None, None])).sum(0)
-            gs = geq + (1 - 1 / self.taus) * w_[:, None, None] * 3 * (
-                jx[None] * c * EX9[:qs, None, None] + jz[None] * c * EZ9[:qs, None, None]) / c2
+            if self.pf:
+                # conservative Allen-Cahn collision (ref: collision.cu:190-223):
+                # g* = g - (g - geq)/tau_phi + (tau_phi - 1/2)/tau_phi Fp, with
+                # Fp_k = dt w_k [(1 - 4 (phi - 1/2)^2)/W c e.grad(phi)/|grad(phi)|
+                #                + 3 e.d(phi u)/dt / c]
+                nab = (S * u - self.old[0]) / dt, (S * w - self.old[1]) / dt
+                self.old = np.stack([S * u, S * w])
+                nrm = np.sqrt(dpx ** 2 + dpz ** 2 + 1e-8)
+                ed = EX9[:qs, None, None] * dpx[None] + EZ9[:qs, None, None] * dpz[None]
+                en = EX9[:qs, None, None] * nab[0][None] + EZ9[:qs, None, None] * nab[1][None]
+                Fp = dt * w_[:, None, None] * ((1 - 4 * (S - 0.5) ** 2)[None] / self.pfw * c * ed / nrm[None]
+                                               + 3 * en / c)
+                ts = self.taus
+                gs = self.g - (self.g - geq) / ts + (ts - 0.5) / ts * Fp
+            else:
+                ne = self.g - geq
+                jx = (ne * (c * EX9[:qs, None, None])).sum(0)
+                jz = (ne * (c * EZ9[:qs, None, None])).sum(0)
+                gs = geq + (1 - 1 / self.taus) * w_[:, None, None] * 3 * (
+                    jx[None] * c * EX9[:qs, None, None] + jz[None] * c * EZ9[:qs, None, None]) / c2
             self.g = self._stream(gs, qs)
             S = self.g.sum(0)
         self.f = self._stream(fs, 9)
         p2 = self.f.sum(0)
-        rho2 = self.rho0 + self.rho_sal * S
+        rho2 = self.rho_of(S)
         h = dt / (2 * rho2)
         self.ux = (self.f * (c * EX9[:, None, None])).sum(0) + Fx * h
         self.uz = (self.f * (c * EZ9[:, None, None])).sum(0) + Fz * h

@@ -8,7 +8,7 @@ from types import SimpleNamespace
 import numpy as np
 
 from ip_cu_lbm_b200 import cases
-from ip_cu_lbm_b200.lockexchange import ibm_step, le_step
+from ip_cu_lbm_b200.lockexchange import ibm_step, le_step, pf_step
 
 RHO_SAL = 0.824493
 
@@ -77,6 +77,22 @@ def random_state(case, seed, *, rhoL=1.0, rhoH=1000.0, tau=0.6, taus=0.55, amp=1
     return st
 
 
+def random_pf_state(case, seed, *, rhoL=1.0, rhoH=3.0, tau=0.6, taus=0.58, amp=1e-3, noise=0.2):
+    """A two-phase state: the smooth random scalar becomes the order
+    parameter phi in [0.02, 0.98] (no salinity), rho the mixture density, and
+    the previous-step fields phi_old, u_old equal the current ones (so the
+    d(phi u)/dt term starts at zero, as in the reference driver)."""
+    st = random_state(case, seed, rhoL=rhoL, rhoH=rhoH, tau=tau, taus=taus, amp=amp, smin=0.02, smax=0.98,
+                      noise=noise)
+    dt = case["dtype"]
+    phi = st["sal"].copy()
+    st["phi"] = phi
+    st["sal"] = np.zeros_like(phi)
+    st["rho"] = density(st["sal"], phi, rhoL, rhoH, dt)
+    st["phiold"], st["uold"], st["vold"], st["wold"] = phi.copy(), st["u"].copy(), st["v"].copy(), st["w"].copy()
+    return st
+
+
 def mrt_mats(Q=9):
     M, Minv, S = cases.d2q9_mrt()
     _, So, _, MM = cases.set_M(Q, M, S, Minv)
@@ -130,6 +146,8 @@ def oracle_chain(case, state, nsteps, *, prec=None, slip=1, mats=None, kind="le"
         if kind == "le":
             le_step(call, ip, B, num_F=case["nt"], wall_sizes=tuple(len(w) for w in case["walls"]),
                     mrt=mats is not None, **kw)
+        elif kind == "pf":
+            pf_step(call, ip, B, num_F=case["nt"], mrt=mats is not None, **kw)
         else:
             ibm_step(call, ip, B, num_F=case["nt"], num_Gw=case["n_ib"] * 3, mrt=mats is not None, **kw)
     return B
@@ -186,6 +204,8 @@ def gpu_chain(case, state, nsteps, backend, *, slip=1, mats=None, kind="le", **k
         if kind == "le":
             le_step(call, ip, B, num_F=nt, wall_sizes=tuple(len(w) for w in case["walls"]), mrt=mats is not None,
                     **kw)
+        elif kind == "pf":
+            pf_step(call, ip, B, num_F=nt, mrt=mats is not None, **kw)
         else:
             ibm_step(call, ip, B, num_F=nt, num_Gw=case["n_ib"] * 3, mrt=mats is not None, **kw)
     torch.cuda.synchronize()

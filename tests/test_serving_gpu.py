@@ -6,7 +6,7 @@ import numpy as np
 import pytest
 
 from ip_cu_lbm_b200 import Sim
-from ip_cu_lbm_b200.serving import Batch, Server, lock_exchange_request, request_bytes
+from ip_cu_lbm_b200.serving import Batch, Server, lock_exchange_request, rayleigh_taylor_request, request_bytes
 
 pytestmark = pytest.mark.gpu
 
@@ -41,6 +41,26 @@ def test_results_same_alone_and_in_mix(cuda, storage):
         plain = _alone(r, batched=False)
         for k in ("S", "ux", "uz"):
             np.testing.assert_allclose(r.result[k], plain[k], rtol=0, atol=1e-6 * max(1.0, np.abs(plain[k]).max()))
+
+
+@pytest.mark.parametrize("storage", ["f32", "f16"])
+def test_mixed_salinity_and_phase_field_batch(cuda, storage):
+    """Lock-exchange (salinity) and Rayleigh-Taylor (Allen-Cahn phase field)
+    requests served together: each kernel class gets its own launch per step
+    and every result equals the request run alone."""
+    reqs = [lock_exchange_request(0, 96, 64, 120, storage=storage, seed=0),
+            rayleigh_taylor_request(1, 128, 128, 160, storage=storage, seed=1),
+            lock_exchange_request(2, 64, 48, 80, arrival=0.01, storage=storage, seed=2),
+            rayleigh_taylor_request(3, 64, 96, 100, arrival=0.02, storage=storage, seed=3)]
+    srv = Server(budget_bytes=1e9, tick_steps=40)
+    stats = srv.run(reqs)
+    srv.close()
+    assert stats["requests"] == len(reqs)
+    for r in srv.done:
+        same = _alone(r, batched=True)
+        for k in ("S", "ux", "uz"):
+            assert np.array_equal(r.result[k], same[k]), (r.rid, k)
+        assert np.isfinite(r.result["ux"]).all()
 
 
 def test_budget_limits_admission(cuda):

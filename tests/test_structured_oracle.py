@@ -6,7 +6,7 @@ import numpy as np
 import pytest
 
 from ip_cu_lbm_b200 import cases
-from helpers import mrt_mats, oracle_chain, random_state, rel_l2
+from helpers import mrt_mats, oracle_chain, random_pf_state, random_state, rel_l2
 from oracle.structured import Box
 
 BOXES = [
@@ -52,6 +52,33 @@ def test_structured_oracle_matches_kernel_chain(bx, slip, nsteps):
     f = chain.f.reshape(-1, 9)[: c["nc"]]
     err = rel_l2(b.f, np.stack([grid(f[:, k]) for k in range(9)]))
     assert err <= 1e-12, ("f", err)
+
+
+PF_PHYS = dict(rhoL=1.0, rhoH=3.0)
+
+
+@pytest.mark.parametrize("bx", BOXES)
+@pytest.mark.parametrize("slip", [0, 1])
+@pytest.mark.parametrize("nsteps", [1, 6])
+def test_structured_phase_field_matches_kernel_chain(bx, slip, nsteps):
+    """Two-phase (Allen-Cahn) mode against the reference's two-phase kernel
+    order on the oracle chain: surface tension, the mixture's weight,
+    col_PF with its d(phi u)/dt term. The reference fixes tau_phi = 0.58."""
+    c = cases.box_case(prec="f64", nx0=bx["nx0"], nz=bx["nz"], divx=bx["divx"], dx=1e-3, dt=1e-4, sigma=2e-4)
+    st = random_pf_state(c, 11 + nsteps, tau=0.63, taus=0.58, **PF_PHYS)
+    mats = mrt_mats()
+    chain = oracle_chain(c, st, nsteps, slip=slip, mats=mats, kind="pf", **PF_PHYS)
+    st_b = dict(st)
+    st_b["sal"] = st["phi"]
+    it = c["items"]
+    b = structured_from_case(c, st_b, slip=slip, mats=mats, phase_field=True, sigma=float(it[16]),
+                             pf_width=float(it[9]), gravity=9.81, **PF_PHYS)
+    b.old = np.stack([b.S * b.ux, b.S * b.uz])
+    b.step(nsteps)
+    grid = lambda a: cases.compact_to_grid(c, a)
+    for name, mine, ref in (("u", b.ux, chain.u), ("w", b.uz, chain.w), ("phi", b.S, chain.phi), ("p", b.p, chain.p)):
+        err = rel_l2(mine, grid(ref), floor=1e-300)
+        assert err <= 1e-12, (name, err)
 
 
 def test_uniform_streaming_is_an_exact_shift():
