@@ -153,6 +153,38 @@ int ipcu_batch_sync(ipcu_batch *batch);
  * waits for it. A server keeps the host one tick ahead of the GPU with them. */
 int ipcu_batch_mark(ipcu_batch *batch);
 int ipcu_batch_wait_mark(ipcu_batch *batch, int mark);
+/* Moving immersed boundary: one rigid body per simulation (uniform
+ * lattice, salinity or no scalar). Markers on the outline (body frame,
+ * physical units) carry arc lengths dS; each step, after the fluid step,
+ * multi-direct forcing with the reference's 4-point Peskin kernel
+ * (ref: function/ibm.cu:61-66 weightFunction) makes the fluid follow the
+ * body at the markers, the force density enters the next fluid step, and
+ * the body moves by an FP64 momentum balance built on the reference's
+ * update_IBbody / update_IBpoint (ref: function/ibm.cu:367-447): the
+ * reaction of the IB force, buoyancy -(1 - rho_f/rho_s) m gravity along z
+ * and the change of the fluid momentum inside the body. No counterpart of
+ * the reference's own IB coupling (get_IBMGw2), which stays available
+ * through the kernel-entry API above. */
+typedef struct ipcu_ib_body2d {
+  double xc, zc, theta;   /* centre (cell centres at (i + 1/2) dz) and angle */
+  double u, w, omega;     /* initial velocity and angular velocity */
+  double rho_s, rho_f;    /* body and fluid density */
+  double area, inertia;   /* area and polar second moment of area (integral of r^2 dA) */
+  double semi_a, semi_b;  /* ellipse semi-axes (body frame x, z): cells whose centre lies inside
+                             carry the fluid momentum the body update adds back */
+  double gravity;
+  int32_t iters;          /* multi-direct forcing iterations (3) */
+  int32_t pad;
+} ipcu_ib_body2d;
+/* Attaches the body (n <= 512 markers, [n][2] x, z); IPCU_ERR_UNSUPPORTED
+ * for stretched geometries and the phase field. Drops recorded graphs;
+ * snapshots of a simulation with a body are refused. Status bit 8: the
+ * body's stencils outgrew the kernel's window (the update was skipped). */
+int ipcu_sim_ib_attach(ipcu_sim *sim, const ipcu_ib_body2d *body, const double *markers, const double *dS, int32_t n);
+/* Body state: x, z, u, w, theta, omega and the IB force (x, z) and torque
+ * the markers put on the fluid in the last step (9 values). Synchronises.
+ * ipcu_sim_get serves the force density as fields "ibfx", "ibfz". */
+int ipcu_sim_ib_body(ipcu_sim *sim, double *out);
 /* Device bytes a simulation holds (state, ping-pong, tables). */
 int64_t ipcu_sim_device_bytes(const ipcu_sim *sim);
 

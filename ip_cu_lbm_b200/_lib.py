@@ -71,6 +71,18 @@ class SimConfig(ctypes.Structure):
     ]
 
 
+class IBBody2D(ctypes.Structure):
+    """Mirror of ipcu_ib_body2d (include/ipcu_sim.h)."""
+    _fields_ = [
+        ("xc", ctypes.c_double), ("zc", ctypes.c_double), ("theta", ctypes.c_double),
+        ("u", ctypes.c_double), ("w", ctypes.c_double), ("omega", ctypes.c_double),
+        ("rho_s", ctypes.c_double), ("rho_f", ctypes.c_double),
+        ("area", ctypes.c_double), ("inertia", ctypes.c_double),
+        ("semi_a", ctypes.c_double), ("semi_b", ctypes.c_double),
+        ("gravity", ctypes.c_double), ("iters", ctypes.c_int32), ("pad", ctypes.c_int32),
+    ]
+
+
 class Sim3DConfig(ctypes.Structure):
     """Mirror of ipcu_sim3d_config (include/ipcu_sim3d.h)."""
     _fields_ = [
@@ -130,6 +142,8 @@ def _declare(L: ctypes.CDLL) -> None:
         "ipcu_batch_mark": ([P], I),
         "ipcu_batch_wait_mark": ([P, I], I),
         "ipcu_sim_device_bytes": ([P], I64),
+        "ipcu_sim_ib_attach": ([P, ctypes.POINTER(IBBody2D), P, P, ctypes.c_int32], I),
+        "ipcu_sim_ib_body": ([P, P], I),
         "ipcu_sim3d_create": ([ctypes.POINTER(Sim3DConfig), P, P, ctypes.POINTER(P)], I),
         "ipcu_sim3d_destroy": ([P], None),
         "ipcu_sim3d_step": ([P, I64], I),

@@ -231,3 +231,14 @@ def ibm_ellipse_case(nx0=40, nz=60, n_markers=24, dx=1e-3, dt=1e-3, tilt_deg=45.
                 angleVB=f32(np.zeros(3)), posw=f32(posw), oposw=f32(op), Gw=f32(np.zeros(3 * n_markers)),
                 velw=f32(np.zeros(3 * n_markers)), nB=f32(nB), onB=f32(onB), quatold=f32(q))
     return c, body
+
+
+def ellipse_markers(a, b, n):
+    """Lagrangian markers of an ellipse (x/a)^2 + (z/b)^2 = 1 in the body
+    frame: n points at equal arc length (dense polyline of the perimeter,
+    inverted by interpolation) and the arc length each one carries."""
+    t = np.linspace(0.0, 2.0 * np.pi, 40001)
+    x, z = a * np.cos(t), b * np.sin(t)
+    s = np.concatenate([[0.0], np.cumsum(np.hypot(np.diff(x), np.diff(z)))])
+    tt = np.interp(np.arange(n) * s[-1] / n, s, t)
+    return np.stack([a * np.cos(tt), b * np.sin(tt)], 1), np.full(n, s[-1] / n)

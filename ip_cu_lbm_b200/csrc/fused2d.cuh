@@ -61,6 +61,12 @@ struct alignas(64) Params {
   int8_t slipB9[16 * 9], slipK9[16 * 9];  // per wall class: owner neighbour and population
   int8_t slipB5[16 * 9], slipK5[16 * 9];
   unsigned *status;
+  // immersed boundary: force density [2][N] added to the cell force where the
+  // cell's tile is flagged in ibflag ([tiles z][ibtx]: some cell of the tile
+  // or of its halo carries a force); null without a body
+  const float *fext;
+  const uint8_t *ibflag;
+  int ibtx;
 };
 
 // prepare_only: set the kernel's shared-memory attribute (call once before any capture);

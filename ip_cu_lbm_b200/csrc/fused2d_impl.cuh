@@ -229,6 +229,8 @@ __device__ __forceinline__ void step_tile(const Params &p, int parity, int tile_
   static_assert(PHYS == 0 || QS > 0, "the phase field lives on the scalar lattice");
   const float rho0 = p.rho_base, rsal = p.rho_sal_f;
   auto rho_of = [&](float S) { return fmaf(S, rsal, rho0); };
+  // immersed-boundary force on this tile (block-uniform)
+  const bool ibt = p.fext != nullptr && p.ibflag[tile_z * p.ibtx + tile_x] != 0;
 
   // ---- phase 0: stage the tile (TMA) or the salinity ring, and the axis weights
   if (tid == 0) *qcount = 0;
@@ -347,6 +349,11 @@ __device__ __forceinline__ void step_tile(const Params &p, int parity, int tile_
       Fz += mu * dpz - rho * p.grav;  // the mixture's weight (Boussi_flag off)
     } else {
       Fz -= S * p.g_bouss_f;  // Boussinesq buoyancy of the salinity
+    }
+    if (ibt) {  // immersed-boundary force density of the previous coupled step
+      const long long ci = (long long)gz * nx + gx;
+      Fx += p.fext[ci];
+      Fz += p.fext[N + ci];
     }
     const float uc = u * ic, wc = w * ic;
     const float usq = uc * uc + wc * wc;

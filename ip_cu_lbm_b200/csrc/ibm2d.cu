@@ -1,0 +1,456 @@
+// Moving immersed boundary for the fused 2-D solver: one CTA per body runs,
+// after each fluid step, the whole coupled update on the body's footprint.
+//
+// The fluid step added the previous IB force density f_ib to the cell force
+// (fused kernel), so the new velocity u = c j + (F + f_ib) dt / 2 rho holds
+// half of it. The update (uniform lattice, cell centres (i + 1/2) dz):
+//   1. markers X_l = X + R(theta) X0_l, U_b,l = U + omega x r_l (FP64, as
+//      update_IBpoint, ref: function/ibm.cu:426-447), and their 4x4 Peskin
+//      stencils (ref: function/ibm.cu:61-66 weightFunction);
+//   2. the cells of the previous and the new stencils get shared-memory
+//      slots (a window map over their bounding box); the old force's half
+//      is taken out of u there and f_ib restarts at zero;
+//   3. multi-direct forcing, `iters` times: U*_l = sum phi u (16 lanes per
+//      marker, shuffle reduction), dF_l = 2 rho_f (U_b,l - U*_l) / dt,
+//      spread df = dF_l phi dS_l / dz^2 onto f_ib and df dt / 2 rho onto u
+//      (shared-memory atomics), F_l += dF_l;
+//   4. u and f_ib go back to HBM (16-bit storage re-expresses the stored
+//      deviations about the new u, so the populations stay as they were),
+//      and the tile flags the fluid kernel reads follow the footprint;
+//   5. FP64 sums: F_ib = sum F_l dS_l, T_ib = sum r_l x F_l dS_l and the
+//      fluid momentum P, angular momentum L of the cells whose centre lies
+//      inside the body (ellipse);
+//   6. one thread steps the body in FP64 (update_IBbody's force, torque and
+//      buoyancy (1 - rho_f/rho_s) m g, ref: function/ibm.cu:367-424): the
+//      body takes the reaction of the mean of this step's and the previous
+//      step's IB force (the fluid's momentum changes by that mean) plus the
+//      change of the fluid momentum inside it, with forward Euler for the
+//      velocities and the trapezoidal rule for position and angle:
+//        m (U' - U) = -dt (F_ib + F_ib,old)/2 + rho_f (P - P_old) + buoyancy,
+//        I (w' - w) = -dt (T_ib + T_ib,old)/2 + rho_f (L - L_old).
+// Overflow of the marker, window or slot capacity sets status bit 8 and
+// leaves the state untouched.
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+
+#include "fused2d_impl.cuh"
+#include "ibm2d.cuh"
+#include "ipcu_common.cuh"
+#include "storage.cuh"
+
+namespace ipcu {
+namespace ib2d {
+
+namespace {
+
+constexpr int kWarps = kThreads / 32;
+constexpr int kGroups = kThreads / 16;  // 16 lanes (one 4x4 stencil) per marker
+
+// 4-point Peskin kernel (ref: function/ibm.cu:61-66), r in lattice spacings
+__device__ __forceinline__ float peskin4(float r) {
+  r = fabsf(r);
+  if (r < 1.0f) return (3.0f - 2.0f * r + sqrtf(fmaxf(1.0f + 4.0f * r - 4.0f * r * r, 0.0f))) * 0.125f;
+  if (r < 2.0f) return (5.0f - 2.0f * r - sqrtf(fmaxf(-7.0f + 12.0f * r - 4.0f * r * r, 0.0f))) * 0.125f;
+  return 0.0f;
+}
+
+struct Layout {
+  // markers
+  static constexpr size_t I0 = 0;                                   // int [nl] stencil origin x
+  static constexpr size_t K0 = I0 + 4 * kMaxMarkers;                 // int [nl] origin z
+  static constexpr size_t WX = K0 + 4 * kMaxMarkers;                 // float [nl][4]
+  static constexpr size_t WZ = WX + 16 * kMaxMarkers;                // float [nl][4]
+  static constexpr size_t UB = WZ + 16 * kMaxMarkers;                // float [nl][2] body velocity at the marker
+  static constexpr size_t DF = UB + 8 * kMaxMarkers;                 // float [nl][2] this iteration's force
+  static constexpr size_t FT = DF + 8 * kMaxMarkers;                 // float [nl][2] accumulated force
+  static constexpr size_t DS = FT + 8 * kMaxMarkers;                 // float [nl] dS / dz^2
+  // slots
+  static constexpr size_t CELL = DS + 4 * kMaxMarkers;               // int [slots] cell index
+  static constexpr size_t SU = CELL + 4 * kMaxSlots;                 // float [slots] u_x
+  static constexpr size_t SW = SU + 4 * kMaxSlots;                   // float [slots] u_z
+  static constexpr size_t SFX = SW + 4 * kMaxSlots;                  // float [slots] f_ib x
+  static constexpr size_t SFZ = SFX + 4 * kMaxSlots;                 // float [slots] f_ib z
+  static constexpr size_t SH = SFZ + 4 * kMaxSlots;                  // float [slots] dt / 2 rho
+  static constexpr size_t MAP = SH + 4 * kMaxSlots;                  // short [window] slot of a window cell
+  static constexpr size_t RED = (MAP + 2 * kMaxWindow + 15) / 16 * 16;  // double [kWarps][6]
+  static constexpr size_t BYTES = RED + 8 * 6 * kWarps;
+};
+
+template <class ST, int QS>
+__device__ void coupled_update(const Job &j, int parity) {
+  extern __shared__ __align__(16) unsigned char sm[];
+  int *sI0 = reinterpret_cast<int *>(sm + Layout::I0);
+  int *sK0 = reinterpret_cast<int *>(sm + Layout::K0);
+  float *sWX = reinterpret_cast<float *>(sm + Layout::WX);
+  float *sWZ = reinterpret_cast<float *>(sm + Layout::WZ);
+  float *sUB = reinterpret_cast<float *>(sm + Layout::UB);
+  float *sDF = reinterpret_cast<float *>(sm + Layout::DF);
+  float *sFT = reinterpret_cast<float *>(sm + Layout::FT);
+  float *sDS = reinterpret_cast<float *>(sm + Layout::DS);
+  int *sCell = reinterpret_cast<int *>(sm + Layout::CELL);
+  float *sU = reinterpret_cast<float *>(sm + Layout::SU);
+  float *sW = reinterpret_cast<float *>(sm + Layout::SW);
+  float *sFX = reinterpret_cast<float *>(sm + Layout::SFX);
+  float *sFZ = reinterpret_cast<float *>(sm + Layout::SFZ);
+  float *sH = reinterpret_cast<float *>(sm + Layout::SH);
+  short *sMap = reinterpret_cast<short *>(sm + Layout::MAP);
+  double *sRed = reinterpret_cast<double *>(sm + Layout::RED);
+  __shared__ Body B;
+  __shared__ int bnd[4];  // window bounds imin, imax, kmin, kmax
+  __shared__ int nslot, fail;
+
+  const f2d::Params &p = j.fp;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int nx = p.nx, nz = p.nz, nl = j.nl;
+  const long long N = (long long)nx * nz;
+  const int b = p.cur ^ parity ^ 1;  // the buffer the fluid step wrote
+  float *mac = p.mbuf[b];
+  const double dz = j.dz, idz = 1.0 / dz;
+
+  if (tid == 0) {
+    B = *j.body;
+    bnd[0] = bnd[2] = INT_MAX;
+    bnd[1] = bnd[3] = INT_MIN;
+    nslot = 0;
+    fail = nl > kMaxMarkers ? 1 : 0;
+  }
+  __syncthreads();
+  if (fail) {
+    if (tid == 0) atomicOr(p.status, 8u);
+    return;
+  }
+  const bool have_prev = B.have_prev != 0;
+  const double cth = cos(B.th), sth = sin(B.th);
+
+  // ---- 1. markers: position, velocity, stencil origin and weights
+  for (int l = tid; l < nl; l += kThreads) {
+    const double x0 = j.X0[2 * l], z0 = j.X0[2 * l + 1];
+    const double rx = cth * x0 - sth * z0, rz = sth * x0 + cth * z0;
+    const double X = B.X[0] + rx, Z = B.X[1] + rz;
+    const double xs = X * idz - 0.5, zs = Z * idz - 0.5;  // in cell-index units
+    const int i0 = (int)floor(xs) - 1, k0 = (int)floor(zs) - 1;
+    sI0[l] = i0;
+    sK0[l] = k0;
+#pragma unroll
+    for (int a = 0; a < 4; a++) {
+      sWX[4 * l + a] = peskin4((float)((double)(i0 + a) - xs));
+      sWZ[4 * l + a] = peskin4((float)((double)(k0 + a) - zs));
+    }
+    sUB[2 * l] = (float)(B.U[0] - B.om * rz);
+    sUB[2 * l + 1] = (float)(B.U[1] + B.om * rx);
+    sFT[2 * l] = sFT[2 * l + 1] = 0.f;
+    sDS[l] = (float)(j.dS[l] * idz * idz);
+    atomicMin(&bnd[0], i0);
+    atomicMax(&bnd[1], i0 + 3);
+    atomicMin(&bnd[2], k0);
+    atomicMax(&bnd[3], k0 + 3);
+    if (have_prev) {
+      const int oi = j.org[2 * l], ok = j.org[2 * l + 1];
+      atomicMin(&bnd[0], oi);
+      atomicMax(&bnd[1], oi + 3);
+      atomicMin(&bnd[2], ok);
+      atomicMax(&bnd[3], ok + 3);
+    }
+  }
+  __syncthreads();
+  const int wi0 = bnd[0], wk0 = bnd[2], WW = bnd[1] - bnd[0] + 1, WH = bnd[3] - bnd[2] + 1;
+  if (nl == 0 || (long long)WW * WH > kMaxWindow) {
+    if (tid == 0 && nl > 0) atomicOr(p.status, 8u);
+    return;
+  }
+  const int nwin = WW * WH;
+
+  // ---- 2. slots for the cells of the old and new stencils inside the box
+  for (int e = tid; e < nwin; e += kThreads) sMap[e] = -1;
+  __syncthreads();
+  for (int e = tid; e < 16 * nl * (have_prev ? 2 : 1); e += kThreads) {
+    const int l = (e >> 4) % nl, a = e & 3, c = (e >> 2) & 3;
+    const bool old = (e >> 4) >= nl;
+    const int i = (old ? j.org[2 * l] : sI0[l]) + a, k = (old ? j.org[2 * l + 1] : sK0[l]) + c;
+    if (i >= 0 && i < nx && k >= 0 && k < nz) sMap[(k - wk0) * WW + (i - wi0)] = -2;
+  }
+  __syncthreads();
+  for (int e = tid; e < nwin; e += kThreads) {
+    if (sMap[e] != -2) continue;
+    const int s = atomicAdd(&nslot, 1);
+    if (s < kMaxSlots) {
+      sMap[e] = (short)s;
+      const int k = wk0 + e / WW, i = wi0 + e % WW;
+      sCell[s] = k * nx + i;
+    }
+  }
+  __syncthreads();
+  const int ns = nslot;
+  if (ns > kMaxSlots) {
+    if (tid == 0) atomicOr(p.status, 8u);
+    return;
+  }
+  const float rho0 = p.rho_base, rsal = p.rho_sal_f, hdt = p.hdt;
+  for (int s = tid; s < ns; s += kThreads) {
+    const long long ci = sCell[s];
+    const float S = mac[ci];
+    const float h = hdt / fmaf(S, rsal, rho0);
+    sH[s] = h;
+    sU[s] = mac[N + ci] - j.fext[ci] * h;
+    sW[s] = mac[2 * N + ci] - j.fext[N + ci] * h;
+    sFX[s] = sFZ[s] = 0.f;
+  }
+  __syncthreads();
+
+  // ---- 3. multi-direct forcing
+  const int g = tid >> 4, q = tid & 15, qa = q & 3, qc = q >> 2;
+  auto slot_of = [&](int l) -> int {
+    const int i = sI0[l] + qa, k = sK0[l] + qc;
+    if (i < 0 || i >= nx || k < 0 || k >= nz) return -1;
+    return sMap[(k - wk0) * WW + (i - wi0)];
+  };
+  const float two_rf_dt = (float)(2.0 * j.rho_f / j.dt);
+  for (int it = 0; it < j.iters; it++) {
+    for (int lb = 0; lb < nl; lb += kGroups) {
+      const int l = lb + g;
+      float vx = 0.f, vz = 0.f;
+      if (l < nl) {
+        const int s = slot_of(l);
+        if (s >= 0) {
+          const float w = sWX[4 * l + qa] * sWZ[4 * l + qc];
+          vx = w * sU[s];
+          vz = w * sW[s];
+        }
+      }
+#pragma unroll
+      for (int o = 8; o > 0; o >>= 1) {
+        vx += __shfl_xor_sync(0xffffffffu, vx, o, 16);
+        vz += __shfl_xor_sync(0xffffffffu, vz, o, 16);
+      }
+      if (l < nl && q == 0) {
+        const float dfx = two_rf_dt * (sUB[2 * l] - vx), dfz = two_rf_dt * (sUB[2 * l + 1] - vz);
+        sDF[2 * l] = dfx;
+        sDF[2 * l + 1] = dfz;
+        sFT[2 * l] += dfx;
+        sFT[2 * l + 1] += dfz;
+      }
+    }
+    __syncthreads();
+    for (int lb = 0; lb < nl; lb += kGroups) {
+      const int l = lb + g;
+      if (l >= nl) continue;
+      const int s = slot_of(l);
+      if (s < 0) continue;
+      const float wd = sWX[4 * l + qa] * sWZ[4 * l + qc] * sDS[l];
+      const float fx = sDF[2 * l] * wd, fz = sDF[2 * l + 1] * wd;
+      atomicAdd(&sFX[s], fx);
+      atomicAdd(&sFZ[s], fz);
+      atomicAdd(&sU[s], fx * sH[s]);
+      atomicAdd(&sW[s], fz * sH[s]);
+    }
+    __syncthreads();
+  }
+
+  // ---- 4. write back; tile flags follow the footprint
+  const int ibtx = p.ibtx;
+  auto flag_around = [&](int i, int k, uint8_t v) {
+    const int ia = max(i - kHalo, 0) / f2d::kTX, ib = min(i + kHalo, nx - 1) / f2d::kTX;
+    const int ka = max(k - kHalo, 0) / f2d::kTZ, kb = min(k + kHalo, nz - 1) / f2d::kTZ;
+    j.flag[ka * ibtx + ia] = v;
+    j.flag[ka * ibtx + ib] = v;
+    j.flag[kb * ibtx + ia] = v;
+    j.flag[kb * ibtx + ib] = v;
+  };
+  if (have_prev) {
+    for (int e = tid; e < 16 * nl; e += kThreads) {
+      const int l = e >> 4, i = j.org[2 * l] + (e & 3), k = j.org[2 * l + 1] + ((e >> 2) & 3);
+      if (i >= 0 && i < nx && k >= 0 && k < nz) flag_around(i, k, 0);
+    }
+  }
+  __syncthreads();
+  constexpr bool RES = sizeof(ST) == 2;
+  const float ic = 1.0f / p.c;
+  for (int s = tid; s < ns; s += kThreads) {
+    const long long ci = sCell[s];
+    const float un = sU[s], wn = sW[s];
+    if constexpr (RES) {
+      // re-express the stored deviations about the new velocity
+      ST *fb = static_cast<ST *>(p.fbuf[b]);
+      const float uo = mac[N + ci] * ic, wo = mac[2 * N + ci] * ic, u2o = rstore::usq(uo, wo);
+      const float uc = un * ic, wc = wn * ic, u2 = rstore::usq(uc, wc);
+      const float pr = mac[3 * N + ci];
+      float amax = 0.f;
+#pragma unroll
+      for (int k = 0; k < 9; k++) {
+        const float fv = f2d::ld(fb, k * N + ci, p.inv_fscale) + rstore::feq(k, pr, uo, wo, u2o);
+        const float r = fv - rstore::feq(k, pr, uc, wc, u2);
+        amax = fmaxf(amax, fabsf(r) * p.fscale);
+        f2d::st(fb, k * N + ci, r, p.fscale);
+      }
+      if constexpr (QS > 0) {
+        ST *gb = static_cast<ST *>(p.gbuf[b]);
+        const float S = mac[ci];
+#pragma unroll
+        for (int k = 0; k < QS; k++) {
+          const float eo = QS == 5 ? rstore::geq5(k, S, uo, wo) : rstore::geq9(k, S, uo, wo, u2o);
+          const float en = QS == 5 ? rstore::geq5(k, S, uc, wc) : rstore::geq9(k, S, uc, wc, u2);
+          const float r = f2d::ld(gb, k * N + ci, p.inv_gscale) + eo - en;
+          amax = fmaxf(amax, fabsf(r) * p.gscale);
+          f2d::st(gb, k * N + ci, r, p.gscale);
+        }
+      }
+      if (amax > p.store_max) atomicOr(p.status, 2u);
+    }
+    mac[N + ci] = un;
+    mac[2 * N + ci] = wn;
+    const float fx = sFX[s], fz = sFZ[s];
+    j.fext[ci] = fx;
+    j.fext[N + ci] = fz;
+    if (fx != 0.f || fz != 0.f) flag_around((int)(ci % nx), (int)(ci / nx), 1);
+    if (!(isfinite(un) && isfinite(wn))) atomicOr(p.status, 1u);
+  }
+  __syncthreads();
+
+  // ---- 5. FP64 sums: marker force and torque, fluid momentum inside the body
+  double acc[6] = {0, 0, 0, 0, 0, 0};
+  for (int l = tid; l < nl; l += kThreads) {
+    const double x0 = j.X0[2 * l], z0 = j.X0[2 * l + 1];
+    const double rx = cth * x0 - sth * z0, rz = sth * x0 + cth * z0;
+    const double fx = (double)sFT[2 * l] * j.dS[l], fz = (double)sFT[2 * l + 1] * j.dS[l];
+    acc[0] += fx;
+    acc[1] += fz;
+    acc[2] += rx * fz - rz * fx;
+    j.org[2 * l] = sI0[l];  // this step's footprint is the next step's old one
+    j.org[2 * l + 1] = sK0[l];
+  }
+  {
+    const double a = j.semi_a, bb = j.semi_b;
+    const double hx = sqrt(a * a * cth * cth + bb * bb * sth * sth), hz = sqrt(a * a * sth * sth + bb * bb * cth * cth);
+    const int ia = max((int)ceil((B.X[0] - hx) * idz - 0.5), 0), ib = min((int)floor((B.X[0] + hx) * idz - 0.5), nx - 1);
+    const int ka = max((int)ceil((B.X[1] - hz) * idz - 0.5), 0), kb = min((int)floor((B.X[1] + hz) * idz - 0.5), nz - 1);
+    const int bw = ib - ia + 1, bh = kb - ka + 1;
+    const double dA = dz * dz;
+    if (bw > 0 && bh > 0) {
+      for (int e = tid; e < bw * bh; e += kThreads) {
+        const int i = ia + e % bw, k = ka + e / bw;
+        const double dx = (i + 0.5) * dz - B.X[0], dzz = (k + 0.5) * dz - B.X[1];
+        const double xb = cth * dx + sth * dzz, zb = -sth * dx + cth * dzz;
+        if ((xb / a) * (xb / a) + (zb / bb) * (zb / bb) < 1.0) {
+          const long long ci = (long long)k * nx + i;
+          const double ux = mac[N + ci], uz = mac[2 * N + ci];
+          acc[3] += ux * dA;
+          acc[4] += uz * dA;
+          acc[5] += (dx * uz - dzz * ux) * dA;
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int v = 0; v < 6; v++) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc[v] += __shfl_down_sync(0xffffffffu, acc[v], o);
+  }
+  if (lane == 0) {
+#pragma unroll
+    for (int v = 0; v < 6; v++) sRed[warp * 6 + v] = acc[v];
+  }
+  __syncthreads();
+
+  // ---- 6. rigid-body step (FP64, one thread)
+  if (tid == 0) {
+    double t[6] = {0, 0, 0, 0, 0, 0};
+    for (int w = 0; w < kWarps; w++)
+      for (int v = 0; v < 6; v++) t[v] += sRed[w * 6 + v];
+    Body nb = B;
+    const double dt = j.dt, rf = j.rho_f;
+    double Fb[2] = {-(t[0] + B.Fib[0]) / 2, -(t[1] + B.Fib[1]) / 2};
+    const double Tb = -(t[2] + B.Tib) / 2;
+    Fb[1] += -(1.0 - rf / j.rho_s) * j.m * j.grav;
+    const double P0 = have_prev ? B.P[0] : t[3], P1 = have_prev ? B.P[1] : t[4], L0 = have_prev ? B.L : t[5];
+    nb.U[0] = B.U[0] + (dt * Fb[0] + rf * (t[3] - P0)) / j.m;
+    nb.U[1] = B.U[1] + (dt * Fb[1] + rf * (t[4] - P1)) / j.m;
+    nb.om = B.om + (dt * Tb + rf * (t[5] - L0)) / j.I;
+    nb.X[0] = B.X[0] + dt * (B.U[0] + nb.U[0]) / 2;
+    nb.X[1] = B.X[1] + dt * (B.U[1] + nb.U[1]) / 2;
+    nb.th = B.th + dt * (B.om + nb.om) / 2;
+    nb.P[0] = t[3];
+    nb.P[1] = t[4];
+    nb.L = t[5];
+    nb.Fib[0] = t[0];
+    nb.Fib[1] = t[1];
+    nb.Tib = t[2];
+    nb.have_prev = 1;
+    *j.body = nb;
+  }
+}
+
+template <class ST, int QS>
+__global__ void __launch_bounds__(kThreads, 1) ib_kernel(const __grid_constant__ Job j, int parity) {
+  coupled_update<ST, QS>(j, parity);
+}
+
+template <class ST, int QS>
+__global__ void __launch_bounds__(kThreads, 1) ib_kernel_batched(const Job *__restrict__ jobs, int parity) {
+  coupled_update<ST, QS>(jobs[blockIdx.x], parity);
+}
+
+template <class ST, int QS>
+int prep1() {
+  cudaError_t e = cudaFuncSetAttribute(ib_kernel<ST, QS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Layout::BYTES);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(ib_kernel_batched<ST, QS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)Layout::BYTES);
+  return status_from_cuda(e);
+}
+
+template <class ST>
+int prep_q() {
+  int st = prep1<ST, 0>();
+  if (!st) st = prep1<ST, 5>();
+  if (!st) st = prep1<ST, 9>();
+  return st;
+}
+
+template <class ST, int QS>
+int go(const Job *jp, const Job *jobs, int njobs, int parity, cudaStream_t s) {
+  if (jp) ib_kernel<ST, QS><<<1, kThreads, Layout::BYTES, s>>>(*jp, parity);
+  else ib_kernel_batched<ST, QS><<<njobs, kThreads, Layout::BYTES, s>>>(jobs, parity);
+  return status_from_cuda(cudaGetLastError());
+}
+
+template <class ST>
+int go_q(const Job *jp, const Job *jobs, int njobs, int parity, int qs, cudaStream_t s) {
+  switch (qs) {
+    case 0: return go<ST, 0>(jp, jobs, njobs, parity, s);
+    case 5: return go<ST, 5>(jp, jobs, njobs, parity, s);
+    case 9: return go<ST, 9>(jp, jobs, njobs, parity, s);
+  }
+  return IPCU_ERR_UNSUPPORTED;
+}
+
+int dispatch(const Job *jp, const Job *jobs, int njobs, int parity, int storage, int qs, cudaStream_t s) {
+  switch (storage) {
+    case IPCU_STORE_F32: return go_q<float>(jp, jobs, njobs, parity, qs, s);
+    case IPCU_STORE_F16: return go_q<__half>(jp, jobs, njobs, parity, qs, s);
+    case IPCU_STORE_BF16: return go_q<__nv_bfloat16>(jp, jobs, njobs, parity, qs, s);
+  }
+  return IPCU_ERR_UNSUPPORTED;
+}
+
+}  // namespace
+
+size_t smem_bytes() { return Layout::BYTES; }
+
+int prepare() {
+  int st = prep_q<float>();
+  if (!st) st = prep_q<__half>();
+  if (!st) st = prep_q<__nv_bfloat16>();
+  return st;
+}
+
+int launch(const Job &j, int parity, int storage, int qs, cudaStream_t s) {
+  return dispatch(&j, nullptr, 1, parity, storage, qs, s);
+}
+
+int launch_batched(const Job *jobs, int njobs, int parity, int storage, int qs, cudaStream_t s) {
+  if (njobs <= 0) return IPCU_OK;
+  return dispatch(nullptr, jobs, njobs, parity, storage, qs, s);
+}
+
+}  // namespace ib2d
+}  // namespace ipcu

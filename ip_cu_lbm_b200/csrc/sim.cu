@@ -14,6 +14,7 @@
 #include <cudaTypedefs.h>
 
 #include "fused2d.cuh"
+#include "ibm2d.cuh"
 #include "ipcu_common.cuh"
 #include "storage.cuh"
 
@@ -41,6 +42,9 @@ struct ipcu_sim {
   std::vector<double> X, Z, DX, DZ;
   std::vector<double> M, Minv, Srates;  // MRT matrices as given (for snapshots)
   long long steps = 0;                  // time steps taken since creation / restore
+  // moving immersed boundary (null without a body): device state and the
+  // coupled update's parameters (fp filled per launch)
+  ib2d::Job *ib = nullptr;
 };
 
 // Macroscopic planes: S, u_x, u_z (+ p* with 16-bit storage)
@@ -323,6 +327,15 @@ void free_sim(ipcu_sim *s) {
   fr(s->obuf[1]);
   fr(s->ilx2);
   fr(s->ilz2);
+  if (s->ib) {
+    fr(s->ib->body);
+    fr((void *)s->ib->X0);
+    fr((void *)s->ib->dS);
+    fr(s->ib->org);
+    fr(s->ib->fext);
+    fr(s->ib->flag);
+    delete s->ib;
+  }
   if (s->ready) cudaEventDestroy(s->ready);
   delete s;
 }
@@ -584,6 +597,11 @@ static int launch_one(ipcu_sim *s) {
   f2d::Params P = s->P;
   P.cur = s->cur;
   int st = f2d::launch_step(P, s->cfg.storage, s->cfg.q_scalar, s->cfg.geometry, s->stream);
+  if (st == IPCU_OK && s->ib) {
+    ib2d::Job j = *s->ib;
+    j.fp = P;
+    st = ib2d::launch(j, 0, s->cfg.storage, s->cfg.q_scalar, s->stream);
+  }
   if (st == IPCU_OK) {
     s->cur ^= 1;
     s->steps++;
@@ -645,6 +663,93 @@ extern "C" int ipcu_sim_step_graph(ipcu_sim *sim, int64_t nsteps, int32_t chunk)
 }
 
 extern "C" int64_t ipcu_sim_cells(const ipcu_sim *sim) { return sim ? sim->N : 0; }
+
+// ---------------------------------------------------------------------------
+// Moving immersed boundary: one rigid body per simulation (ibm2d.cu).
+extern "C" int ipcu_sim_ib_attach(ipcu_sim *s, const ipcu_ib_body2d *bd, const double *markers, const double *dS,
+                                  int32_t n) {
+  if (!s || !bd || !markers || !dS || n <= 0 || s->ib) return IPCU_ERR_ARG;
+  if (n > ib2d::kMaxMarkers) return IPCU_ERR_CAPACITY;
+  if (s->cfg.geometry != IPCU_GEO_UNIFORM || s->cfg.scalar_kind == IPCU_SCALAR_PHASE) return IPCU_ERR_UNSUPPORTED;
+  if (!(bd->rho_s > 0 && bd->rho_f > 0 && bd->area > 0 && bd->inertia > 0 && bd->semi_a > 0 && bd->semi_b > 0 &&
+        bd->iters >= 0 && bd->iters <= 64))
+    return IPCU_ERR_ARG;
+  for (int i = 0; i < n; i++)
+    if (!(dS[i] > 0) || !std::isfinite(markers[2 * i]) || !std::isfinite(markers[2 * i + 1])) return IPCU_ERR_ARG;
+  {
+    static bool prepared[64] = {false};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return IPCU_ERR_CUDA;
+    if (!prepared[dev]) {
+      const int st = ib2d::prepare();
+      if (st) return st;
+      prepared[dev] = true;
+    }
+  }
+  // recorded graphs hold the parameters without the body: drop them
+  if (cudaStreamSynchronize(s->stream) != cudaSuccess) return IPCU_ERR_CUDA;
+  for (int i = 0; i < 2; i++)
+    if (s->graph[i]) {
+      cudaGraphExecDestroy(s->graph[i]);
+      s->graph[i] = nullptr;
+    }
+  s->graph_chunk = 0;
+  ib2d::Job *j = new ib2d::Job();
+  std::memset(j, 0, sizeof *j);
+  const long long N = s->N;
+  const int tx = (s->nx + f2d::kTX - 1) / f2d::kTX, tz = (s->nz + f2d::kTZ - 1) / f2d::kTZ;
+  ib2d::Body b0;
+  std::memset(&b0, 0, sizeof b0);
+  b0.X[0] = bd->xc;
+  b0.X[1] = bd->zc;
+  b0.U[0] = bd->u;
+  b0.U[1] = bd->w;
+  b0.th = bd->theta;
+  b0.om = bd->omega;
+  std::vector<double> X0(markers, markers + 2 * n), dSv(dS, dS + n);
+  bool ok = salloc(s, &j->body, sizeof(ib2d::Body)) && salloc(s, &j->org, sizeof(int) * 2 * n) &&
+            salloc(s, &j->fext, sizeof(float) * 2 * N) && salloc(s, &j->flag, (size_t)tx * tz);
+  double *dX0 = nullptr, *ddS = nullptr;
+  ok = ok && salloc(s, &dX0, sizeof(double) * 2 * n) && salloc(s, &ddS, sizeof(double) * n);
+  j->X0 = dX0;
+  j->dS = ddS;
+  s->ib = j;  // freed with the simulation from here on
+  if (!ok) return IPCU_ERR_NOMEM;
+  cudaError_t e = cudaMemcpyAsync(j->body, &b0, sizeof b0, cudaMemcpyHostToDevice, s->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(dX0, X0.data(), sizeof(double) * 2 * n, cudaMemcpyHostToDevice, s->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(ddS, dSv.data(), sizeof(double) * n, cudaMemcpyHostToDevice, s->stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(j->org, 0, sizeof(int) * 2 * n, s->stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(j->fext, 0, sizeof(float) * 2 * N, s->stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(j->flag, 0, (size_t)tx * tz, s->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+  if (e != cudaSuccess) return IPCU_ERR_CUDA;
+  j->nl = n;
+  j->iters = bd->iters;
+  j->m = bd->rho_s * bd->area;
+  j->I = bd->rho_s * bd->inertia;
+  j->rho_s = bd->rho_s;
+  j->rho_f = bd->rho_f;
+  j->grav = bd->gravity;
+  j->semi_a = bd->semi_a;
+  j->semi_b = bd->semi_b;
+  j->dz = s->cfg.dz;
+  j->dt = s->cfg.dt;
+  s->P.fext = j->fext;
+  s->P.ibflag = j->flag;
+  s->P.ibtx = tx;
+  return IPCU_OK;
+}
+
+extern "C" int ipcu_sim_ib_body(ipcu_sim *s, double *out) {
+  if (!s || !out || !s->ib) return IPCU_ERR_ARG;
+  ib2d::Body b;
+  if (cudaStreamSynchronize(s->stream) != cudaSuccess ||
+      cudaMemcpy(&b, s->ib->body, sizeof b, cudaMemcpyDeviceToHost) != cudaSuccess)
+    return IPCU_ERR_CUDA;
+  const double v[9] = {b.X[0], b.X[1], b.U[0], b.U[1], b.th, b.om, b.Fib[0], b.Fib[1], b.Tib};
+  std::memcpy(out, v, sizeof v);
+  return IPCU_OK;
+}
 
 extern "C" int64_t ipcu_sim_bytes_per_cell(const ipcu_sim *sim) {
   if (!sim) return 0;
@@ -781,6 +886,17 @@ extern "C" int ipcu_sim_get(ipcu_sim *s, const char *field, double *out, int64_t
   const long long N = s->N;
   const int q = s->cfg.q_scalar;
   const std::string fd(field);
+  if (fd == "ibfx" || fd == "ibfz") {  // immersed-boundary force density
+    if (!s->ib) return IPCU_ERR_ARG;
+    if (n < N) return IPCU_ERR_CAPACITY;
+    std::vector<float> m(N);
+    if (cudaStreamSynchronize(s->stream) != cudaSuccess ||
+        cudaMemcpy(m.data(), s->ib->fext + (fd == "ibfz" ? N : 0), sizeof(float) * N, cudaMemcpyDeviceToHost) !=
+            cudaSuccess)
+      return IPCU_ERR_CUDA;
+    for (long long i = 0; i < N; i++) out[i] = m[i];
+    return IPCU_OK;
+  }
   const long long need = fd == "f" ? 9 * N : (fd == "g" ? (long long)q * N : N);
   if (fd == "g" && !q) return IPCU_ERR_ARG;
   const int slot = fd == "S" ? 0 : (fd == "ux" ? 1 : (fd == "uz" ? 2 : (fd == "rho" ? 0 : (fd == "p" ? 3 : -1))));
@@ -940,6 +1056,7 @@ extern "C" int64_t ipcu_sim_steps(const ipcu_sim *s) { return s ? s->steps : -1;
 
 extern "C" int ipcu_sim_save(ipcu_sim *s, const char *path) {
   if (!s || !path) return IPCU_ERR_ARG;
+  if (s->ib) return IPCU_ERR_UNSUPPORTED;  // the snapshot format holds no body
   if (cudaStreamSynchronize(s->stream) != cudaSuccess) return IPCU_ERR_CUDA;
   const long long N = s->N;
   const int q = s->cfg.q_scalar;
@@ -1070,7 +1187,8 @@ struct ipcu_batch {
   int next_mark = 0;
   f2d::Params *d_params = nullptr;
   f2d::WorkItem *d_work = nullptr;
-  size_t cap_params = 0, cap_work = 0;
+  ib2d::Job *d_jobs = nullptr;  // coupled bodies of the listed simulations
+  size_t cap_params = 0, cap_work = 0, cap_jobs = 0;
   int grid_cap = 0;
 };
 
@@ -1097,6 +1215,7 @@ extern "C" void ipcu_batch_destroy(ipcu_batch *b) {
   cudaStreamSynchronize(b->stream);
   cudaFree(b->d_params);
   cudaFree(b->d_work);
+  cudaFree(b->d_jobs);
   if (b->done) cudaEventDestroy(b->done);
   for (int i = 0; i < 4; i++)
     if (b->mark[i]) cudaEventDestroy(b->mark[i]);
@@ -1126,7 +1245,8 @@ static int batch_enqueue(ipcu_batch *b, ipcu_sim *const *sims, int n, int64_t ns
   });
   std::vector<f2d::Params> hp(n);
   std::vector<f2d::WorkItem> hw;
-  struct Group { int storage, qs, geo, pf, w0, w1; };
+  std::vector<ib2d::Job> hj;
+  struct Group { int storage, qs, geo, pf, w0, w1, j0, j1; };
   std::vector<Group> groups;
   for (int oi = 0; oi < n; oi++) {
     ipcu_sim *s = sims[order[oi]];
@@ -1135,11 +1255,17 @@ static int batch_enqueue(ipcu_batch *b, ipcu_sim *const *sims, int n, int64_t ns
     const ipcu_sim_config &c = s->cfg;
     if (groups.empty() || groups.back().storage != c.storage || groups.back().qs != c.q_scalar ||
         groups.back().geo != c.geometry || groups.back().pf != c.scalar_kind)
-      groups.push_back({c.storage, c.q_scalar, c.geometry, c.scalar_kind, (int)hw.size(), (int)hw.size()});
+      groups.push_back({c.storage, c.q_scalar, c.geometry, c.scalar_kind, (int)hw.size(), (int)hw.size(),
+                        (int)hj.size(), (int)hj.size()});
     const int tx = (s->nx + f2d::kTX - 1) / f2d::kTX, tz = (s->nz + f2d::kTZ - 1) / f2d::kTZ;
     for (int z = 0; z < tz; z++)
       for (int x = 0; x < tx; x++) hw.push_back({oi, x, z, 0});
     groups.back().w1 = (int)hw.size();
+    if (s->ib) {
+      hj.push_back(*s->ib);
+      hj.back().fp = hp[oi];
+      groups.back().j1 = (int)hj.size();
+    }
   }
   if (hp.size() > b->cap_params) {
     cudaFree(b->d_params);
@@ -1151,7 +1277,15 @@ static int batch_enqueue(ipcu_batch *b, ipcu_sim *const *sims, int n, int64_t ns
     if (cudaMalloc((void **)&b->d_work, sizeof(f2d::WorkItem) * hw.size()) != cudaSuccess) return IPCU_ERR_NOMEM;
     b->cap_work = hw.size();
   }
-  if (cudaMemcpyAsync(b->d_params, hp.data(), sizeof(f2d::Params) * hp.size(), cudaMemcpyHostToDevice, b->stream) !=
+  if (hj.size() > b->cap_jobs) {
+    cudaFree(b->d_jobs);
+    if (cudaMalloc((void **)&b->d_jobs, sizeof(ib2d::Job) * hj.size()) != cudaSuccess) return IPCU_ERR_NOMEM;
+    b->cap_jobs = hj.size();
+  }
+  if ((!hj.empty() &&
+       cudaMemcpyAsync(b->d_jobs, hj.data(), sizeof(ib2d::Job) * hj.size(), cudaMemcpyHostToDevice, b->stream) !=
+           cudaSuccess) ||
+      cudaMemcpyAsync(b->d_params, hp.data(), sizeof(f2d::Params) * hp.size(), cudaMemcpyHostToDevice, b->stream) !=
           cudaSuccess ||
       cudaMemcpyAsync(b->d_work, hw.data(), sizeof(f2d::WorkItem) * hw.size(), cudaMemcpyHostToDevice, b->stream) !=
           cudaSuccess)
@@ -1166,6 +1300,8 @@ static int batch_enqueue(ipcu_batch *b, ipcu_sim *const *sims, int n, int64_t ns
       const int grid = std::min(nw, b->grid_cap);
       int st = f2d::launch_batched(b->d_params, b->d_work + g.w0, nw, (int)(k & 1), g.storage, g.qs, g.geo, g.pf, grid,
                                    b->stream, false);
+      if (!st && g.j1 > g.j0)
+        st = ib2d::launch_batched(b->d_jobs + g.j0, g.j1 - g.j0, (int)(k & 1), g.storage, g.qs, b->stream);
       if (st) return st;
     }
   }

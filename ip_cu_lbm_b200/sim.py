@@ -6,7 +6,7 @@ import ctypes
 import numpy as np
 
 from . import _lib
-from .cases import d2q9_mrt
+from .cases import d2q9_mrt, ellipse_markers
 
 GEOMETRY = {"uniform": 0, "x5": 1, "x3": 2, "z5": 3, "z3": 4}
 STORAGE = {"f32": 0, "f16": 1, "bf16": 2}
@@ -85,6 +85,28 @@ class Sim:
 
     def step_graph(self, n, chunk=64):
         _lib.check(_lib.lib().ipcu_sim_step_graph(self._h, int(n), int(chunk)), "ipcu_sim_step_graph")
+
+    # ---------------------------------------------------------------- immersed body
+    def attach_ellipse(self, xc, zc, a, b, *, markers=240, theta=0.0, rho_s=1.1, rho_f=1.0, gravity=0.0,
+                       iters=3, u=0.0, w=0.0, omega=0.0):
+        """Attaches a rigid ellipse (semi-axes a along the body x axis, b along
+        its z axis, physical units) with `markers` markers at equal arc length;
+        it settles under gravity by multi-direct forcing (ipcu_sim_ib_attach)."""
+        X0, dS = ellipse_markers(a, b, markers)
+        body = _lib.IBBody2D(xc=xc, zc=zc, theta=theta, u=u, w=w, omega=omega, rho_s=rho_s, rho_f=rho_f,
+                             area=np.pi * a * b, inertia=np.pi * a * b * (a * a + b * b) / 4, semi_a=a, semi_b=b,
+                             gravity=gravity, iters=iters, pad=0)
+        X0 = np.ascontiguousarray(X0, dtype=np.float64)
+        dS = np.ascontiguousarray(dS, dtype=np.float64)
+        _lib.check(_lib.lib().ipcu_sim_ib_attach(self._h, ctypes.byref(body), X0.ctypes.data, dS.ctypes.data,
+                                                 len(dS)), "ipcu_sim_ib_attach")
+
+    def body(self):
+        """Body state: dict of x, z, u, w, theta, omega, Fx, Fz, T (the IB
+        force and torque on the fluid in the last step)."""
+        out = np.zeros(9)
+        _lib.check(_lib.lib().ipcu_sim_ib_body(self._h, out.ctypes.data), "ipcu_sim_ib_body")
+        return dict(zip(("x", "z", "u", "w", "theta", "omega", "Fx", "Fz", "T"), out.tolist()))
 
     # ---------------------------------------------------------------- fields
     def get(self, field):

@@ -130,6 +130,7 @@ class Box:
         self.ux = np.zeros((nz, nx))
         self.uz = np.zeros((nz, nx))
         self.old = np.zeros((2, nz, nx))  # phase field: phi u, phi w of the previous step
+        self.fext = np.zeros((2, nz, nx))  # external force density (immersed boundary), added to F
 
     # ------------------------------------------------------------------ pieces
     def _interp(self, fs, s):
@@ -246,6 +247,8 @@ class Box:
             Fz = Fz + mu * dpz - rho * self.grav
         else:
             Fz = Fz - S * self.g_bouss
+        Fx = Fx + self.fext[0]
+        Fz = Fz + self.fext[1]
         eu = c * (EX9[:, None, None] * u[None] + EZ9[:, None, None] * w[None]) / c2
         us = (u * u + w * w) / c2
         feq = W9[:, None, None] * (p[None] + 3 * eu + 4.5 * eu ** 2 - 1.5 * us[None])
