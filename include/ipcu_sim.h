@@ -164,7 +164,10 @@ int ipcu_batch_wait_mark(ipcu_batch *batch, int mark);
  * reaction of the IB force, buoyancy -(1 - rho_f/rho_s) m gravity along z
  * and the change of the fluid momentum inside the body. No counterpart of
  * the reference's own IB coupling (get_IBMGw2), which stays available
- * through the kernel-entry API above. */
+ * through the kernel-entry API above. The coupling is stable at density
+ * ratios down to about one for bodies at least 4 cells thick (semi-axes
+ * >= 4 dz): a thinner body lies wholly inside its own 4-point stencils and
+ * its interior fluid no longer follows it. */
 typedef struct ipcu_ib_body2d {
   double xc, zc, theta;   /* centre (cell centres at (i + 1/2) dz) and angle */
   double u, w, omega;     /* initial velocity and angular velocity */

@@ -34,8 +34,12 @@ struct alignas(64) Params {
   // interpolated axis: weights [2][NA][NS], fin scale [2][NA], fout scale [NA],
   // and the interior cells' combined flux weights [2][NS+1][NA]
   const float *wA, *scin, *scout, *wC;
-  // 1/(x_{i+1} - x_{i-1} + dz/1000) with clamped neighbours (density gradient)
+  // 1/(x_{i+1} - x_{i-1} + dz/1000) with clamped neighbours (density gradient);
+  // gconst bit 0 (x) / bit 1 (z): the table is first, mid..., last, given
+  // in gix3 / giz3, so the kernel needs no load for it
   const float *ginvx, *ginvz;
+  float gix3[3], giz3[3];
+  int gconst;
   float c, dt, tau, taus;
   float fk3, hdt;  // 3 dt / c (forcing term per unit density) and dt / 2
   // rho = rho_base + rho_sal_f * S: salinity (base rhoL + (rhoH - rhoL) phi)

@@ -332,7 +332,10 @@ __device__ __forceinline__ void step_tile(const Params &p, int parity, int tile_
     // force: buoyancy (salinity) or surface tension + weight (phase field),
     // plus the pressure gradient on the density (ref: collision.cu:57-112)
     const float pc = pr * c2 / 3.0f;
-    const float gix = __ldg(p.ginvx + gx), giz = __ldg(p.ginvz + gz);
+    const float gix = (p.gconst & 1) ? (gx == 0 ? p.gix3[0] : (gx == nx - 1 ? p.gix3[2] : p.gix3[1]))
+                                     : __ldg(p.ginvx + gx);
+    const float giz = (p.gconst & 2) ? (gz == 0 ? p.giz3[0] : (gz == nz - 1 ? p.giz3[2] : p.giz3[1]))
+                                     : __ldg(p.ginvz + gz);
     float Fx = -pc * ((rho_of(sS[rs + 1]) - rho_of(sS[rs - 1])) * gix);
     float Fz = -pc * ((rho_of(sS[rs + RX]) - rho_of(sS[rs - RX])) * giz);
     float dpx = 0.f, dpz = 0.f;  // grad(phi) (phase field)

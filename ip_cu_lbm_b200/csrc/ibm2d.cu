@@ -12,14 +12,19 @@
 //      is taken out of u there and f_ib restarts at zero;
 //   3. multi-direct forcing, `iters` times: U*_l = sum phi u (16 lanes per
 //      marker, shuffle reduction), dF_l = 2 rho_f (U_b,l - U*_l) / dt,
-//      spread df = dF_l phi dS_l / dz^2 onto f_ib and df dt / 2 rho onto u
-//      (shared-memory atomics), F_l += dF_l;
+//      spread df = dF_l phi dS_l / dz^2 onto f_ib and df dt / 2 rho onto u,
+//      F_l += dF_l; each slot gathers its (marker, cell) pairs from a list
+//      sorted by pair index, so every sum runs in a fixed order and a
+//      body's update is the same whatever runs beside it;
 //   4. u and f_ib go back to HBM (16-bit storage re-expresses the stored
 //      deviations about the new u, so the populations stay as they were),
 //      and the tile flags the fluid kernel reads follow the footprint;
 //   5. FP64 sums: F_ib = sum F_l dS_l, T_ib = sum r_l x F_l dS_l and the
-//      fluid momentum P, angular momentum L of the cells whose centre lies
-//      inside the body (ellipse);
+//      fluid momentum P, angular momentum L inside the body, each cell
+//      weighted by its volume fraction alpha = clamp(1/2 - d/dz, 0, 1), d the
+//      signed distance of its centre from the ellipse (first-order estimate
+//      F/|grad F| of F = (x/a)^2 + (z/b)^2 - 1 in the body frame; a binary
+//      inside test would kick the body whenever a centre crosses the outline);
 //   6. one thread steps the body in FP64 (update_IBbody's force, torque and
 //      buoyancy (1 - rho_f/rho_s) m g, ref: function/ibm.cu:367-424): the
 //      body takes the reaction of the mean of this step's and the previous
@@ -71,7 +76,10 @@ struct Layout {
   static constexpr size_t SFX = SW + 4 * kMaxSlots;                  // float [slots] f_ib x
   static constexpr size_t SFZ = SFX + 4 * kMaxSlots;                 // float [slots] f_ib z
   static constexpr size_t SH = SFZ + 4 * kMaxSlots;                  // float [slots] dt / 2 rho
-  static constexpr size_t MAP = SH + 4 * kMaxSlots;                  // short [window] slot of a window cell
+  static constexpr size_t OFF = SH + 4 * kMaxSlots;                  // int [slots + 1] first pair of a slot
+  static constexpr size_t CUR = OFF + 4 * (kMaxSlots + 1);           // int [slots] count, then write cursor
+  static constexpr size_t LIST = CUR + 4 * kMaxSlots;                // short [16 nl] pairs l*16+q by slot
+  static constexpr size_t MAP = LIST + 2 * 16 * kMaxMarkers;         // short [window] slot of a window cell
   static constexpr size_t RED = (MAP + 2 * kMaxWindow + 15) / 16 * 16;  // double [kWarps][6]
   static constexpr size_t BYTES = RED + 8 * 6 * kWarps;
 };
@@ -93,6 +101,9 @@ __device__ void coupled_update(const Job &j, int parity) {
   float *sFX = reinterpret_cast<float *>(sm + Layout::SFX);
   float *sFZ = reinterpret_cast<float *>(sm + Layout::SFZ);
   float *sH = reinterpret_cast<float *>(sm + Layout::SH);
+  int *sOff = reinterpret_cast<int *>(sm + Layout::OFF);
+  int *sCur = reinterpret_cast<int *>(sm + Layout::CUR);
+  short *sList = reinterpret_cast<short *>(sm + Layout::LIST);
   short *sMap = reinterpret_cast<short *>(sm + Layout::MAP);
   double *sRed = reinterpret_cast<double *>(sm + Layout::RED);
   __shared__ Body B;
@@ -194,16 +205,84 @@ __device__ void coupled_update(const Job &j, int parity) {
     sU[s] = mac[N + ci] - j.fext[ci] * h;
     sW[s] = mac[2 * N + ci] - j.fext[N + ci] * h;
     sFX[s] = sFZ[s] = 0.f;
+    sCur[s] = 0;
+  }
+  __syncthreads();
+
+  // ---- pairs of the new stencils listed by slot, in pair order
+  auto slot_at = [&](int l, int qq) -> int {
+    const int i = sI0[l] + (qq & 3), k = sK0[l] + (qq >> 2);
+    if (i < 0 || i >= nx || k < 0 || k >= nz) return -1;
+    return sMap[(k - wk0) * WW + (i - wi0)];
+  };
+  for (int e = tid; e < 16 * nl; e += kThreads) {
+    const int s = slot_at(e >> 4, e & 15);
+    if (s >= 0) atomicAdd(&sCur[s], 1);
+  }
+  __syncthreads();
+  {
+    // exclusive scan of the counts: kPer consecutive slots per thread, then
+    // across lanes and warps
+    constexpr int kPer = (kMaxSlots + kThreads - 1) / kThreads;
+    int *wtot = reinterpret_cast<int *>(sRed);
+    int loc[kPer], sum = 0;
+#pragma unroll
+    for (int i = 0; i < kPer; i++) {
+      const int s = tid * kPer + i;
+      loc[i] = sum;
+      sum += s < ns ? sCur[s] : 0;
+    }
+    int x = sum;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += y;
+    }
+    if (lane == 31) wtot[warp] = x;
+    __syncthreads();
+    if (tid == 0) {
+      int run = 0;
+      for (int w = 0; w < kWarps; w++) {
+        const int t = wtot[w];
+        wtot[w] = run;
+        run += t;
+      }
+      sOff[ns] = run;
+    }
+    __syncthreads();
+    const int base = wtot[warp] + x - sum;
+    __syncthreads();  // every warp has read wtot before sRed is reused
+#pragma unroll
+    for (int i = 0; i < kPer; i++) {
+      const int s = tid * kPer + i;
+      if (s < ns) sOff[s] = base + loc[i];
+    }
+  }
+  __syncthreads();
+  for (int s = tid; s < ns; s += kThreads) sCur[s] = sOff[s];
+  __syncthreads();
+  for (int e = tid; e < 16 * nl; e += kThreads) {
+    const int s = slot_at(e >> 4, e & 15);
+    if (s >= 0) sList[atomicAdd(&sCur[s], 1)] = (short)e;
+  }
+  __syncthreads();
+  for (int s = tid; s < ns; s += kThreads) {  // insertion sort of each slot's short list
+    const int a0 = sOff[s], a1 = sOff[s + 1];
+    for (int a = a0 + 1; a < a1; a++) {
+      const short v = sList[a];
+      int b2 = a - 1;
+      while (b2 >= a0 && sList[b2] > v) {
+        sList[b2 + 1] = sList[b2];
+        b2--;
+      }
+      sList[b2 + 1] = v;
+    }
   }
   __syncthreads();
 
   // ---- 3. multi-direct forcing
   const int g = tid >> 4, q = tid & 15, qa = q & 3, qc = q >> 2;
-  auto slot_of = [&](int l) -> int {
-    const int i = sI0[l] + qa, k = sK0[l] + qc;
-    if (i < 0 || i >= nx || k < 0 || k >= nz) return -1;
-    return sMap[(k - wk0) * WW + (i - wi0)];
-  };
+  auto slot_of = [&](int l) -> int { return slot_at(l, q); };
   const float two_rf_dt = (float)(2.0 * j.rho_f / j.dt);
   for (int it = 0; it < j.iters; it++) {
     for (int lb = 0; lb < nl; lb += kGroups) {
@@ -231,17 +310,18 @@ __device__ void coupled_update(const Job &j, int parity) {
       }
     }
     __syncthreads();
-    for (int lb = 0; lb < nl; lb += kGroups) {
-      const int l = lb + g;
-      if (l >= nl) continue;
-      const int s = slot_of(l);
-      if (s < 0) continue;
-      const float wd = sWX[4 * l + qa] * sWZ[4 * l + qc] * sDS[l];
-      const float fx = sDF[2 * l] * wd, fz = sDF[2 * l + 1] * wd;
-      atomicAdd(&sFX[s], fx);
-      atomicAdd(&sFZ[s], fz);
-      atomicAdd(&sU[s], fx * sH[s]);
-      atomicAdd(&sW[s], fz * sH[s]);
+    for (int s = tid; s < ns; s += kThreads) {
+      float fx = 0.f, fz = 0.f;
+      for (int a = sOff[s]; a < sOff[s + 1]; a++) {
+        const int e = sList[a], l = e >> 4, qq = e & 15;
+        const float wd = sWX[4 * l + (qq & 3)] * sWZ[4 * l + (qq >> 2)] * sDS[l];
+        fx = fmaf(sDF[2 * l], wd, fx);
+        fz = fmaf(sDF[2 * l + 1], wd, fz);
+      }
+      sFX[s] += fx;
+      sFZ[s] += fz;
+      sU[s] = fmaf(fx, sH[s], sU[s]);
+      sW[s] = fmaf(fz, sH[s], sW[s]);
     }
     __syncthreads();
   }
@@ -320,7 +400,9 @@ __device__ void coupled_update(const Job &j, int parity) {
   }
   {
     const double a = j.semi_a, bb = j.semi_b;
-    const double hx = sqrt(a * a * cth * cth + bb * bb * sth * sth), hz = sqrt(a * a * sth * sth + bb * bb * cth * cth);
+    // half extents of the ellipse, widened by one cell for the fraction ramp
+    const double hx = sqrt(a * a * cth * cth + bb * bb * sth * sth) + dz;
+    const double hz = sqrt(a * a * sth * sth + bb * bb * cth * cth) + dz;
     const int ia = max((int)ceil((B.X[0] - hx) * idz - 0.5), 0), ib = min((int)floor((B.X[0] + hx) * idz - 0.5), nx - 1);
     const int ka = max((int)ceil((B.X[1] - hz) * idz - 0.5), 0), kb = min((int)floor((B.X[1] + hz) * idz - 0.5), nz - 1);
     const int bw = ib - ia + 1, bh = kb - ka + 1;
@@ -330,12 +412,15 @@ __device__ void coupled_update(const Job &j, int parity) {
         const int i = ia + e % bw, k = ka + e / bw;
         const double dx = (i + 0.5) * dz - B.X[0], dzz = (k + 0.5) * dz - B.X[1];
         const double xb = cth * dx + sth * dzz, zb = -sth * dx + cth * dzz;
-        if ((xb / a) * (xb / a) + (zb / bb) * (zb / bb) < 1.0) {
+        const double F = (xb / a) * (xb / a) + (zb / bb) * (zb / bb) - 1.0;
+        const double G = 2.0 * hypot(xb / (a * a), zb / (bb * bb));
+        const double al = fmin(fmax(0.5 - F / fmax(G, 1e-300) * idz, 0.0), 1.0) * dA;
+        if (al > 0.0) {
           const long long ci = (long long)k * nx + i;
           const double ux = mac[N + ci], uz = mac[2 * N + ci];
-          acc[3] += ux * dA;
-          acc[4] += uz * dA;
-          acc[5] += (dx * uz - dzz * ux) * dA;
+          acc[3] += al * ux;
+          acc[4] += al * uz;
+          acc[5] += al * (dx * uz - dzz * ux);
         }
       }
     }

@@ -462,6 +462,21 @@ extern "C" int ipcu_sim_create(const ipcu_sim_config *cfg, const double *s0, ipc
   P.wC = s->wC;
   P.ginvx = s->ginvx;
   P.ginvz = s->ginvz;
+  {
+    // tables of an evenly spaced axis hold three values: first, interior, last
+    auto three = [](const std::vector<float> &t, float *o) {
+      const size_t n = t.size();
+      if (n < 3) return false;
+      for (size_t i = 2; i + 1 < n; i++)
+        if (t[i] != t[1]) return false;
+      o[0] = t[0];
+      o[1] = t[1];
+      o[2] = t[n - 1];
+      return true;
+    };
+    const std::vector<float> tx = grad_inv(s->X, dz), tz = grad_inv(s->Z, dz);
+    P.gconst = (three(tx, P.gix3) ? 1 : 0) | (three(tz, P.giz3) ? 2 : 0);
+  }
   P.c = (float)(dz / c.dt);
   P.dt = (float)c.dt;
   P.fk3 = (float)(3.0 * c.dt * c.dt / dz);
@@ -1347,5 +1362,8 @@ extern "C" int64_t ipcu_sim_device_bytes(const ipcu_sim *s) {
   const long long N = s->N;
   return 2 * ((long long)s->esz * (9 + std::max(s->cfg.q_scalar, 1)) * N + 4LL * (nmac(s) + (s->cfg.scalar_kind == IPCU_SCALAR_PHASE ? 2 : 0)) * N) +
          4LL * (3 * (s->nx + s->nz) + 2 * 5 * std::max(s->nx, s->nz)) + 2048 +
-         (s->cfg.scalar_kind == IPCU_SCALAR_PHASE ? 4LL * (s->nx + s->nz) : 0);  // 1/dx^2, 1/dz^2
+         (s->cfg.scalar_kind == IPCU_SCALAR_PHASE ? 4LL * (s->nx + s->nz) : 0) +  // 1/dx^2, 1/dz^2
+         (s->ib ? 8LL * N + ((s->nx + f2d::kTX - 1) / f2d::kTX) * ((s->nz + f2d::kTZ - 1) / f2d::kTZ) +
+                      32LL * s->ib->nl + (long long)sizeof(ib2d::Body)
+                : 0);  // immersed body: force density, tile flags, markers, body state
 }

@@ -83,6 +83,7 @@ class Request:
     steps: int = field(compare=False)
     kwargs: dict = field(default_factory=dict, compare=False)
     s0: np.ndarray = field(default=None, compare=False)
+    body: dict = field(default=None, compare=False)  # Sim.attach_ellipse arguments (immersed body)
     # filled by the server
     sim: Sim = field(default=None, compare=False, repr=False)
     remaining: int = field(default=0, compare=False)
@@ -104,8 +105,11 @@ def request_bytes(req: Request) -> int:
         nmac += 2  # previous step's phi u, phi w
     q = max(req.kwargs.get("q_scalar", 5), 1)
     N = req.cells
+    ib = 0
+    if req.body is not None:  # force density, tile flags, markers, body state
+        ib = 8 * N + ((req.nx + 31) // 32) * ((req.nz + 15) // 16) + 32 * req.body.get("markers", 240) + 104
     return (2 * (esz * (9 + q) * N + 4 * nmac * N) + 4 * (3 * (req.nx + req.nz) + 10 * max(req.nx, req.nz)) + 2048
-            + (4 * (req.nx + req.nz) if pf else 0))
+            + (4 * (req.nx + req.nz) if pf else 0) + ib)
 
 
 class Server:
@@ -135,6 +139,8 @@ class Server:
         while self.waiting and self.in_use + request_bytes(self.waiting[0]) <= self.budget:
             r = heapq.heappop(self.waiting)
             r.sim = Sim(r.nx, r.nz, s0=r.s0, stream=self.stream, **r.kwargs)
+            if r.body is not None:
+                r.sim.attach_ellipse(**r.body)
             r.admitted = now
             self.in_use += r.sim.device_bytes()
             self.active.append(r)
@@ -200,6 +206,8 @@ class Server:
             a = buf.numpy()
             r.result = {k: a[planes[k] * r.cells:(planes[k] + 1) * r.cells].astype(np.float64).reshape(r.nz, r.nx)
                         for k in self.keep}
+            if r.body is not None:
+                r.result["body"] = r.sim.body()
             r.finished = clock()
             self.in_use -= r.sim.device_bytes()
             r.sim.close()
@@ -250,6 +258,28 @@ def lock_exchange_request(rid, nx, nz, steps, arrival=0.0, storage="f16", seed=0
     kw = dict(q_scalar=5, geometry="uniform", storage=storage, wall="bb", mrt=True, tau=0.53, taus=0.503,
               rho_sal=gp, g_bouss=gp)
     return Request(arrival=arrival, rid=rid, nx=nx, nz=nz, steps=steps, kwargs=kw, s0=S0.ravel())
+
+
+def falling_ellipse_request(rid, nx, nz, steps, arrival=0.0, storage="f16", seed=0):
+    """A 2-D settling-ellipse request after the immersed-boundary case,
+    scaled to the grid: semi-axes a = max(nx/40, 8), b = a/2 (20 x 10 on an
+    800-wide box; the coupling needs b >= 4 cells at this density ratio, a
+    body thinner than that lies wholly inside its own Peskin stencils and
+    its interior fluid no longer moves with it), markers at about 2.5 per
+    unit arc length (48..512), density ratio 1.1, tilt 45 degrees, released
+    from rest at (nx/2, 0.85 nz) with a seeded +-2 % jitter; gravity
+    1e-5 (20/a)^2 keeps the settling speed comparable across sizes; D2Q9
+    MRT, nu = 0.02, bounce-back, no scalar, lattice units."""
+    rng = np.random.default_rng(seed)
+    a = max(nx / 40.0, 8.0)
+    b = a / 2.0
+    per = np.pi * (3 * (a + b) - np.sqrt((3 * a + b) * (a + 3 * b)))
+    markers = int(min(max(round(2.5 * per), 48), 512))
+    j = 1.0 + rng.uniform(-0.02, 0.02, 2)
+    kw = dict(q_scalar=0, geometry="uniform", storage=storage, wall="bb", mrt=True, tau=0.56)
+    body = dict(xc=nx / 2 * j[0], zc=0.85 * nz * j[1], a=a, b=b, markers=markers, theta=np.pi / 4, rho_s=1.1,
+                rho_f=1.0, gravity=1e-5 * (20.0 / a) ** 2, iters=3)
+    return Request(arrival=arrival, rid=rid, nx=nx, nz=nz, steps=steps, kwargs=kw, s0=np.zeros(nx * nz), body=body)
 
 
 def rayleigh_taylor_request(rid, nx, nz, steps, arrival=0.0, storage="f16", seed=0):

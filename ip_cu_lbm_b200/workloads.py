@@ -73,3 +73,37 @@ def lock_exchange_uniform(nx=512, nz=64, seed=20261203):
                   tau=3 * nu + 0.5, taus=3 * kappa + 0.5, rhoL=1.0, rhoH=1.0, phi=1.0, rho_sal=1e-4, g_bouss=1e-4,
                   s_ref=0.5)
     return params, S, dict(nx=nx, nz=nz)
+
+
+# gravities of the settling-ellipse sweep (lattice units), intended to span
+# terminal Reynolds numbers 2 a U / nu of about 1 to 30 for the 20 x 10
+# ellipse at nu = 0.02
+ELLIPSE_GRAVITIES = (2.5e-6, 1e-5, 4e-5, 1.6e-4)
+
+
+def settling_ellipse(nx=800, nz=3000, storage="f32", gravity=1e-5, N2=0.0, seed=20261203):
+    """An ellipse settling from rest: 800 x 3000 uniform D2Q9 MRT box,
+    nu = 0.02, bounce-back walls, semi-axes 20 x 10 cells, 240 markers at
+    equal arc length, density ratio 1.1, initial tilt 45 degrees, released at
+    (nx/2, 0.85 nz) with a seeded +-2 % jitter of the release point; with
+    N2 > 0, a linear salinity stratification N^2 = g' dS/dz on D2Q5
+    (kappa = 0.0005). The Boussinesq force -g' S carries the whole
+    hydrostatic load, whose pressure range N^2 nz^2 / 2 must stay well below
+    c_s^2 = 1/3 for the weakly compressible lattice: N^2 = 1e-6 over 3000
+    cells (range 4.5) is beyond it, 1e-8 (0.045) is not. Returns
+    (sim params, S0, body dict, meta)."""
+    rng = np.random.default_rng(seed)
+    nu = 0.02
+    S0 = np.zeros((nz, nx))
+    qs, gp = 0, 0.0
+    if N2 > 0:
+        S0 = 1.0 - (np.arange(nz)[:, None] + 0.5) / nz * np.ones((1, nx))
+        qs, gp = 5, N2 * nz  # N^2 = g' |dS/dz| with dS/dz = 1/nz
+    params = dict(q_scalar=qs, geometry="uniform", storage=storage, wall="bb", mrt=True, dz=1.0, dt=1.0,
+                  tau=3 * nu + 0.5, taus=3 * 0.0005 + 0.5, rhoL=1.0, rhoH=1.0, phi=1.0, rho_sal=1e-3, g_bouss=gp,
+                  s_ref=0.5)
+    j = 1.0 + rng.uniform(-0.02, 0.02, 2)
+    body = dict(xc=nx / 2 * j[0], zc=0.85 * nz * j[1], a=20.0, b=10.0, markers=240, theta=np.pi / 4, rho_s=1.1,
+                rho_f=1.0, gravity=gravity, iters=3)
+    meta = dict(nx=nx, nz=nz, nu=nu, N2=N2)
+    return params, S0, body, meta

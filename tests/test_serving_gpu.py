@@ -6,13 +6,16 @@ import numpy as np
 import pytest
 
 from ip_cu_lbm_b200 import Sim
-from ip_cu_lbm_b200.serving import Batch, Server, lock_exchange_request, rayleigh_taylor_request, request_bytes
+from ip_cu_lbm_b200.serving import (Batch, Server, falling_ellipse_request, lock_exchange_request,
+                                    rayleigh_taylor_request, request_bytes)
 
 pytestmark = pytest.mark.gpu
 
 
 def _alone(req, batched):
     s = Sim(req.nx, req.nz, s0=req.s0, **req.kwargs)
+    if req.body is not None:
+        s.attach_ellipse(**req.body)
     if batched:
         b = Batch()
         b.step([s], req.steps)
@@ -20,6 +23,8 @@ def _alone(req, batched):
     else:
         s.step(req.steps)
     out = {k: s.get(k) for k in ("S", "ux", "uz")}
+    if req.body is not None:
+        out["body"] = s.body()
     s.close()
     return out
 
@@ -76,3 +81,35 @@ def test_budget_limits_admission(cuda):
     stats = srv.run([])
     srv.close()
     assert stats["requests"] == 4
+
+
+@pytest.mark.parametrize("storage", ["f32", "f16"])
+def test_immersed_body_requests_in_the_mix(cuda, storage):
+    """Falling-ellipse requests batched with lock-exchange requests: each
+    body's one-CTA update runs in one launch per step for all bodies, its
+    sums in a fixed order, so every result -- fields and body -- is the
+    request's own result run alone, bit for bit."""
+    reqs = [falling_ellipse_request(0, 192, 576, 150, storage=storage, seed=0),
+            lock_exchange_request(1, 96, 64, 120, storage=storage, seed=1),
+            falling_ellipse_request(2, 224, 672, 90, arrival=0.01, storage=storage, seed=2)]
+    srv = Server(budget_bytes=2e9, tick_steps=40)
+    stats = srv.run(reqs)
+    srv.close()
+    assert stats["requests"] == len(reqs)
+    for r in srv.done:
+        same = _alone(r, batched=True)
+        for k in ("S", "ux", "uz"):
+            assert np.array_equal(r.result[k], same[k]), (r.rid, k)
+        if r.body is not None:
+            assert r.result["body"] == same["body"]
+            assert r.result["body"]["z"] < r.body["zc"]  # the ellipse sinks
+
+
+def test_request_bytes_match_device_bytes(cuda):
+    for r in (lock_exchange_request(0, 96, 64, 10, storage="f16"), rayleigh_taylor_request(1, 64, 96, 10),
+              falling_ellipse_request(2, 192, 576, 10), falling_ellipse_request(3, 256, 768, 10, storage="f32")):
+        s = Sim(r.nx, r.nz, s0=r.s0, **r.kwargs)
+        if r.body is not None:
+            s.attach_ellipse(**r.body)
+        assert s.device_bytes() == request_bytes(r), (r.rid, s.device_bytes(), request_bytes(r))
+        s.close()
