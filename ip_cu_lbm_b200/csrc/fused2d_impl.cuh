@@ -229,8 +229,13 @@ __device__ __forceinline__ void step_tile(const Params &p, int parity, int tile_
   static_assert(PHYS == 0 || QS > 0, "the phase field lives on the scalar lattice");
   const float rho0 = p.rho_base, rsal = p.rho_sal_f;
   auto rho_of = [&](float S) { return fmaf(S, rsal, rho0); };
-  // immersed-boundary force on this tile (block-uniform)
-  const bool ibt = p.fext != nullptr && p.ibflag[tile_z * p.ibtx + tile_x] != 0;
+  // immersed-boundary force on this tile (block-uniform). The body's update
+  // of the previous step may still be running (programmatic dependent
+  // launch): a flagged tile waits for it before it reads anything. The flag
+  // is read past L1 (the update sets it just before it lets this kernel go).
+  const bool ibt = p.fext != nullptr &&
+                   *reinterpret_cast<const volatile uint8_t *>(p.ibflag + tile_z * p.ibtx + tile_x) != 0;
+  if (ibt) asm volatile("griddepcontrol.wait;" ::: "memory");
 
   // ---- phase 0: stage the tile (TMA) or the salinity ring, and the axis weights
   if (tid == 0) *qcount = 0;
@@ -751,6 +756,23 @@ int launch_bg(const Params *ps, const WorkItem *work, int nwork, int parity, int
   return IPCU_ERR_UNSUPPORTED;
 }
 
+// Launch that may begin while the previous kernel on the stream (a body's
+// update) still runs; the kernel orders itself with griddepcontrol.wait.
+template <class K, class... A>
+int launch_pdl(K kernel, dim3 grid, size_t smem, cudaStream_t s, A... args) {
+  cudaLaunchConfig_t cfg = {};
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.gridDim = grid;
+  cfg.blockDim = dim3(kThreads);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  return status_from_cuda(cudaLaunchKernelEx(&cfg, kernel, args...));
+}
+
 template <class ST, int QS, int GEO, bool TMA, int PHYS>
 int launch_t1(const Params &p, cudaStream_t s, bool prepare_only) {
   constexpr size_t sm = smem_bytes<QS, GEO, TMA>();
@@ -759,6 +781,7 @@ int launch_t1(const Params &p, cudaStream_t s, bool prepare_only) {
                                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
   }
   dim3 grid((p.nx + kTX - 1) / kTX, (p.nz + kTZ - 1) / kTZ);
+  if (p.fext) return launch_pdl(step_kernel<ST, QS, GEO, TMA, PHYS>, grid, sm, s, p);
   step_kernel<ST, QS, GEO, TMA, PHYS><<<grid, kThreads, sm, s>>>(p);
   return status_from_cuda(cudaGetLastError());
 }

@@ -17,8 +17,15 @@
 //      sorted by pair index, so every sum runs in a fixed order and a
 //      body's update is the same whatever runs beside it;
 //   4. u and f_ib go back to HBM (16-bit storage re-expresses the stored
-//      deviations about the new u, so the populations stay as they were),
-//      and the tile flags the fluid kernel reads follow the footprint;
+//      deviations about the new u, so the populations stay as they were).
+//      The tile flags the fluid kernel reads follow the footprint: the new
+//      footprint's tiles are flagged before any write, then the kernel lets
+//      the next fluid step launch (programmatic dependent launch): its
+//      flagged tiles wait for this update, the others run beside it. This
+//      update writes the cells of the previous and the new footprints, so
+//      only the tiles of the footprint two steps back that neither covers
+//      are unflagged (the fluid step that may run beside it needs none of
+//      them);
 //   5. FP64 sums: F_ib = sum F_l dS_l, T_ib = sum r_l x F_l dS_l and the
 //      fluid momentum P, angular momentum L inside the body, each cell
 //      weighted by its volume fraction alpha = clamp(1/2 - d/dz, 0, 1), d the
@@ -50,6 +57,7 @@ namespace {
 
 constexpr int kWarps = kThreads / 32;
 constexpr int kGroups = kThreads / 16;  // 16 lanes (one 4x4 stencil) per marker
+constexpr int kTileMap = 1024;          // tiles tracked around the footprints for the flag clean-up
 
 // 4-point Peskin kernel (ref: function/ibm.cu:61-66), r in lattice spacings
 __device__ __forceinline__ float peskin4(float r) {
@@ -79,7 +87,8 @@ struct Layout {
   static constexpr size_t OFF = SH + 4 * kMaxSlots;                  // int [slots + 1] first pair of a slot
   static constexpr size_t CUR = OFF + 4 * (kMaxSlots + 1);           // int [slots] count, then write cursor
   static constexpr size_t LIST = CUR + 4 * kMaxSlots;                // short [16 nl] pairs l*16+q by slot
-  static constexpr size_t MAP = LIST + 2 * 16 * kMaxMarkers;         // short [window] slot of a window cell
+  static constexpr size_t PS = LIST + 2 * 16 * kMaxMarkers;          // short [16 nl] slot of each pair (-1 outside)
+  static constexpr size_t MAP = PS + 2 * 16 * kMaxMarkers;           // short [window] slot of a window cell
   static constexpr size_t RED = (MAP + 2 * kMaxWindow + 15) / 16 * 16;  // double [kWarps][6]
   static constexpr size_t BYTES = RED + 8 * 6 * kWarps;
 };
@@ -104,10 +113,13 @@ __device__ void coupled_update(const Job &j, int parity) {
   int *sOff = reinterpret_cast<int *>(sm + Layout::OFF);
   int *sCur = reinterpret_cast<int *>(sm + Layout::CUR);
   short *sList = reinterpret_cast<short *>(sm + Layout::LIST);
+  short *sPS = reinterpret_cast<short *>(sm + Layout::PS);
   short *sMap = reinterpret_cast<short *>(sm + Layout::MAP);
   double *sRed = reinterpret_cast<double *>(sm + Layout::RED);
   __shared__ Body B;
-  __shared__ int bnd[4];  // window bounds imin, imax, kmin, kmax
+  __shared__ int bnd[4];   // window bounds imin, imax, kmin, kmax
+  __shared__ int bnd2[4];  // bounds of the footprint two steps back
+  __shared__ uint8_t tmap[kTileMap];  // tiles of the previous and new footprints
   __shared__ int nslot, fail;
 
   const f2d::Params &p = j.fp;
@@ -120,8 +132,8 @@ __device__ void coupled_update(const Job &j, int parity) {
 
   if (tid == 0) {
     B = *j.body;
-    bnd[0] = bnd[2] = INT_MAX;
-    bnd[1] = bnd[3] = INT_MIN;
+    bnd[0] = bnd[2] = bnd2[0] = bnd2[2] = INT_MAX;
+    bnd[1] = bnd[3] = bnd2[1] = bnd2[3] = INT_MIN;
     nslot = 0;
     fail = nl > kMaxMarkers ? 1 : 0;
   }
@@ -155,6 +167,13 @@ __device__ void coupled_update(const Job &j, int parity) {
     atomicMax(&bnd[1], i0 + 3);
     atomicMin(&bnd[2], k0);
     atomicMax(&bnd[3], k0 + 3);
+    if (B.have_prev2) {
+      const int oi = j.org2[2 * l], ok = j.org2[2 * l + 1];
+      atomicMin(&bnd2[0], oi);
+      atomicMax(&bnd2[1], oi + 3);
+      atomicMin(&bnd2[2], ok);
+      atomicMax(&bnd2[3], ok + 3);
+    }
     if (have_prev) {
       const int oi = j.org[2 * l], ok = j.org[2 * l + 1];
       atomicMin(&bnd[0], oi);
@@ -174,12 +193,15 @@ __device__ void coupled_update(const Job &j, int parity) {
   // ---- 2. slots for the cells of the old and new stencils inside the box
   for (int e = tid; e < nwin; e += kThreads) sMap[e] = -1;
   __syncthreads();
-  for (int e = tid; e < 16 * nl * (have_prev ? 2 : 1); e += kThreads) {
-    const int l = (e >> 4) % nl, a = e & 3, c = (e >> 2) & 3;
-    const bool old = (e >> 4) >= nl;
-    const int i = (old ? j.org[2 * l] : sI0[l]) + a, k = (old ? j.org[2 * l + 1] : sK0[l]) + c;
+  for (int e = tid; e < 16 * nl; e += kThreads) {
+    const int l = e >> 4, i = sI0[l] + (e & 3), k = sK0[l] + ((e >> 2) & 3);
     if (i >= 0 && i < nx && k >= 0 && k < nz) sMap[(k - wk0) * WW + (i - wi0)] = -2;
   }
+  if (have_prev)
+    for (int e = tid; e < 16 * nl; e += kThreads) {
+      const int l = e >> 4, i = j.org[2 * l] + (e & 3), k = j.org[2 * l + 1] + ((e >> 2) & 3);
+      if (i >= 0 && i < nx && k >= 0 && k < nz) sMap[(k - wk0) * WW + (i - wi0)] = -2;
+    }
   __syncthreads();
   for (int e = tid; e < nwin; e += kThreads) {
     if (sMap[e] != -2) continue;
@@ -196,6 +218,39 @@ __device__ void coupled_update(const Job &j, int parity) {
     if (tid == 0) atomicOr(p.status, 8u);
     return;
   }
+  // flags: the new footprint's tiles go up before anything is written; tmap
+  // marks the tiles of the previous and new footprints for the clean-up
+  const int ibtx = p.ibtx;
+  const int tx0 = max(min(wi0, bnd2[0]) - kHalo, 0) / f2d::kTX, tz0 = max(min(wk0, bnd2[2]) - kHalo, 0) / f2d::kTZ;
+  const int tmw = min(max(wi0 + WW - 1, bnd2[1]) + kHalo, nx - 1) / f2d::kTX - tx0 + 1;
+  const int tmh = min(max(wk0 + WH - 1, bnd2[3]) + kHalo, nz - 1) / f2d::kTZ - tz0 + 1;
+  const bool tmap_ok = tmw > 0 && tmh > 0 && tmw * tmh <= kTileMap;
+  if (tmap_ok)
+    for (int e = tid; e < tmw * tmh; e += kThreads) tmap[e] = 0;
+  __syncthreads();
+  // tiles whose halo may reach a marker's 4x4 stencil: the stencil widened
+  // by the margin spans at most two tiles per axis, those of its ends
+  auto corners = [&](int i0, int k0, int (&tx)[2], int (&tz)[2]) {
+    tx[0] = min(max(i0 - kHalo, 0), nx - 1) / f2d::kTX;
+    tx[1] = min(max(i0 + 3 + kHalo, 0), nx - 1) / f2d::kTX;
+    tz[0] = min(max(k0 - kHalo, 0), nz - 1) / f2d::kTZ;
+    tz[1] = min(max(k0 + 3 + kHalo, 0), nz - 1) / f2d::kTZ;
+  };
+  for (int e = tid; e < nl * (have_prev ? 2 : 1); e += kThreads) {
+    const bool old = e >= nl;
+    const int l = old ? e - nl : e;
+    int tx[2], tz[2];
+    corners(old ? j.org[2 * l] : sI0[l], old ? j.org[2 * l + 1] : sK0[l], tx, tz);
+#pragma unroll
+    for (int c = 0; c < 4; c++) {
+      const int x = tx[c & 1], z = tz[c >> 1];
+      if (!old) j.flag[z * ibtx + x] = 1;
+      if (tmap_ok) tmap[(z - tz0) * tmw + (x - tx0)] = 1;
+    }
+  }
+  __threadfence();
+  __syncthreads();
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
   const float rho0 = p.rho_base, rsal = p.rho_sal_f, hdt = p.hdt;
   for (int s = tid; s < ns; s += kThreads) {
     const long long ci = sCell[s];
@@ -209,14 +264,11 @@ __device__ void coupled_update(const Job &j, int parity) {
   }
   __syncthreads();
 
-  // ---- pairs of the new stencils listed by slot, in pair order
-  auto slot_at = [&](int l, int qq) -> int {
-    const int i = sI0[l] + (qq & 3), k = sK0[l] + (qq >> 2);
-    if (i < 0 || i >= nx || k < 0 || k >= nz) return -1;
-    return sMap[(k - wk0) * WW + (i - wi0)];
-  };
+  // ---- pairs of the new stencils: their slots, then listed by slot in pair order
   for (int e = tid; e < 16 * nl; e += kThreads) {
-    const int s = slot_at(e >> 4, e & 15);
+    const int l = e >> 4, i = sI0[l] + (e & 3), k = sK0[l] + ((e >> 2) & 3);
+    const int s = (i < 0 || i >= nx || k < 0 || k >= nz) ? -1 : sMap[(k - wk0) * WW + (i - wi0)];
+    sPS[e] = (short)s;
     if (s >= 0) atomicAdd(&sCur[s], 1);
   }
   __syncthreads();
@@ -262,7 +314,7 @@ __device__ void coupled_update(const Job &j, int parity) {
   for (int s = tid; s < ns; s += kThreads) sCur[s] = sOff[s];
   __syncthreads();
   for (int e = tid; e < 16 * nl; e += kThreads) {
-    const int s = slot_at(e >> 4, e & 15);
+    const int s = sPS[e];
     if (s >= 0) sList[atomicAdd(&sCur[s], 1)] = (short)e;
   }
   __syncthreads();
@@ -282,7 +334,7 @@ __device__ void coupled_update(const Job &j, int parity) {
 
   // ---- 3. multi-direct forcing
   const int g = tid >> 4, q = tid & 15, qa = q & 3, qc = q >> 2;
-  auto slot_of = [&](int l) -> int { return slot_at(l, q); };
+  auto slot_of = [&](int l) -> int { return sPS[16 * l + q]; };
   const float two_rf_dt = (float)(2.0 * j.rho_f / j.dt);
   for (int it = 0; it < j.iters; it++) {
     for (int lb = 0; lb < nl; lb += kGroups) {
@@ -326,23 +378,7 @@ __device__ void coupled_update(const Job &j, int parity) {
     __syncthreads();
   }
 
-  // ---- 4. write back; tile flags follow the footprint
-  const int ibtx = p.ibtx;
-  auto flag_around = [&](int i, int k, uint8_t v) {
-    const int ia = max(i - kHalo, 0) / f2d::kTX, ib = min(i + kHalo, nx - 1) / f2d::kTX;
-    const int ka = max(k - kHalo, 0) / f2d::kTZ, kb = min(k + kHalo, nz - 1) / f2d::kTZ;
-    j.flag[ka * ibtx + ia] = v;
-    j.flag[ka * ibtx + ib] = v;
-    j.flag[kb * ibtx + ia] = v;
-    j.flag[kb * ibtx + ib] = v;
-  };
-  if (have_prev) {
-    for (int e = tid; e < 16 * nl; e += kThreads) {
-      const int l = e >> 4, i = j.org[2 * l] + (e & 3), k = j.org[2 * l + 1] + ((e >> 2) & 3);
-      if (i >= 0 && i < nx && k >= 0 && k < nz) flag_around(i, k, 0);
-    }
-  }
-  __syncthreads();
+  // ---- 4. write back
   constexpr bool RES = sizeof(ST) == 2;
   const float ic = 1.0f / p.c;
   for (int s = tid; s < ns; s += kThreads) {
@@ -378,11 +414,22 @@ __device__ void coupled_update(const Job &j, int parity) {
     }
     mac[N + ci] = un;
     mac[2 * N + ci] = wn;
-    const float fx = sFX[s], fz = sFZ[s];
-    j.fext[ci] = fx;
-    j.fext[N + ci] = fz;
-    if (fx != 0.f || fz != 0.f) flag_around((int)(ci % nx), (int)(ci / nx), 1);
+    j.fext[ci] = sFX[s];
+    j.fext[N + ci] = sFZ[s];
     if (!(isfinite(un) && isfinite(wn))) atomicOr(p.status, 1u);
+  }
+  // tiles of the footprint two steps back that neither the previous nor the
+  // new footprint covers: no fluid step needs to wait there any more
+  if (B.have_prev2 && tmap_ok) {
+    for (int l = tid; l < nl; l += kThreads) {
+      int tx[2], tz[2];
+      corners(j.org2[2 * l], j.org2[2 * l + 1], tx, tz);
+#pragma unroll
+      for (int c = 0; c < 4; c++) {
+        const int x = tx[c & 1], z = tz[c >> 1];
+        if (!tmap[(z - tz0) * tmw + (x - tx0)]) j.flag[z * ibtx + x] = 0;
+      }
+    }
   }
   __syncthreads();
 
@@ -395,11 +442,13 @@ __device__ void coupled_update(const Job &j, int parity) {
     acc[0] += fx;
     acc[1] += fz;
     acc[2] += rx * fz - rz * fx;
-    j.org[2 * l] = sI0[l];  // this step's footprint is the next step's old one
+    j.org2[2 * l] = j.org[2 * l];  // the footprints move back one step
+    j.org2[2 * l + 1] = j.org[2 * l + 1];
+    j.org[2 * l] = sI0[l];
     j.org[2 * l + 1] = sK0[l];
   }
   {
-    const double a = j.semi_a, bb = j.semi_b;
+    const double a = j.semi_a, bb = j.semi_b, ra = 1.0 / a, rb = 1.0 / bb;
     // half extents of the ellipse, widened by one cell for the fraction ramp
     const double hx = sqrt(a * a * cth * cth + bb * bb * sth * sth) + dz;
     const double hz = sqrt(a * a * sth * sth + bb * bb * cth * cth) + dz;
@@ -412,8 +461,9 @@ __device__ void coupled_update(const Job &j, int parity) {
         const int i = ia + e % bw, k = ka + e / bw;
         const double dx = (i + 0.5) * dz - B.X[0], dzz = (k + 0.5) * dz - B.X[1];
         const double xb = cth * dx + sth * dzz, zb = -sth * dx + cth * dzz;
-        const double F = (xb / a) * (xb / a) + (zb / bb) * (zb / bb) - 1.0;
-        const double G = 2.0 * hypot(xb / (a * a), zb / (bb * bb));
+        const double xa = xb * ra, zc = zb * rb;
+        const double F = xa * xa + zc * zc - 1.0;
+        const double G = 2.0 * hypot(xa * ra, zc * rb);
         const double al = fmin(fmax(0.5 - F / fmax(G, 1e-300) * idz, 0.0), 1.0) * dA;
         if (al > 0.0) {
           const long long ci = (long long)k * nx + i;
@@ -459,6 +509,7 @@ __device__ void coupled_update(const Job &j, int parity) {
     nb.Fib[0] = t[0];
     nb.Fib[1] = t[1];
     nb.Tib = t[2];
+    nb.have_prev2 = B.have_prev;
     nb.have_prev = 1;
     *j.body = nb;
   }

@@ -14,7 +14,7 @@ namespace ib2d {
 constexpr int kThreads = 512;
 constexpr int kMaxMarkers = 512;
 constexpr int kMaxWindow = 12288;  // cells of the footprint window (old + new stencils)
-constexpr int kMaxSlots = 4096;    // distinct cells the stencils touch
+constexpr int kMaxSlots = 3072;    // distinct cells the stencils touch
 constexpr int kHalo = 4;           // a forced cell flags every tile whose halo may reach it
 
 // Device-resident FP64 body state.
@@ -23,7 +23,7 @@ struct Body {
   double P[2], L;             // fluid momentum and angular momentum inside the body, previous step
   double Fib[2], Tib;         // force and torque (about the centre) the markers put on the fluid, previous step
   int have_prev;              // a coupled step has run: the fields above and the old footprint are valid
-  int pad;
+  int have_prev2;             // two have: the footprint of two steps back is valid
 };
 
 // One coupled body: the fluid's buffers come from the simulation's
@@ -34,6 +34,7 @@ struct Job {
   const double *X0;  // [nl][2] marker positions in the body frame
   const double *dS;  // [nl] arc length per marker
   int *org;          // [nl][2] stencil origin of the previous step's markers
+  int *org2;         // [nl][2] ... and of the step before
   float *fext;       // [2][N] force density on the fluid (also fp.fext)
   uint8_t *flag;     // [tiles] (also fp.ibflag)
   int nl, iters;

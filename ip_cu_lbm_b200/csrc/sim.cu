@@ -332,6 +332,7 @@ void free_sim(ipcu_sim *s) {
     fr((void *)s->ib->X0);
     fr((void *)s->ib->dS);
     fr(s->ib->org);
+    fr(s->ib->org2);
     fr(s->ib->fext);
     fr(s->ib->flag);
     delete s->ib;
@@ -723,6 +724,7 @@ extern "C" int ipcu_sim_ib_attach(ipcu_sim *s, const ipcu_ib_body2d *bd, const d
   b0.om = bd->omega;
   std::vector<double> X0(markers, markers + 2 * n), dSv(dS, dS + n);
   bool ok = salloc(s, &j->body, sizeof(ib2d::Body)) && salloc(s, &j->org, sizeof(int) * 2 * n) &&
+            salloc(s, &j->org2, sizeof(int) * 2 * n) &&
             salloc(s, &j->fext, sizeof(float) * 2 * N) && salloc(s, &j->flag, (size_t)tx * tz);
   double *dX0 = nullptr, *ddS = nullptr;
   ok = ok && salloc(s, &dX0, sizeof(double) * 2 * n) && salloc(s, &ddS, sizeof(double) * n);
@@ -734,6 +736,7 @@ extern "C" int ipcu_sim_ib_attach(ipcu_sim *s, const ipcu_ib_body2d *bd, const d
   if (e == cudaSuccess) e = cudaMemcpyAsync(dX0, X0.data(), sizeof(double) * 2 * n, cudaMemcpyHostToDevice, s->stream);
   if (e == cudaSuccess) e = cudaMemcpyAsync(ddS, dSv.data(), sizeof(double) * n, cudaMemcpyHostToDevice, s->stream);
   if (e == cudaSuccess) e = cudaMemsetAsync(j->org, 0, sizeof(int) * 2 * n, s->stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(j->org2, 0, sizeof(int) * 2 * n, s->stream);
   if (e == cudaSuccess) e = cudaMemsetAsync(j->fext, 0, sizeof(float) * 2 * N, s->stream);
   if (e == cudaSuccess) e = cudaMemsetAsync(j->flag, 0, (size_t)tx * tz, s->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
@@ -1364,6 +1367,6 @@ extern "C" int64_t ipcu_sim_device_bytes(const ipcu_sim *s) {
          4LL * (3 * (s->nx + s->nz) + 2 * 5 * std::max(s->nx, s->nz)) + 2048 +
          (s->cfg.scalar_kind == IPCU_SCALAR_PHASE ? 4LL * (s->nx + s->nz) : 0) +  // 1/dx^2, 1/dz^2
          (s->ib ? 8LL * N + ((s->nx + f2d::kTX - 1) / f2d::kTX) * ((s->nz + f2d::kTZ - 1) / f2d::kTZ) +
-                      32LL * s->ib->nl + (long long)sizeof(ib2d::Body)
+                      40LL * s->ib->nl + (long long)sizeof(ib2d::Body)
                 : 0);  // immersed body: force density, tile flags, markers, body state
 }

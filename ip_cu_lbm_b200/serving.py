@@ -107,7 +107,7 @@ def request_bytes(req: Request) -> int:
     N = req.cells
     ib = 0
     if req.body is not None:  # force density, tile flags, markers, body state
-        ib = 8 * N + ((req.nx + 31) // 32) * ((req.nz + 15) // 16) + 32 * req.body.get("markers", 240) + 104
+        ib = 8 * N + ((req.nx + 31) // 32) * ((req.nz + 15) // 16) + 40 * req.body.get("markers", 240) + 104
     return (2 * (esz * (9 + q) * N + 4 * nmac * N) + 4 * (3 * (req.nx + req.nz) + 10 * max(req.nx, req.nz)) + 2048
             + (4 * (req.nx + req.nz) if pf else 0) + ib)
 
