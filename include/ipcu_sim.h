@@ -188,6 +188,12 @@ int ipcu_sim_ib_attach(ipcu_sim *sim, const ipcu_ib_body2d *body, const double *
  * the markers put on the fluid in the last step (9 values). Synchronises.
  * ipcu_sim_get serves the force density as fields "ibfx", "ibfz". */
 int ipcu_sim_ib_body(ipcu_sim *sim, double *out);
+/* A new non-blocking CUDA stream (it does not synchronise with the legacy
+ * default stream) and its release; work still queued on a released stream
+ * completes. A server gives each admitted simulation one, so that a
+ * simulation's set-up never waits for the batch in flight. */
+int ipcu_stream_create(ipcu_stream_t *out);
+int ipcu_stream_destroy(ipcu_stream_t stream);
 /* Device bytes a simulation holds (state, ping-pong, tables). */
 int64_t ipcu_sim_device_bytes(const ipcu_sim *sim);
 

@@ -13,15 +13,17 @@ constexpr int kTX = 32;  // tile width along x (one warp per row)
 constexpr int kTZ = 16;  // tile height along z
 constexpr int kThreads = 256;
 constexpr int kMinBlocks = 4;  // resident CTAs per SM the register budget is sized for
-constexpr int kTmaBoxX = kTX + 8;  // TMA box width: [x0-4, x0+kTX+4), 16-byte aligned start
+constexpr int kTmaBoxX = kTX + 8;     // TMA box width, FP32: [x0-4, x0+kTX+4), 16-byte aligned start
+constexpr int kTmaBoxX16 = kTX + 16;  // TMA box width, 16-bit: [x0-8, x0+kTX+8)
 
 // halo rows of the streaming stencil along z (1 unless z is the interpolated axis)
 inline int halo_z(int geo) { return geo == IPCU_GEO_Z5 ? 3 : (geo == IPCU_GEO_Z3 ? 2 : 1); }
 
 struct alignas(64) Params {
-  // TMA descriptors of the ping-pong buffers (FP32 storage, nx % 4 == 0):
-  // f [9][nz][nx], g [q][nz][nx], macroscopic [3][nz][nx]; boxes sized for
-  // the tile + halo (f, g) and the salinity ring rows (macroscopic)
+  // TMA descriptors of the ping-pong buffers (FP32 storage with nx % 4 == 0,
+  // 16-bit storage with nx % 8 == 0): f [9][nz][nx], g [q][nz][nx],
+  // macroscopic [3 or 4][nz][nx]; boxes sized for the tile + halo (f, g) and
+  // the salinity ring rows (macroscopic)
   CUtensorMap tm_f[2], tm_g[2], tm_m[2];
   int tma;  // 1: the single-simulation kernel stages with the maps above
   int nx, nz;
@@ -84,9 +86,10 @@ struct WorkItem {
 // Advances every simulation referenced by `work` (all of the same storage,
 // scalar lattice and geometry) by one step; `params` and `work` are device
 // arrays; `parity` flips the ping-pong buffers of all of them. `grid` CTAs
-// loop over the work list.
+// loop over the work list. tma: every one of them has tensor maps (staged
+// with TMA box loads, the maps read from `params`).
 int launch_batched(const Params *params, const WorkItem *work, int nwork, int parity, int storage, int qs, int geo,
-                   int pf, int grid, cudaStream_t s, bool prepare_only = false);
+                   int pf, int grid, cudaStream_t s, bool prepare_only, bool tma);
 
 }  // namespace f2d
 }  // namespace ipcu

@@ -91,21 +91,30 @@ struct Geo {
 constexpr int kQueue = 127;
 
 // Shared-memory layout in floats; TMA destinations start on 128-byte boundaries.
-template <int QS, int GEO, bool TMA>
+// SB: bytes of a stored population. TMA staging of 16-bit storage lands the
+// f and g boxes ([planes][EZ][kTmaBoxX16] 16-bit values, starting at
+// x0 - 8 so the x coordinate stays 16-byte aligned) in their own area H0,
+// from which the collision phase reads them into the float tile, and stages
+// four macroscopic planes (S, u_x, u_z, p*).
+template <int QS, int GEO, bool TMA, int SB = 4>
 struct Smem {
   using G = Geo<GEO, TMA>;
   static constexpr int al(int v, int a) { return (v + a - 1) / a * a; }
+  static constexpr bool H16 = TMA && SB == 2;
   static constexpr int G0 = al(9 * G::NE, 32);                   // g tile
-  static constexpr int S0 = al(G0 + QS * G::NE, 32);             // ring (TMA: S, u_x, u_z planes)
-  static constexpr int F0 = S0 + (TMA ? 3 : 1) * G::SZ * G::RX;  // registers: interior force
+  static constexpr int S0 = al(G0 + QS * G::NE, 32);             // ring (TMA: S, u_x, u_z [, p*] planes)
+  static constexpr int F0 = S0 + (TMA ? (H16 ? 4 : 3) : 1) * G::SZ * G::RX;  // registers: interior force
   static constexpr int W0 = F0 + (TMA ? 0 : 2 * kTX * kTZ);      // axis weights
   static constexpr int C0 = W0 + 2 * G::WREC * G::NWA;            // combined interior weights
   static constexpr int B0 = al(C0 + 2 * (G::NS + 1) * G::NWA, 2);  // mbarrier
   static constexpr int Q0 = B0 + 4;                                // wall-cell queue: count + kQueue slots
-  static constexpr size_t bytes = sizeof(float) * (size_t)(Q0 + 1 + kQueue);
+  static constexpr int E16 = G::EZ * kTmaBoxX16;                   // 16-bit values per staged plane
+  static constexpr int H0 = al(Q0 + 1 + kQueue, 32);               // 16-bit staging: f planes, then g
+  static constexpr int HG = al(H0 + 9 * E16 / 2, 32);              // TMA destinations: 128-byte aligned
+  static constexpr size_t bytes = sizeof(float) * (size_t)(H16 ? HG + QS * E16 / 2 : Q0 + 1 + kQueue);
 };
-template <int QS, int GEO, bool TMA>
-constexpr size_t smem_bytes() { return Smem<QS, GEO, TMA>::bytes; }
+template <int QS, int GEO, bool TMA, int SB = 4>
+constexpr size_t smem_bytes() { return Smem<QS, GEO, TMA, SB>::bytes; }
 
 __device__ __forceinline__ unsigned smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
 __device__ __forceinline__ void mbar_init(unsigned bar, unsigned count) {
@@ -115,6 +124,12 @@ __device__ __forceinline__ void mbar_init(unsigned bar, unsigned count) {
 }
 __device__ __forceinline__ void mbar_expect_tx(unsigned bar, unsigned bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+// Acquires a tensor map written to global memory by the generic proxy (the
+// batched kernel's parameter array is rewritten between launches)
+__device__ __forceinline__ void tensormap_acquire(const CUtensorMap *map) {
+  asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(reinterpret_cast<uint64_t>(map))
+               : "memory");
 }
 // 3-D tiled TMA load (no multicast) into this CTA's shared memory
 __device__ __forceinline__ void tma_load_3d(unsigned dst, const CUtensorMap *map, int x, int y, int z, unsigned bar) {
@@ -191,16 +206,19 @@ struct Fast {
 // the kernel's constant bank) and the batched kernel (parameters in global
 // memory). TMA: stage with tensor-map box loads (single-simulation FP32
 // kernel; the tensor maps live in the __grid_constant__ parameters).
+// tm: the tensor maps (tm_f[2], tm_g[2], tm_m[2], contiguous) of the
+// simulation, in parameter or global memory (TMA staging only).
 template <class ST, int QS, int GEO, bool TMA, int PHYS>
-__device__ __forceinline__ void step_tile(const Params &p, int parity, int tile_x, int tile_z, float *smem) {
+__device__ __forceinline__ void step_tile(const Params &p, int parity, int tile_x, int tile_z, float *smem,
+                                          const CUtensorMap *tm = nullptr) {
   using G = Geo<GEO, TMA>;
-  using SL = Smem<QS, GEO, TMA>;
+  using SL = Smem<QS, GEO, TMA, (int)sizeof(ST)>;
   constexpr int HZ = G::HZ, EX = G::EX, NE = G::NE, SZ = G::SZ, RX = G::RX, RO = G::RO;
   constexpr int XO = G::XO, NWA = G::NWA, WREC = G::WREC;
   // RES (16-bit storage): f and g hold deviations from the local
   // equilibrium, p* comes from its own FP32 plane
   constexpr bool RES = sizeof(ST) == 2;
-  static_assert(!TMA || sizeof(ST) == 4, "TMA staging is for FP32 storage");
+
   float *sf = smem;            // [9][EZ][EX] f, collided in place
   float *sg = smem + SL::G0;   // [QS][EZ][EX] g
   float *sS = smem + SL::S0;   // [SZ][RX] salinity ring (TMA: then the u_x, u_z planes)
@@ -245,11 +263,20 @@ __device__ __forceinline__ void step_tile(const Params &p, int parity, int tile_
     if (tid == 0) mbar_init(bar_a, 1);
     __syncthreads();
     if (tid == 0) {
-      constexpr unsigned bytes = 4u * (unsigned)((9 + QS) * NE + 3 * SZ * RX);
-      mbar_expect_tx(bar_a, bytes);
-      tma_load_3d(smem_u32(sf), &p.tm_f[bi], ox, oz, 0, bar_a);
-      if constexpr (QS > 0) tma_load_3d(smem_u32(sg), &p.tm_g[bi], ox, oz, 0, bar_a);
-      tma_load_3d(smem_u32(sS), &p.tm_m[bi], ox, oz - 1, 0, bar_a);
+      if constexpr (RES) {
+        // 16-bit boxes from x0 - 8 (= ox - 4), four FP32 macroscopic planes
+        constexpr unsigned bytes = 2u * (unsigned)((9 + QS) * SL::E16) + 4u * (unsigned)(4 * SZ * RX);
+        mbar_expect_tx(bar_a, bytes);
+        tma_load_3d(smem_u32(smem + SL::H0), &tm[bi], ox - 4, oz, 0, bar_a);
+        if constexpr (QS > 0) tma_load_3d(smem_u32(smem + SL::HG), &tm[2 + bi], ox - 4, oz, 0, bar_a);
+        tma_load_3d(smem_u32(sS), &tm[4 + bi], ox, oz - 1, 0, bar_a);
+      } else {
+        constexpr unsigned bytes = 4u * (unsigned)((9 + QS) * NE + 3 * SZ * RX);
+        mbar_expect_tx(bar_a, bytes);
+        tma_load_3d(smem_u32(sf), &tm[bi], ox, oz, 0, bar_a);
+        if constexpr (QS > 0) tma_load_3d(smem_u32(sg), &tm[2 + bi], ox, oz, 0, bar_a);
+        tma_load_3d(smem_u32(sS), &tm[4 + bi], ox, oz - 1, 0, bar_a);
+      }
     }
   } else {
     for (int e = tid; e < SZ * RX; e += kThreads) {
@@ -312,10 +339,21 @@ __device__ __forceinline__ void step_tile(const Params &p, int parity, int tile_
     const int rs = (lz + 1) * RX + lx + RO;  // ring slot
     float f[9], g[QS > 0 ? QS : 1], u, w, pr = 0.f;
     if constexpr (TMA) {
+      if constexpr (RES) {
+        const ST *h16 = reinterpret_cast<const ST *>(smem + SL::H0);
+        const int e16 = lz * kTmaBoxX16 + lx + 4;  // the 16-bit box starts 4 columns left of the float tile
 #pragma unroll
-      for (int k = 0; k < 9; k++) f[k] = sf[k * NE + e];
+        for (int k = 0; k < 9; k++) f[k] = ld(h16, k * SL::E16 + e16, ifs);
+        const ST *g16 = reinterpret_cast<const ST *>(smem + SL::HG);
 #pragma unroll
-      for (int k = 0; k < QS; k++) g[k] = sg[k * NE + e];
+        for (int k = 0; k < QS; k++) g[k] = ld(g16, k * SL::E16 + e16, igs);
+        pr = sS[3 * SZ * RX + rs];
+      } else {
+#pragma unroll
+        for (int k = 0; k < 9; k++) f[k] = sf[k * NE + e];
+#pragma unroll
+        for (int k = 0; k < QS; k++) g[k] = sg[k * NE + e];
+      }
       u = sS[SZ * RX + rs];
       w = sS[2 * SZ * RX + rs];
     } else {
@@ -705,13 +743,15 @@ __device__ __forceinline__ void step_tile(const Params &p, int parity, int tile_
 template <class ST, int QS, int GEO, bool TMA, int PHYS>
 __global__ void __launch_bounds__(kThreads, kMinBlocks) step_kernel(const __grid_constant__ Params p) {
   extern __shared__ __align__(128) float smem[];
-  step_tile<ST, QS, GEO, TMA, PHYS>(p, 0, blockIdx.x, blockIdx.y, smem);
+  step_tile<ST, QS, GEO, TMA, PHYS>(p, 0, blockIdx.x, blockIdx.y, smem, p.tm_f);
 }
 
 // The batched kernel copies each work item's parameters (past the tensor
 // maps, which register staging does not use) into shared memory, so that
 // the tile reads them as shared loads rather than global ones.
-template <class ST, int QS, int GEO, int PHYS>
+// TMA: stage with each simulation's tensor maps, read in place from the
+// global parameter array (all simulations of the launch have them).
+template <class ST, int QS, int GEO, bool TMA, int PHYS>
 __global__ void __launch_bounds__(kThreads, kMinBlocks)
     step_kernel_batched(const Params *__restrict__ ps, const WorkItem *__restrict__ work, int nwork, int parity) {
   extern __shared__ __align__(128) float smem[];
@@ -724,34 +764,46 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
       const uint32_t *src = reinterpret_cast<const uint32_t *>(ps + w.sim);
       uint32_t *dst = reinterpret_cast<uint32_t *>(&sp);
       for (int j = kSkip + threadIdx.x; j < kWords; j += kThreads) dst[j] = src[j];
+      if (TMA && threadIdx.x < 6) tensormap_acquire(ps[w.sim].tm_f + threadIdx.x);
       cur_sim = w.sim;
       __syncthreads();
     }
-    step_tile<ST, QS, GEO, false, PHYS>(sp, parity, w.tx, w.tz, smem);
+    step_tile<ST, QS, GEO, TMA, PHYS>(sp, parity, w.tx, w.tz, smem, ps[w.sim].tm_f);
     __syncthreads();  // the next item reuses shared memory
   }
 }
 
-template <class ST, int QS, int GEO, int PHYS>
-int launch_b(const Params *ps, const WorkItem *work, int nwork, int parity, int grid, cudaStream_t s, bool prep) {
-  constexpr size_t sm = smem_bytes<QS, GEO, false>();
+template <class ST, int QS, int GEO, bool TMA, int PHYS>
+int launch_b1(const Params *ps, const WorkItem *work, int nwork, int parity, int grid, cudaStream_t s, bool prep) {
+  constexpr size_t sm = smem_bytes<QS, GEO, TMA, (int)sizeof(ST)>();
   if (prep)
-    return status_from_cuda(cudaFuncSetAttribute(step_kernel_batched<ST, QS, GEO, PHYS>,
+    return status_from_cuda(cudaFuncSetAttribute(step_kernel_batched<ST, QS, GEO, TMA, PHYS>,
                                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
   if (nwork <= 0) return IPCU_OK;
-  step_kernel_batched<ST, QS, GEO, PHYS><<<grid, kThreads, sm, s>>>(ps, work, nwork, parity);
+  step_kernel_batched<ST, QS, GEO, TMA, PHYS><<<grid, kThreads, sm, s>>>(ps, work, nwork, parity);
   return status_from_cuda(cudaGetLastError());
+}
+// tma: every simulation of the launch has tensor maps
+template <class ST, int QS, int GEO, int PHYS>
+int launch_b(const Params *ps, const WorkItem *work, int nwork, int parity, int grid, cudaStream_t s, bool prep,
+             bool tma) {
+  if (prep) {
+    const int st = launch_b1<ST, QS, GEO, false, PHYS>(ps, work, nwork, parity, grid, s, true);
+    return st ? st : launch_b1<ST, QS, GEO, true, PHYS>(ps, work, nwork, parity, grid, s, true);
+  }
+  if (tma) return launch_b1<ST, QS, GEO, true, PHYS>(ps, work, nwork, parity, grid, s, false);
+  return launch_b1<ST, QS, GEO, false, PHYS>(ps, work, nwork, parity, grid, s, false);
 }
 
 template <class ST, int QS, int PHYS>
 int launch_bg(const Params *ps, const WorkItem *work, int nwork, int parity, int geo, int grid, cudaStream_t s,
-              bool prep) {
+              bool prep, bool tma) {
   switch (geo) {
-    case IPCU_GEO_UNIFORM: return launch_b<ST, QS, IPCU_GEO_UNIFORM, PHYS>(ps, work, nwork, parity, grid, s, prep);
-    case IPCU_GEO_X5: return launch_b<ST, QS, IPCU_GEO_X5, PHYS>(ps, work, nwork, parity, grid, s, prep);
-    case IPCU_GEO_X3: return launch_b<ST, QS, IPCU_GEO_X3, PHYS>(ps, work, nwork, parity, grid, s, prep);
-    case IPCU_GEO_Z5: return launch_b<ST, QS, IPCU_GEO_Z5, PHYS>(ps, work, nwork, parity, grid, s, prep);
-    case IPCU_GEO_Z3: return launch_b<ST, QS, IPCU_GEO_Z3, PHYS>(ps, work, nwork, parity, grid, s, prep);
+    case IPCU_GEO_UNIFORM: return launch_b<ST, QS, IPCU_GEO_UNIFORM, PHYS>(ps, work, nwork, parity, grid, s, prep, tma);
+    case IPCU_GEO_X5: return launch_b<ST, QS, IPCU_GEO_X5, PHYS>(ps, work, nwork, parity, grid, s, prep, tma);
+    case IPCU_GEO_X3: return launch_b<ST, QS, IPCU_GEO_X3, PHYS>(ps, work, nwork, parity, grid, s, prep, tma);
+    case IPCU_GEO_Z5: return launch_b<ST, QS, IPCU_GEO_Z5, PHYS>(ps, work, nwork, parity, grid, s, prep, tma);
+    case IPCU_GEO_Z3: return launch_b<ST, QS, IPCU_GEO_Z3, PHYS>(ps, work, nwork, parity, grid, s, prep, tma);
   }
   return IPCU_ERR_UNSUPPORTED;
 }
@@ -775,7 +827,7 @@ int launch_pdl(K kernel, dim3 grid, size_t smem, cudaStream_t s, A... args) {
 
 template <class ST, int QS, int GEO, bool TMA, int PHYS>
 int launch_t1(const Params &p, cudaStream_t s, bool prepare_only) {
-  constexpr size_t sm = smem_bytes<QS, GEO, TMA>();
+  constexpr size_t sm = smem_bytes<QS, GEO, TMA, (int)sizeof(ST)>();
   if (prepare_only) {  // once per sim, outside any stream capture
     return status_from_cuda(cudaFuncSetAttribute(step_kernel<ST, QS, GEO, TMA, PHYS>,
                                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
@@ -789,9 +841,7 @@ int launch_t1(const Params &p, cudaStream_t s, bool prepare_only) {
 // TMA staging for FP32 storage when the host built the tensor maps (p.tma)
 template <class ST, int QS, int GEO, int PHYS>
 int launch_t(const Params &p, cudaStream_t s, bool prepare_only) {
-  if constexpr (sizeof(ST) == 4) {
-    if (p.tma) return launch_t1<ST, QS, GEO, true, PHYS>(p, s, prepare_only);
-  }
+  if (p.tma) return launch_t1<ST, QS, GEO, true, PHYS>(p, s, prepare_only);
   return launch_t1<ST, QS, GEO, false, PHYS>(p, s, prepare_only);
 }
 
@@ -821,13 +871,13 @@ int launch_q(const Params &p, int qs, int geo, cudaStream_t s, bool prep) {
 }
 template <class ST, int PHYS>
 int launch_bq(const Params *ps, const WorkItem *work, int nwork, int parity, int qs, int geo, int grid,
-              cudaStream_t s, bool prep) {
+              cudaStream_t s, bool prep, bool tma) {
   if (qs == 0) {
-    if constexpr (PHYS == 0) return launch_bg<ST, 0, 0>(ps, work, nwork, parity, geo, grid, s, prep);
+    if constexpr (PHYS == 0) return launch_bg<ST, 0, 0>(ps, work, nwork, parity, geo, grid, s, prep, tma);
     return IPCU_ERR_UNSUPPORTED;
   }
-  if (qs == 5) return launch_bg<ST, 5, PHYS>(ps, work, nwork, parity, geo, grid, s, prep);
-  if (qs == 9) return launch_bg<ST, 9, PHYS>(ps, work, nwork, parity, geo, grid, s, prep);
+  if (qs == 5) return launch_bg<ST, 5, PHYS>(ps, work, nwork, parity, geo, grid, s, prep, tma);
+  if (qs == 9) return launch_bg<ST, 9, PHYS>(ps, work, nwork, parity, geo, grid, s, prep, tma);
   return IPCU_ERR_UNSUPPORTED;
 }
 #define IPCU_F2D_INSTANTIATE(ST, NAME, PHYS)                                                              \
@@ -835,8 +885,8 @@ int launch_bq(const Params *ps, const WorkItem *work, int nwork, int parity, int
     return launch_q<ST, PHYS>(p, qs, geo, s, prep);                                                       \
   }                                                                                                       \
   int launch_batched_##NAME(const Params *ps, const WorkItem *work, int nwork, int parity, int qs, int geo, \
-                            int grid, cudaStream_t s, bool prep) {                                        \
-    return launch_bq<ST, PHYS>(ps, work, nwork, parity, qs, geo, grid, s, prep);                          \
+                            int grid, cudaStream_t s, bool prep, bool tma) {                              \
+    return launch_bq<ST, PHYS>(ps, work, nwork, parity, qs, geo, grid, s, prep, tma);                     \
   }
 
 }  // namespace f2d

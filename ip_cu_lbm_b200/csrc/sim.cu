@@ -133,18 +133,20 @@ PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
   return fn;
 }
 
-// FP32 planes [planes][nz][nx] read as boxes of [planes][rows][kTmaBoxX];
-// cells outside the array read as zero
-bool encode_planes(CUtensorMap *map, void *base, int nx, int nz, int planes, int rows) {
+// Planes [planes][nz][nx] of 4-byte (FP32) or 2-byte (16-bit storage, moved
+// as raw bits) values read as boxes of [planes][rows][kTmaBoxX] or
+// [planes][rows][kTmaBoxX16]; cells outside the array read as zero
+bool encode_planes(CUtensorMap *map, void *base, int nx, int nz, int planes, int rows, int esz = 4) {
   PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
-  if (!enc || nx % 4 != 0) return false;
+  if (!enc || (nx * esz) % 16 != 0) return false;
   const cuuint64_t dims[3] = {(cuuint64_t)nx, (cuuint64_t)nz, (cuuint64_t)planes};
-  const cuuint64_t strides[2] = {(cuuint64_t)nx * 4, (cuuint64_t)nx * nz * 4};
-  const cuuint32_t box[3] = {(cuuint32_t)f2d::kTmaBoxX, (cuuint32_t)rows, (cuuint32_t)planes};
+  const cuuint64_t strides[2] = {(cuuint64_t)nx * esz, (cuuint64_t)nx * nz * esz};
+  const cuuint32_t box[3] = {(cuuint32_t)(esz == 4 ? f2d::kTmaBoxX : f2d::kTmaBoxX16), (cuuint32_t)rows,
+                             (cuuint32_t)planes};
   const cuuint32_t es[3] = {1, 1, 1};
-  return enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, base, dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
-             CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
-             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+  return enc(map, esz == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_UINT16, 3, base, dims,
+             strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+             CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
 // 1/(x_{i+1} - x_{i-1} + dz/1000) in float, clamped neighbours
@@ -557,14 +559,19 @@ extern "C" int ipcu_sim_create(const ipcu_sim_config *cfg, const double *s0, ipc
   }
   // TMA staging for FP32 storage: tile + halo rows for f and g, ring rows
   // (one more on each side) for the S, u_x, u_z planes
+  // TMA staging: FP32 storage with nx % 4 == 0; 16-bit storage with
+  // nx % 8 == 0 and no scalar lattice (with one, the staged 16-bit boxes
+  // beside the float tile leave room for 2 CTAs per SM instead of 4, which
+  // measured slower than register staging)
   P.tma = 0;
-  if (c.storage == IPCU_STORE_F32 && c.nx % 4 == 0) {
-    const int rows = f2d::kTZ + 2 * f2d::halo_z(c.geometry);
+  if ((c.storage == IPCU_STORE_F32 && c.nx % 4 == 0) ||
+      (c.storage != IPCU_STORE_F32 && c.nx % 8 == 0 && c.q_scalar == 0)) {
+    const int rows = f2d::kTZ + 2 * f2d::halo_z(c.geometry), esz = (int)s->esz;
     bool ok = true;
     for (int i = 0; i < 2 && ok; i++) {
-      ok = encode_planes(&P.tm_f[i], s->f[i], c.nx, c.nz, 9, rows) &&
-           encode_planes(&P.tm_m[i], s->mac[i], c.nx, c.nz, 3, rows + 2) &&
-           (c.q_scalar == 0 || encode_planes(&P.tm_g[i], s->g[i], c.nx, c.nz, c.q_scalar, rows));
+      ok = encode_planes(&P.tm_f[i], s->f[i], c.nx, c.nz, 9, rows, esz) &&
+           encode_planes(&P.tm_m[i], s->mac[i], c.nx, c.nz, nmac(s), rows + 2) &&
+           (c.q_scalar == 0 || encode_planes(&P.tm_g[i], s->g[i], c.nx, c.nz, c.q_scalar, rows, esz));
     }
     P.tma = ok ? 1 : 0;
   }
@@ -679,6 +686,19 @@ extern "C" int ipcu_sim_step_graph(ipcu_sim *sim, int64_t nsteps, int32_t chunk)
 }
 
 extern "C" int64_t ipcu_sim_cells(const ipcu_sim *sim) { return sim ? sim->N : 0; }
+
+extern "C" int ipcu_stream_create(ipcu_stream_t *out) {
+  if (!out) return IPCU_ERR_ARG;
+  cudaStream_t s = nullptr;
+  if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) return IPCU_ERR_CUDA;
+  *out = (ipcu_stream_t)s;
+  return IPCU_OK;
+}
+
+extern "C" int ipcu_stream_destroy(ipcu_stream_t stream) {
+  if (!stream) return IPCU_ERR_ARG;
+  return cudaStreamDestroy((cudaStream_t)stream) == cudaSuccess ? IPCU_OK : IPCU_ERR_CUDA;
+}
 
 // ---------------------------------------------------------------------------
 // Moving immersed boundary: one rigid body per simulation (ibm2d.cu).
@@ -1258,13 +1278,13 @@ static int batch_enqueue(ipcu_batch *b, ipcu_sim *const *sims, int n, int64_t ns
   for (int i = 0; i < n; i++) order[i] = i;
   std::stable_sort(order.begin(), order.end(), [&](int a, int c) {
     const ipcu_sim_config &A = sims[a]->cfg, &C = sims[c]->cfg;
-    return std::make_tuple(A.storage, A.q_scalar, A.geometry, A.scalar_kind) <
-           std::make_tuple(C.storage, C.q_scalar, C.geometry, C.scalar_kind);
+    return std::make_tuple(A.storage, A.q_scalar, A.geometry, A.scalar_kind, sims[a]->P.tma) <
+           std::make_tuple(C.storage, C.q_scalar, C.geometry, C.scalar_kind, sims[c]->P.tma);
   });
   std::vector<f2d::Params> hp(n);
   std::vector<f2d::WorkItem> hw;
   std::vector<ib2d::Job> hj;
-  struct Group { int storage, qs, geo, pf, w0, w1, j0, j1; };
+  struct Group { int storage, qs, geo, pf, tma, w0, w1, j0, j1; };
   std::vector<Group> groups;
   for (int oi = 0; oi < n; oi++) {
     ipcu_sim *s = sims[order[oi]];
@@ -1272,9 +1292,9 @@ static int batch_enqueue(ipcu_batch *b, ipcu_sim *const *sims, int n, int64_t ns
     hp[oi].cur = s->cur;
     const ipcu_sim_config &c = s->cfg;
     if (groups.empty() || groups.back().storage != c.storage || groups.back().qs != c.q_scalar ||
-        groups.back().geo != c.geometry || groups.back().pf != c.scalar_kind)
-      groups.push_back({c.storage, c.q_scalar, c.geometry, c.scalar_kind, (int)hw.size(), (int)hw.size(),
-                        (int)hj.size(), (int)hj.size()});
+        groups.back().geo != c.geometry || groups.back().pf != c.scalar_kind || groups.back().tma != s->P.tma)
+      groups.push_back({c.storage, c.q_scalar, c.geometry, c.scalar_kind, s->P.tma, (int)hw.size(),
+                        (int)hw.size(), (int)hj.size(), (int)hj.size()});
     const int tx = (s->nx + f2d::kTX - 1) / f2d::kTX, tz = (s->nz + f2d::kTZ - 1) / f2d::kTZ;
     for (int z = 0; z < tz; z++)
       for (int x = 0; x < tx; x++) hw.push_back({oi, x, z, 0});
@@ -1309,7 +1329,7 @@ static int batch_enqueue(ipcu_batch *b, ipcu_sim *const *sims, int n, int64_t ns
           cudaSuccess)
     return IPCU_ERR_CUDA;
   for (const Group &g : groups) {
-    int st = f2d::launch_batched(nullptr, nullptr, 0, 0, g.storage, g.qs, g.geo, g.pf, 0, b->stream, true);
+    int st = f2d::launch_batched(nullptr, nullptr, 0, 0, g.storage, g.qs, g.geo, g.pf, 0, b->stream, true, g.tma);
     if (st) return st;
   }
   for (int64_t k = 0; k < nsteps; k++) {
@@ -1317,7 +1337,7 @@ static int batch_enqueue(ipcu_batch *b, ipcu_sim *const *sims, int n, int64_t ns
       const int nw = g.w1 - g.w0;
       const int grid = std::min(nw, b->grid_cap);
       int st = f2d::launch_batched(b->d_params, b->d_work + g.w0, nw, (int)(k & 1), g.storage, g.qs, g.geo, g.pf, grid,
-                                   b->stream, false);
+                                   b->stream, false, g.tma != 0);
       if (!st && g.j1 > g.j0)
         st = ib2d::launch_batched(b->d_jobs + g.j0, g.j1 - g.j0, (int)(k & 1), g.storage, g.qs, b->stream);
       if (st) return st;

@@ -26,6 +26,13 @@ from . import _lib
 from .sim import Sim
 
 
+def new_stream():
+    """A dedicated non-blocking CUDA stream (ipcu_stream_create), as an int handle."""
+    h = ctypes.c_void_p()
+    _lib.check(_lib.lib().ipcu_stream_create(ctypes.byref(h)), "ipcu_stream_create")
+    return h.value
+
+
 class Batch:
     """Owner of an ipcu_batch (device parameter array and work list)."""
 
@@ -84,6 +91,7 @@ class Request:
     kwargs: dict = field(default_factory=dict, compare=False)
     s0: np.ndarray = field(default=None, compare=False)
     body: dict = field(default=None, compare=False)  # Sim.attach_ellipse arguments (immersed body)
+    stream: object = field(default=None, compare=False, repr=False)  # the simulation's own CUDA stream
     # filled by the server
     sim: Sim = field(default=None, compare=False, repr=False)
     remaining: int = field(default=0, compare=False)
@@ -113,9 +121,21 @@ def request_bytes(req: Request) -> int:
 
 
 class Server:
-    def __init__(self, budget_bytes=150e9, tick_steps=200, keep_results=("S", "ux", "uz"), stream=None):
+    def __init__(self, budget_bytes=150e9, tick_steps=200, keep_results=("S", "ux", "uz"), stream=None,
+                 admit_per_tick=64):
         """keep_results: macroscopic planes copied back per finished request
-        ("S", "ux", "uz"; "p" too with 16-bit storage)."""
+        ("S", "ux", "uz"; "p" too with 16-bit storage). stream: the batch's
+        CUDA stream handle (default: a new non-blocking stream). Every
+        admitted simulation gets a non-blocking stream of its own, so that
+        its set-up (which synchronises that stream) never waits for the
+        batch in flight. admit_per_tick bounds the set-ups done between two
+        launches, so the GPU starts on the first requests while the host
+        sets up the next ones."""
+        self.admit_per_tick = int(admit_per_tick)
+        self._own_stream = None
+        if stream is None:
+            self._own_stream = new_stream()
+            stream = self._own_stream
         self.budget = float(budget_bytes)
         self.tick_steps = int(tick_steps)
         self.keep = keep_results
@@ -136,9 +156,13 @@ class Server:
 
     def _admit(self, now):
         t0 = time.perf_counter()
-        while self.waiting and self.in_use + request_bytes(self.waiting[0]) <= self.budget:
+        admitted = 0
+        while (self.waiting and admitted < self.admit_per_tick
+               and self.in_use + request_bytes(self.waiting[0]) <= self.budget):
+            admitted += 1
             r = heapq.heappop(self.waiting)
-            r.sim = Sim(r.nx, r.nz, s0=r.s0, stream=self.stream, **r.kwargs)
+            r.stream = new_stream()
+            r.sim = Sim(r.nx, r.nz, s0=r.s0, stream=r.stream, **r.kwargs)
             if r.body is not None:
                 r.sim.attach_ellipse(**r.body)
             r.admitted = now
@@ -204,14 +228,16 @@ class Server:
         for r, buf in retiring:
             r.sim.sync()
             a = buf.numpy()
-            r.result = {k: a[planes[k] * r.cells:(planes[k] + 1) * r.cells].astype(np.float64).reshape(r.nz, r.nx)
-                        for k in self.keep}
+            # FP32 views of the pinned copy (the buffer stays with the result)
+            r.result = {k: a[planes[k] * r.cells:(planes[k] + 1) * r.cells].reshape(r.nz, r.nx) for k in self.keep}
             if r.body is not None:
                 r.result["body"] = r.sim.body()
             r.finished = clock()
             self.in_use -= r.sim.device_bytes()
             r.sim.close()
             r.sim = None
+            _lib.lib().ipcu_stream_destroy(r.stream)  # the frees queued on it still run
+            r.stream = None
             self.done.append(r)
 
     def run(self, requests, clock=time.perf_counter):
@@ -243,7 +269,14 @@ class Server:
         for r in self.active + [r for r, _ in self.retiring]:
             if r.sim is not None:
                 r.sim.close()
+                r.sim = None
+            if r.stream is not None:
+                _lib.lib().ipcu_stream_destroy(r.stream)
+                r.stream = None
         self.batch.close()
+        if self._own_stream is not None:
+            _lib.lib().ipcu_stream_destroy(self._own_stream)
+            self._own_stream = None
 
 
 def lock_exchange_request(rid, nx, nz, steps, arrival=0.0, storage="f16", seed=0):
