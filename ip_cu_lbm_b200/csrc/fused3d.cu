@@ -99,12 +99,16 @@ __global__ void __launch_bounds__(kThreads, 3) step3d_kernel(const __grid_consta
     __syncthreads();
     if (own) {
       const long long i = (long long)z * P + (long long)y * nx + x;
+      // per-cell base pointers: every access below is base + a warp-uniform offset
+      const float *__restrict__ fi = p.f_in + i;
+      const float *__restrict__ gi = p.g_in + i;
+      const float *__restrict__ Fi = p.F_in + i;
       float f[19], g[7];
 #pragma unroll
-      for (int k = 0; k < 19; k++) f[k] = p.f_in[k * N + i];
+      for (int k = 0; k < 19; k++) f[k] = fi[k * N];
 #pragma unroll
-      for (int k = 0; k < 7; k++) g[k] = p.g_in[k * N + i];
-      const float Fpx = p.F_in[i], Fpy = p.F_in[N + i], Fpz = p.F_in[2 * N + i];
+      for (int k = 0; k < 7; k++) g[k] = gi[k * N];
+      const float Fpx = Fi[0], Fpy = Fi[N], Fpz = Fi[2 * N];
       const int s0 = z % 3, sm = (z + 2) % 3, sp = (z + 1) % 3;
       const int lx = tx + 1, ly = ty + 1;
       // moments (ref: collision.cu:238-257): p*, S, u with the previous force
@@ -187,26 +191,30 @@ __global__ void __launch_bounds__(kThreads, 3) step3d_kernel(const __grid_consta
       go[4] = w7(4) * (S - by);
       go[5] = w7(5) * (S + bz);
       go[6] = w7(6) * (S - bz);
-      // push streaming with halfway bounce-back (ref: propagation.cu, set_bound.cu:155-159)
+      // push streaming with halfway bounce-back (ref: propagation.cu, set_bound.cu:155-159):
+      // population k goes to the cell e_k away, or back into this cell's
+      // opposite slot where that cell lies outside the box
+      float *__restrict__ fo_ = p.f_out + i;
+      float *__restrict__ go_ = p.g_out + i;
+      const bool bx0 = x > 0, bx1 = x < nx - 1, by0 = y > 0, by1 = y < ny - 1, bz0 = z > 0, bz1 = z < nz - 1;
+      auto inside = [&](int k) {
+        return (cx(k) > 0 ? bx1 : (cx(k) < 0 ? bx0 : true)) && (cy(k) > 0 ? by1 : (cy(k) < 0 ? by0 : true)) &&
+               (cz(k) > 0 ? bz1 : (cz(k) < 0 ? bz0 : true));
+      };
 #pragma unroll
       for (int k = 0; k < 19; k++) {
-        const int xt = x + cx(k), yt = y + cy(k), zt = z + cz(k);
-        if (xt >= 0 && xt < nx && yt >= 0 && yt < ny && zt >= 0 && zt < nz)
-          p.f_out[k * N + (long long)zt * P + (long long)yt * nx + xt] = fo[k];
-        else
-          p.f_out[opp(k) * N + i] = fo[k];
+        if (inside(k)) fo_[k * N + cz(k) * P + cy(k) * nx + cx(k)] = fo[k];
+        else fo_[opp(k) * N] = fo[k];
       }
 #pragma unroll
       for (int k = 0; k < 7; k++) {
-        const int xt = x + cx(k), yt = y + cy(k), zt = z + cz(k);
-        if (xt >= 0 && xt < nx && yt >= 0 && yt < ny && zt >= 0 && zt < nz)
-          p.g_out[k * N + (long long)zt * P + (long long)yt * nx + xt] = go[k];
-        else
-          p.g_out[opp(k) * N + i] = go[k];
+        if (inside(k)) go_[k * N + cz(k) * P + cy(k) * nx + cx(k)] = go[k];
+        else go_[opp(k) * N] = go[k];
       }
-      p.F_out[i] = Fx;
-      p.F_out[N + i] = Fy;
-      p.F_out[2 * N + i] = Fz;
+      float *__restrict__ Fo = p.F_out + i;
+      Fo[0] = Fx;
+      Fo[N] = Fy;
+      Fo[2 * N] = Fz;
       if (!(isfinite(uc) && isfinite(wc) && isfinite(S) && isfinite(pr))) atomicOr(p.status, 1u);
     }
     __syncthreads();  // the ring slot of z - 1 is overwritten next
