@@ -110,6 +110,16 @@ def measured_traffic(args):
     return d["dram_bytes_per_launch"] if d else None
 
 
+def traffic3d(N):
+    """DRAM bytes per launch of the 3-D step at N cells, scaled from the
+    committed 128^3 ncu capture (profiles/traffic.json), else None."""
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    if not os.path.exists(p):
+        return None
+    d = json.load(open(p)).get("step3d_kernel@128x128x128")
+    return int(d["dram_bytes_per_cell"] * N) if d else None
+
+
 def load_peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -298,8 +308,10 @@ def run_3d(args):
                    "lbm_steps_per_step": inner, "cells": N, "storage": "f32", "parallelism": f"replicas x{world}",
                    "l2": f"inputs ({4 * 29 * N / 1e9:.2f} GB) larger than L2"},
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                     "frac": round(achieved / peak, 4), "traffic": None, "bytes_per_cell": bpc,
-                     "peak_source": f"{peak_src} (MEASURED_PEAKS.json hbm_gbs)" if peak_src == "measured" else peak_src},
+                     "frac": round(achieved / peak, 4), "traffic": traffic3d(N), "bytes_per_cell": bpc,
+                     "peak_source": f"{peak_src} (MEASURED_PEAKS.json hbm_gbs)" if peak_src == "measured" else peak_src,
+                     "traffic_note": "DRAM read+write bytes per launch from the 128^3 ncu capture (profiles/traffic.json), "
+                                     "scaled by cells; it grows in proportion to the cells streamed"},
         "e2e": {"value": round(e2e, 2), "unit": METRIC,
                 "h2d_bytes_per_step": int(4 * (19 + 7 + 3) * N), "d2h_bytes_per_step": int(4 * 7 * N)},
         "gpu_launches": args.steps * inner, "clocks": clk.summary(),

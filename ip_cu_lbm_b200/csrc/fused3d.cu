@@ -67,7 +67,7 @@ constexpr bool check_opp() {
 }
 static_assert(check_opp(), "D3Q19 opposite table");
 
-__global__ void __launch_bounds__(kThreads, 3) step3d_kernel(const __grid_constant__ Params3 p) {
+__global__ void __launch_bounds__(kThreads, 4) step3d_kernel(const __grid_constant__ Params3 p) {
   __shared__ float sS[3][kRY][kRX];
   const int nx = p.nx, ny = p.ny, nz = p.nz;
   const long long N = (long long)nx * ny * nz, P = (long long)nx * ny;
@@ -83,10 +83,10 @@ __global__ void __launch_bounds__(kThreads, 3) step3d_kernel(const __grid_consta
     for (int e = threadIdx.x; e < kRX * kRY; e += kThreads) {
       const int ly = e / kRX, lx = e - ly * kRX;
       const int gx = min(max(x0 - 1 + lx, 0), nx - 1), gy = min(max(y0 - 1 + ly, 0), ny - 1);
-      const long long i = (long long)zc * P + (long long)gy * nx + gx;
+      const float *__restrict__ gp = p.g_in + ((long long)zc * P + (long long)gy * nx + gx);
       float S = 0.f;
 #pragma unroll
-      for (int k = 0; k < 7; k++) S += p.g_in[k * N + i];
+      for (int k = 0; k < 7; k++) S += gp[k * N];
       sS[((z % 3) + 3) % 3][ly][lx] = S;
     }
   };

@@ -83,7 +83,8 @@ extern "C" int ipcu_sim3d_create(const ipcu_sim3d_config *cfg, const double *s0,
   P.nx = c.nx;
   P.ny = c.ny;
   P.nz = c.nz;
-  // z cells per CTA: enough CTAs for several waves of 3 per SM on 148 SMs
+  // z cells per CTA: enough CTAs for several waves on 148 SMs (about 27 z
+  // chunks of 24 at 160 x 160 x 640, measured against 18)
   const long long cols = (long long)((c.nx + 31) / 32) * ((c.ny + 7) / 8);
   P.zchunk = (int)std::max(4LL, std::min<long long>(64, (long long)c.nz * cols / (148LL * 3 * 6)));
   const double cl = c.dz / c.dt;
