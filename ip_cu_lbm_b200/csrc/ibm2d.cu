@@ -18,14 +18,17 @@
 //      body's update is the same whatever runs beside it;
 //   4. u and f_ib go back to HBM (16-bit storage re-expresses the stored
 //      deviations about the new u, so the populations stay as they were).
-//      The tile flags the fluid kernel reads follow the footprint: the new
-//      footprint's tiles are flagged before any write, then the kernel lets
-//      the next fluid step launch (programmatic dependent launch): its
-//      flagged tiles wait for this update, the others run beside it. This
-//      update writes the cells of the previous and the new footprints, so
-//      only the tiles of the footprint two steps back that neither covers
-//      are unflagged (the fluid step that may run beside it needs none of
-//      them);
+//      The tile flags the fluid kernel reads follow the footprint. The
+//      next fluid step may run beside this update (programmatic dependent
+//      launch; the update lets it go at its start): its flagged tiles wait
+//      for the update, the others run on. It needs flags on the previous
+//      and this step's footprints, the cells this update writes; both are
+//      set one update ahead, since each update ends by flagging the
+//      footprint its successor will have (the successor starts from the
+//      body state this one leaves). The first update flags its own
+//      footprint before it lets the fluid step go. Tiles of the footprint
+//      two steps back that none of the previous, current and next
+//      footprints covers are unflagged;
 //   5. FP64 sums: F_ib = sum F_l dS_l, T_ib = sum r_l x F_l dS_l and the
 //      fluid momentum P, angular momentum L inside the body, each cell
 //      weighted by its volume fraction alpha = clamp(1/2 - d/dz, 0, 1), d the
@@ -119,7 +122,8 @@ __device__ void coupled_update(const Job &j, int parity) {
   __shared__ Body B;
   __shared__ int bnd[4];   // window bounds imin, imax, kmin, kmax
   __shared__ int bnd2[4];  // bounds of the footprint two steps back
-  __shared__ uint8_t tmap[kTileMap];  // tiles of the previous and new footprints
+  __shared__ int bnd3[4];  // bounds of the next step's footprint
+  __shared__ uint8_t tmap[kTileMap];  // tiles of the previous, current and next footprints
   __shared__ int nslot, fail;
 
   const f2d::Params &p = j.fp;
@@ -132,8 +136,8 @@ __device__ void coupled_update(const Job &j, int parity) {
 
   if (tid == 0) {
     B = *j.body;
-    bnd[0] = bnd[2] = bnd2[0] = bnd2[2] = INT_MAX;
-    bnd[1] = bnd[3] = bnd2[1] = bnd2[3] = INT_MIN;
+    bnd[0] = bnd[2] = bnd2[0] = bnd2[2] = bnd3[0] = bnd3[2] = INT_MAX;
+    bnd[1] = bnd[3] = bnd2[1] = bnd2[3] = bnd3[1] = bnd3[3] = INT_MIN;
     nslot = 0;
     fail = nl > kMaxMarkers ? 1 : 0;
   }
@@ -142,7 +146,9 @@ __device__ void coupled_update(const Job &j, int parity) {
     if (tid == 0) atomicOr(p.status, 8u);
     return;
   }
-  const bool have_prev = B.have_prev != 0;
+  const bool have_prev = B.have_prev != 0, have_prev2 = B.have_prev2 != 0;
+  // the footprint of this step was flagged by the previous update
+  if (have_prev) asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
   const double cth = cos(B.th), sth = sin(B.th);
 
   // ---- 1. markers: position, velocity, stencil origin and weights
@@ -167,7 +173,7 @@ __device__ void coupled_update(const Job &j, int parity) {
     atomicMax(&bnd[1], i0 + 3);
     atomicMin(&bnd[2], k0);
     atomicMax(&bnd[3], k0 + 3);
-    if (B.have_prev2) {
+    if (have_prev2) {
       const int oi = j.org2[2 * l], ok = j.org2[2 * l + 1];
       atomicMin(&bnd2[0], oi);
       atomicMax(&bnd2[1], oi + 3);
@@ -218,39 +224,26 @@ __device__ void coupled_update(const Job &j, int parity) {
     if (tid == 0) atomicOr(p.status, 8u);
     return;
   }
-  // flags: the new footprint's tiles go up before anything is written; tmap
-  // marks the tiles of the previous and new footprints for the clean-up
-  const int ibtx = p.ibtx;
-  const int tx0 = max(min(wi0, bnd2[0]) - kHalo, 0) / f2d::kTX, tz0 = max(min(wk0, bnd2[2]) - kHalo, 0) / f2d::kTZ;
-  const int tmw = min(max(wi0 + WW - 1, bnd2[1]) + kHalo, nx - 1) / f2d::kTX - tx0 + 1;
-  const int tmh = min(max(wk0 + WH - 1, bnd2[3]) + kHalo, nz - 1) / f2d::kTZ - tz0 + 1;
-  const bool tmap_ok = tmw > 0 && tmh > 0 && tmw * tmh <= kTileMap;
-  if (tmap_ok)
-    for (int e = tid; e < tmw * tmh; e += kThreads) tmap[e] = 0;
-  __syncthreads();
   // tiles whose halo may reach a marker's 4x4 stencil: the stencil widened
   // by the margin spans at most two tiles per axis, those of its ends
+  const int ibtx = p.ibtx;
   auto corners = [&](int i0, int k0, int (&tx)[2], int (&tz)[2]) {
     tx[0] = min(max(i0 - kHalo, 0), nx - 1) / f2d::kTX;
     tx[1] = min(max(i0 + 3 + kHalo, 0), nx - 1) / f2d::kTX;
     tz[0] = min(max(k0 - kHalo, 0), nz - 1) / f2d::kTZ;
     tz[1] = min(max(k0 + 3 + kHalo, 0), nz - 1) / f2d::kTZ;
   };
-  for (int e = tid; e < nl * (have_prev ? 2 : 1); e += kThreads) {
-    const bool old = e >= nl;
-    const int l = old ? e - nl : e;
-    int tx[2], tz[2];
-    corners(old ? j.org[2 * l] : sI0[l], old ? j.org[2 * l + 1] : sK0[l], tx, tz);
+  if (!have_prev) {  // the first update flags its own footprint before the next fluid step may start
+    for (int l = tid; l < nl; l += kThreads) {
+      int tx[2], tz[2];
+      corners(sI0[l], sK0[l], tx, tz);
 #pragma unroll
-    for (int c = 0; c < 4; c++) {
-      const int x = tx[c & 1], z = tz[c >> 1];
-      if (!old) j.flag[z * ibtx + x] = 1;
-      if (tmap_ok) tmap[(z - tz0) * tmw + (x - tx0)] = 1;
+      for (int c = 0; c < 4; c++) j.flag[tz[c >> 1] * ibtx + tx[c & 1]] = 1;
     }
+    __threadfence();
+    __syncthreads();
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
   }
-  __threadfence();
-  __syncthreads();
-  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
   const float rho0 = p.rho_base, rsal = p.rho_sal_f, hdt = p.hdt;
   for (int s = tid; s < ns; s += kThreads) {
     const long long ci = sCell[s];
@@ -418,19 +411,6 @@ __device__ void coupled_update(const Job &j, int parity) {
     j.fext[N + ci] = sFZ[s];
     if (!(isfinite(un) && isfinite(wn))) atomicOr(p.status, 1u);
   }
-  // tiles of the footprint two steps back that neither the previous nor the
-  // new footprint covers: no fluid step needs to wait there any more
-  if (B.have_prev2 && tmap_ok) {
-    for (int l = tid; l < nl; l += kThreads) {
-      int tx[2], tz[2];
-      corners(j.org2[2 * l], j.org2[2 * l + 1], tx, tz);
-#pragma unroll
-      for (int c = 0; c < 4; c++) {
-        const int x = tx[c & 1], z = tz[c >> 1];
-        if (!tmap[(z - tz0) * tmw + (x - tx0)]) j.flag[z * ibtx + x] = 0;
-      }
-    }
-  }
   __syncthreads();
 
   // ---- 5. FP64 sums: marker force and torque, fluid momentum inside the body
@@ -442,10 +422,6 @@ __device__ void coupled_update(const Job &j, int parity) {
     acc[0] += fx;
     acc[1] += fz;
     acc[2] += rx * fz - rz * fx;
-    j.org2[2 * l] = j.org[2 * l];  // the footprints move back one step
-    j.org2[2 * l + 1] = j.org[2 * l + 1];
-    j.org[2 * l] = sI0[l];
-    j.org[2 * l + 1] = sK0[l];
   }
   {
     const double a = j.semi_a, bb = j.semi_b, ra = 1.0 / a, rb = 1.0 / bb;
@@ -512,6 +488,71 @@ __device__ void coupled_update(const Job &j, int parity) {
     nb.have_prev2 = B.have_prev;
     nb.have_prev = 1;
     *j.body = nb;
+    B = nb;
+  }
+  __syncthreads();
+
+  // ---- 7. flags for the next step's footprint (from the body state just
+  // written, as the next update will compute it), clean-up two steps back,
+  // and the footprints move back one step
+  int *sPI = reinterpret_cast<int *>(sUB);  // predicted stencil origins [nl][2]
+  {
+    const double c2 = cos(B.th), s2 = sin(B.th);
+    for (int l = tid; l < nl; l += kThreads) {
+      const double x0 = j.X0[2 * l], z0 = j.X0[2 * l + 1];
+      const double X = B.X[0] + (c2 * x0 - s2 * z0), Z = B.X[1] + (s2 * x0 + c2 * z0);
+      const int pi = (int)floor(X * idz - 0.5) - 1, pk = (int)floor(Z * idz - 0.5) - 1;
+      sPI[2 * l] = pi;
+      sPI[2 * l + 1] = pk;
+      atomicMin(&bnd3[0], pi);
+      atomicMax(&bnd3[1], pi + 3);
+      atomicMin(&bnd3[2], pk);
+      atomicMax(&bnd3[3], pk + 3);
+    }
+  }
+  __syncthreads();
+  const int lo_i = min(min(wi0, bnd2[0]), bnd3[0]), hi_i = max(max(wi0 + WW - 1, bnd2[1]), bnd3[1]);
+  const int lo_k = min(min(wk0, bnd2[2]), bnd3[2]), hi_k = max(max(wk0 + WH - 1, bnd2[3]), bnd3[3]);
+  const int tx0 = min(max(lo_i - kHalo, 0), nx - 1) / f2d::kTX, tz0 = min(max(lo_k - kHalo, 0), nz - 1) / f2d::kTZ;
+  const int tmw = min(max(hi_i + kHalo, 0), nx - 1) / f2d::kTX - tx0 + 1;
+  const int tmh = min(max(hi_k + kHalo, 0), nz - 1) / f2d::kTZ - tz0 + 1;
+  const bool tmap_ok = tmw > 0 && tmh > 0 && tmw * tmh <= kTileMap;
+  if (tmap_ok)
+    for (int e = tid; e < tmw * tmh; e += kThreads) tmap[e] = 0;
+  __syncthreads();
+  // previous, current and next footprints: kept (the next one flagged now)
+  for (int e = tid; e < 3 * nl; e += kThreads) {
+    const int which = e / nl, l = e - which * nl;
+    if (which == 0 && !have_prev) continue;
+    const int i0 = which == 0 ? j.org[2 * l] : (which == 1 ? sI0[l] : sPI[2 * l]);
+    const int k0 = which == 0 ? j.org[2 * l + 1] : (which == 1 ? sK0[l] : sPI[2 * l + 1]);
+    int tx[2], tz[2];
+    corners(i0, k0, tx, tz);
+#pragma unroll
+    for (int c = 0; c < 4; c++) {
+      const int x = tx[c & 1], z = tz[c >> 1];
+      if (which == 2) j.flag[z * ibtx + x] = 1;
+      if (tmap_ok) tmap[(z - tz0) * tmw + (x - tx0)] = 1;
+    }
+  }
+  __syncthreads();
+  if (have_prev2 && tmap_ok) {
+    for (int l = tid; l < nl; l += kThreads) {
+      int tx[2], tz[2];
+      corners(j.org2[2 * l], j.org2[2 * l + 1], tx, tz);
+#pragma unroll
+      for (int c = 0; c < 4; c++) {
+        const int x = tx[c & 1], z = tz[c >> 1];
+        if (!tmap[(z - tz0) * tmw + (x - tx0)]) j.flag[z * ibtx + x] = 0;
+      }
+    }
+  }
+  __syncthreads();
+  for (int l = tid; l < nl; l += kThreads) {
+    j.org2[2 * l] = j.org[2 * l];
+    j.org2[2 * l + 1] = j.org[2 * l + 1];
+    j.org[2 * l] = sI0[l];
+    j.org[2 * l + 1] = sK0[l];
   }
 }
 
