@@ -88,7 +88,7 @@ struct Geo {
 // Cells next to a wall are queued in shared memory and processed after the
 // interior cells by a compacted set of threads (up to kQueue per tile; more
 // are processed in place). At the C2 size a tile has at most ~80 of them.
-constexpr int kQueue = 127;
+constexpr int kQueue = 111;
 
 // Shared-memory layout in floats; TMA destinations start on 128-byte boundaries.
 // SB: bytes of a stored population. TMA staging of 16-bit storage lands the
@@ -106,7 +106,8 @@ struct Smem {
   static constexpr int F0 = S0 + (TMA ? (H16 ? 4 : 3) : 1) * G::SZ * G::RX;  // registers: interior force
   static constexpr int W0 = F0 + (TMA ? 0 : 2 * kTX * kTZ);      // axis weights
   static constexpr int C0 = W0 + 2 * G::WREC * G::NWA;            // combined interior weights
-  static constexpr int B0 = al(C0 + 2 * (G::NS + 1) * G::NWA, 2);  // mbarrier
+  static constexpr int GI0 = C0 + 2 * (G::NS + 1) * G::NWA;       // density-gradient factors of the rows [EZ]
+  static constexpr int B0 = al(GI0 + G::EZ, 2);                     // mbarrier
   static constexpr int Q0 = B0 + 4;                                // wall-cell queue: count + kQueue slots
   static constexpr int E16 = G::EZ * kTmaBoxX16;                   // 16-bit values per staged plane
   static constexpr int H0 = al(Q0 + 1 + kQueue, 32);               // 16-bit staging: f planes, then g
@@ -225,6 +226,7 @@ __device__ __forceinline__ void step_tile(const Params &p, int parity, int tile_
   float *sF = smem + SL::F0;   // registers: [2][kTZ][kTX] interior force
   float *sW = smem + SL::W0;   // [2][WREC][NWA] axis weights
   float *sC = smem + SL::C0;   // [2][NS+1][NWA] combined interior weights
+  float *sGI = smem + SL::GI0;  // gradient factors of the tile's rows [EZ]
   uint64_t *bar = reinterpret_cast<uint64_t *>(smem + SL::B0);
   int *qcount = reinterpret_cast<int *>(smem + SL::Q0), *queue = qcount + 1;
 
@@ -284,6 +286,13 @@ __device__ __forceinline__ void step_tile(const Params &p, int parity, int tile_
       const int gx = min(max(ox - RO + lx, 0), nx - 1), gz = min(max(oz - 1 + lz, 0), nz - 1);
       sS[e] = mac_in[(long long)gz * nx + gx];
     }
+  }
+  // the density-gradient factors 1/(z_{k+1} - z_{k-1} + dz/1000) of the
+  // tile's rows, so the collision reads no table from memory (an evenly
+  // spaced x axis uses its three constants, a stretched one its table)
+  for (int e = tid; e < G::EZ; e += kThreads) {
+    const int gz = min(max(oz + e, 0), nz - 1);
+    sGI[e] = (p.gconst & 2) ? (gz == 0 ? p.giz3[0] : (gz == nz - 1 ? p.giz3[2] : p.giz3[1])) : __ldg(p.ginvz + gz);
   }
   if constexpr (G::AX >= 0) {
     const int NA = (G::AX == 0) ? nx : nz, oA = (G::AX == 0) ? ox : oz;
@@ -377,8 +386,7 @@ __device__ __forceinline__ void step_tile(const Params &p, int parity, int tile_
     const float pc = pr * c2 / 3.0f;
     const float gix = (p.gconst & 1) ? (gx == 0 ? p.gix3[0] : (gx == nx - 1 ? p.gix3[2] : p.gix3[1]))
                                      : __ldg(p.ginvx + gx);
-    const float giz = (p.gconst & 2) ? (gz == 0 ? p.giz3[0] : (gz == nz - 1 ? p.giz3[2] : p.giz3[1]))
-                                     : __ldg(p.ginvz + gz);
+    const float giz = sGI[lz];
     float Fx = -pc * ((rho_of(sS[rs + 1]) - rho_of(sS[rs - 1])) * gix);
     float Fz = -pc * ((rho_of(sS[rs + RX]) - rho_of(sS[rs - RX])) * giz);
     float dpx = 0.f, dpz = 0.f;  // grad(phi) (phase field)
