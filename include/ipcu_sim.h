@@ -147,6 +147,11 @@ int ipcu_batch_step(ipcu_batch *batch, ipcu_sim *const *sims, int n, int64_t nst
  * see the results; ipcu_batch_sync waits for everything enqueued. A server
  * admits new requests on the host while the GPU runs the batch. */
 int ipcu_batch_launch(ipcu_batch *batch, ipcu_sim *const *sims, int n, int64_t nsteps);
+/* The same with a step count per simulation (nsteps[i] >= 0; 0 leaves it
+ * out): the simulations still stepping at each step share one launch per
+ * kernel class, so a server advances every admitted request to its own end
+ * of the tick with one call. */
+int ipcu_batch_launch_each(ipcu_batch *batch, ipcu_sim *const *sims, const int64_t *nsteps, int n);
 int ipcu_batch_sync(ipcu_batch *batch);
 /* Progress marks: ipcu_batch_mark records the point reached by everything
  * enqueued so far and returns its handle (a ring of 4); ipcu_batch_wait_mark

@@ -138,6 +138,7 @@ def _declare(L: ctypes.CDLL) -> None:
         "ipcu_batch_destroy": ([P], None),
         "ipcu_batch_step": ([P, P, I, I64], I),
         "ipcu_batch_launch": ([P, P, I, I64], I),
+        "ipcu_batch_launch_each": ([P, P, P, I], I),
         "ipcu_batch_sync": ([P], I),
         "ipcu_batch_mark": ([P], I),
         "ipcu_batch_wait_mark": ([P, I], I),

@@ -8,7 +8,7 @@ namespace f2d {
 
 #define IPCU_F2D_DECL(NAME)                                                                        \
   int launch_##NAME(const Params &p, int qs, int geo, cudaStream_t s, bool prep);                  \
-  int launch_batched_##NAME(const Params *, const WorkItem *, int, int, int, int, int, cudaStream_t, bool, bool);
+  int launch_batched_##NAME(const Params *, const WorkItem *, int, int, int, int, int, cudaStream_t, bool, bool, bool);
 IPCU_F2D_DECL(f32)
 IPCU_F2D_DECL(f16)
 IPCU_F2D_DECL(bf16)
@@ -18,17 +18,17 @@ IPCU_F2D_DECL(pf_bf16)
 #undef IPCU_F2D_DECL
 
 int launch_batched(const Params *ps, const WorkItem *work, int nwork, int parity, int storage, int qs, int geo,
-                   int pf, int grid, cudaStream_t s, bool prep, bool tma) {
+                   int pf, int grid, cudaStream_t s, bool prep, bool tma, bool pdl) {
   switch (storage) {
     case IPCU_STORE_F32:
-      return pf ? launch_batched_pf_f32(ps, work, nwork, parity, qs, geo, grid, s, prep, tma)
-                : launch_batched_f32(ps, work, nwork, parity, qs, geo, grid, s, prep, tma);
+      return pf ? launch_batched_pf_f32(ps, work, nwork, parity, qs, geo, grid, s, prep, tma, pdl)
+                : launch_batched_f32(ps, work, nwork, parity, qs, geo, grid, s, prep, tma, pdl);
     case IPCU_STORE_F16:
-      return pf ? launch_batched_pf_f16(ps, work, nwork, parity, qs, geo, grid, s, prep, tma)
-                : launch_batched_f16(ps, work, nwork, parity, qs, geo, grid, s, prep, tma);
+      return pf ? launch_batched_pf_f16(ps, work, nwork, parity, qs, geo, grid, s, prep, tma, pdl)
+                : launch_batched_f16(ps, work, nwork, parity, qs, geo, grid, s, prep, tma, pdl);
     case IPCU_STORE_BF16:
-      return pf ? launch_batched_pf_bf16(ps, work, nwork, parity, qs, geo, grid, s, prep, tma)
-                : launch_batched_bf16(ps, work, nwork, parity, qs, geo, grid, s, prep, tma);
+      return pf ? launch_batched_pf_bf16(ps, work, nwork, parity, qs, geo, grid, s, prep, tma, pdl)
+                : launch_batched_bf16(ps, work, nwork, parity, qs, geo, grid, s, prep, tma, pdl);
   }
   return IPCU_ERR_UNSUPPORTED;
 }

@@ -87,9 +87,12 @@ struct WorkItem {
 // scalar lattice and geometry) by one step; `params` and `work` are device
 // arrays; `parity` flips the ping-pong buffers of all of them. `grid` CTAs
 // loop over the work list. tma: every one of them has tensor maps (staged
-// with TMA box loads, the maps read from `params`).
+// with TMA box loads, the maps read from `params`). pdl: launched as a
+// programmatic dependent of the previous launch, a batch of body updates
+// (ib2d::launch_batched): the tiles those bodies flagged wait for it, the
+// rest of the work list runs beside it.
 int launch_batched(const Params *params, const WorkItem *work, int nwork, int parity, int storage, int qs, int geo,
-                   int pf, int grid, cudaStream_t s, bool prepare_only, bool tma);
+                   int pf, int grid, cudaStream_t s, bool prepare_only, bool tma, bool pdl = false);
 
 }  // namespace f2d
 }  // namespace ipcu

@@ -779,41 +779,10 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
     step_tile<ST, QS, GEO, TMA, PHYS>(sp, parity, w.tx, w.tz, smem, ps[w.sim].tm_f);
     __syncthreads();  // the next item reuses shared memory
   }
-}
-
-template <class ST, int QS, int GEO, bool TMA, int PHYS>
-int launch_b1(const Params *ps, const WorkItem *work, int nwork, int parity, int grid, cudaStream_t s, bool prep) {
-  constexpr size_t sm = smem_bytes<QS, GEO, TMA, (int)sizeof(ST)>();
-  if (prep)
-    return status_from_cuda(cudaFuncSetAttribute(step_kernel_batched<ST, QS, GEO, TMA, PHYS>,
-                                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-  if (nwork <= 0) return IPCU_OK;
-  step_kernel_batched<ST, QS, GEO, TMA, PHYS><<<grid, kThreads, sm, s>>>(ps, work, nwork, parity);
-  return status_from_cuda(cudaGetLastError());
-}
-// tma: every simulation of the launch has tensor maps
-template <class ST, int QS, int GEO, int PHYS>
-int launch_b(const Params *ps, const WorkItem *work, int nwork, int parity, int grid, cudaStream_t s, bool prep,
-             bool tma) {
-  if (prep) {
-    const int st = launch_b1<ST, QS, GEO, false, PHYS>(ps, work, nwork, parity, grid, s, true);
-    return st ? st : launch_b1<ST, QS, GEO, true, PHYS>(ps, work, nwork, parity, grid, s, true);
-  }
-  if (tma) return launch_b1<ST, QS, GEO, true, PHYS>(ps, work, nwork, parity, grid, s, false);
-  return launch_b1<ST, QS, GEO, false, PHYS>(ps, work, nwork, parity, grid, s, false);
-}
-
-template <class ST, int QS, int PHYS>
-int launch_bg(const Params *ps, const WorkItem *work, int nwork, int parity, int geo, int grid, cudaStream_t s,
-              bool prep, bool tma) {
-  switch (geo) {
-    case IPCU_GEO_UNIFORM: return launch_b<ST, QS, IPCU_GEO_UNIFORM, PHYS>(ps, work, nwork, parity, grid, s, prep, tma);
-    case IPCU_GEO_X5: return launch_b<ST, QS, IPCU_GEO_X5, PHYS>(ps, work, nwork, parity, grid, s, prep, tma);
-    case IPCU_GEO_X3: return launch_b<ST, QS, IPCU_GEO_X3, PHYS>(ps, work, nwork, parity, grid, s, prep, tma);
-    case IPCU_GEO_Z5: return launch_b<ST, QS, IPCU_GEO_Z5, PHYS>(ps, work, nwork, parity, grid, s, prep, tma);
-    case IPCU_GEO_Z3: return launch_b<ST, QS, IPCU_GEO_Z3, PHYS>(ps, work, nwork, parity, grid, s, prep, tma);
-  }
-  return IPCU_ERR_UNSUPPORTED;
+  // Launched as a programmatic dependent of a batch of body updates, the
+  // kernel ends only after them, so that whatever follows it on the stream
+  // follows them too (a no-op after a plain launch).
+  asm volatile("griddepcontrol.wait;" ::: "memory");
 }
 
 // Launch that may begin while the previous kernel on the stream (a body's
@@ -831,6 +800,45 @@ int launch_pdl(K kernel, dim3 grid, size_t smem, cudaStream_t s, A... args) {
   cfg.attrs = at;
   cfg.numAttrs = 1;
   return status_from_cuda(cudaLaunchKernelEx(&cfg, kernel, args...));
+}
+
+// pdl: the previous launch on the stream is a batch of body updates, which
+// the flagged tiles wait for (griddepcontrol.wait) while the rest run.
+template <class ST, int QS, int GEO, bool TMA, int PHYS>
+int launch_b1(const Params *ps, const WorkItem *work, int nwork, int parity, int grid, cudaStream_t s, bool prep,
+              bool pdl) {
+  constexpr size_t sm = smem_bytes<QS, GEO, TMA, (int)sizeof(ST)>();
+  if (prep)
+    return status_from_cuda(cudaFuncSetAttribute(step_kernel_batched<ST, QS, GEO, TMA, PHYS>,
+                                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  if (nwork <= 0) return IPCU_OK;
+  if (pdl) return launch_pdl(step_kernel_batched<ST, QS, GEO, TMA, PHYS>, dim3(grid), sm, s, ps, work, nwork, parity);
+  step_kernel_batched<ST, QS, GEO, TMA, PHYS><<<grid, kThreads, sm, s>>>(ps, work, nwork, parity);
+  return status_from_cuda(cudaGetLastError());
+}
+// tma: every simulation of the launch has tensor maps
+template <class ST, int QS, int GEO, int PHYS>
+int launch_b(const Params *ps, const WorkItem *work, int nwork, int parity, int grid, cudaStream_t s, bool prep,
+             bool tma, bool pdl) {
+  if (prep) {
+    const int st = launch_b1<ST, QS, GEO, false, PHYS>(ps, work, nwork, parity, grid, s, true, false);
+    return st ? st : launch_b1<ST, QS, GEO, true, PHYS>(ps, work, nwork, parity, grid, s, true, false);
+  }
+  if (tma) return launch_b1<ST, QS, GEO, true, PHYS>(ps, work, nwork, parity, grid, s, false, pdl);
+  return launch_b1<ST, QS, GEO, false, PHYS>(ps, work, nwork, parity, grid, s, false, pdl);
+}
+
+template <class ST, int QS, int PHYS>
+int launch_bg(const Params *ps, const WorkItem *work, int nwork, int parity, int geo, int grid, cudaStream_t s,
+              bool prep, bool tma, bool pdl) {
+  switch (geo) {
+    case IPCU_GEO_UNIFORM: return launch_b<ST, QS, IPCU_GEO_UNIFORM, PHYS>(ps, work, nwork, parity, grid, s, prep, tma, pdl);
+    case IPCU_GEO_X5: return launch_b<ST, QS, IPCU_GEO_X5, PHYS>(ps, work, nwork, parity, grid, s, prep, tma, pdl);
+    case IPCU_GEO_X3: return launch_b<ST, QS, IPCU_GEO_X3, PHYS>(ps, work, nwork, parity, grid, s, prep, tma, pdl);
+    case IPCU_GEO_Z5: return launch_b<ST, QS, IPCU_GEO_Z5, PHYS>(ps, work, nwork, parity, grid, s, prep, tma, pdl);
+    case IPCU_GEO_Z3: return launch_b<ST, QS, IPCU_GEO_Z3, PHYS>(ps, work, nwork, parity, grid, s, prep, tma, pdl);
+  }
+  return IPCU_ERR_UNSUPPORTED;
 }
 
 template <class ST, int QS, int GEO, bool TMA, int PHYS>
@@ -879,13 +887,13 @@ int launch_q(const Params &p, int qs, int geo, cudaStream_t s, bool prep) {
 }
 template <class ST, int PHYS>
 int launch_bq(const Params *ps, const WorkItem *work, int nwork, int parity, int qs, int geo, int grid,
-              cudaStream_t s, bool prep, bool tma) {
+              cudaStream_t s, bool prep, bool tma, bool pdl) {
   if (qs == 0) {
-    if constexpr (PHYS == 0) return launch_bg<ST, 0, 0>(ps, work, nwork, parity, geo, grid, s, prep, tma);
+    if constexpr (PHYS == 0) return launch_bg<ST, 0, 0>(ps, work, nwork, parity, geo, grid, s, prep, tma, pdl);
     return IPCU_ERR_UNSUPPORTED;
   }
-  if (qs == 5) return launch_bg<ST, 5, PHYS>(ps, work, nwork, parity, geo, grid, s, prep, tma);
-  if (qs == 9) return launch_bg<ST, 9, PHYS>(ps, work, nwork, parity, geo, grid, s, prep, tma);
+  if (qs == 5) return launch_bg<ST, 5, PHYS>(ps, work, nwork, parity, geo, grid, s, prep, tma, pdl);
+  if (qs == 9) return launch_bg<ST, 9, PHYS>(ps, work, nwork, parity, geo, grid, s, prep, tma, pdl);
   return IPCU_ERR_UNSUPPORTED;
 }
 #define IPCU_F2D_INSTANTIATE(ST, NAME, PHYS)                                                              \
@@ -893,8 +901,8 @@ int launch_bq(const Params *ps, const WorkItem *work, int nwork, int parity, int
     return launch_q<ST, PHYS>(p, qs, geo, s, prep);                                                       \
   }                                                                                                       \
   int launch_batched_##NAME(const Params *ps, const WorkItem *work, int nwork, int parity, int qs, int geo, \
-                            int grid, cudaStream_t s, bool prep, bool tma) {                              \
-    return launch_bq<ST, PHYS>(ps, work, nwork, parity, qs, geo, grid, s, prep, tma);                     \
+                            int grid, cudaStream_t s, bool prep, bool tma, bool pdl) {                    \
+    return launch_bq<ST, PHYS>(ps, work, nwork, parity, qs, geo, grid, s, prep, tma, pdl);                \
   }
 
 }  // namespace f2d

@@ -1260,50 +1260,72 @@ extern "C" void ipcu_batch_destroy(ipcu_batch *b) {
   delete b;
 }
 
-// Enqueues nsteps batched steps on the batch stream and orders every listed
-// simulation's own stream after them (event wait), so that later work on a
-// simulation -- reads, more steps, destruction -- sees the results.
-static int batch_enqueue(ipcu_batch *b, ipcu_sim *const *sims, int n, int64_t nsteps) {
-  if (!b || (n > 0 && !sims) || nsteps < 0) return IPCU_ERR_ARG;
-  if (n == 0 || nsteps == 0) return IPCU_OK;
+// Enqueues batched steps on the batch stream -- simulation i advances by
+// nsteps[i] -- and orders every listed simulation's own stream after them
+// (event wait), so that later work on a simulation -- reads, more steps,
+// destruction -- sees the results.
+//
+// Within each kernel class the simulations are laid out by decreasing step
+// count, so the ones still stepping at step k own a prefix of the class's
+// work list (and of its bodies): one launch per class per step, its grid the
+// prefix, however ragged the counts. Classes with bodies go first, each
+// fluid launch right after a batch of body updates is a programmatic
+// dependent of it (only the tiles the bodies flagged wait), and a class
+// without bodies follows one with bodies, so their fluid step runs beside
+// the body updates.
+static int batch_enqueue(ipcu_batch *b, ipcu_sim *const *sims, int n, const int64_t *nsteps) {
+  if (!b || (n > 0 && (!sims || !nsteps))) return IPCU_ERR_ARG;
+  std::vector<int> order;
+  int64_t kmax = 0;
   for (int i = 0; i < n; i++) {
-    if (!sims[i]) return IPCU_ERR_ARG;
+    if (!sims[i] || nsteps[i] < 0) return IPCU_ERR_ARG;
+    if (nsteps[i] == 0) continue;
+    order.push_back(i);
+    kmax = std::max(kmax, nsteps[i]);
+  }
+  if (order.empty()) return IPCU_OK;
+  for (int i : order) {
     // the batch stream waits (on the device) for the simulation's own work
     if (cudaEventRecord(sims[i]->ready, sims[i]->stream) != cudaSuccess ||
         cudaStreamWaitEvent(b->stream, sims[i]->ready, 0) != cudaSuccess)
       return IPCU_ERR_CUDA;
   }
-  // group by kernel class, keeping order
-  std::vector<int> order(n);
-  for (int i = 0; i < n; i++) order[i] = i;
+  // group by (bodies first, kernel class), then by decreasing step count
+  auto key = [&](int a) {
+    const ipcu_sim_config &A = sims[a]->cfg;
+    return std::make_tuple(sims[a]->ib == nullptr, A.storage, A.q_scalar, A.geometry, A.scalar_kind, sims[a]->P.tma);
+  };
   std::stable_sort(order.begin(), order.end(), [&](int a, int c) {
-    const ipcu_sim_config &A = sims[a]->cfg, &C = sims[c]->cfg;
-    return std::make_tuple(A.storage, A.q_scalar, A.geometry, A.scalar_kind, sims[a]->P.tma) <
-           std::make_tuple(C.storage, C.q_scalar, C.geometry, C.scalar_kind, sims[c]->P.tma);
+    const auto ka = key(a), kc = key(c);
+    return ka < kc || (ka == kc && nsteps[a] > nsteps[c]);
   });
-  std::vector<f2d::Params> hp(n);
+  const int m = (int)order.size();
+  std::vector<f2d::Params> hp(m);
   std::vector<f2d::WorkItem> hw;
   std::vector<ib2d::Job> hj;
-  struct Group { int storage, qs, geo, pf, tma, w0, w1, j0, j1; };
+  // per class: its simulations' end offsets in the work and body lists,
+  // with their step counts (decreasing)
+  struct Member { int64_t steps; int w1, j1; };
+  struct Group { int storage, qs, geo, pf, tma, w0, j0; std::vector<Member> mem; size_t live; };
   std::vector<Group> groups;
-  for (int oi = 0; oi < n; oi++) {
+  for (int oi = 0; oi < m; oi++) {
     ipcu_sim *s = sims[order[oi]];
     hp[oi] = s->P;
     hp[oi].cur = s->cur;
     const ipcu_sim_config &c = s->cfg;
-    if (groups.empty() || groups.back().storage != c.storage || groups.back().qs != c.q_scalar ||
-        groups.back().geo != c.geometry || groups.back().pf != c.scalar_kind || groups.back().tma != s->P.tma)
-      groups.push_back({c.storage, c.q_scalar, c.geometry, c.scalar_kind, s->P.tma, (int)hw.size(),
-                        (int)hw.size(), (int)hj.size(), (int)hj.size()});
+    if (oi == 0 || key(order[oi]) != key(order[oi - 1]))
+      groups.push_back({c.storage, c.q_scalar, c.geometry, c.scalar_kind, s->P.tma, (int)hw.size(), (int)hj.size(),
+                        {}, 0});
     const int tx = (s->nx + f2d::kTX - 1) / f2d::kTX, tz = (s->nz + f2d::kTZ - 1) / f2d::kTZ;
     for (int z = 0; z < tz; z++)
       for (int x = 0; x < tx; x++) hw.push_back({oi, x, z, 0});
-    groups.back().w1 = (int)hw.size();
     if (s->ib) {
       hj.push_back(*s->ib);
       hj.back().fp = hp[oi];
-      groups.back().j1 = (int)hj.size();
     }
+    Group &g = groups.back();
+    g.mem.push_back({nsteps[order[oi]], (int)hw.size(), (int)hj.size()});
+    g.live = g.mem.size();
   }
   if (hp.size() > b->cap_params) {
     cudaFree(b->d_params);
@@ -1332,33 +1354,50 @@ static int batch_enqueue(ipcu_batch *b, ipcu_sim *const *sims, int n, int64_t ns
     int st = f2d::launch_batched(nullptr, nullptr, 0, 0, g.storage, g.qs, g.geo, g.pf, 0, b->stream, true, g.tma);
     if (st) return st;
   }
-  for (int64_t k = 0; k < nsteps; k++) {
-    for (const Group &g : groups) {
-      const int nw = g.w1 - g.w0;
+  bool after_bodies = false;  // the last launch on the stream is a batch of body updates
+  for (int64_t k = 0; k < kmax; k++) {
+    for (Group &g : groups) {
+      while (g.live > 0 && g.mem[g.live - 1].steps <= k) g.live--;  // members done after k steps
+      if (g.live == 0) continue;
+      const int nw = g.mem[g.live - 1].w1 - g.w0, nj = g.mem[g.live - 1].j1 - g.j0;
       const int grid = std::min(nw, b->grid_cap);
       int st = f2d::launch_batched(b->d_params, b->d_work + g.w0, nw, (int)(k & 1), g.storage, g.qs, g.geo, g.pf, grid,
-                                   b->stream, false, g.tma != 0);
-      if (!st && g.j1 > g.j0)
-        st = ib2d::launch_batched(b->d_jobs + g.j0, g.j1 - g.j0, (int)(k & 1), g.storage, g.qs, b->stream);
+                                   b->stream, false, g.tma != 0, after_bodies);
+      after_bodies = false;
+      if (!st && nj > 0) {
+        st = ib2d::launch_batched(b->d_jobs + g.j0, nj, (int)(k & 1), g.storage, g.qs, b->stream);
+        after_bodies = true;
+      }
       if (st) return st;
     }
   }
   if (cudaEventRecord(b->done, b->stream) != cudaSuccess) return IPCU_ERR_CUDA;
-  for (int i = 0; i < n; i++) {
+  for (int i : order) {
     if (cudaStreamWaitEvent(sims[i]->stream, b->done, 0) != cudaSuccess) return IPCU_ERR_CUDA;
-    sims[i]->cur ^= (int)(nsteps & 1);
-    sims[i]->steps += nsteps;
+    sims[i]->cur ^= (int)(nsteps[i] & 1);
+    sims[i]->steps += nsteps[i];
   }
   return IPCU_OK;
 }
 
+static int batch_enqueue_all(ipcu_batch *b, ipcu_sim *const *sims, int n, int64_t nsteps) {
+  if (!b || n < 0 || (n > 0 && !sims) || nsteps < 0) return IPCU_ERR_ARG;
+  const std::vector<int64_t> each((size_t)n, nsteps);
+  return batch_enqueue(b, sims, n, each.data());
+}
+
 extern "C" int ipcu_batch_step(ipcu_batch *b, ipcu_sim *const *sims, int n, int64_t nsteps) {
-  const int st = batch_enqueue(b, sims, n, nsteps);
+  const int st = batch_enqueue_all(b, sims, n, nsteps);
   if (st != IPCU_OK || n == 0 || nsteps == 0) return st;
   return cudaStreamSynchronize(b->stream) == cudaSuccess ? IPCU_OK : IPCU_ERR_CUDA;
 }
 
 extern "C" int ipcu_batch_launch(ipcu_batch *b, ipcu_sim *const *sims, int n, int64_t nsteps) {
+  return batch_enqueue_all(b, sims, n, nsteps);
+}
+
+extern "C" int ipcu_batch_launch_each(ipcu_batch *b, ipcu_sim *const *sims, const int64_t *nsteps, int n) {
+  if (n < 0) return IPCU_ERR_ARG;
   return batch_enqueue(b, sims, n, nsteps);
 }
 

@@ -3,9 +3,10 @@
 Requests (a 2-D case and a step count) arrive over time. The server admits
 them first-in first-out while the device memory they need fits the HBM
 budget, keeps every admitted simulation resident, and advances all of them
-together: each tick is one batched call (ipcu_batch_step) that runs one launch
-per step for every kernel class, CTAs walking a device work list of
-(simulation, tile). Finished simulations are retired at the tick boundary,
+together: each tick is one batched call (ipcu_batch_launch_each) that takes
+every simulation to its own end of the tick with one launch per step for
+every kernel class, CTAs walking a device work list of (simulation, tile).
+Finished simulations are retired at the tick boundary,
 their memory freed, and waiting requests admitted into the space -- requests
 that arrive while others are on the GPU join the running batch.
 
@@ -55,6 +56,15 @@ class Batch:
             return
         arr = (ctypes.c_void_p * len(sims))(*[s._h.value for s in sims])
         _lib.check(_lib.lib().ipcu_batch_launch(self._h, arr, len(sims), int(n)), "ipcu_batch_launch")
+
+    def launch_each(self, sims, steps):
+        """Enqueues steps[i] steps of sims[i] without waiting, in one call
+        (ipcu_batch_launch_each): those still stepping share each launch."""
+        if not sims:
+            return
+        arr = (ctypes.c_void_p * len(sims))(*[s._h.value for s in sims])
+        cnt = (ctypes.c_int64 * len(sims))(*[int(n) for n in steps])
+        _lib.check(_lib.lib().ipcu_batch_launch_each(self._h, arr, cnt, len(sims)), "ipcu_batch_launch_each")
 
     def sync(self):
         _lib.check(_lib.lib().ipcu_batch_sync(self._h), "ipcu_batch_sync")
@@ -181,14 +191,12 @@ class Server:
             if not self.active:
                 return 0
         t0 = time.perf_counter()
-        groups = {}
-        for r in self.active:
-            groups.setdefault(min(self.tick_steps, r.remaining), []).append(r)
-        for n, rs in sorted(groups.items(), reverse=True):
-            self.batch.launch([r.sim for r in rs], n)
-            for r in rs:
-                r.remaining -= n
-                self.cell_updates += r.cells * n
+        # every active simulation to its own end of the tick, in one call
+        steps = [min(self.tick_steps, r.remaining) for r in self.active]
+        self.batch.launch_each([r.sim for r in self.active], steps)
+        for r, n in zip(self.active, steps):
+            r.remaining -= n
+            self.cell_updates += r.cells * n
         mark = self.batch.mark()
         # finishers: copy the macroscopic planes back on their own streams,
         # which the batch launch ordered after their last steps

@@ -113,3 +113,45 @@ def test_request_bytes_match_device_bytes(cuda):
             s.attach_ellipse(**r.body)
         assert s.device_bytes() == request_bytes(r), (r.rid, s.device_bytes(), request_bytes(r))
         s.close()
+
+
+@pytest.mark.parametrize("storage", ["f32", "f16"])
+def test_ragged_step_counts_in_one_call(cuda, storage):
+    """ipcu_batch_launch_each: bodies, salinity and phase-field simulations
+    with different step counts (one of them 0) in one call. The fluid
+    launches that follow a batch of body updates start beside it, and every
+    result equals the simulation stepped one synchronised step at a time,
+    where nothing overlaps, bit for bit."""
+    reqs = [falling_ellipse_request(0, 192, 576, 70, storage=storage, seed=0),
+            lock_exchange_request(1, 96, 64, 120, storage=storage, seed=1),
+            falling_ellipse_request(2, 224, 672, 33, storage=storage, seed=2),
+            rayleigh_taylor_request(3, 128, 128, 0, storage=storage, seed=3),
+            lock_exchange_request(4, 64, 48, 57, storage=storage, seed=4),
+            rayleigh_taylor_request(5, 64, 96, 91, storage=storage, seed=5)]
+
+    def make(r):
+        s = Sim(r.nx, r.nz, s0=r.s0, **r.kwargs)
+        if r.body is not None:
+            s.attach_ellipse(**r.body)
+        return s
+
+    sims = [make(r) for r in reqs]
+    b = Batch()
+    b.launch_each(sims, [r.steps for r in reqs])
+    b.sync()
+    with pytest.raises(RuntimeError):
+        b.launch_each(sims[:1], [-1])
+    b.close()
+    for r, s in zip(reqs, sims):
+        ref = make(r)
+        for _ in range(r.steps):
+            ref.step(1)
+            ref.sync()  # the next step's launch waits for this one to end
+        assert s.steps() == r.steps
+        for k in ("S", "ux", "uz"):
+            assert np.array_equal(s.get(k), ref.get(k)), (r.rid, k)
+        if r.body is not None:
+            assert s.body() == ref.body()
+        assert s.status() == 0
+        ref.close()
+        s.close()
