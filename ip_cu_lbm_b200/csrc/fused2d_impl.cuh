@@ -748,8 +748,20 @@ __device__ __forceinline__ void step_tile(const Params &p, int parity, int tile_
   for (int j = tid; j < nq; j += kThreads) general(queue[j]);
 }
 
+// Resident CTAs per SM the single-run kernel's registers are sized for. The
+// FP32 TMA flow-only tile (36 KB of shared memory) fits 48 registers with a
+// 4-byte spill and runs 5 CTAs per SM: the step is bound by the latency of
+// staging a tile, and a fifth CTA hides more of it (+4.7 % MLUPS on an
+// 800 x 3000 box). The scalar lattices spill 30-70 bytes at 48 registers
+// and stay at 4.
+template <class ST, int QS, bool TMA>
+constexpr int step_min_blocks() {
+  return (QS == 0 && TMA && sizeof(ST) == 4) ? 5 : kMinBlocks;
+}
+
 template <class ST, int QS, int GEO, bool TMA, int PHYS>
-__global__ void __launch_bounds__(kThreads, kMinBlocks) step_kernel(const __grid_constant__ Params p) {
+__global__ void __launch_bounds__(kThreads, step_min_blocks<ST, QS, TMA>())
+    step_kernel(const __grid_constant__ Params p) {
   extern __shared__ __align__(128) float smem[];
   step_tile<ST, QS, GEO, TMA, PHYS>(p, 0, blockIdx.x, blockIdx.y, smem, p.tm_f);
 }
