@@ -1,25 +1,28 @@
 #!/usr/bin/env python
 """Benchmark of the per-step lattice Boltzmann path (MLUPS).
 
-Workload (one bench step = INNER lattice Boltzmann time steps of the fused
-kernel on one resident simulation): the nonuniform-grid two-layer case,
-1024 x 256 cells, uniform x, tanh-stretched z (spacing ratio ~4), D2Q9 MRT +
-D2Q5 salinity, 3-point upwind-biased quadratic interpolated streaming,
-bounce-back walls, FP32 (see ip_cu_lbm_b200/workloads.py).
+Default workload (one bench step = --inner coupled lattice Boltzmann time
+steps on one resident simulation): the settling-ellipse case, an 800 x 3000
+uniform D2Q9 MRT box with bounce-back walls, nu = 0.02, and a 20 x 10-cell
+ellipse carried by 240 markers (density ratio 1.1, tilt 45 degrees, lattice
+gravity 1e-5) released from rest; FP32 (see ip_cu_lbm_b200/workloads.py).
+Its 230 MB state is far larger than L2, so the step is HBM-bound.
 
     python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+                    [--case ib|2d|3d] [--serving]
 
 N > 1 runs one independent replica per GPU (torchrun, one process per GPU):
 the path has no exchange step, so no data-path collective is used; the
 timing is a barrier + synchronize on both sides and the max over ranks.
-Between timed steps L2 is flushed by writing a 256 MiB buffer (the 36 MB
-state is L2-resident inside a step). Rank 0 prints one JSON line.
+Between timed steps L2 is flushed by writing a 256 MiB buffer. Rank 0 prints
+one JSON line.
 
---impl reference times the reference's own implementation of this path,
-its CUDA kernel library built unmodified for sm_100a (oracle/_ref), running
-the LockExchange kernel chain on the closest workload it supports: the same
-262,144 cells with the stretched axis along x (the reference interpolates
-x only), Q9 scalar, its 5-point stencil.
+--impl reference times the reference's own implementation of this path, its
+CUDA kernel library built unmodified for sm_100a (oracle/_ref), running the
+case driver's kernel chain on the same workload: for the settling ellipse the
+EllipticalFall2 order (equ_f .. get_IBMGw2 .. update_IBbody) on the identical
+grid, body and walls, set up with the reference's own host functions
+(oracle/refcase.py); nothing of this package is loaded in that process.
 """
 from __future__ import annotations
 
@@ -40,7 +43,11 @@ INNER = 1000
 METRIC = "MLUPS"
 
 
-from ip_cu_lbm_b200.replicas import env_int  # noqa: E402
+def env_int(k, d):
+    try:
+        return int(os.environ.get(k, d))
+    except ValueError:
+        return d
 
 
 class Clocks:
@@ -104,7 +111,7 @@ def measured_traffic(args):
     """DRAM bytes per launch of the default FP32 workload's step kernel from
     the committed ncu summary (profiles/traffic.json), else None."""
     p = os.path.join(ROOT, "profiles", "traffic.json")
-    if args.storage != "f32" or args.inner != INNER or not os.path.exists(p):
+    if args.storage != "f32" or (args.inner or INNER) != INNER or not os.path.exists(p):
         return None
     d = json.load(open(p)).get("step_kernel<float,5,z3,TMA>@1024x256")
     return d["dram_bytes_per_launch"] if d else None
@@ -145,8 +152,57 @@ def peak_label(src):
     return "fallback (6.65 TB/s copy bandwidth measured earlier on this hardware; MEASURED_PEAKS.json absent)"
 
 
-def cpu_baseline(params, S0, meta, budget_s=12.0):
-    """The FP64 structured-grid oracle (numpy port of the path) on the same
+def host_cores():
+    """nproc and the CPU model of this host (lscpu), for the CPU baseline."""
+    model, sockets = None, None
+    try:
+        out = subprocess.run(["lscpu"], capture_output=True, text=True, timeout=10).stdout
+        for line in out.splitlines():
+            k, _, v = line.partition(":")
+            if k.strip() == "Model name":
+                model = v.strip()
+            elif k.strip() == "Socket(s)":
+                sockets = v.strip()
+    except (OSError, subprocess.SubprocessError):
+        pass
+    return {"nproc": os.cpu_count(), "model": model, "sockets": sockets}
+
+
+def cpu_baseline_ib(budget_s=15.0):
+    """The reference's kernels restated in C++ (oracle/ipcu_oracle.cpp, FP32,
+    OpenMP over all host threads), run in the EllipticalFall2 driver order on
+    the settling-ellipse workload with the reference's layout (compacted
+    cells, ghosts, AoS populations): as many steps as fit in budget_s."""
+    import ctypes
+
+    from oracle import oracle as _o
+    from oracle import refcase
+
+    c, host, meta = refcase.settling_ellipse_ref()
+    O = _o.oracle().lib
+    O.oracle_ibm_steps_f32.argtypes = [ctypes.c_void_p] * 3
+    O.oracle_ibm_steps_f32.restype = ctypes.c_int
+    arrs = {k: np.ascontiguousarray(v) for k, v in host.items()}
+    slots = (ctypes.c_void_p * len(_o.REF_BUFS))(*[arrs[k].ctypes.data if k in arrs else None for k in _o.REF_BUFS])
+    nt = meta["nt"]
+    ip = (ctypes.c_longlong * 16)(nt, 1, 1, 1, 0, 0, 1, *[len(w) for w in c["walls"]], nt, 3 * meta["markers"])
+    fp = (ctypes.c_float * 2)(1.0, meta["rhoH"])
+    O.oracle_ibm_steps_f32(slots, ip, fp)  # warm (first touch of every page)
+    n, t0 = 0, time.perf_counter()
+    while n < 200 and (n < 3 or time.perf_counter() - t0 < budget_s):
+        O.oracle_ibm_steps_f32(slots, ip, fp)
+        n += 1
+    dt = time.perf_counter() - t0
+    hc = host_cores()
+    return {"value": round(meta["nc"] * n / dt / 1e6, 3), "unit": METRIC, "cores": int(O.oracle_num_threads()),
+            "kind": "port", "host": hc,
+            "sample": f"{n} steps of the full 800x3000 settling-ellipse workload in the reference's EllipticalFall2 "
+                      "kernel order, FP32, the reference kernels restated in C++ with OpenMP "
+                      "(oracle/ipcu_oracle.cpp, oracle_ibm_steps_f32)"}
+
+
+def cpu_baseline_2d(params, S0, meta, budget_s=12.0):
+    """The FP64 structured-grid oracle (numpy port of the path) on the C2
     workload, single host thread, bounded number of steps."""
     from ip_cu_lbm_b200.cases import d2q9_mrt
     from oracle.structured import Box
@@ -181,7 +237,7 @@ def run_ours(args):
     stream = torch.cuda.current_stream(dev)
     sim = Sim(meta["nx"], meta["nz"], s0=S0.ravel(), stream=stream.cuda_stream, **params)
     N = sim.N
-    inner = args.inner
+    inner = args.inner or INNER
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
     chunk = min(inner, 200)
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
@@ -253,7 +309,7 @@ def run_ours(args):
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
-            line["cpu_baseline"] = cpu_baseline(params, S0, meta)
+            line["cpu_baseline"] = cpu_baseline_2d(params, S0, meta)
         except Exception as e:  # reported, not fatal
             line["cpu_baseline"] = {"value": None, "error": str(e)[:200]}
     if rank == 0:
@@ -281,7 +337,7 @@ def run_3d(args):
     rng = np.random.default_rng(20261203)
     S0 = 1.0 - zz + 1e-4 * rng.uniform(-1, 1, (nz, ny, nx))  # linear stratification, seeded noise
     sim = Sim3D(nx, ny, nz, tau=0.55, taus=0.52, rho_sal=1e-3, g_bouss=1e-5, s0=S0.ravel(), stream=stream.cuda_stream)
-    N, inner = sim.N, args.inner if args.inner != INNER else 20
+    N, inner = sim.N, args.inner or 20
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     with Clocks(local) as clk:
         time.sleep(0.3)
@@ -338,16 +394,27 @@ def run_3d(args):
     R.close()
 
 
+def ib_config(nx=800, nz=3000):
+    """The settling-ellipse workload as both arms name it (identical dicts)."""
+    return {"workload": f"settling ellipse: {nx}x{nz} uniform D2Q9 MRT box, bounce-back walls, nu 0.02 (lattice "
+                        "units), rigid ellipse with semi-axes 20x10 cells and 240 markers at equal arc length, "
+                        "density ratio 1.1, tilt 45 deg, lattice gravity 1e-5, released from rest near "
+                        "(0.5, 0.85) of the box",
+            "cells": nx * nz, "storage": "f32",
+            "l2": "flushed (256 MiB write) between timed steps; the state is larger than L2"}
+
+
 def run_ib(args):
-    """The moving-immersed-boundary case: an ellipse (20 x 10 cells, 240
-    markers, density ratio 1.1, tilt 45 degrees) settling from rest in an
-    800 x 3000 uniform D2Q9 MRT box, gravity 1e-5 (the second of the sweep's
-    four values), without the optional salinity stratification (N^2 = 1e-6
-    over 3000 cells puts a hydrostatic pressure range of 4.5 on the weakly
-    compressible lattice; see workloads.settling_ellipse). One bench step =
-    --inner coupled steps (fused fluid step + the one-CTA immersed-boundary
-    update) replayed from CUDA graphs; the 230 MB FP32 state exceeds L2 and a
-    256 MiB flush separates timed steps."""
+    """The moving-immersed-boundary case (the default bench line): an
+    ellipse (20 x 10 cells, 240 markers, density ratio 1.1, tilt 45 degrees)
+    settling from rest in an 800 x 3000 uniform D2Q9 MRT box, gravity 1e-5
+    (the second of the sweep's four values), without the optional salinity
+    stratification (N^2 = 1e-6 over 3000 cells puts a hydrostatic pressure
+    range of 4.5 on the weakly compressible lattice; see
+    workloads.settling_ellipse). One bench step = --inner coupled steps
+    (fused fluid step + the one-CTA immersed-boundary update) replayed from
+    CUDA graphs; the 230 MB FP32 state exceeds L2 and a 256 MiB flush
+    separates timed steps."""
     import torch
 
     from ip_cu_lbm_b200 import Sim, workloads
@@ -362,7 +429,7 @@ def run_ib(args):
     sim.attach_ellipse(body["xc"], body["zc"], body["a"], body["b"], markers=body["markers"], theta=body["theta"],
                        rho_s=body["rho_s"], rho_f=body["rho_f"], gravity=body["gravity"], iters=body["iters"])
     N = sim.N
-    inner = args.inner if args.inner != INNER else 200
+    inner = args.inner if args.inner else 3000
     chunk = min(inner, 100)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
@@ -388,8 +455,9 @@ def run_ib(args):
     peak, peak_src = load_peaks()
     achieved = N * bpc / (step_ms / 1e3) / 1e9
     b = sim.body()
-    # end to end: upload the fluid state from pinned host memory, advance,
-    # read u_x, u_z and the body state back
+    # end to end through the C ABI: every bench step uploads the whole state
+    # from pinned host memory, advances --inner steps and downloads the whole
+    # state and the body (the state lives on the host between steps)
     esz = sim.storage_bytes()
     hdt = torch.float32 if esz == 4 else torch.float16
     q = params["q_scalar"]
@@ -404,42 +472,57 @@ def run_ib(args):
     for _ in range(e2e_steps):
         sim.upload(hf, hg if q else None, hm)
         sim.step_graph(inner, chunk=chunk)
-        sim.download(None, None, hm)
-        sim.body()
+        sim.download(hf, hg if q else None, hm)
+        sim.body()  # synchronises the stream
     R.barrier()
     e2e = world * N * inner * e2e_steps / R.max(time.perf_counter() - t0) / 1e6
-    h2d = hf.numel() * esz + (hg.numel() * esz if q else 0) + hm.numel() * 4
+    state_bytes = hf.numel() * esz + (hg.numel() * esz if q else 0) + hm.numel() * 4
     line = {
         "metric": METRIC, "value": round(value, 2), "unit": METRIC, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(total_ms / args.steps, 4), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None,
         "dtype": "f32" if args.storage == "f32" else f"{args.storage}-storage/f32",
         "data": "synthetic (seeded release-point jitter)",
-        "config": {"workload": f"settling ellipse, {meta['nx']}x{meta['nz']} D2Q9 MRT, 20x10 ellipse, 240 markers, "
-                               "density ratio 1.1, MDF x3, Peskin-4, FP64 body",
-                   "lbm_steps_per_step": inner, "cells": N, "storage": args.storage,
-                   "parallelism": f"replicas x{world}", "gravity": body["gravity"],
-                   "body_after": {k: round(v, 6) for k, v in b.items() if k in ("x", "z", "w", "theta")},
-                   "l2": "flushed (256 MiB write) between timed steps; state larger than L2"},
+        "config": ib_config(meta["nx"], meta["nz"]) if args.storage == "f32" else
+        dict(ib_config(meta["nx"], meta["nz"]), storage=args.storage),
+        "lbm_steps_per_step": inner, "parallelism": f"replicas x{world}",
+        "scheme": "fused collide-and-stream step + multi-direct forcing (3 iterations, Peskin-4) with an FP64 "
+                  "rigid-body update, CUDA-graph replay",
+        "body_after": {k: round(v, 6) for k, v in b.items() if k in ("x", "z", "w", "theta")},
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4), "traffic": traffic_ib(args), "bytes_per_cell": bpc,
                      "peak_source": peak_label(peak_src),
                      "note": "fluid step's algorithmic bytes / (fluid + immersed-boundary kernel time per step); "
-                             "traffic = ncu dram read+write bytes of one fluid launch (cold, 4 CTAs per SM build), "
-                             "below the algorithmic bytes because L2 still holds part of the written state"},
-        "e2e": {"value": round(e2e, 2), "unit": METRIC, "h2d_bytes_per_step": int(h2d),
-                "d2h_bytes_per_step": int(hm.numel() * 4 + 72)},
+                             "traffic = ncu dram read+write bytes of one fluid launch"},
+        "e2e": {"value": round(e2e, 2), "unit": METRIC, "h2d_bytes_per_step": int(state_bytes),
+                "d2h_bytes_per_step": int(state_bytes + 72)},
         "gpu_launches": 2 * args.steps * inner, "clocks": clk.summary(),
     }
+    if R.rank == 0 and world == 1 and not args.no_cpu_baseline and args.storage == "f32":
+        try:
+            line["cpu_baseline"] = cpu_baseline_ib()
+        except Exception as e:  # reported, not fatal
+            line["cpu_baseline"] = {"value": None, "error": str(e)[:200]}
     if R.rank == 0:
         print(json.dumps(line), flush=True)
     sim.close()
     R.close()
 
 
+def _standalone_module(relpath, name):
+    """A pure-Python file of this repository loaded as a module of its own
+    (no package import, so no product library is loaded)."""
+    import importlib.util
+
+    spec = importlib.util.spec_from_file_location(name, os.path.join(ROOT, relpath))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
 def run_reference(args):
-    """The reference's CUDA kernel chain (oracle/_ref) on the closest
-    supported workload; rank 0 only."""
+    """The reference's CUDA kernel chain (oracle/_ref) on the bench's
+    workload; rank 0 only. Nothing of ip_cu_lbm_b200 is imported or loaded."""
     rank = env_int("RANK", 0)
     if rank != 0:
         return
@@ -448,23 +531,126 @@ def run_reference(args):
     if not _o.ref_available():
         print(json.dumps({"impl": "reference", "unavailable": "reference build oracle/_ref/libipcu_ref.so missing"}))
         return
+    if args.case == "3d":
+        print(json.dumps({"impl": "reference", "unavailable": "the reference has no D3Q19/D3Q7 path (3-D is D3Q27 "
+                                                              "only), and 160x160x640 exceeds its 2^24 float "
+                                                              "cell-count limit"}))
+        return
+    if args.case == "2d":
+        return run_reference_2d(args)
+    run_reference_ib(args)
+
+
+def _ref_tensors(host, dev):
     import torch
 
-    from ip_cu_lbm_b200 import cases, workloads
+    return {k: torch.as_tensor(np.ascontiguousarray(v), device=dev,
+                               dtype=torch.float32 if np.asarray(v).dtype.kind == "f" else torch.int32)
+            for k, v in host.items()}
+
+
+def run_reference_ib(args):
+    """The reference's EllipticalFall2 kernel chain (ref:
+    EllipticalFall2/EllipticalFallxz.cu:344-430: equ_f, Force, col_f_MRT,
+    IP_process, update_rho, resetF, set_f_ftmp, get_IBMGw2, update_velIBM,
+    update_IBbody, update_IBpoint, search_IBlattice, resetF x2) on the
+    settling-ellipse workload, in the reference's physical units (gravity
+    9.81 is hard-coded there, so dt gives the lattice gravity 1e-5)."""
+    import ctypes
+
+    import torch
+
+    from oracle import oracle as _o
+    from oracle import refcase
 
     dev = torch.device("cuda", env_int("LOCAL_RANK", 0))
     torch.cuda.set_device(dev)
-    params, S0, meta = workloads.stratified_nonuniform()
-    nzs, nxs = meta["nz"], meta["nx"]  # stretched axis becomes the reference's x axis
-    c = cases.box_case(Q=9, nx0=nzs, nz=nxs, dx=1.0, dt=1.0, prec="f32")
-    # stretched x coordinates (the reference accepts any posx/delX >= dz)
-    xs, ws = np.asarray(params["z"]), np.asarray(params["wz"])
-    nc, own = c["nc"], c["owner"]
-    px = np.repeat(xs, nxs)
-    dX = np.repeat(ws, nxs)
-    c["posx"] = np.concatenate([px, px[own]]).astype(np.float32)
-    c["delX"] = np.concatenate([dX, dX[own]]).astype(np.float32)
-    Q, nt = 9, c["nt"]
+    c, host, meta = refcase.settling_ellipse_ref()
+    T = _ref_tensors(host, dev)
+    slots = (ctypes.c_void_p * len(_o.REF_BUFS))(*[T[k].data_ptr() if k in T else None for k in _o.REF_BUFS])
+    nt, nc = meta["nt"], meta["nc"]
+    inner = args.ref_inner
+    ip = (ctypes.c_longlong * 16)(nt, inner, 1, 1, 0, 0, 1, *[len(w) for w in c["walls"]], nt, 3 * meta["markers"])
+    fp = (ctypes.c_float * 2)(1.0, meta["rhoH"])
+    Rf = _o.ref()
+    for _ in range(args.warmup):
+        assert Rf.lib.ref_ibm_steps_f32(slots, ip, fp) == 0
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    torch.cuda.synchronize()
+    total = 0.0
+    with Clocks(dev.index or 0) as clk:
+        time.sleep(0.3)
+        t_start = time.perf_counter()
+        for k in range(args.steps):
+            flush.fill_(float(k))
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            assert Rf.lib.ref_ibm_steps_f32(slots, ip, fp) == 0
+            e1.record()
+            torch.cuda.synchronize()
+            total += e0.elapsed_time(e1)
+        clk.window(t_start, time.perf_counter())
+    value = nc * inner * args.steps / (total / 1e3) / 1e6
+    # end to end: the driver's state (populations and the per-cell moments the
+    # chain carries) uploaded from pinned host memory, the steps, and the
+    # state read back, every bench step
+    state = ["f", "p", "u", "w", "rho", "Fx", "Fz"]
+    hb = {k: torch.empty(T[k].numel(), dtype=torch.float32, pin_memory=True) for k in state}
+    for k in state:
+        hb[k].copy_(T[k])
+    torch.cuda.synchronize()
+    e2e_steps = max(3, args.steps)
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        for k in state:
+            T[k].copy_(hb[k], non_blocking=True)
+        assert Rf.lib.ref_ibm_steps_f32(slots, ip, fp) == 0
+        for k in state:
+            hb[k].copy_(T[k], non_blocking=True)
+        torch.cuda.synchronize()
+    e2e = nc * inner * e2e_steps / (time.perf_counter() - t0) / 1e6
+    state_bytes = sum(hb[k].numel() * 4 for k in state)
+    posB = T["posB"].cpu().numpy()
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": round(value, 2), "unit": METRIC, "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(total / args.steps, 4),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (the same ellipse, grid and walls)",
+        "config": ib_config(),
+        "lbm_steps_per_step": inner,
+        "scheme": "the reference's EllipticalFall2 kernel chain, its CUDA built unmodified for sm_100a: "
+                  "get_IBMGw2 stress-jump forcing (one pass), float body update, "
+                  "<<<ceil(Nt/64),64>>> launches on the legacy stream; grid and ghosts from its own host functions",
+        "body_after_m": [round(float(v), 6) for v in posB],
+        "cpu_baseline": {"value": round(value, 2), "unit": METRIC, "kind": "reference", "cores": 0,
+                         "sample": "the reference's own CUDA build on the GPU (it has no CPU implementation)"},
+        "e2e": {"value": round(e2e, 2), "unit": METRIC, "h2d_bytes_per_step": int(state_bytes),
+                "d2h_bytes_per_step": int(state_bytes)},
+        "clocks": clk.summary(),
+    }), flush=True)
+
+
+def run_reference_2d(args):
+    """The reference's LockExchange kernel chain on the closest workload to
+    the nonuniform two-layer case it supports: the same 262,144 cells with
+    the stretched axis along x (the reference interpolates x only), Q9
+    scalar, its 5-point stencil, bounce-back."""
+    import ctypes
+
+    import torch
+
+    from oracle import oracle as _o
+    from oracle import refcase
+
+    dev = torch.device("cuda", env_int("LOCAL_RANK", 0))
+    torch.cuda.set_device(dev)
+    # the workload's definition (pure numpy) loaded on its own, without the package
+    wl = _standalone_module("ip_cu_lbm_b200/workloads.py", "ipcu_workloads_def")
+    params, S0, meta = wl.stratified_nonuniform()
+    nzs, nxs = S0.shape  # stretched axis (rows of S0) becomes the reference's x axis
+    c = refcase.box2d(nzs, nxs, 1.0, 1.0, 1e-6, xs=params["z"], wxs=params["wz"])
+    Q, nt, nc, own = 9, c["nt"], c["nc"], c["owner"]
     # S[z, x] -> reference cell (i = z, l = x); scaled by 1e-3 because the
     # reference hard-codes g = 9.81 and rho ~ 1000 (function/collision.cu:78)
     Sg = 1e-3 * S0.T.reshape(-1)
@@ -474,28 +660,24 @@ def run_reference(args):
     st = dict(f=np.zeros(nt * Q, np.float32), g=np.concatenate([g, np.zeros((len(own), Q), np.float32)]).ravel(),
               p=np.zeros(nt, np.float32), sal=ext(Sg.astype(np.float32)), phi=np.ones(nt, np.float32),
               u=np.zeros(nt, np.float32), v=np.zeros(nt, np.float32), w=np.zeros(nt, np.float32),
-              tau=np.full(nt, params["tau"], np.float32), taus=np.full(nt, params["taus"], np.float32))
+              tau=np.full(nt, 3 * 0.005 + 0.5, np.float32), taus=np.full(nt, 3 * 0.0005 + 0.5, np.float32))
     st["rho"] = (1000.0 + st["sal"].astype(np.float64) * 0.824493).astype(np.float32)
-    M, Minv, S = cases.d2q9_mrt()
-    _, S, _, MM = cases.set_M(9, M, S, Minv)
+    M, Mi, S, MM = refcase.mrt9()
     host = dict(items=c["items"], neib=c["neib"], nextB=c["nextB"], nextK=c["nextK"], posx=c["posx"],
-                posy=c["posy"], posz=c["posz"], delX=c["delX"], delY=c["delY"], M=M.ravel(), Minv=Minv.ravel(),
+                posy=c["posy"], posz=c["posz"], delX=c["delX"], delY=c["delY"], M=M.ravel(), Minv=Mi.ravel(),
                 S=S, MM=MM.ravel(), ftmp=st["f"], fout=st["f"], feq=np.zeros(nt * Q), Fk=np.zeros(nt * Q),
                 Fx=np.zeros(nt), Fy=np.zeros(nt), Fz=np.zeros(nt), **st)
     for a in range(6):
         wl = c["walls"][a]
         host[f"w{a + 1}"] = wl if len(wl) else np.zeros(1, np.int32)
-    T = {k: torch.as_tensor(np.ascontiguousarray(v), device=dev,
-                            dtype=torch.float32 if np.asarray(v).dtype.kind == "f" else torch.int32)
-         for k, v in host.items()}
-    import ctypes
-
+    T = _ref_tensors(host, dev)
     slots = (ctypes.c_void_p * len(_o.REF_BUFS))(*[T[k].data_ptr() if k in T else None for k in _o.REF_BUFS])
-    ip = (ctypes.c_longlong * 16)(nt, INNER, 1, 1, 1, 0, 1, *[len(w) for w in c["walls"]], nt, 0)
+    inner = args.ref_inner
+    ip = (ctypes.c_longlong * 16)(nt, inner, 1, 1, 1, 0, 1, *[len(w) for w in c["walls"]], nt, 0)
     fp = (ctypes.c_float * 2)(1.0, 1000.0)
-    R = _o.ref()
+    Rf = _o.ref()
     for _ in range(args.warmup):
-        assert R.lib.ref_le_steps_f32(slots, ip, fp) == 0
+        assert Rf.lib.ref_le_steps_f32(slots, ip, fp) == 0
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
     torch.cuda.synchronize()
     total = 0.0
@@ -506,19 +688,20 @@ def run_reference(args):
             torch.cuda.synchronize()
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record()
-            assert R.lib.ref_le_steps_f32(slots, ip, fp) == 0
+            assert Rf.lib.ref_le_steps_f32(slots, ip, fp) == 0
             e1.record()
             torch.cuda.synchronize()
             total += e0.elapsed_time(e1)
         clk.window(t_start, time.perf_counter())
-    value = nc * INNER * args.steps / (total / 1e3) / 1e6
+    value = nc * inner * args.steps / (total / 1e3) / 1e6
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": round(value, 2), "unit": METRIC, "n_gpus": 1,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(total / args.steps, 4),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": f"reference LockExchange kernel chain, {nzs}x{nxs} cells (stretched axis along x, "
                                "5-point stencil, Q9 scalar, MRT, bounce-back), reference CUDA built for sm_100a",
-                   "lbm_steps_per_step": INNER, "cells": nc},
+                   "cells": nc},
+        "lbm_steps_per_step": inner,
         "cpu_baseline": {"value": round(value, 2), "unit": METRIC, "kind": "reference", "cores": 0,
                          "sample": "the reference's own CUDA build on the GPU (it has no CPU implementation)"},
         "e2e": {"value": round(value, 2), "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -656,12 +839,14 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--storage", default="f32", choices=["f32", "f16", "bf16"])
-    ap.add_argument("--inner", type=int, default=INNER)
+    ap.add_argument("--inner", type=int, default=0, help="LBM steps per bench step (0: the case's default)")
+    ap.add_argument("--ref-inner", type=int, default=20, help="LBM steps per bench step of the reference arm")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--serving", action="store_true", help="run the continuous-batching serving stream instead")
     ap.add_argument("--requests", type=int, default=512)
-    ap.add_argument("--case", default="2d", choices=["2d", "3d", "ib"],
-                    help="3d: the C4-sized 3-D box; ib: the settling-ellipse immersed-boundary case")
+    ap.add_argument("--case", default="ib", choices=["ib", "2d", "3d"],
+                    help="ib: the settling-ellipse immersed-boundary case (default); 2d: the nonuniform "
+                         "two-layer 1024x256 case; 3d: the C4-sized 3-D box")
     ap.add_argument("--dims", default="160,160,640", help="3-D box nx,ny,nz (--case 3d)")
     args = ap.parse_args()
     if args.warmup < 3:

@@ -21,6 +21,18 @@
 #include <cstring>
 #include <vector>
 
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+// Per-cell loops whose iterations write only their own cell run on all host
+// threads; the result is bitwise that of the sequential loop. Scatters (the
+// Q27 flux hand-back, the immersed-boundary spreading) stay sequential, in
+// cell order.
+#define OMP_CELLS _Pragma("omp parallel for schedule(static)")
+#define OMP_STR(x) #x
+#define OMP_CELLS_IF(c) _Pragma(OMP_STR(omp parallel for schedule(static) if (c)))
+
 namespace {
 
 // Parameter-block layout (ref: itemIndex.hpp:4-33).
@@ -149,12 +161,14 @@ inline void quat_rot(T q0, T q1, T q2, T q3, T *R) {
 template <class T>
 void o_equ_f(const T *it, T *feq, const T *pr, const T *u, const T *v, const T *w) {  // collision.cu:3-14
   P<T> p(it);
+  OMP_CELLS
   for (long i = 0; i < p.nc; i++)
     for (int k = 0; k < p.Q; k++) feq[i * p.Q + k] = equil<T>(p, k, 1, pr[i], u[i], v[i], w[i]);
 }
 template <class T>
 void o_equ_g(const T *it, T *feq, const T *s, const T *u, const T *v, const T *w) {  // collision.cu:16-27
   P<T> p(it);
+  OMP_CELLS
   for (long i = 0; i < p.nc; i++)
     for (int k = 0; k < p.Q; k++) feq[i * p.Q + k] = equil<T>(p, k, s[i], 1, u[i], v[i], w[i]);
 }
@@ -197,6 +211,7 @@ void o_Force(const T *it, int bouss, const int *nb, const T *, const T *, const 
   const int Q = p.Q, up = (Q == 27) ? 5 : 2, dn = (Q == 27) ? 6 : 4;
   const T reg = p.dz / 1000;
   const T sig = it[I_sigma], W = it[I_PFthick];
+  OMP_CELLS
   for (long i = 0; i < p.nc; i++) {
     const int *n = nb + i * Q;
     auto grad = [&](const T *a, const T *pos, int d1, int d2) {
@@ -234,8 +249,9 @@ void o_col_f_MRT(const T *it, const T *tau, T *f, T *ftmp, T *feq, const T *Fk, 
                  const T *Mi, const T *, const T *MM) {
   P<T> p(it);
   const int Q = p.Q, s0 = (Q == 27) ? 5 : 7, ns = (Q == 27) ? 5 : 2;
-  std::vector<T> d(Q), mles(Q);
+  OMP_CELLS
   for (long i = 0; i < p.nc; i++) {
+    T d[27], mles[27];
     T *fi = f + i * Q;
     for (int k = 0; k < Q; k++) d[k] = fi[k] - feq[i * Q + k] + Fk[i * Q + k] / 2.0;
     for (int a = 0; a < Q; a++) {
@@ -260,12 +276,14 @@ void o_col_f_MRT(const T *it, const T *tau, T *f, T *ftmp, T *feq, const T *Fk, 
 template <class T>
 void o_col_f_SRT(const T *it, const T *tau, T *f, T *ftmp, T *feq, const T *Fk) {
   P<T> p(it);
+  OMP_CELLS
   for (long i = 0; i < p.nc; i++)
     for (int k = 0; k < p.Q; k++) {
       long j = i * p.Q + k;
       f[j] = f[j] - (f[j] - feq[j] + Fk[j] / 2.0) / tau[i] + Fk[j];
       ftmp[j] = f[j];
     }
+  OMP_CELLS
   for (long i = 0; i < p.nc; i++)
     for (int k = 0; k < p.Q; k++) f[i * p.Q + k] = feq[i * p.Q + k] = 0;
 }
@@ -276,6 +294,7 @@ void o_col_g_reg(const T *it, const T *taus, T *g, T *gtmp, T *geq, const T *s, 
                  const T *v, const T *w) {
   P<T> p(it);
   const int Q = p.Q;
+  OMP_CELLS
   for (long i = 0; i < p.nc; i++) {
     T jx = 0, jy = 0, jz = 0;
     for (int k = 0; k < Q; k++) {
@@ -304,6 +323,7 @@ void o_col_PF(const T *it, const int *nb, const T *, T *g, T *gtmp, T *geq, cons
   P<T> p(it);
   const int Q = p.Q, up = (Q == 27) ? 5 : 2, dn = (Q == 27) ? 6 : 4;
   const T reg = p.dz / 1000, W = it[I_PFthick];
+  OMP_CELLS
   for (long i = 0; i < p.nc; i++) {
     const int *n = nb + i * Q;
     T gx = (phi[n[1]] - phi[n[3]]) / (px[n[1]] - px[n[3]] + reg);
@@ -333,6 +353,7 @@ void o_col_PF(const T *it, const int *nb, const T *, T *g, T *gtmp, T *geq, cons
 template <class T>
 void o_update_scalar(const T *it, const T *g, T *s) {  // collision.cu:225-236
   P<T> p(it);
+  OMP_CELLS
   for (long i = 0; i < p.nc; i++) {
     T a = 0;
     for (int k = 0; k < p.Q; k++) a += g[i * p.Q + k];
@@ -345,6 +366,7 @@ template <class T>
 void o_update_rho(const T *it, T rhoL, T rhoH, const T *f, const T *Fx, const T *Fy, const T *Fz, T *pr,
                   const T *sal, const T *phi, T *rho, T *u, T *v, T *w) {
   P<T> p(it);
+  OMP_CELLS
   for (long i = 0; i < p.nc; i++) {
     T a = 0, b = 0, c = 0, d = 0;
     for (int k = 0; k < p.Q; k++) {
@@ -364,6 +386,7 @@ void o_update_rho(const T *it, T rhoL, T rhoH, const T *f, const T *Fx, const T 
 
 template <class T>
 void o_resetF(const T *, T *Fx, T *Fy, T *Fz, int n) {  // collision.cu:258-264
+  OMP_CELLS
   for (int i = 0; i < n; i++) Fx[i] = Fy[i] = Fz[i] = 0;
 }
 
@@ -371,6 +394,7 @@ void o_resetF(const T *, T *Fx, T *Fy, T *Fz, int n) {  // collision.cu:258-264
 template <class T>
 void o_set_wall_f(const T *it, const int *nb, T *f) {  // adv.cu:3-13 (ghost <- owner copy)
   P<T> p(it);
+  OMP_CELLS
   for (long g = p.nc; g < p.nc + p.nw; g++) {
     long o = nb[g * p.Q];
     for (int k = 0; k < p.Q; k++) f[g * p.Q + k] = f[o * p.Q + k];
@@ -400,6 +424,7 @@ void o_set_out(const T *it, const int *nb, const T *ftmp, T *fout, T *fin, T *fi
       kd[k + 8] = 23 + k;
     }
   }
+  OMP_CELLS_IF(Q == 9)
   for (long i = 0; i < p.nc; i++) {
     const long b = i * Q;
     if (Q == 9) {
@@ -508,6 +533,7 @@ void o_set_fin(const T *it, const int *nb, const int *, T *fin, T *finy) {
 template <class T>
 void o_reset_f(const T *it, const T *ftmp, T *fin, T *f) {  // adv.cu:176-187
   P<T> p(it);
+  OMP_CELLS
   for (long j = 0; j < p.nc * p.Q; j++) {
     fin[j] += f[j];
     f[j] = ftmp[j];
@@ -519,6 +545,7 @@ template <class T>
 void o_set_wall_f_inv(const T *it, const int *nb, const int *nextB, const int *nextK, T *f) {
   P<T> p(it);
   const int Q = p.Q;
+  OMP_CELLS_IF(Q == 9)
   for (long g = p.nc; g < p.nc + p.nw; g++) {
     const long b = g * Q, o = nb[b];
     if (Q == 9) {
@@ -558,6 +585,7 @@ template <class T>
 void o_set_tmp(const T *it, const int *nb, const T *f, T *ftmp, const T *fout, const T *fin) {
   P<T> p(it);
   Dirs D(p.Q);
+  OMP_CELLS
   for (long i = 0; i < p.nc; i++)
     for (int k = 0; k < p.Q; k++) {
       long s = nb[i * p.Q + D.cp[k]];
@@ -572,6 +600,7 @@ void o_set_wall_propagation(const T *it, int bc, const int *nb, const int *nextK
   P<T> p(it);
   const int Q = p.Q;
   Dirs D(Q);
+  OMP_CELLS_IF(bc == 1)
   for (long g = p.nc; g < p.nc + p.nw; g++) {
     const long b = g * Q, o = nb[b], wb = (g - p.nc) * Q;
     if (bc == 1) {
@@ -589,6 +618,7 @@ template <class T>
 void o_propagation(const T *it, const int *nb, T *f, const T *ftmp) {  // propagation.cu:2-12
   P<T> p(it);
   Dirs D(p.Q);
+  OMP_CELLS
   for (long i = 0; i < p.nc; i++)
     for (int k = 0; k < p.Q; k++) f[i * p.Q + k] = ftmp[(long)nb[i * p.Q + D.kinv[k]] * p.Q + k];
 }
@@ -596,12 +626,14 @@ void o_propagation(const T *it, const int *nb, T *f, const T *ftmp) {  // propag
 template <class T>
 void o_reset_wall_fin(const T *it, T *fin, T *finy) {  // basic.cu:274-284
   P<T> p(it);
+  OMP_CELLS
   for (long j = p.nc * p.Q; j < (p.nc + p.nw) * p.Q; j++) fin[j] = finy[j] = 0;
 }
 
 template <class T>
 void o_set_wall_rho(const T *it, const int *nb, T *rho) {  // basic.cu:254-261
   P<T> p(it);
+  OMP_CELLS
   for (long g = p.nc; g < p.nc + p.nw; g++) rho[g] = rho[nb[g * p.Q]];
 }
 
@@ -835,6 +867,7 @@ template <class T>
 void o_update_velIBM(const T *it, const int *, T *f, const T *, T *pr, const T *, T *u, T *v, T *w,
                      const T *, const T *, const T *, const T *Fx, const T *Fy, const T *Fz) {
   P<T> p(it);
+  OMP_CELLS
   for (long i = 0; i < p.nc; i++) {
     T a = 0, b = 0, c = 0, d = 0;
     for (int k = 0; k < p.Q; k++) {
@@ -1122,4 +1155,114 @@ extern "C" void oracle_nearest_cells_f32(const float *px, const float *py, const
     }
     lid[k] = near_id;
   }
+}
+
+// ======================================================================= driver step orders
+// The case drivers' per-step kernel order on host buffers, for the timed CPU
+// baseline: the same buffer slots as oracle/ref_harness.cu's step chains
+// (enum order below), so one buffer table drives the reference build on the
+// GPU and this restatement on the host cores.
+namespace {
+enum OBuf {
+  O_items, O_neib, O_nextB, O_nextK, O_f, O_ftmp, O_fout, O_feq, O_Fk, O_g, O_p, O_sal, O_phi, O_tau,
+  O_taus, O_Fx, O_Fy, O_Fz, O_rho, O_px, O_py, O_pz, O_dX, O_dY, O_u, O_v, O_w, O_M, O_Minv, O_S, O_MM,
+  O_w1, O_w2, O_w3, O_w4, O_w5, O_w6,
+  O_lid, O_uo, O_vo, O_wo, O_massB, O_densB, O_inertia, O_FB, O_posB, O_Torque, O_velB, O_quat,
+  O_quaS, O_angleVB, O_posw, O_oposw, O_Gw, O_velw, O_nB, O_onB, O_quatold,
+  O_COUNT
+};
+}  // namespace
+
+// LockExchange order (ref: LockExchange/LockExchange.cu:214-278).
+// ip[]: 0 unused, 1 nsteps, 2 slip(0)/bounce-back(1), 3 use_mrt, 4 use_scalar,
+//       5 use_wall_function, 6 boussi, 7..12 wall sizes, 13 num_F
+// fp[]: 0 rhoL, 1 rhoH
+extern "C" int oracle_le_steps_f32(void *const *b, const long long *ip, const float *fp) {
+#define F(x) ((float *)b[x])
+#define I(x) ((int *)b[x])
+  const float *it = F(O_items);
+  const int *nb = I(O_neib);
+  for (long long s = 0; s < ip[1]; s++) {
+    if (ip[5]) {
+      o_wall_function<float>(it, F(O_dX), F(O_dY), 1, 0, 0, (int)ip[7], I(O_w1), F(O_v), F(O_w), F(O_u), F(O_Fy), F(O_Fz), F(O_rho));
+      o_wall_function<float>(it, F(O_dX), F(O_dY), 1, 0, 0, (int)ip[9], I(O_w3), F(O_v), F(O_w), F(O_u), F(O_Fy), F(O_Fz), F(O_rho));
+      o_wall_function<float>(it, F(O_dX), F(O_dY), 0, 0, 1, (int)ip[11], I(O_w5), F(O_u), F(O_v), F(O_w), F(O_Fx), F(O_Fy), F(O_rho));
+      o_wall_function<float>(it, F(O_dX), F(O_dY), 0, 0, 1, (int)ip[12], I(O_w6), F(O_u), F(O_v), F(O_w), F(O_Fx), F(O_Fy), F(O_rho));
+      o_wall_function<float>(it, F(O_dX), F(O_dY), 0, 1, 0, (int)ip[8], I(O_w2), F(O_u), F(O_w), F(O_v), F(O_Fx), F(O_Fz), F(O_rho));
+      o_wall_function<float>(it, F(O_dX), F(O_dY), 0, 1, 0, (int)ip[10], I(O_w4), F(O_u), F(O_w), F(O_v), F(O_Fx), F(O_Fz), F(O_rho));
+    }
+    o_equ_f<float>(it, F(O_feq), F(O_p), F(O_u), F(O_v), F(O_w));
+    o_Force<float>(it, (int)ip[6], nb, F(O_f), F(O_feq), F(O_tau), F(O_Fk), F(O_Fx), F(O_Fy), F(O_Fz), F(O_p), F(O_rho),
+                   F(O_sal), F(O_phi), F(O_u), F(O_v), F(O_w), F(O_dX), F(O_dY), F(O_px), F(O_py), F(O_pz));
+    if (ip[3])
+      o_col_f_MRT<float>(it, F(O_tau), F(O_f), F(O_ftmp), F(O_feq), F(O_Fk), F(O_M), F(O_Minv), F(O_S), F(O_MM));
+    else
+      o_col_f_SRT<float>(it, F(O_tau), F(O_f), F(O_ftmp), F(O_feq), F(O_Fk));
+    o_IP_process<float>(it, nb, F(O_f), F(O_feq), F(O_ftmp), F(O_fout), I(O_nextB), I(O_nextK), F(O_px), F(O_py),
+                        F(O_dX), F(O_dY), (int)ip[2]);
+    if (ip[4]) {
+      o_col_g_reg<float>(it, F(O_taus), F(O_g), F(O_ftmp), F(O_feq), F(O_sal), F(O_u), F(O_v), F(O_w));
+      o_IP_process<float>(it, nb, F(O_g), F(O_feq), F(O_ftmp), F(O_fout), I(O_nextB), I(O_nextK), F(O_px), F(O_py),
+                          F(O_dX), F(O_dY), (int)ip[2]);
+      o_update_scalar<float>(it, F(O_g), F(O_sal));
+    }
+    o_update_rho<float>(it, fp[0], fp[1], F(O_f), F(O_Fx), F(O_Fy), F(O_Fz), F(O_p), F(O_sal), F(O_phi), F(O_rho),
+                        F(O_u), F(O_v), F(O_w));
+    o_set_wall_rho<float>(it, nb, F(O_rho));
+    o_resetF<float>(it, F(O_Fx), F(O_Fy), F(O_Fz), (int)ip[13]);
+  }
+  return 0;
+}
+
+// Moving-IBM order (ref: EllipticalFall2/EllipticalFallxz.cu:344-430).
+// ip[]: 1 nsteps, 2 bc, 3 use_mrt, 6 boussi, 13 num_F, 14 num_Gw; fp[]: 0 rhoL, 1 rhoH
+extern "C" int oracle_ibm_steps_f32(void *const *b, const long long *ip, const float *fp) {
+  const float *it = F(O_items);
+  const int *nb = I(O_neib);
+  const P<float> p(it);
+  for (long long s = 0; s < ip[1]; s++) {
+    o_equ_f<float>(it, F(O_feq), F(O_p), F(O_u), F(O_v), F(O_w));
+    o_Force<float>(it, (int)ip[6], nb, F(O_f), F(O_feq), F(O_tau), F(O_Fk), F(O_Fx), F(O_Fy), F(O_Fz), F(O_p), F(O_rho),
+                   F(O_sal), F(O_phi), F(O_u), F(O_v), F(O_w), F(O_dX), F(O_dY), F(O_px), F(O_py), F(O_pz));
+    if (ip[3])
+      o_col_f_MRT<float>(it, F(O_tau), F(O_f), F(O_ftmp), F(O_feq), F(O_Fk), F(O_M), F(O_Minv), F(O_S), F(O_MM));
+    else
+      o_col_f_SRT<float>(it, F(O_tau), F(O_f), F(O_ftmp), F(O_feq), F(O_Fk));
+    o_IP_process<float>(it, nb, F(O_f), F(O_feq), F(O_ftmp), F(O_fout), I(O_nextB), I(O_nextK), F(O_px), F(O_py),
+                        F(O_dX), F(O_dY), (int)ip[2]);
+    o_update_rho<float>(it, fp[0], fp[1], F(O_f), F(O_Fx), F(O_Fy), F(O_Fz), F(O_p), F(O_sal), F(O_phi), F(O_rho),
+                        F(O_u), F(O_v), F(O_w));
+    o_resetF<float>(it, F(O_Fx), F(O_Fy), F(O_Fz), (int)ip[13]);
+    {  // driver-local set_f_ftmp (ref: EllipticalFallxz.cu:4-13)
+      float *f = F(O_f), *ft = F(O_ftmp);
+      const long n = p.nc * p.Q;
+      OMP_CELLS
+      for (long j = 0; j < n; j++) ft[j] = f[j];
+    }
+    o_get_IBMGw2<float>(it, I(O_lid), nb, F(O_f), F(O_tau), F(O_px), F(O_py), F(O_pz), F(O_posw), F(O_posB), F(O_nB),
+                        F(O_u), F(O_v), F(O_w), F(O_velw), F(O_Fx), F(O_Fy), F(O_Fz), F(O_Gw), fp[1]);
+    o_update_velIBM<float>(it, I(O_lid), F(O_f), F(O_ftmp), F(O_p), F(O_tau), F(O_u), F(O_v), F(O_w), F(O_uo), F(O_vo),
+                           F(O_wo), F(O_Fx), F(O_Fy), F(O_Fz));
+    o_update_IBbody<float>(it, 0, F(O_massB), F(O_densB), F(O_inertia), F(O_FB), F(O_posB), F(O_Torque), F(O_velB),
+                           F(O_quat), F(O_quaS), F(O_angleVB), F(O_posw), F(O_Gw), F(O_quatold), fp[1]);
+    o_update_IBpoint<float>(it, 0, F(O_posB), F(O_velB), F(O_angleVB), F(O_quaS), F(O_posw), F(O_oposw), F(O_nB),
+                            F(O_onB), F(O_velw));
+    o_search_IBlattice<float>(it, 0, I(O_lid), nb, F(O_px), F(O_py), F(O_pz), F(O_posw));
+    o_resetF<float>(it, F(O_Fx), F(O_Fy), F(O_Fz), (int)ip[13]);
+    o_resetF<float>(it, F(O_Gw), F(O_Gw), F(O_Gw), (int)ip[14]);
+  }
+  return 0;
+#undef F
+#undef I
+}
+
+extern "C" int oracle_buf_count() { return O_COUNT; }
+
+// Host threads the OpenMP loops use (1 without OpenMP).
+extern "C" int oracle_num_threads() {
+#ifdef _OPENMP
+  return omp_get_max_threads();
+#else
+  return 1;
+#endif
 }

@@ -23,7 +23,24 @@ ROOT = os.path.dirname(HERE)
 if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 
-from ip_cu_lbm_b200._abi import Binder, ptr  # noqa: E402  (signature tables only)
+
+def _load_abi_tables():
+    """ip_cu_lbm_b200/_abi.py (pure-Python signature tables) loaded as a
+    standalone module, so that the checkers never import the product package."""
+    import importlib.util
+
+    name = "ipcu_abi_tables"
+    if name in sys.modules:
+        return sys.modules[name]
+    spec = importlib.util.spec_from_file_location(name, os.path.join(ROOT, "ip_cu_lbm_b200", "_abi.py"))
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules[name] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+_abi_tables = _load_abi_tables()
+Binder, ptr = _abi_tables.Binder, _abi_tables.ptr
 
 ORACLE_SO = os.path.join(HERE, "_build", "libipcu_oracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libipcu_ref.so")
