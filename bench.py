@@ -127,13 +127,15 @@ def traffic3d(N):
     return int(d["dram_bytes_per_cell"] * N) if d else None
 
 
-def traffic_ib(args):
+def traffic_ib(args, lean):
     """DRAM bytes per launch of the settling-ellipse fluid step (FP32,
-    800 x 3000) from the committed ncu summary (profiles/traffic.json), else None."""
+    800 x 3000; the lean flow-only step or the full one) from the committed
+    ncu summary (profiles/traffic.json), else None."""
     p = os.path.join(ROOT, "profiles", "traffic.json")
     if args.storage != "f32" or not os.path.exists(p):
         return None
-    d = json.load(open(p)).get("step_kernel<float,0,uniform,TMA>@800x3000")
+    key = "step_kernel<float,0,uniform,TMA,lean>@800x3000" if lean else "step_kernel<float,0,uniform,TMA>@800x3000"
+    d = json.load(open(p)).get(key)
     return d["dram_bytes_per_launch"] if d else None
 
 
@@ -486,11 +488,14 @@ def run_ib(args):
         "config": ib_config(meta["nx"], meta["nz"]) if args.storage == "f32" else
         dict(ib_config(meta["nx"], meta["nz"]), storage=args.storage),
         "lbm_steps_per_step": inner, "parallelism": f"replicas x{world}",
-        "scheme": "fused collide-and-stream step + multi-direct forcing (3 iterations, Peskin-4) with an FP64 "
+        "scheme": "fused collide-and-stream step (lean flow-only form: populations only, velocity planes near "
+                  "the body) + multi-direct forcing (3 iterations, Peskin-4) with an FP64 rigid-body update, "
+                  "CUDA-graph replay" if sim.lean() else
+                  "fused collide-and-stream step + multi-direct forcing (3 iterations, Peskin-4) with an FP64 "
                   "rigid-body update, CUDA-graph replay",
         "body_after": {k: round(v, 6) for k, v in b.items() if k in ("x", "z", "w", "theta")},
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                     "frac": round(achieved / peak, 4), "traffic": traffic_ib(args), "bytes_per_cell": bpc,
+                     "frac": round(achieved / peak, 4), "traffic": traffic_ib(args, sim.lean()), "bytes_per_cell": bpc,
                      "peak_source": peak_label(peak_src),
                      "note": "fluid step's algorithmic bytes / (fluid + immersed-boundary kernel time per step); "
                              "traffic = ncu dram read+write bytes of one fluid launch"},

@@ -103,12 +103,15 @@ int ipcu_sim_sync(ipcu_sim *sim);
  * and of S (mac[i]) with cell weights wx[x]*wz[z], written to out[0..1]
  * (all device pointers), without allocating anything. No counterpart in the
  * reference: it exists for callers that cannot allocate device memory where
- * they need the check -- code inside CUDA graph capture, hosts that give all
- * device memory to their own pool, loops that must not enter the driver's
- * allocator. Its scratch is a fixed file-scope device array, so it accepts
- * at most 16,777,216 cells (IPCU_ERR_CAPACITY beyond), the first call on a
- * device resolves that array's address (make it before any capture), and
- * concurrent calls race on the shared array. */
+ * they need the check -- hosts that give all device memory to their own
+ * pool, loops that must not enter the driver's allocator. Its scratch is a
+ * fixed file-scope device array, so it accepts at most 16,777,216 cells
+ * (IPCU_ERR_CAPACITY beyond); the first call on a device resolves that
+ * array's address (make it before any capture, with the stream's device
+ * current); concurrent calls race on the shared array. FP32 populations
+ * only (16-bit storage keeps p* in its own plane: use ipcu_sim_totals).
+ * The result equals ipcu_sim_totals' to rounding, not bit for bit (more
+ * blocks, another FP64 summation order). */
 int ipcu_totals_noalloc_f32(const float *f, const float *mac, const float *wx, const float *wz, int nx, int nz,
                             double *out, ipcu_stream_t stream);
 /* Time steps taken since creation or restore. */
@@ -130,6 +133,19 @@ int64_t ipcu_sim_bytes_per_cell(const ipcu_sim *sim);
 /* FP64 domain sums of S and p* weighted by cell area (dx*dz/dz^2), the
  * reference's conservation diagnostic (ref: function/basic.cu:9-15). */
 int ipcu_sim_totals(ipcu_sim *sim, double *sum_p, double *sum_s);
+/* Lean flow-only step (on by default where allowed: FP32 storage, nx % 4 ==
+ * 0, no scalar lattice, uniform S). The step kernel then moves the nine
+ * populations only: the constant S plane is neither read nor written, and
+ * the velocity planes are stored only in tiles where an immersed body's
+ * force acted; elsewhere the velocity is recomputed from the populations,
+ * bit for bit the value the full step stores (ref: the update_rho moments,
+ * function/collision.cu:238-257). Field reads, downloads and snapshots
+ * complete the planes first. Uploading a non-uniform S plane turns it off.
+ * ipcu_sim_set_lean(sim, 0) forces the full step (IPCU_ERR_UNSUPPORTED when
+ * enabling a configuration that does not allow it); ipcu_sim_lean reports
+ * whether it is on. */
+int ipcu_sim_set_lean(ipcu_sim *sim, int enable);
+int ipcu_sim_lean(const ipcu_sim *sim);
 
 /* Batched stepping of many resident simulations (continuous-batching
  * serving): each call advances every listed simulation by nsteps with one

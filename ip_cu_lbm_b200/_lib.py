@@ -124,6 +124,8 @@ def _declare(L: ctypes.CDLL) -> None:
         "ipcu_sim_device_state": ([P, ctypes.POINTER(P), ctypes.POINTER(P), ctypes.POINTER(P)], I),
         "ipcu_sim_bytes_per_cell": ([P], I64),
         "ipcu_sim_totals": ([P, ctypes.POINTER(D), ctypes.POINTER(D)], I),
+        "ipcu_sim_set_lean": ([P, I], I),
+        "ipcu_sim_lean": ([P], I),
         "ipcu_sim_upload": ([P, P, P, P], I),
         "ipcu_sim_download": ([P, P, P, P], I),
         "ipcu_sim_sync": ([P], I),

@@ -73,7 +73,35 @@ struct alignas(64) Params {
   const float *fext;
   const uint8_t *ibflag;
   int ibtx;
+  // Lean flow-only step (FP32 storage, TMA staging, no scalar lattice, S
+  // uniform): the S plane is constant and never read or written; the
+  // velocity planes of buffer b hold a tile's values only where
+  // ustore[b][tile] = 1 (tiles that carried an immersed-boundary force in
+  // the step that wrote b). Elsewhere the velocity is c j + F0 dt / 2 rho,
+  // recomputed from the populations (F0 = (0, -s_uni g_bouss)), bit for bit
+  // what the step would have stored.
+  uint8_t *ustore[2];
+  int lean, ntx, ntz;
+  float s_uni;
 };
+
+// p*, j_x, j_z of nine populations in the one summation order every kernel
+// and the host use (k = 0..8, starting from zero), so that a velocity
+// recomputed from stored populations equals the one stored beside them.
+__host__ __device__ __forceinline__ void moments9(const float (&f)[9], float &pr, float &jx, float &jz) {
+  constexpr int ex[9] = {0, 1, 0, -1, 0, 1, -1, -1, 1}, ez[9] = {0, 0, 1, 0, -1, 1, 1, -1, -1};
+  pr = 0.f;
+  jx = 0.f;
+  jz = 0.f;
+#pragma unroll
+  for (int k = 0; k < 9; k++) {
+    pr += f[k];
+    if (ex[k] > 0) jx += f[k];
+    if (ex[k] < 0) jx -= f[k];
+    if (ez[k] > 0) jz += f[k];
+    if (ez[k] < 0) jz -= f[k];
+  }
+}
 
 // prepare_only: set the kernel's shared-memory attribute (call once before any capture);
 // p.pf selects the phase-field kernels

@@ -209,9 +209,11 @@ struct Fast {
 // kernel; the tensor maps live in the __grid_constant__ parameters).
 // tm: the tensor maps (tm_f[2], tm_g[2], tm_m[2], contiguous) of the
 // simulation, in parameter or global memory (TMA staging only).
-template <class ST, int QS, int GEO, bool TMA, int PHYS>
+// LEAN: the lean flow-only step (Params::lean; FP32, TMA, no scalar lattice).
+template <class ST, int QS, int GEO, bool TMA, int PHYS, bool LEAN = false>
 __device__ __forceinline__ void step_tile(const Params &p, int parity, int tile_x, int tile_z, float *smem,
                                           const CUtensorMap *tm = nullptr) {
+  static_assert(!LEAN || (TMA && QS == 0 && PHYS == 0 && sizeof(ST) == 4), "lean step: FP32 TMA flow only");
   using G = Geo<GEO, TMA>;
   using SL = Smem<QS, GEO, TMA, (int)sizeof(ST)>;
   constexpr int HZ = G::HZ, EX = G::EX, NE = G::NE, SZ = G::SZ, RX = G::RX, RO = G::RO;
@@ -256,6 +258,24 @@ __device__ __forceinline__ void step_tile(const Params &p, int parity, int tile_
   const bool ibt = p.fext != nullptr &&
                    *reinterpret_cast<const volatile uint8_t *>(p.ibflag + tile_z * p.ibtx + tile_x) != 0;
   if (ibt) asm volatile("griddepcontrol.wait;" ::: "memory");
+  // lean step: which of the 3 x 3 tiles around this one hold their velocity
+  // planes in the input buffer (bit (dz + 1) * 3 + (dx + 1)); the staged
+  // macroscopic box is loaded only when one of them does. The mask sits in
+  // the spare word after the mbarrier (no static shared memory: the z3 tile
+  // fills four CTAs' share of the SM exactly).
+  unsigned &lean_nbf = *reinterpret_cast<unsigned *>(smem + SL::B0 + 2);
+  if constexpr (LEAN) {
+    if (tid == 0) {
+      unsigned m = 0;
+      const uint8_t *us = p.ustore[bi];
+      for (int dzz = -1; dzz <= 1; dzz++)
+        for (int dxx = -1; dxx <= 1; dxx++) {
+          const int tx = tile_x + dxx, tz = tile_z + dzz;
+          if (tx >= 0 && tx < p.ntx && tz >= 0 && tz < p.ntz && us[tz * p.ntx + tx]) m |= 1u << ((dzz + 1) * 3 + dxx + 1);
+        }
+      lean_nbf = m;
+    }
+  }
 
   // ---- phase 0: stage the tile (TMA) or the salinity ring, and the axis weights
   if (tid == 0) *qcount = 0;
@@ -272,6 +292,12 @@ __device__ __forceinline__ void step_tile(const Params &p, int parity, int tile_
         tma_load_3d(smem_u32(smem + SL::H0), &tm[bi], ox - 4, oz, 0, bar_a);
         if constexpr (QS > 0) tma_load_3d(smem_u32(smem + SL::HG), &tm[2 + bi], ox - 4, oz, 0, bar_a);
         tma_load_3d(smem_u32(sS), &tm[4 + bi], ox, oz - 1, 0, bar_a);
+      } else if constexpr (LEAN) {
+        const bool need_mac = lean_nbf != 0;
+        const unsigned bytes = 4u * (unsigned)(9 * NE + (need_mac ? 3 * SZ * RX : 0));
+        mbar_expect_tx(bar_a, bytes);
+        tma_load_3d(smem_u32(sf), &tm[bi], ox, oz, 0, bar_a);
+        if (need_mac) tma_load_3d(smem_u32(sS), &tm[4 + bi], ox, oz - 1, 0, bar_a);
       } else {
         constexpr unsigned bytes = 4u * (unsigned)((9 + QS) * NE + 3 * SZ * RX);
         mbar_expect_tx(bar_a, bytes);
@@ -321,8 +347,9 @@ __device__ __forceinline__ void step_tile(const Params &p, int parity, int tile_
       return;
     }
     // the box reads zeros outside the domain: give the ring's outside cells
-    // their clamped (owner) salinity, as the ghosts carry it
-    if (ox < 0 || ox + EX > nx || oz - 1 < 0 || oz - 1 + SZ > nz) {
+    // their clamped (owner) salinity, as the ghosts carry it (the lean step
+    // reads no salinity)
+    if (!LEAN && (ox < 0 || ox + EX > nx || oz - 1 < 0 || oz - 1 + SZ > nz)) {
       for (int e = tid; e < SZ * RX; e += kThreads) {
         const int lz = e / RX, lx = e - lz * RX;
         const int gx = ox + lx, gz = oz - 1 + lz;
@@ -363,8 +390,24 @@ __device__ __forceinline__ void step_tile(const Params &p, int parity, int tile_
 #pragma unroll
         for (int k = 0; k < QS; k++) g[k] = sg[k * NE + e];
       }
-      u = sS[SZ * RX + rs];
-      w = sS[2 * SZ * RX + rs];
+      if constexpr (LEAN) {
+        // the owner tile's velocity planes, or the velocity its last step
+        // formed without a body force: c j + F0 dt / 2 rho
+        const int otx = lx < XO ? 0 : (lx >= XO + kTX ? 2 : 1), otz = lz < HZ ? 0 : (lz >= HZ + kTZ ? 2 : 1);
+        if ((lean_nbf >> (otz * 3 + otx)) & 1u) {
+          u = sS[SZ * RX + rs];
+          w = sS[2 * SZ * RX + rs];
+        } else {
+          float p0, jx0, jz0;
+          moments9(f, p0, jx0, jz0);
+          const float h0 = __fdividef(p.hdt, rho_of(p.s_uni));
+          u = fmaf(0.0f, h0, c * jx0);
+          w = fmaf(-(p.s_uni * p.g_bouss_f), h0, c * jz0);
+        }
+      } else {
+        u = sS[SZ * RX + rs];
+        w = sS[2 * SZ * RX + rs];
+      }
     } else {
       const long long ci = (long long)gz * nx + gx;
 #pragma unroll
@@ -375,7 +418,7 @@ __device__ __forceinline__ void step_tile(const Params &p, int parity, int tile_
       w = mac_in[2 * N + ci];
       if constexpr (RES) pr = mac_in[3 * N + ci];
     }
-    const float S = sS[rs], rho = rho_of(S);
+    const float S = LEAN ? p.s_uni : sS[rs], rho = rho_of(S);
     // p* (ref: collision.cu:244-246)
     if constexpr (!RES) {
 #pragma unroll
@@ -387,8 +430,9 @@ __device__ __forceinline__ void step_tile(const Params &p, int parity, int tile_
     const float gix = (p.gconst & 1) ? (gx == 0 ? p.gix3[0] : (gx == nx - 1 ? p.gix3[2] : p.gix3[1]))
                                      : __ldg(p.ginvx + gx);
     const float giz = sGI[lz];
-    float Fx = -pc * ((rho_of(sS[rs + 1]) - rho_of(sS[rs - 1])) * gix);
-    float Fz = -pc * ((rho_of(sS[rs + RX]) - rho_of(sS[rs - RX])) * giz);
+    // (uniform S in the lean step: no density gradient)
+    float Fx = LEAN ? 0.0f : -pc * ((rho_of(sS[rs + 1]) - rho_of(sS[rs - 1])) * gix);
+    float Fz = LEAN ? 0.0f : -pc * ((rho_of(sS[rs + RX]) - rho_of(sS[rs - RX])) * giz);
     float dpx = 0.f, dpz = 0.f;  // grad(phi) (phase field)
     if constexpr (PHYS == 1) {
       // chemical potential of the double well, mu = 4 beta phi (phi - 1)(phi - 1/2)
@@ -628,25 +672,21 @@ __device__ __forceinline__ void step_tile(const Params &p, int parity, int tile_
 
   // moments and store of one cell from its streamed populations
   auto finish = [&](int e, long long ci, int rc, const float (&fv)[9], const float (&gv)[QS > 0 ? QS : 1]) {
-    float pr = 0.f, jx = 0.f, jz = 0.f;
-#pragma unroll
-    for (int k = 0; k < 9; k++) {
-      const float v = fv[k];
-      pr += v;
-      if (ex(k)) jx += ex(k) * v;
-      if (ez(k)) jz += ez(k) * v;
-    }
+    float pr, jx, jz;
+    moments9(fv, pr, jx, jz);
     float S = 0.f;
     if constexpr (QS > 0) {
 #pragma unroll
       for (int k = 0; k < QS; k++) S += gv[k];
+    } else if constexpr (LEAN) {
+      S = p.s_uni;
     } else {
       S = sS[rc];
     }
     // moments (ref: collision.cu:244-254)
     const float h = __fdividef(p.hdt, rho_of(S));
     const float Fx = TMA ? sS[SZ * RX + rc] : sF[e], Fz = TMA ? sS[2 * SZ * RX + rc] : sF[kTX * kTZ + e];
-    const float ux = c * jx + Fx * h, uz = c * jz + Fz * h;
+    const float ux = fmaf(Fx, h, c * jx), uz = fmaf(Fz, h, c * jz);
     if constexpr (RES) {
       // deviations from the equilibrium of the moments stored beside them
       const float ucn = ux * ic, wcn = uz * ic, u2 = rstore::usq(ucn, wcn);
@@ -671,9 +711,17 @@ __device__ __forceinline__ void step_tile(const Params &p, int parity, int tile_
 #pragma unroll
       for (int k = 0; k < QS; k++) st(g_out, k * N + ci, gv[k], 1.0f);
     }
-    mac_out[ci] = S;
-    mac_out[N + ci] = ux;
-    mac_out[2 * N + ci] = uz;
+    if constexpr (LEAN) {
+      // velocity planes only where a body force acted (recomputable elsewhere)
+      if (ibt) {
+        mac_out[N + ci] = ux;
+        mac_out[2 * N + ci] = uz;
+      }
+    } else {
+      mac_out[ci] = S;
+      mac_out[N + ci] = ux;
+      mac_out[2 * N + ci] = uz;
+    }
     if (!(isfinite(ux) && isfinite(uz) && isfinite(S) && isfinite(pr))) atomicOr(p.status, 1u);
   };
   // general path: clamped stencils, ghost rules (cells next to a wall)
@@ -746,6 +794,9 @@ __device__ __forceinline__ void step_tile(const Params &p, int parity, int tile_
   __syncthreads();
   const int nq = min(*qcount, kQueue);
   for (int j = tid; j < nq; j += kThreads) general(queue[j]);
+  if constexpr (LEAN) {
+    if (tid == 0) p.ustore[bo][tile_z * p.ntx + tile_x] = ibt ? 1 : 0;
+  }
 }
 
 // Resident CTAs per SM the single-run kernel's registers are sized for. The
@@ -759,11 +810,11 @@ constexpr int step_min_blocks() {
   return (QS == 0 && TMA && sizeof(ST) == 4) ? 5 : kMinBlocks;
 }
 
-template <class ST, int QS, int GEO, bool TMA, int PHYS>
+template <class ST, int QS, int GEO, bool TMA, int PHYS, bool LEAN = false>
 __global__ void __launch_bounds__(kThreads, step_min_blocks<ST, QS, TMA>())
     step_kernel(const __grid_constant__ Params p) {
   extern __shared__ __align__(128) float smem[];
-  step_tile<ST, QS, GEO, TMA, PHYS>(p, 0, blockIdx.x, blockIdx.y, smem, p.tm_f);
+  step_tile<ST, QS, GEO, TMA, PHYS, LEAN>(p, 0, blockIdx.x, blockIdx.y, smem, p.tm_f);
 }
 
 // The batched kernel copies each work item's parameters (past the tensor
@@ -853,22 +904,29 @@ int launch_bg(const Params *ps, const WorkItem *work, int nwork, int parity, int
   return IPCU_ERR_UNSUPPORTED;
 }
 
-template <class ST, int QS, int GEO, bool TMA, int PHYS>
+template <class ST, int QS, int GEO, bool TMA, int PHYS, bool LEAN = false>
 int launch_t1(const Params &p, cudaStream_t s, bool prepare_only) {
   constexpr size_t sm = smem_bytes<QS, GEO, TMA, (int)sizeof(ST)>();
   if (prepare_only) {  // once per sim, outside any stream capture
-    return status_from_cuda(cudaFuncSetAttribute(step_kernel<ST, QS, GEO, TMA, PHYS>,
+    return status_from_cuda(cudaFuncSetAttribute(step_kernel<ST, QS, GEO, TMA, PHYS, LEAN>,
                                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
   }
   dim3 grid((p.nx + kTX - 1) / kTX, (p.nz + kTZ - 1) / kTZ);
-  if (p.fext) return launch_pdl(step_kernel<ST, QS, GEO, TMA, PHYS>, grid, sm, s, p);
-  step_kernel<ST, QS, GEO, TMA, PHYS><<<grid, kThreads, sm, s>>>(p);
+  if (p.fext) return launch_pdl(step_kernel<ST, QS, GEO, TMA, PHYS, LEAN>, grid, sm, s, p);
+  step_kernel<ST, QS, GEO, TMA, PHYS, LEAN><<<grid, kThreads, sm, s>>>(p);
   return status_from_cuda(cudaGetLastError());
 }
 
-// TMA staging for FP32 storage when the host built the tensor maps (p.tma)
+// TMA staging for FP32 storage when the host built the tensor maps (p.tma);
+// the lean flow-only step where the host enabled it (p.lean)
 template <class ST, int QS, int GEO, int PHYS>
 int launch_t(const Params &p, cudaStream_t s, bool prepare_only) {
+  if constexpr (QS == 0 && PHYS == 0 && sizeof(ST) == 4) {
+    if (p.tma && (p.lean || prepare_only)) {
+      const int st = launch_t1<ST, QS, GEO, true, PHYS, true>(p, s, prepare_only);
+      if (!prepare_only || st) return st;
+    }
+  }
   if (p.tma) return launch_t1<ST, QS, GEO, true, PHYS>(p, s, prepare_only);
   return launch_t1<ST, QS, GEO, false, PHYS>(p, s, prepare_only);
 }

@@ -58,6 +58,31 @@ namespace ib2d {
 
 namespace {
 
+// Velocity of cell ci in buffer b, the one the fluid step wrote: its
+// velocity planes, or, after a lean flow-only step in a tile without a body
+// force, c j + F0 dt / 2 rho from the populations (the value that step
+// would have stored, bit for bit).
+__device__ __forceinline__ void vel_at(const f2d::Params &p, int b, const float *mac, long long ci, long long N,
+                                       float &ux, float &uz) {
+  if (p.lean) {
+    const int x = (int)(ci % p.nx), z = (int)(ci / p.nx);
+    if (!p.ustore[b][(z / f2d::kTZ) * p.ntx + x / f2d::kTX]) {
+      const float *fb = static_cast<const float *>(p.fbuf[b]);
+      float fv[9];
+#pragma unroll
+      for (int k = 0; k < 9; k++) fv[k] = fb[k * N + ci];
+      float pr, jx, jz;
+      f2d::moments9(fv, pr, jx, jz);
+      const float h0 = __fdividef(p.hdt, fmaf(p.s_uni, p.rho_sal_f, p.rho_base));
+      ux = fmaf(0.0f, h0, p.c * jx);
+      uz = fmaf(-(p.s_uni * p.g_bouss_f), h0, p.c * jz);
+      return;
+    }
+  }
+  ux = mac[N + ci];
+  uz = mac[2 * N + ci];
+}
+
 constexpr int kWarps = kThreads / 32;
 constexpr int kGroups = kThreads / 16;  // 16 lanes (one 4x4 stencil) per marker
 constexpr int kTileMap = 1024;          // tiles tracked around the footprints for the flag clean-up
@@ -247,11 +272,13 @@ __device__ void coupled_update(const Job &j, int parity) {
   const float rho0 = p.rho_base, rsal = p.rho_sal_f, hdt = p.hdt;
   for (int s = tid; s < ns; s += kThreads) {
     const long long ci = sCell[s];
-    const float S = mac[ci];
+    const float S = p.lean ? p.s_uni : mac[ci];
     const float h = hdt / fmaf(S, rsal, rho0);
+    float ux, uz;
+    vel_at(p, b, mac, ci, N, ux, uz);
     sH[s] = h;
-    sU[s] = mac[N + ci] - j.fext[ci] * h;
-    sW[s] = mac[2 * N + ci] - j.fext[N + ci] * h;
+    sU[s] = ux - j.fext[ci] * h;
+    sW[s] = uz - j.fext[N + ci] * h;
     sFX[s] = sFZ[s] = 0.f;
     sCur[s] = 0;
   }
@@ -443,7 +470,9 @@ __device__ void coupled_update(const Job &j, int parity) {
         const double al = fmin(fmax(0.5 - F / fmax(G, 1e-300) * idz, 0.0), 1.0) * dA;
         if (al > 0.0) {
           const long long ci = (long long)k * nx + i;
-          const double ux = mac[N + ci], uz = mac[2 * N + ci];
+          float uxf, uzf;
+          vel_at(p, b, mac, ci, N, uxf, uzf);
+          const double ux = uxf, uz = uzf;
           acc[3] += al * ux;
           acc[4] += al * uz;
           acc[5] += al * (dx * uz - dzz * ux);

@@ -45,6 +45,13 @@ struct ipcu_sim {
   // moving immersed boundary (null without a body): device state and the
   // coupled update's parameters (fp filled per launch)
   ib2d::Job *ib = nullptr;
+  // lean flow-only step (f2d::Params::lean): per-parity tile flags of
+  // stored velocity planes; lean_ok: the configuration allows it
+  uint8_t *ustore[2] = {nullptr, nullptr};
+  bool lean_ok = false;
+  int ntiles = 0;
+  // area weights dx dz / dz^2 per column and row (conservation totals)
+  float *twx = nullptr, *twz = nullptr;
 };
 
 // Macroscopic planes: S, u_x, u_z (+ p* with 16-bit storage)
@@ -227,6 +234,27 @@ __global__ void k_init_g(const float *S, int q, float *g, long long N) {
   }
 }
 
+// Lean flow-only step: completes the velocity planes of buffer b in the
+// tiles whose last step did not store them (ustore[b][tile] == 0), with the
+// value that step formed, c j + F0 dt / 2 rho from the populations.
+__global__ void k_lean_fill(const __grid_constant__ f2d::Params P, int b) {
+  const long long N = (long long)P.nx * P.nz;
+  const float *fb = static_cast<const float *>(P.fbuf[b]);
+  float *mac = P.mbuf[b];
+  const float h0 = __fdividef(P.hdt, fmaf(P.s_uni, P.rho_sal_f, P.rho_base));
+  IPCU_FOR(i, 0, N) {
+    const int x = (int)(i % P.nx), z = (int)(i / P.nx);
+    if (P.ustore[b][(z / f2d::kTZ) * P.ntx + x / f2d::kTX]) continue;
+    float fv[9];
+#pragma unroll
+    for (int k = 0; k < 9; k++) fv[k] = fb[k * N + i];
+    float pr, jx, jz;
+    f2d::moments9(fv, pr, jx, jz);
+    mac[N + i] = fmaf(0.0f, h0, P.c * jx);
+    mac[2 * N + i] = fmaf(-(P.s_uni * P.g_bouss_f), h0, P.c * jz);
+  }
+}
+
 // FP64 area-weighted sums of p* (sum of f) and S, two-pass deterministic
 // (per-block partials, then one block in fixed order).
 // (16-bit storage keeps p* in the 4th macroscopic plane; pass f = nullptr)
@@ -329,6 +357,10 @@ void free_sim(ipcu_sim *s) {
   fr(s->obuf[1]);
   fr(s->ilx2);
   fr(s->ilz2);
+  fr(s->ustore[0]);
+  fr(s->ustore[1]);
+  fr(s->twx);
+  fr(s->twz);
   if (s->ib) {
     fr(s->ib->body);
     fr((void *)s->ib->X0);
@@ -349,6 +381,46 @@ int upload(V **dst, const std::vector<V> &src) {
   if (cudaMalloc((void **)dst, sizeof(V) * src.size()) != cudaSuccess) return IPCU_ERR_NOMEM;
   return cudaMemcpy(*dst, src.data(), sizeof(V) * src.size(), cudaMemcpyHostToDevice) == cudaSuccess ? IPCU_OK
                                                                                                       : IPCU_ERR_CUDA;
+}
+
+// ---- lean flow-only step bookkeeping
+// The current buffer's velocity planes made complete (before anything reads
+// them from outside the lean kernels: field reads, downloads, snapshots,
+// batched steps).
+int lean_fill(ipcu_sim *s) {
+  if (!s->P.lean) return IPCU_OK;
+  const Launch L = launch_for(s->N);
+  k_lean_fill<<<L.grid, L.block, 0, s->stream>>>(s->P, s->cur);
+  return status_from_cuda(cudaGetLastError());
+}
+// Every tile of the current buffer holds its velocity planes (after an
+// upload, or after batched steps).
+int lean_mark_all(ipcu_sim *s) {
+  if (!s->ustore[0]) return IPCU_OK;
+  return status_from_cuda(cudaMemsetAsync(s->ustore[s->cur], 1, (size_t)s->ntiles, s->stream));
+}
+void drop_graphs(ipcu_sim *s) {
+  cudaStreamSynchronize(s->stream);
+  for (int i = 0; i < 2; i++)
+    if (s->graph[i]) {
+      cudaGraphExecDestroy(s->graph[i]);
+      s->graph[i] = nullptr;
+    }
+  s->graph_chunk = 0;
+}
+// A new S plane was written to the current buffer: the lean step stays on
+// only while S is uniform at the value it was set up with.
+void lean_check_s(ipcu_sim *s, const float *S) {
+  if (!s->lean_ok) return;
+  for (long long i = 0; i < s->N; i++)
+    if (S[i] != s->P.s_uni) {
+      s->lean_ok = false;
+      if (s->P.lean) {
+        s->P.lean = 0;
+        drop_graphs(s);
+      }
+      return;
+    }
 }
 
 }  // namespace
@@ -575,6 +647,37 @@ extern "C" int ipcu_sim_create(const ipcu_sim_config *cfg, const double *s0, ipc
     }
     P.tma = ok ? 1 : 0;
   }
+  // tiles, and the lean flow-only step where the configuration allows it:
+  // FP32 storage with TMA staging, no scalar lattice, a uniform S
+  P.ntx = (c.nx + f2d::kTX - 1) / f2d::kTX;
+  P.ntz = (c.nz + f2d::kTZ - 1) / f2d::kTZ;
+  s->ntiles = P.ntx * P.ntz;
+  {
+    bool uni = true;
+    const float s00 = s0 ? (float)s0[0] : 0.f;
+    for (long long i = 1; s0 && i < s->N && uni; i++) uni = (float)s0[i] == s00;
+    s->lean_ok = c.storage == IPCU_STORE_F32 && c.q_scalar == 0 && !pf && P.tma && uni;
+    P.s_uni = s00;
+    if (s->lean_ok) {
+      if (!salloc(s, &s->ustore[0], (size_t)s->ntiles) || !salloc(s, &s->ustore[1], (size_t)s->ntiles)) {
+        free_sim(s);
+        return IPCU_ERR_NOMEM;
+      }
+      P.ustore[0] = s->ustore[0];
+      P.ustore[1] = s->ustore[1];
+      P.lean = 1;
+    }
+  }
+  {
+    std::vector<float> wxv(c.nx), wzv(c.nz);
+    for (int i = 0; i < c.nx; i++) wxv[i] = (float)(s->DX[i] / dz);
+    for (int l = 0; l < c.nz; l++) wzv[l] = (float)(s->DZ[l] / dz);
+    if ((st = supload(s, &s->twx, wxv)) == IPCU_OK) st = supload(s, &s->twz, wzv);
+    if (st != IPCU_OK) {
+      free_sim(s);
+      return st;
+    }
+  }
   st = f2d::launch_step(P, c.storage, c.q_scalar, c.geometry, s->stream, true);
   if (st != IPCU_OK) {
     free_sim(s);
@@ -590,9 +693,17 @@ extern "C" int ipcu_sim_create(const ipcu_sim_config *cfg, const double *s0, ipc
     const int cb = s->cur;
     cudaError_t e = cudaMemsetAsync(s->f[cb], 0, s->esz * 9 * N, s->stream);
     if (e == cudaSuccess && c.q_scalar) e = cudaMemsetAsync(s->g[cb], 0, s->esz * c.q_scalar * N, s->stream);
-    if (e == cudaSuccess) e = cudaMemsetAsync(s->mac[cb], 0, sizeof(float) * nmac(s) * N, s->stream);
-    if (e == cudaSuccess)
-      e = cudaMemcpyAsync(s->mac[cb], S0f.data(), sizeof(float) * N, cudaMemcpyHostToDevice, s->stream);
+    // both buffers' macroscopic planes start at S0, u = 0 (the lean step
+    // never writes the S plane)
+    for (int i = 0; i < 2 && e == cudaSuccess; i++) {
+      e = cudaMemsetAsync(s->mac[i], 0, sizeof(float) * nmac(s) * N, s->stream);
+      if (e == cudaSuccess)
+        e = cudaMemcpyAsync(s->mac[i], S0f.data(), sizeof(float) * N, cudaMemcpyHostToDevice, s->stream);
+    }
+    if (e == cudaSuccess && s->ustore[0]) {
+      e = cudaMemsetAsync(s->ustore[cb], 1, (size_t)s->ntiles, s->stream);
+      if (e == cudaSuccess) e = cudaMemsetAsync(s->ustore[cb ^ 1], 0, (size_t)s->ntiles, s->stream);
+    }
     if (e == cudaSuccess && c.q_scalar && c.storage == IPCU_STORE_F32) {
       Launch L = launch_for(N);
       k_init_g<<<L.grid, L.block, 0, s->stream>>>(s->mac[cb], c.q_scalar, (float *)s->g[cb], N);
@@ -758,7 +869,25 @@ extern "C" int ipcu_sim_ib_attach(ipcu_sim *s, const ipcu_ib_body2d *bd, const d
   if (e == cudaSuccess) e = cudaMemsetAsync(j->org, 0, sizeof(int) * 2 * n, s->stream);
   if (e == cudaSuccess) e = cudaMemsetAsync(j->org2, 0, sizeof(int) * 2 * n, s->stream);
   if (e == cudaSuccess) e = cudaMemsetAsync(j->fext, 0, sizeof(float) * 2 * N, s->stream);
-  if (e == cudaSuccess) e = cudaMemsetAsync(j->flag, 0, (size_t)tx * tz, s->stream);
+  // the tiles whose halo may reach the initial markers' 4x4 stencils are
+  // flagged from the start, as each update flags its successor's footprint:
+  // the first fluid step then already stores the velocity the first update
+  // reads there (lean flow-only step)
+  std::vector<uint8_t> fl((size_t)tx * tz, 0);
+  {
+    const double ct = std::cos(bd->theta), sn = std::sin(bd->theta), idz = 1.0 / s->cfg.dz;
+    auto tile_of = [&](int v, int nmax, int t) { return std::min(std::max(v, 0), nmax - 1) / t; };
+    for (int l = 0; l < n; l++) {
+      const double X = bd->xc + ct * markers[2 * l] - sn * markers[2 * l + 1];
+      const double Z = bd->zc + sn * markers[2 * l] + ct * markers[2 * l + 1];
+      const int i0 = (int)std::floor(X * idz - 0.5) - 1, k0 = (int)std::floor(Z * idz - 0.5) - 1;
+      const int xa = tile_of(i0 - ib2d::kHalo, s->nx, f2d::kTX), xb = tile_of(i0 + 3 + ib2d::kHalo, s->nx, f2d::kTX);
+      const int za = tile_of(k0 - ib2d::kHalo, s->nz, f2d::kTZ), zb = tile_of(k0 + 3 + ib2d::kHalo, s->nz, f2d::kTZ);
+      for (int zt : {za, zb})
+        for (int xt : {xa, xb}) fl[(size_t)zt * tx + xt] = 1;
+    }
+  }
+  if (e == cudaSuccess) e = cudaMemcpyAsync(j->flag, fl.data(), fl.size(), cudaMemcpyHostToDevice, s->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
   if (e != cudaSuccess) return IPCU_ERR_CUDA;
   j->nl = n;
@@ -794,11 +923,14 @@ extern "C" int64_t ipcu_sim_bytes_per_cell(const ipcu_sim *sim) {
   // every stored distribution and the macroscopic planes are read once and written once
   // (the phase field also reads and writes the previous step's phi u, phi w)
   const int old = sim->cfg.scalar_kind == IPCU_SCALAR_PHASE ? 2 : 0;
+  // (the lean flow-only step reads and writes the nine populations only)
+  if (sim->P.lean) return 2 * (int64_t)sim->esz * 9;
   return 2 * ((int64_t)sim->esz * (9 + sim->cfg.q_scalar) + 4 * (nmac(sim) + old));
 }
 
 extern "C" int ipcu_sim_device_state(ipcu_sim *sim, void **f, void **g, float **mac) {
   if (!sim) return IPCU_ERR_ARG;
+  if (int st = lean_fill(sim)) return st;
   if (f) *f = sim->f[sim->cur];
   if (g) *g = sim->g[sim->cur];
   if (mac) *mac = sim->mac[sim->cur];
@@ -818,6 +950,7 @@ static int state_download(ipcu_sim *s, HostState &h) {
   h.f.resize(9 * N);
   h.g.resize((size_t)q * N);
   h.mac.assign(4 * N, 0.f);
+  if (int st = lean_fill(s)) return st;
   if (cudaStreamSynchronize(s->stream) != cudaSuccess ||
       cudaMemcpy(fb.data(), s->f[s->cur], fb.size(), cudaMemcpyDeviceToHost) != cudaSuccess ||
       (q && cudaMemcpy(gb.data(), s->g[s->cur], gb.size(), cudaMemcpyDeviceToHost) != cudaSuccess) ||
@@ -873,6 +1006,8 @@ static int state_upload(ipcu_sim *s, const HostState &h) {
       (q && cudaMemcpy(s->g[s->cur], gb.data(), gb.size(), cudaMemcpyHostToDevice) != cudaSuccess) ||
       cudaMemcpy(s->mac[s->cur], h.mac.data(), sizeof(float) * nm * N, cudaMemcpyHostToDevice) != cudaSuccess)
     return IPCU_ERR_CUDA;
+  lean_check_s(s, h.mac.data());
+  if (int st = lean_mark_all(s)) return st;
   if (s->obuf[s->cur]) {
     // phase field: the previous step's phi u is taken equal to this state's,
     // so the d(phi u)/dt term starts at zero (the reference driver's
@@ -943,6 +1078,7 @@ extern "C" int ipcu_sim_get(ipcu_sim *s, const char *field, double *out, int64_t
   // macroscopic planes straight from the device; p* with FP32 storage and
   // the populations need the whole state
   if (slot >= 0 && (slot < 3 || nmac(s) == 4)) {
+    if (int st = lean_fill(s)) return st;
     std::vector<float> m(N);
     if (cudaStreamSynchronize(s->stream) != cudaSuccess ||
         cudaMemcpy(m.data(), s->mac[s->cur] + (long long)slot * N, sizeof(float) * N, cudaMemcpyDeviceToHost) !=
@@ -978,24 +1114,13 @@ extern "C" int ipcu_sim_status(ipcu_sim *s, uint32_t *flags) {
 
 extern "C" int ipcu_sim_totals(ipcu_sim *s, double *sum_p, double *sum_s) {
   if (!s) return IPCU_ERR_ARG;
-  // area weights (dx dz / dz^2) from the cell widths, FP32 copies on the device
-  std::vector<float> wx(s->nx), wz(s->nz);
-  for (int i = 0; i < s->nx; i++) wx[i] = (float)(s->DX[i] / s->cfg.dz);
-  for (int l = 0; l < s->nz; l++) wz[l] = (float)(s->DZ[l] / s->cfg.dz);
-  float *dwx = nullptr, *dwz = nullptr;
-  if (upload(&dwx, wx) || upload(&dwz, wz)) {
-    cudaFree(dwx);
-    cudaFree(dwz);
-    return IPCU_ERR_NOMEM;
-  }
+  // area weights (dx dz / dz^2) resident on the device since creation
   const float *f32 = s->cfg.storage == IPCU_STORE_F32 ? (const float *)s->f[s->cur] : nullptr;
-  k_totals<<<kTotBlocks, 256, 0, s->stream>>>(f32, s->mac[s->cur], dwx, dwz, s->nx, s->nz, s->partials);
+  k_totals<<<kTotBlocks, 256, 0, s->stream>>>(f32, s->mac[s->cur], s->twx, s->twz, s->nx, s->nz, s->partials);
   k_totals_final<<<1, 32, 0, s->stream>>>(s->partials, kTotBlocks, s->partials + 2 * kTotBlocks);
   double h[2] = {0, 0};
   cudaError_t e = cudaMemcpyAsync(h, s->partials + 2 * kTotBlocks, sizeof h, cudaMemcpyDeviceToHost, s->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
-  cudaFree(dwx);
-  cudaFree(dwz);
   if (e != cudaSuccess) return IPCU_ERR_CUDA;
   if (sum_p) *sum_p = h[0];
   if (sum_s) *sum_s = h[1];
@@ -1010,12 +1135,20 @@ extern "C" int ipcu_sim_upload(ipcu_sim *s, const void *f, const void *g, const 
   if (e == cudaSuccess && g && s->cfg.q_scalar)
     e = cudaMemcpyAsync(s->g[s->cur], g, s->esz * s->cfg.q_scalar * N, cudaMemcpyHostToDevice, s->stream);
   if (e == cudaSuccess && mac) e = cudaMemcpyAsync(s->mac[s->cur], mac, sizeof(float) * nmac(s) * N, cudaMemcpyHostToDevice, s->stream);
-  return e == cudaSuccess ? IPCU_OK : IPCU_ERR_CUDA;
+  if (e != cudaSuccess) return IPCU_ERR_CUDA;
+  if (mac) {
+    lean_check_s(s, mac);  // (reads the host buffer, which the copy only reads too)
+    return lean_mark_all(s);
+  }
+  return IPCU_OK;
 }
 
 extern "C" int ipcu_sim_download(ipcu_sim *s, void *f, void *g, float *mac) {
   if (!s) return IPCU_ERR_ARG;
   const long long N = s->N;
+  if (mac) {
+    if (int st = lean_fill(s)) return st;
+  }
   cudaError_t e = cudaSuccess;
   if (f) e = cudaMemcpyAsync(f, s->f[s->cur], s->esz * 9 * N, cudaMemcpyDeviceToHost, s->stream);
   if (e == cudaSuccess && g && s->cfg.q_scalar)
@@ -1033,16 +1166,16 @@ extern "C" int32_t ipcu_sim_storage_bytes(const ipcu_sim *s) { return s ? (int32
 
 // ---------------------------------------------------------------------------
 // Allocation-free totals. Some callers cannot allocate device memory at the
-// point where they need the conservation check: code running inside CUDA
-// graph capture (an allocation is not a capturable stream operation), hosts
-// that hand all device memory to their own pool at start-up, and real-time
-// loops that must not hit the driver's allocator. This entry point runs the
-// same two-pass reduction as ipcu_sim_totals but keeps its per-block partial
-// sums in a file-scope device array instead of allocated scratch.
+// point where they need the conservation check: hosts that hand all device
+// memory to their own pool at start-up, and real-time loops that must not
+// hit the driver's allocator. This entry point runs the same two-pass
+// reduction as ipcu_sim_totals (with up to 1024 blocks instead of 296, so
+// the two agree to rounding, not bit for bit) but keeps its per-block
+// partial sums in a file-scope device array instead of allocated scratch.
 //
 // Limit: kNoAllocBlocks partials of kNoAllocCells cells each, i.e. at most
 // 1024 * 16384 = 16,777,216 cells; larger fields are rejected with
-// IPCU_ERR_CAPACITY. The array occupies 16.4 KB on every device that loads
+// IPCU_ERR_CAPACITY. The array occupies 16 KB on every device that loads
 // the library, until the process exits. Every call shares it and it keeps
 // the last call's contents: each call writes every partial it reads, so
 // nothing needs clearing, but calls whose kernels overlap on the GPU (two
@@ -1050,7 +1183,7 @@ extern "C" int32_t ipcu_sim_storage_bytes(const ipcu_sim *s) { return s ? (int32
 // caller.
 constexpr int kNoAllocBlocks = 1024;
 constexpr long long kNoAllocCells = 16384;
-static __device__ __align__(256) double g_noalloc_partials[2 * kNoAllocBlocks + 2];
+static __device__ __align__(256) double g_noalloc_partials[2 * kNoAllocBlocks];
 
 extern "C" int ipcu_totals_noalloc_f32(const float *f, const float *mac, const float *wx, const float *wz, int nx,
                                        int nz, double *out, ipcu_stream_t stream) {
@@ -1059,7 +1192,9 @@ extern "C" int ipcu_totals_noalloc_f32(const float *f, const float *mac, const f
   if (N > (long long)kNoAllocBlocks * kNoAllocCells) return IPCU_ERR_CAPACITY;
   // host code cannot use the array's name as a device address: resolve it
   // once per device (the first call on a device does this set-up, so it
-  // should come before any stream capture)
+  // should come before any stream capture). The cache is keyed on the
+  // current device, which must be the one `stream` belongs to; concurrent
+  // first calls write the same address.
   static double *dev_ptr[64] = {nullptr};
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return IPCU_ERR_CUDA;
@@ -1095,6 +1230,7 @@ extern "C" int64_t ipcu_sim_steps(const ipcu_sim *s) { return s ? s->steps : -1;
 extern "C" int ipcu_sim_save(ipcu_sim *s, const char *path) {
   if (!s || !path) return IPCU_ERR_ARG;
   if (s->ib) return IPCU_ERR_UNSUPPORTED;  // the snapshot format holds no body
+  if (int st = lean_fill(s)) return st;
   if (cudaStreamSynchronize(s->stream) != cudaSuccess) return IPCU_ERR_CUDA;
   const long long N = s->N;
   const int q = s->cfg.q_scalar;
@@ -1173,10 +1309,32 @@ extern "C" int ipcu_sim_load(const char *path, ipcu_stream_t stream, ipcu_sim **
     ipcu_sim_destroy(s);
     return IPCU_ERR_CUDA;
   }
+  lean_check_s(s, mb.data());
+  if (lean_mark_all(s) != IPCU_OK) {
+    ipcu_sim_destroy(s);
+    return IPCU_ERR_CUDA;
+  }
   s->steps = steps;
   *out = s;
   return IPCU_OK;
 }
+
+extern "C" int ipcu_sim_set_lean(ipcu_sim *s, int enable) {
+  if (!s) return IPCU_ERR_ARG;
+  if (enable && !s->lean_ok) return IPCU_ERR_UNSUPPORTED;
+  if ((s->P.lean != 0) == (enable != 0)) return IPCU_OK;
+  if (!enable) {
+    if (int st = lean_fill(s)) return st;  // the planes of the current buffer made complete
+    s->P.lean = 0;
+  } else {
+    s->P.lean = 1;  // after full steps every plane of the current buffer is valid
+    if (int st = lean_mark_all(s)) return st;
+  }
+  drop_graphs(s);
+  return IPCU_OK;
+}
+
+extern "C" int ipcu_sim_lean(const ipcu_sim *s) { return s && s->P.lean ? 1 : 0; }
 
 // Field CSV in the reference's column order (ref: function/basic.cu:16-28):
 // "num_calc,N" then x,y,z,delx,dely,pressure,salinity,phi,rho,u,v,w,Fx,Fy,Fz
@@ -1285,6 +1443,11 @@ static int batch_enqueue(ipcu_batch *b, ipcu_sim *const *sims, int n, const int6
   }
   if (order.empty()) return IPCU_OK;
   for (int i : order) {
+    // the batched kernel reads and writes every plane: a simulation that
+    // ran lean steps completes its velocity planes first
+    if (sims[i]->P.lean) {
+      if (int st = lean_fill(sims[i])) return st;
+    }
     // the batch stream waits (on the device) for the simulation's own work
     if (cudaEventRecord(sims[i]->ready, sims[i]->stream) != cudaSuccess ||
         cudaStreamWaitEvent(b->stream, sims[i]->ready, 0) != cudaSuccess)
@@ -1312,6 +1475,7 @@ static int batch_enqueue(ipcu_batch *b, ipcu_sim *const *sims, int n, const int6
     ipcu_sim *s = sims[order[oi]];
     hp[oi] = s->P;
     hp[oi].cur = s->cur;
+    hp[oi].lean = 0;
     const ipcu_sim_config &c = s->cfg;
     if (oi == 0 || key(order[oi]) != key(order[oi - 1]))
       groups.push_back({c.storage, c.q_scalar, c.geometry, c.scalar_kind, s->P.tma, (int)hw.size(), (int)hj.size(),
@@ -1376,6 +1540,9 @@ static int batch_enqueue(ipcu_batch *b, ipcu_sim *const *sims, int n, const int6
     if (cudaStreamWaitEvent(sims[i]->stream, b->done, 0) != cudaSuccess) return IPCU_ERR_CUDA;
     sims[i]->cur ^= (int)(nsteps[i] & 1);
     sims[i]->steps += nsteps[i];
+    // the batched kernel wrote every velocity plane: the lean step's flags
+    // of the new current buffer all hold
+    if (int st = lean_mark_all(sims[i])) return st;
   }
   return IPCU_OK;
 }

@@ -132,6 +132,14 @@ class Sim:
         _lib.check(_lib.lib().ipcu_sim_totals(self._h, ctypes.byref(a), ctypes.byref(b)), "ipcu_sim_totals")
         return a.value, b.value
 
+    def set_lean(self, on=True):
+        """Turns the lean flow-only step on or off (ipcu_sim_set_lean)."""
+        _lib.check(_lib.lib().ipcu_sim_set_lean(self._h, 1 if on else 0), "ipcu_sim_set_lean")
+
+    def lean(self):
+        """True while the step kernel runs the lean flow-only step."""
+        return bool(_lib.lib().ipcu_sim_lean(self._h))
+
     def bytes_per_cell(self):
         return int(_lib.lib().ipcu_sim_bytes_per_cell(self._h))
 

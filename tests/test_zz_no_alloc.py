@@ -1,8 +1,8 @@
 """The allocation-free totals entry point (ipcu_totals_noalloc_f32).
 
 Some callers cannot allocate device memory where they need the domain
-totals: code running inside CUDA graph capture, hosts that hand all device
-memory to their own pool, loops that must not enter the driver's allocator.
+totals: hosts that hand all device memory to their own pool, loops that must
+not enter the driver's allocator.
 For them the library keeps the reduction's scratch in a fixed device array.
 This file checks, through the C ABI, that two calls in a row return the same
 totals as the allocating path (ipcu_sim_totals, same FP64 reduction) within
