@@ -117,13 +117,14 @@ def measured_traffic(args):
     return d["dram_bytes_per_launch"] if d else None
 
 
-def traffic3d(N):
+def traffic3d(N, stretched):
     """DRAM bytes per launch of the 3-D step at N cells, scaled from the
-    committed 128^3 ncu capture (profiles/traffic.json), else None."""
+    committed 128^3 ncu capture of the same kernel (profiles/traffic.json),
+    else None."""
     p = os.path.join(ROOT, "profiles", "traffic.json")
     if not os.path.exists(p):
         return None
-    d = json.load(open(p)).get("step3d_kernel@128x128x128")
+    d = json.load(open(p)).get("step3s_kernel<3>@128x128x128" if stretched else "step3d_kernel@128x128x128")
     return int(d["dram_bytes_per_cell"] * N) if d else None
 
 
@@ -321,12 +322,16 @@ def run_ours(args):
 
 
 def run_3d(args):
-    """The 3-D path at the C4 size: 160 x 160 x 640 uniform box (16.4M cells,
-    state 3.8 GB > L2), D3Q19 MRT + D3Q7 salinity with a linear stratification,
-    bounce-back, FP32. A step is --inner LBM steps (default 20) replayed from
-    a CUDA graph; the inputs are far larger than L2, so no flush is needed."""
+    """The 3-D path at the C4 size: 160 x 160 x 640 cells (16.4M, state
+    3.8 GB > L2), x and y tanh-clustered toward the centreline (spacing ratio
+    3) with the 3-point conservative flux form, z uniform (--uniform3d: the
+    uniform box), D3Q19 MRT + D3Q7 salinity with a linear stratification,
+    bounce-back, FP32 (the configuration's falling sphere is not part of
+    it). A step is --inner LBM steps (default 20) replayed from a CUDA graph;
+    the inputs are far larger than L2, so no flush is needed."""
     import torch
 
+    from ip_cu_lbm_b200 import workloads
     from ip_cu_lbm_b200.replicas import Replicas
     from ip_cu_lbm_b200.sim3d import Sim3D
 
@@ -335,10 +340,11 @@ def run_3d(args):
     nx, ny, nz = (int(v) for v in args.dims.split(","))
     dev = torch.device("cuda", local)
     stream = torch.cuda.current_stream(dev)
-    zz = np.broadcast_to((np.arange(nz) + 0.5)[:, None, None] / nz, (nz, ny, nx))
-    rng = np.random.default_rng(20261203)
-    S0 = 1.0 - zz + 1e-4 * rng.uniform(-1, 1, (nz, ny, nx))  # linear stratification, seeded noise
-    sim = Sim3D(nx, ny, nz, tau=0.55, taus=0.52, rho_sal=1e-3, g_bouss=1e-5, s0=S0.ravel(), stream=stream.cuda_stream)
+    kw, S0 = workloads.clustered_box_3d(nx, ny, nz)
+    if args.uniform3d:
+        for k in ("x", "wx", "y", "wy", "ns"):
+            kw.pop(k)
+    sim = Sim3D(nx, ny, nz, s0=S0.ravel(), stream=stream.cuda_stream, **kw)
     N, inner = sim.N, args.inner or 20
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     with Clocks(local) as clk:
@@ -379,11 +385,14 @@ def run_3d(args):
         "metric": METRIC, "value": round(value, 2), "unit": METRIC, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(total_ms / args.steps, 4), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded linear stratification)",
-        "config": {"workload": f"3-D uniform box {nx}x{ny}x{nz} D3Q19 MRT + D3Q7, bounce-back",
+        "config": {"workload": (f"3-D uniform box {nx}x{ny}x{nz} D3Q19 MRT + D3Q7, bounce-back" if args.uniform3d else
+                                f"3-D box {nx}x{ny}x{nz}, x and y tanh-clustered toward the centreline (ratio 3, "
+                                "3-point conservative flux form, corner transport on the xy diagonals), z uniform, "
+                                "D3Q19 MRT + D3Q7 linear stratification, bounce-back; no body"),
                    "lbm_steps_per_step": inner, "cells": N, "storage": "f32", "parallelism": f"replicas x{world}",
                    "l2": f"inputs ({4 * 29 * N / 1e9:.2f} GB) larger than L2"},
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                     "frac": round(achieved / peak, 4), "traffic": traffic3d(N), "bytes_per_cell": bpc,
+                     "frac": round(achieved / peak, 4), "traffic": traffic3d(N, not args.uniform3d), "bytes_per_cell": bpc,
                      "peak_source": peak_label(peak_src),
                      "traffic_note": "DRAM read+write bytes per launch from the 128^3 ncu capture (profiles/traffic.json), "
                                      "scaled by cells; it grows in proportion to the cells streamed"},
@@ -853,6 +862,7 @@ def main():
                     help="ib: the settling-ellipse immersed-boundary case (default); 2d: the nonuniform "
                          "two-layer 1024x256 case; 3d: the C4-sized 3-D box")
     ap.add_argument("--dims", default="160,160,640", help="3-D box nx,ny,nz (--case 3d)")
+    ap.add_argument("--uniform3d", action="store_true", help="--case 3d on a uniform box (no stretched axes)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

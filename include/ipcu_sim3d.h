@@ -1,7 +1,8 @@
 /*
  * ipcu_sim3d.h -- 3-D structured solver of libipcu (included by ipcu.h).
  *
- * One simulation = one box of nx x ny x nz cells on a uniform lattice:
+ * One simulation = one box of nx x ny x nz cells on a uniform lattice (or
+ * with stretched x and y axes, ipcu_sim3d_create_stretched):
  * D3Q19 flow (MRT with the d'Humieres moment basis, the five shear moments
  * relaxing with 1/tau and all others with rate 1, as the reference's
  * unit-rate S file; or BGK) and a D3Q7 passive salinity with the
@@ -36,6 +37,24 @@ typedef struct ipcu_sim3d ipcu_sim3d;
 /* Creates a simulation at rest (f = 0, g = w_k S0, F = 0); s0: host, N
  * values x fastest (NULL = 0). */
 int ipcu_sim3d_create(const ipcu_sim3d_config *cfg, const double *s0, ipcu_stream_t stream, ipcu_sim3d **out);
+
+/* Stretched x and y axes (z stays uniform): cell centres and widths per
+ * axis (host arrays; NULL keeps that axis uniform; every width >= dz), and
+ * the interpolation stencil of the reference's conservative flux form
+ * (ref: function/adv.cu:50-257): 3 (quadratic, two upstream nodes and one
+ * downstream) or 5 (the reference's centred 5-point stencil). Populations
+ * moving along x or y take the 1-D flux form, those moving along an xy
+ * diagonal the corner-transport form of set_out (adv.cu:100-145), z is an
+ * exact shift. Ghosts across x and y walls are mirror images of their
+ * owners for every quantity the flux form reads; sources outside the box
+ * bounce back. */
+typedef struct ipcu_sim3d_axes {
+  const double *x, *wx; /* nx cell centres and widths along x */
+  const double *y, *wy; /* ny cell centres and widths along y */
+  int32_t ns;           /* 3 or 5 */
+} ipcu_sim3d_axes;
+int ipcu_sim3d_create_stretched(const ipcu_sim3d_config *cfg, const ipcu_sim3d_axes *axes, const double *s0,
+                                ipcu_stream_t stream, ipcu_sim3d **out);
 void ipcu_sim3d_destroy(ipcu_sim3d *sim);
 /* Advances nsteps (asynchronous on the simulation's stream). */
 int ipcu_sim3d_step(ipcu_sim3d *sim, int64_t nsteps);

@@ -83,6 +83,12 @@ class IBBody2D(ctypes.Structure):
     ]
 
 
+class Sim3DAxes(ctypes.Structure):
+    """Mirror of ipcu_sim3d_axes (include/ipcu_sim3d.h)."""
+    _fields_ = [("x", ctypes.c_void_p), ("wx", ctypes.c_void_p), ("y", ctypes.c_void_p), ("wy", ctypes.c_void_p),
+                ("ns", ctypes.c_int32)]
+
+
 class Sim3DConfig(ctypes.Structure):
     """Mirror of ipcu_sim3d_config (include/ipcu_sim3d.h)."""
     _fields_ = [
@@ -150,6 +156,8 @@ def _declare(L: ctypes.CDLL) -> None:
         "ipcu_stream_create": ([ctypes.POINTER(P)], I),
         "ipcu_stream_destroy": ([P], I),
         "ipcu_sim3d_create": ([ctypes.POINTER(Sim3DConfig), P, P, ctypes.POINTER(P)], I),
+        "ipcu_sim3d_create_stretched": ([ctypes.POINTER(Sim3DConfig), ctypes.POINTER(Sim3DAxes), P, P,
+                                         ctypes.POINTER(P)], I),
         "ipcu_sim3d_destroy": ([P], None),
         "ipcu_sim3d_step": ([P, I64], I),
         "ipcu_sim3d_step_graph": ([P, I64], I),

@@ -1,0 +1,40 @@
+// Parameters of the fused 3-D step on stretched x and y axes (fused3s.cu).
+#pragma once
+#include <cuda_runtime.h>
+
+#include "ipcu.h"
+
+namespace ipcu {
+namespace f3s {
+
+constexpr int kTX = 32, kTY = 8, kThreads = kTX * kTY;
+
+// Flux-form tables of one stretched axis (n cells), built on the host like
+// the 2-D solver's (sim.cu axis_tables): node weights wA [2][n][NS] (sign of
+// the population's motion, cell, node), fin scale scin [2][n], fout scale
+// scout [n] = dz / D, combined interior weights wC [2][NS+1][n], and the
+// density-gradient factors ginv [n] = 1/(x_{i+1} - x_{i-1} + dz/1000)
+// (clamped neighbours).
+struct Axis {
+  const float *wA, *scin, *scout, *wC, *ginv;
+};
+
+struct Params3S {
+  int nx, ny, nz, zchunk;  // z cells per CTA
+  const float *f_in, *g_in, *F_in;
+  float *f_out, *g_out, *F_out;
+  Axis ax, ay;
+  float c, dt, itau, omg_s;  // 1/tau, 1 - 1/tau_s
+  float fk3, hdt;            // 3 dt / c, dt / 2
+  float rho0, rsal, gb;      // rho = rho0 + rsal S; buoyancy -gb S
+  float giz_in, giz_wall;    // z (uniform): 1/(2dz + dz/1000), 1/(dz + dz/1000)
+  int mrt;
+  unsigned *status;
+};
+
+// ns: 3 (quadratic upwind) or 5 (the reference's stencil)
+int launch3s(const Params3S &p, int ns, cudaStream_t s, bool prepare_only = false);
+size_t smem3s(int ns);
+
+}  // namespace f3s
+}  // namespace ipcu

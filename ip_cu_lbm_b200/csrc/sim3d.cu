@@ -5,7 +5,9 @@
 #include <string>
 #include <vector>
 
+#include "axis_tables.hpp"
 #include "fused3d.cuh"
+#include "fused3s.cuh"
 #include "ipcu_common.cuh"
 
 using namespace ipcu;
@@ -20,6 +22,12 @@ struct ipcu_sim3d {
   f3d::Params3 P;
   cudaGraphExec_t graph[2] = {nullptr, nullptr};  // two steps, per starting buffer
   long long steps = 0;
+  // stretched x and y axes (ns 3 or 5; 0: the uniform box kernel): the
+  // step kernel's parameters and the axes' device tables
+  int ns = 0;
+  f3s::Params3S PS;
+  float *tab = nullptr;
+  std::vector<double> X, DX, Y, DY;
 };
 
 namespace {
@@ -38,6 +46,7 @@ void free3(ipcu_sim3d *s) {
     cudaFree(s->F[i]);
   }
   cudaFree(s->status);
+  cudaFree(s->tab);
   delete s;
 }
 
@@ -52,16 +61,51 @@ f3d::Params3 params_for(const ipcu_sim3d *s, int cur) {
   return P;
 }
 
+// one step reading buffer `cur`: the uniform box kernel or the stretched one
+int launch_one(const ipcu_sim3d *s, int cur, cudaStream_t st) {
+  if (!s->ns) return f3d::launch3d(params_for(s, cur), st);
+  f3s::Params3S P = s->PS;
+  P.f_in = s->f[cur];
+  P.g_in = s->g[cur];
+  P.F_in = s->F[cur];
+  P.f_out = s->f[cur ^ 1];
+  P.g_out = s->g[cur ^ 1];
+  P.F_out = s->F[cur ^ 1];
+  return f3s::launch3s(P, s->ns, st);
+}
+
 }  // namespace
 
 extern "C" int ipcu_sim3d_create(const ipcu_sim3d_config *cfg, const double *s0, ipcu_stream_t stream,
                                  ipcu_sim3d **out) {
+  return ipcu_sim3d_create_stretched(cfg, nullptr, s0, stream, out);
+}
+
+extern "C" int ipcu_sim3d_create_stretched(const ipcu_sim3d_config *cfg, const ipcu_sim3d_axes *axes,
+                                           const double *s0, ipcu_stream_t stream, ipcu_sim3d **out) {
   if (!cfg || !out) return IPCU_ERR_ARG;
   *out = nullptr;
   const ipcu_sim3d_config &c = *cfg;
   if (c.nx < 1 || c.ny < 1 || c.nz < 1 || !(c.dz > 0) || !(c.dt > 0) || c.tau <= 0.5 || c.taus <= 0.5)
     return IPCU_ERR_ARG;
+  const bool stretched = axes && (axes->x || axes->wx || axes->y || axes->wy);
+  if (stretched && axes->ns != 3 && axes->ns != 5) return IPCU_ERR_ARG;
+  std::vector<double> X(c.nx), DX(c.nx), Y(c.ny), DY(c.ny);
+  for (int i = 0; i < c.nx; i++) {
+    X[i] = stretched && axes->x ? axes->x[i] : (i + 0.5) * c.dz;
+    DX[i] = stretched && axes->wx ? axes->wx[i] : c.dz;
+    if (DX[i] < c.dz * (1 - 1e-9)) return IPCU_ERR_ARG;  // CFL <= 1 on the interpolated axes
+  }
+  for (int j = 0; j < c.ny; j++) {
+    Y[j] = stretched && axes->y ? axes->y[j] : (j + 0.5) * c.dz;
+    DY[j] = stretched && axes->wy ? axes->wy[j] : c.dz;
+    if (DY[j] < c.dz * (1 - 1e-9)) return IPCU_ERR_ARG;
+  }
   ipcu_sim3d *s = new ipcu_sim3d();
+  s->X = X;
+  s->DX = DX;
+  s->Y = Y;
+  s->DY = DY;
   s->cfg = c;
   s->N = (long long)c.nx * c.ny * c.nz;
   s->stream = (cudaStream_t)stream;
@@ -105,6 +149,59 @@ extern "C" int ipcu_sim3d_create(const ipcu_sim3d_config *cfg, const double *s0,
   P.gi_wall = 1.0f / ((float)c.dz + reg);
   P.mrt = c.mrt ? 1 : 0;
   P.status = s->status;
+  if (stretched) {
+    // flux-form and gradient tables of both axes, one device block
+    s->ns = axes->ns;
+    std::vector<float> wx, six, sox, wcx, wy, siy, soy, wcy;
+    axis_tables(X, DX, c.dz, s->ns, wx, six, sox, wcx);
+    axis_tables(Y, DY, c.dz, s->ns, wy, siy, soy, wcy);
+    const std::vector<float> gx = grad_inv(X, c.dz), gy = grad_inv(Y, c.dz);
+    const std::vector<float> *parts[10] = {&wx, &six, &sox, &wcx, &gx, &wy, &siy, &soy, &wcy, &gy};
+    size_t total = 0;
+    for (auto *v : parts) total += v->size();
+    std::vector<float> all;
+    all.reserve(total);
+    for (auto *v : parts) all.insert(all.end(), v->begin(), v->end());
+    if (cudaMalloc((void **)&s->tab, sizeof(float) * total) != cudaSuccess ||
+        cudaMemcpy(s->tab, all.data(), sizeof(float) * total, cudaMemcpyHostToDevice) != cudaSuccess) {
+      free3(s);
+      return IPCU_ERR_NOMEM;
+    }
+    const float *b[10];
+    size_t off = 0;
+    for (int i = 0; i < 10; i++) {
+      b[i] = s->tab + off;
+      off += parts[i]->size();
+    }
+    f3s::Params3S &Q = s->PS;
+    std::memset(&Q, 0, sizeof Q);
+    Q.nx = c.nx;
+    Q.ny = c.ny;
+    Q.nz = c.nz;
+    // z cells per CTA: the chunk's first planes are collided twice, so
+    // chunks of 32 (6 % extra) while the grid keeps several waves
+    Q.zchunk = (int)std::max(4LL, std::min<long long>(32, (long long)c.nz * cols / (148LL * 2 * 4)));
+    Q.ax = {b[0], b[1], b[2], b[3], b[4]};
+    Q.ay = {b[5], b[6], b[7], b[8], b[9]};
+    Q.c = P.c;
+    Q.dt = P.dt;
+    Q.itau = P.itau;
+    Q.omg_s = P.omg_s;
+    Q.fk3 = P.fk3;
+    Q.hdt = P.hdt;
+    Q.rho0 = P.rho0;
+    Q.rsal = P.rsal;
+    Q.gb = P.gb;
+    Q.giz_in = P.gi_in;
+    Q.giz_wall = P.gi_wall;
+    Q.mrt = P.mrt;
+    Q.status = s->status;
+    const int st = f3s::launch3s(Q, s->ns, s->stream, true);
+    if (st != IPCU_OK) {
+      free3(s);
+      return st;
+    }
+  }
   // state at rest: f = 0, g = w_k S0, F = 0
   std::vector<float> g0(7 * N);
   for (long long i = 0; i < N; i++) {
@@ -131,7 +228,7 @@ extern "C" void ipcu_sim3d_destroy(ipcu_sim3d *s) {
 extern "C" int ipcu_sim3d_step(ipcu_sim3d *s, int64_t nsteps) {
   if (!s || nsteps < 0) return IPCU_ERR_ARG;
   for (int64_t k = 0; k < nsteps; k++) {
-    const int st = f3d::launch3d(params_for(s, s->cur), s->stream);
+    const int st = launch_one(s, s->cur, s->stream);
     if (st != IPCU_OK) return st;
     s->cur ^= 1;
     s->steps++;
@@ -154,8 +251,8 @@ extern "C" int ipcu_sim3d_step_graph(ipcu_sim3d *s, int64_t nsteps) {
         cudaStreamDestroy(cs);
         return IPCU_ERR_CUDA;
       }
-      int st = f3d::launch3d(params_for(s, s->cur), cs);
-      if (st == IPCU_OK) st = f3d::launch3d(params_for(s, s->cur ^ 1), cs);
+      int st = launch_one(s, s->cur, cs);
+      if (st == IPCU_OK) st = launch_one(s, s->cur ^ 1, cs);
       const cudaError_t e = cudaStreamEndCapture(cs, &gr);
       cudaStreamDestroy(cs);
       if (st != IPCU_OK || e != cudaSuccess) return st != IPCU_OK ? st : IPCU_ERR_CUDA;

@@ -14,7 +14,10 @@ class Sim3D:
     as numpy arrays shaped [nz, ny, nx] (x fastest), or [q, nz, ny, nx]."""
 
     def __init__(self, nx, ny, nz, *, mrt=True, dz=1.0, dt=1.0, tau=0.55, taus=0.51, rho0=1.0, rho_sal=0.0,
-                 g_bouss=0.0, s0=None, stream=None):
+                 g_bouss=0.0, s0=None, stream=None, x=None, wx=None, y=None, wy=None, ns=3):
+        """x, wx / y, wy: cell centres and widths of stretched x / y axes
+        (z stays uniform), streamed with the ns-point conservative flux form
+        (ipcu_sim3d_create_stretched); all None: the uniform box kernel."""
         self.nx, self.ny, self.nz = int(nx), int(ny), int(nz)
         self.N = self.nx * self.ny * self.nz
         cfg = _lib.Sim3DConfig()
@@ -28,7 +31,17 @@ class Sim3D:
                 raise ValueError(f"s0 needs {self.N} values")
             s0p = self._s0.ctypes.data
         h = ctypes.c_void_p()
-        _lib.check(_lib.lib().ipcu_sim3d_create(ctypes.byref(cfg), s0p, stream, ctypes.byref(h)), "ipcu_sim3d_create")
+        if any(a is not None for a in (x, wx, y, wy)):
+            self._axes = [None if a is None else np.ascontiguousarray(a, dtype=np.float64) for a in (x, wx, y, wy)]
+            for a, n in zip(self._axes, (self.nx, self.nx, self.ny, self.ny)):
+                if a is not None and a.size != n:
+                    raise ValueError("axis arrays need one value per cell")
+            ax = _lib.Sim3DAxes(*[None if a is None else a.ctypes.data for a in self._axes], int(ns))
+            _lib.check(_lib.lib().ipcu_sim3d_create_stretched(ctypes.byref(cfg), ctypes.byref(ax), s0p, stream,
+                                                              ctypes.byref(h)), "ipcu_sim3d_create_stretched")
+        else:
+            _lib.check(_lib.lib().ipcu_sim3d_create(ctypes.byref(cfg), s0p, stream, ctypes.byref(h)),
+                       "ipcu_sim3d_create")
         self._h = h
 
     def close(self):
