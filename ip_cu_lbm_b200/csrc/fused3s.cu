@@ -32,6 +32,8 @@
 // L2): f [19][N], g [7][N] and the force F [3][N], 232 B per cell in FP32.
 #include <cuda_runtime.h>
 
+#include <type_traits>
+
 #include "d3q19.cuh"
 #include "fused3s.cuh"
 #include "ipcu_common.cuh"
@@ -52,7 +54,8 @@ struct G {
   static constexpr int DN0 = MID0 + 2 * 14 * RC;                // [2][6][RC]
   static constexpr int S0 = DN0 + 2 * 6 * RC;                   // [3][SC]
   static constexpr int FR0 = S0 + 3 * SC;                       // [2][3][kTX * kTY] force of the tile cells
-  static constexpr int NF = FR0 + 2 * 3 * kTX * kTY;
+  static constexpr int Q0 = FR0 + 2 * 3 * kTX * kTY;            // wall-cell queue: count + kTX * kTY cells
+  static constexpr int NF = Q0 + 4 + kTX * kTY;
   static constexpr size_t bytes = sizeof(float) * (size_t)NF;
 };
 
@@ -75,6 +78,133 @@ template <int NS>
 __device__ __forceinline__ int pofs(int k, bool isg, int plane) {
   return cls_base<NS>(k, plane) + (isg ? gidx(k) : fidx(k)) * G<NS>::RC;
 }
+
+
+// The wall path: populations of the boundary-layer cells (first and last
+// cell along x, y or z) whose source c - e lies outside the box bounce back,
+// f(c, k) = ftmp(c, -k), and the partner of that ftmp is across the wall:
+// the flux form with mirror-image ghosts across x and y walls for every
+// quantity it reads, and clamped nodes. The boundary-layer cells of a plane
+// are queued and taken as (population, cell) pairs, consecutive lanes on one
+// population, whose code is instantiated per population (compile-time
+// direction tables; only the mirror choice is decided at run time).
+template <int NS>
+struct Wall {
+  using Gm = G<NS>;
+  static constexpr int h = Gm::h, RX = Gm::RX, RC = Gm::RC;
+  const float *sm;
+  const Params3S *p;
+  int nx, ny, nz, rx0, ry0;
+
+  __device__ __forceinline__ int clx(int v) const { return min(max(v, 0), nx - 1); }
+  __device__ __forceinline__ int cly(int v) const { return min(max(v, 0), ny - 1); }
+  // plane slot of the z-motion class CZ
+  template <int CZ>
+  __device__ __forceinline__ const float *slot(int plane) const {
+    return sm + (CZ > 0 ? Gm::UP0 + (plane % 3) * 6 * RC
+                        : (CZ < 0 ? Gm::DN0 + (plane & 1) * 6 * RC : Gm::MID0 + (plane & 1) * 14 * RC));
+  }
+  // value of slot row `idx` (population within the class) at (gx, gy)
+  __device__ __forceinline__ float V(const float *b, int idx, int gx, int gy) const {
+    return b[idx * RC + (gy - ry0) * RX + (gx - rx0)];
+  }
+  __device__ __forceinline__ float Ix(const float *b, int idx, int s, int gx, int gy) const {
+    const int sg = s == 0 ? 1 : -1;
+    const float *w = p->ax.wA + ((long long)s * nx + gx) * NS;
+    float acc = 0.f;
+#pragma unroll
+    for (int m = 0; m < NS; m++) acc = fmaf(__ldg(w + m), V(b, idx, clx(gx + sg * (m - h)), gy), acc);
+    return acc;
+  }
+  __device__ __forceinline__ float Iy(const float *b, int idx, int s, int gx, int gy) const {
+    const int sg = s == 0 ? 1 : -1;
+    const float *w = p->ay.wA + ((long long)s * ny + gy) * NS;
+    float acc = 0.f;
+#pragma unroll
+    for (int m = 0; m < NS; m++) acc = fmaf(__ldg(w + m), V(b, idx, gx, cly(gy + sg * (m - h))), acc);
+    return acc;
+  }
+  __device__ __forceinline__ float Ixy(const float *b, int idx, int sxi, int syi, int gx, int gy) const {
+    const int sgx = sxi == 0 ? 1 : -1, sgy = syi == 0 ? 1 : -1;
+    const float *wx = p->ax.wA + ((long long)sxi * nx + gx) * NS;
+    const float *wy = p->ay.wA + ((long long)syi * ny + gy) * NS;
+    int xs[NS];
+#pragma unroll
+    for (int m = 0; m < NS; m++) xs[m] = clx(gx + sgx * (m - h));
+    float acc = 0.f;
+#pragma unroll
+    for (int n = 0; n < NS; n++) {
+      const int yy = cly(gy + sgy * (n - h));
+      float row = 0.f;
+#pragma unroll
+      for (int m = 0; m < NS; m++) row = fmaf(__ldg(wx + m), V(b, idx, xs[m], yy), row);
+      acc = fmaf(__ldg(wy + n), row, acc);
+    }
+    return acc;
+  }
+  // ftmp of population K (g: ISG) of plane `plane` at cell (gx, gy) inside the box
+  template <int K, bool ISG>
+  __device__ __forceinline__ float ftmp(int plane, int gx, int gy) const {
+    constexpr int ax = cx(K), ay = cy(K);
+    const float *b = slot<cz(K)>(plane);
+    constexpr int idx = ISG ? gidx(K) : fidx(K);
+    if constexpr (ax == 0 && ay == 0) {
+      return V(b, idx, gx, gy);
+    } else if constexpr (ay == 0) {  // along x
+      constexpr int s = ax > 0 ? 0 : 1, km = mir(K, true, false);
+      constexpr int im = ISG ? gidx(km) : fidx(km);
+      const int px = gx + ax;
+      const float fin = Ix(b, idx, s, gx, gy) * __ldg(p->ax.scin + (long long)s * nx + gx);
+      if (px >= 0 && px < nx) return V(b, idx, px, gy) + (fin - Ix(b, idx, s, px, gy) * __ldg(p->ax.scout + px));
+      return V(b, im, gx, gy) + (fin - Ix(b, im, 1 - s, gx, gy) * __ldg(p->ax.scout + gx));
+    } else if constexpr (ax == 0) {  // along y
+      constexpr int s = ay > 0 ? 0 : 1, km = mir(K, false, true);
+      constexpr int im = ISG ? gidx(km) : fidx(km);
+      const int py = gy + ay;
+      const float fin = Iy(b, idx, s, gx, gy) * __ldg(p->ay.scin + (long long)s * ny + gy);
+      if (py >= 0 && py < ny) return V(b, idx, gx, py) + (fin - Iy(b, idx, s, gx, py) * __ldg(p->ay.scout + py));
+      return V(b, im, gx, gy) + (fin - Iy(b, im, 1 - s, gx, gy) * __ldg(p->ay.scout + gy));
+    } else {  // xy diagonal (corner transport, adv.cu:100-145); f populations only
+      // a quantity (0 f*, 1 fx, 2 fy, 3 fxy) at a possibly ghost cell: the
+      // owner's, for the population mirrored across the crossed walls
+      auto Q = [&](int type, int px, int py) -> float {
+        const bool mx = px < 0 || px >= nx, my = py < 0 || py >= ny;
+        const int qx = clx(px), qy = cly(py);
+        const int i = mx ? (my ? fidx(mir(K, true, true)) : fidx(mir(K, true, false)))
+                         : (my ? fidx(mir(K, false, true)) : fidx(K));
+        const int sxi = (ax > 0) != mx ? 0 : 1, syi = (ay > 0) != my ? 0 : 1;
+        if (type == 0) return V(b, i, qx, qy);
+        if (type == 1) return Ix(b, i, sxi, qx, qy);
+        if (type == 2) return Iy(b, i, syi, qx, qy);
+        return Ixy(b, i, sxi, syi, qx, qy);
+      };
+      const float axs = __ldg(p->ax.scout + clx(gx + ax)), ays = __ldg(p->ay.scout + cly(gy + ay));
+      const float fin = (axs * ays) * Q(3, gx, gy) + ays * (Q(2, gx + ax, gy) - axs * Q(3, gx + ax, gy)) +
+                        axs * (Q(1, gx, gy + ay) - ays * Q(3, gx, gy + ay));
+      const float fout =
+          axs * Q(1, gx + ax, gy + ay) + ays * Q(2, gx + ax, gy + ay) - (axs * ays) * Q(3, gx + ax, gy + ay);
+      return Q(0, gx + ax, gy + ay) + (fin - fout);
+    }
+  }
+  // streamed value of population K at output cell (gx, gy, z) whose source
+  // c - e lies outside the box: halfway bounce-back, ftmp of the opposite
+  // population at the cell itself (its partner is then across the wall)
+  __device__ float bounce_any(int kk, int z, int gx, int gy) const {
+    switch (kk) {
+#define IPCU_W3(k) \
+  case k: return ftmp<opp(k), false>(z, gx, gy);
+      IPCU_W3(0) IPCU_W3(1) IPCU_W3(2) IPCU_W3(3) IPCU_W3(4) IPCU_W3(5) IPCU_W3(6) IPCU_W3(7) IPCU_W3(8)
+      IPCU_W3(9) IPCU_W3(10) IPCU_W3(11) IPCU_W3(12) IPCU_W3(13) IPCU_W3(14) IPCU_W3(15) IPCU_W3(16)
+      IPCU_W3(17) IPCU_W3(18)
+#undef IPCU_W3
+#define IPCU_W3G(k) \
+  case 19 + k: return ftmp<opp(k), true>(z, gx, gy);
+      IPCU_W3G(0) IPCU_W3G(1) IPCU_W3G(2) IPCU_W3G(3) IPCU_W3G(4) IPCU_W3G(5) IPCU_W3G(6)
+#undef IPCU_W3G
+    }
+    return 0.f;
+  }
+};
 
 template <int NS>
 __global__ void __launch_bounds__(kThreads, 2) step3s_kernel(const __grid_constant__ Params3S p) {
@@ -173,110 +303,42 @@ __global__ void __launch_bounds__(kThreads, 2) step3s_kernel(const __grid_consta
       Wy[s][q] = __ldg(p.ay.wC + (long long)(s * (NS + 1) + q) * ny + cly(oy));
     }
 
-  // ---- general path (walls): values, 1-D and tensor interpolants, flux form
-  auto V = [&](int k, bool isg, int plane, int gx, int gy) -> float {
-    return sm[pofs<NS>(k, isg, plane) + (gy - ry0) * RX + (gx - rx0)];
-  };
-  auto Ix = [&](int k, bool isg, int plane, int s, int gx, int gy) -> float {
-    const int sg = s == 0 ? 1 : -1;
-    float acc = 0.f;
-#pragma unroll
-    for (int m = 0; m < NS; m++)
-      acc += __ldg(p.ax.wA + ((long long)s * nx + gx) * NS + m) * V(k, isg, plane, clx(gx + sg * (m - h)), gy);
-    return acc;
-  };
-  auto Iy = [&](int k, bool isg, int plane, int s, int gx, int gy) -> float {
-    const int sg = s == 0 ? 1 : -1;
-    float acc = 0.f;
-#pragma unroll
-    for (int m = 0; m < NS; m++)
-      acc += __ldg(p.ay.wA + ((long long)s * ny + gy) * NS + m) * V(k, isg, plane, gx, cly(gy + sg * (m - h)));
-    return acc;
-  };
-  auto Ixy = [&](int k, int plane, int sxi, int syi, int gx, int gy) -> float {
-    const int sgx = sxi == 0 ? 1 : -1, sgy = syi == 0 ? 1 : -1;
-    float acc = 0.f;
-#pragma unroll
-    for (int n = 0; n < NS; n++) {
-      float row = 0.f;
-      const int yy = cly(gy + sgy * (n - h));
-#pragma unroll
-      for (int m = 0; m < NS; m++)
-        row += __ldg(p.ax.wA + ((long long)sxi * nx + gx) * NS + m) * V(k, false, plane, clx(gx + sgx * (m - h)), yy);
-      acc += __ldg(p.ay.wA + ((long long)syi * ny + gy) * NS + n) * row;
-    }
-    return acc;
-  };
-  // ftmp of population k of plane `plane` at cell (gx, gy) inside the box
-  auto ftmp = [&](int k, bool isg, int plane, int gx, int gy) -> float {
-    const int ax = cx(k), ay = cy(k);
-    if (ax == 0 && ay == 0) return V(k, isg, plane, gx, gy);
-    if (ay == 0) {  // along x
-      const int s = ax > 0 ? 0 : 1, px = gx + ax;
-      const float fin = Ix(k, isg, plane, s, gx, gy) * __ldg(p.ax.scin + (long long)s * nx + gx);
-      if (px >= 0 && px < nx)
-        return V(k, isg, plane, px, gy) + (fin - Ix(k, isg, plane, s, px, gy) * __ldg(p.ax.scout + px));
-      const int km = mir(k, true, false);
-      return V(km, isg, plane, gx, gy) + (fin - Ix(km, isg, plane, 1 - s, gx, gy) * __ldg(p.ax.scout + gx));
-    }
-    if (ax == 0) {  // along y
-      const int s = ay > 0 ? 0 : 1, py = gy + ay;
-      const float fin = Iy(k, isg, plane, s, gx, gy) * __ldg(p.ay.scin + (long long)s * ny + gy);
-      if (py >= 0 && py < ny)
-        return V(k, isg, plane, gx, py) + (fin - Iy(k, isg, plane, s, gx, py) * __ldg(p.ay.scout + py));
-      const int km = mir(k, false, true);
-      return V(km, isg, plane, gx, gy) + (fin - Iy(km, isg, plane, 1 - s, gx, gy) * __ldg(p.ay.scout + gy));
-    }
-    // xy diagonal: the quantities of (possibly ghost) cells, ghosts mirrored
-    auto Q = [&](int type, int px, int py) -> float {
-      const bool mx = px < 0 || px >= nx, my = py < 0 || py >= ny;
-      const int kk = mir(k, mx, my), qx = clx(px), qy = cly(py);
-      const int sxi = cx(kk) > 0 ? 0 : 1, syi = cy(kk) > 0 ? 0 : 1;
-      if (type == 0) return V(kk, false, plane, qx, qy);
-      if (type == 1) return Ix(kk, false, plane, sxi, qx, qy);
-      if (type == 2) return Iy(kk, false, plane, syi, qx, qy);
-      return Ixy(kk, plane, sxi, syi, qx, qy);
-    };
-    const float axs = __ldg(p.ax.scout + clx(gx + ax)), ays = __ldg(p.ay.scout + cly(gy + ay));
-    const float fin = (axs * ays) * Q(3, gx, gy) + ays * (Q(2, gx + ax, gy) - axs * Q(3, gx + ax, gy)) +
-                      axs * (Q(1, gx, gy + ay) - ays * Q(3, gx, gy + ay));
-    const float fout = axs * Q(1, gx + ax, gy + ay) + ays * Q(2, gx + ax, gy + ay) - (axs * ays) * Q(3, gx + ax, gy + ay);
-    return Q(0, gx + ax, gy + ay) + (fin - fout);
-  };
-  // streamed value of population k at output cell (gx, gy, z): pull from
-  // c - e, or bounce back where that source lies outside the box
-  auto general = [&](int k, bool isg, int z, int gx, int gy) -> float {
-    const int sx = gx - cx(k), sy = gy - cy(k), sz = z - cz(k);
-    if (sx >= 0 && sx < nx && sy >= 0 && sy < ny && sz >= 0 && sz < nz) return ftmp(k, isg, sz, sx, sy);
-    return ftmp(opp(k), isg, z, gx, gy);
-  };
-  // interior path: combined weights, nodes around the cell itself
-  auto fast = [&](int k, bool isg, int z) -> float {
+  // combined-weight path, nodes around the cell itself. By linearity the
+  // flux form of a population whose source lies inside the box is this dot
+  // product also next to a wall, with the node addresses clamped into the
+  // box as the ghosts carry their owner's value (CL: the cell lies within
+  // the halo of an x or y wall).
+  auto fast = [&](int k, bool isg, int z, auto clamp_tag) -> float {
+    constexpr bool CL = decltype(clamp_tag)::value;
     const int lx = tx + H, ly = ty + H;
-    const float *b = sm + pofs<NS>(k, isg, z - cz(k)) + ly * RX + lx;
+    const float *b0 = sm + pofs<NS>(k, isg, z - cz(k));
+    auto nx_ = [&](int off) { return CL ? clx(ox + off) - rx0 : lx + off; };
+    auto ny_ = [&](int off) { return CL ? cly(oy + off) - ry0 : ly + off; };
     const int ax = cx(k), ay = cy(k);
-    if (ax == 0 && ay == 0) return b[0];
+    if (ax == 0 && ay == 0) return b0[ly * RX + lx];
     if (ay == 0) {
       const int s = ax > 0 ? 0 : 1;
+      const float *b = b0 + ly * RX;
       float acc = 0.f;
 #pragma unroll
-      for (int q = 0; q <= NS; q++) acc = fmaf(Wx[s][q], b[(q - h - 1) * ax], acc);
+      for (int q = 0; q <= NS; q++) acc = fmaf(Wx[s][q], b[nx_((q - h - 1) * ax)], acc);
       return acc;
     }
     if (ax == 0) {
       const int s = ay > 0 ? 0 : 1;
       float acc = 0.f;
 #pragma unroll
-      for (int r = 0; r <= NS; r++) acc = fmaf(Wy[s][r], b[(r - h - 1) * ay * RX], acc);
+      for (int r = 0; r <= NS; r++) acc = fmaf(Wy[s][r], b0[ny_((r - h - 1) * ay) * RX + lx], acc);
       return acc;
     }
     const int sx = ax > 0 ? 0 : 1, sy = ay > 0 ? 0 : 1;
     float acc = 0.f;
 #pragma unroll
     for (int r = 0; r <= NS; r++) {
+      const float *b = b0 + ny_((r - h - 1) * ay) * RX;
       float row = 0.f;
 #pragma unroll
-      for (int q = 0; q <= NS; q++) row = fmaf(Wx[sx][q], b[(r - h - 1) * ay * RX + (q - h - 1) * ax], row);
+      for (int q = 0; q <= NS; q++) row = fmaf(Wx[sx][q], b[nx_((q - h - 1) * ax)], row);
       acc = fmaf(Wy[sy][r], row, acc);
     }
     return acc;
@@ -304,27 +366,63 @@ __global__ void __launch_bounds__(kThreads, 2) step3s_kernel(const __grid_consta
     __syncthreads();
     if (z + 1 < nz) collide(z + 1);
     __syncthreads();
+    int *qcount = reinterpret_cast<int *>(sm + Gm::Q0), *queue = qcount + 4;
+    if (tid == 0) *qcount = 0;
+    __syncthreads();
+    // populations whose source lies outside the box (boundary layer only)
+    // are left to the wall path below
+    const bool zlo = z == 0, zhi = z == nz - 1;
+    const bool xlo = ox == 0, xhi = ox == nx - 1, ylo = oy == 0, yhi = oy == ny - 1;
+    auto src_in = [&](int k) {
+      return !((cx(k) > 0 && xlo) || (cx(k) < 0 && xhi) || (cy(k) > 0 && ylo) || (cy(k) < 0 && yhi) ||
+               (cz(k) > 0 && zlo) || (cz(k) < 0 && zhi));
+    };
     if (own) {
-      const bool interior = inx && iny && z >= 1 && z <= nz - 2;
       const long long i = (long long)z * P + (long long)oy * nx + ox;
-      float pr = 0.f, S = 0.f;
-#pragma unroll
-      for (int k = 0; k < 19; k++) {
-        const float v = interior ? fast(k, false, z) : general(k, false, z, ox, oy);
-        p.f_out[k * N + i] = v;
-        pr += v;
-      }
-#pragma unroll
-      for (int k = 0; k < 7; k++) {
-        const float v = interior ? fast(k, true, z) : general(k, true, z, ox, oy);
-        p.g_out[k * N + i] = v;
-        S += v;
-      }
       const float *Fr = sm + Gm::FR0 + (z & 1) * 3 * kTX * kTY + ty * kTX + tx;
       p.F_out[i] = Fr[0];
       p.F_out[N + i] = Fr[kTX * kTY];
       p.F_out[2 * N + i] = Fr[2 * kTX * kTY];
+      if (xlo || xhi || ylo || yhi || zlo || zhi) queue[atomicAdd(qcount, 1)] = tid;
+      float pr = 0.f, S = 0.f;
+      auto all = [&](auto tag) {
+#pragma unroll
+        for (int k = 0; k < 19; k++)
+          if (src_in(k)) {
+            const float v = fast(k, false, z, tag);
+            p.f_out[k * N + i] = v;
+            pr += v;
+          }
+#pragma unroll
+        for (int k = 0; k < 7; k++)
+          if (src_in(k)) {
+            const float v = fast(k, true, z, tag);
+            p.g_out[k * N + i] = v;
+            S += v;
+          }
+      };
+      if (inx && iny) all(std::false_type{});
+      else all(std::true_type{});
       if (!(isfinite(pr) && isfinite(S))) atomicOr(p.status, 1u);
+    }
+    // the wall cells of the plane: one (cell, population) pair per thread
+    __syncthreads();
+    {
+      const Wall<NS> wp{sm, &p, nx, ny, nz, rx0, ry0};
+      const int nq = *qcount, nw = nq * 26;
+#pragma unroll 1
+      for (int w = tid; w < nw; w += kThreads) {
+        const int kk = w / nq, cell = queue[w - kk * nq];  // consecutive lanes: one population
+        const int gx = x0 + cell % kTX, gy = y0 + cell / kTX;
+        const int k = kk >= 19 ? kk - 19 : kk;
+        const int sx = gx - cx(k), sy = gy - cy(k), sz = z - cz(k);
+        if (sx >= 0 && sx < nx && sy >= 0 && sy < ny && sz >= 0 && sz < nz) continue;  // done above
+        const float v = wp.bounce_any(kk, z, gx, gy);
+        const long long i = (long long)z * P + (long long)gy * nx + gx;
+        if (kk >= 19) p.g_out[(kk - 19) * N + i] = v;
+        else p.f_out[kk * N + i] = v;
+        if (!isfinite(v)) atomicOr(p.status, 1u);
+      }
     }
     __syncthreads();  // the next collide overwrites the oldest ring slots
   }
