@@ -21,7 +21,7 @@
 // and flux quantities (set_wall_f_inv's mirror, applied to every quantity
 // the flux form reads), halfway bounce-back for sources outside the box.
 //
-// A CTA owns a 32 x 8 column of cells and marches along a chunk of z. Each
+// A CTA owns a 32 x 16 column of cells and marches along a chunk of z. Each
 // plane is collided once into shared memory, tile + halo (H cells in x and
 // y); the post-collision populations are kept by the direction of their z
 // motion: those moving up (needed by the plane above) in a ring of three
@@ -207,7 +207,7 @@ struct Wall {
 };
 
 template <int NS>
-__global__ void __launch_bounds__(kThreads, 2) step3s_kernel(const __grid_constant__ Params3S p) {
+__global__ void __launch_bounds__(kThreads, kMinBlocks) step3s_kernel(const __grid_constant__ Params3S p) {
   using Gm = G<NS>;
   constexpr int h = Gm::h, H = Gm::H, RX = Gm::RX, RC = Gm::RC, SX = Gm::SX, SC = Gm::SC;
   extern __shared__ __align__(16) float sm[];

@@ -7,7 +7,8 @@
 namespace ipcu {
 namespace f3s {
 
-constexpr int kTX = 32, kTY = 8, kThreads = kTX * kTY;
+constexpr int kTX = 32, kTY = 16, kThreads = kTX * kTY;
+constexpr int kMinBlocks = 1;  // one 512-thread CTA per SM (its rings take ~190 KB of shared memory)
 
 // Flux-form tables of one stretched axis (n cells), built on the host like
 // the 2-D solver's (sim.cu axis_tables): node weights wA [2][n][NS] (sign of

@@ -180,7 +180,8 @@ extern "C" int ipcu_sim3d_create_stretched(const ipcu_sim3d_config *cfg, const i
     Q.nz = c.nz;
     // z cells per CTA: the chunk's first planes are collided twice, so
     // chunks of 32 (6 % extra) while the grid keeps several waves
-    Q.zchunk = (int)std::max(4LL, std::min<long long>(32, (long long)c.nz * cols / (148LL * 2 * 4)));
+    const long long cols3 = (long long)((c.nx + f3s::kTX - 1) / f3s::kTX) * ((c.ny + f3s::kTY - 1) / f3s::kTY);
+    Q.zchunk = (int)std::max(4LL, std::min<long long>(32, (long long)c.nz * cols3 / (148LL * f3s::kMinBlocks * 4)));
     Q.ax = {b[0], b[1], b[2], b[3], b[4]};
     Q.ay = {b[5], b[6], b[7], b[8], b[9]};
     Q.c = P.c;
