@@ -117,7 +117,8 @@ int ipcu_totals_noalloc_f32(const float *f, const float *mac, const float *wx, c
 /* Time steps taken since creation or restore. */
 int64_t ipcu_sim_steps(const ipcu_sim *sim);
 /* Versioned binary snapshot (configuration, geometry, MRT matrices, step
- * count, raw state) and its restore into a new simulation; a restored run
+ * count, raw state, and an attached moving body: its description and its
+ * device state) and its restore into a new simulation; a restored run
  * continues bit-identically (replaces basic.cu:31-56 save_status). */
 int ipcu_sim_save(ipcu_sim *sim, const char *path);
 int ipcu_sim_load(const char *path, ipcu_stream_t stream, ipcu_sim **out);
@@ -205,6 +206,14 @@ typedef struct ipcu_ib_body2d {
  * snapshots of a simulation with a body are refused. Status bit 8: the
  * body's stencils outgrew the kernel's window (the update was skipped). */
 int ipcu_sim_ib_attach(ipcu_sim *sim, const ipcu_ib_body2d *body, const double *markers, const double *dS, int32_t n);
+/* Markers of the attached body, 9 values each (x, y, z, u, v, w, Fx, Fy,
+ * Fz: position and velocity now, and the force the marker put on the fluid
+ * in the last update; y = dz/2), cap >= the marker count; returns the
+ * marker count (a negative status on error); and the same as a
+ * CSV in the reference's IB_csv column order, header
+ * "x,y,z,velx,vely,velz,ax,ay,az" (ref: function/ibm.cu:3-14). */
+int32_t ipcu_sim_ib_markers(ipcu_sim *sim, double *out, int32_t cap);
+int ipcu_sim_write_ib_csv(ipcu_sim *sim, const char *path);
 /* Body state: x, z, u, w, theta, omega and the IB force (x, z) and torque
  * the markers put on the fluid in the last step (9 values). Synchronises.
  * ipcu_sim_get serves the force density as fields "ibfx", "ibfz". */

@@ -74,5 +74,11 @@ int ipcu_sim3d_status(ipcu_sim3d *sim, uint32_t *flags);
 int64_t ipcu_sim3d_cells(const ipcu_sim3d *sim);
 /* Algorithmic bytes per cell and step: f, g, F each read and written once. */
 int64_t ipcu_sim3d_bytes_per_cell(const ipcu_sim3d *sim);
+/* Versioned binary snapshot (configuration, axes, stencil, step count, raw
+ * FP32 state) and its restore into a new simulation; a restored run
+ * continues bit-identically. */
+int ipcu_sim3d_save(ipcu_sim3d *sim, const char *path);
+int ipcu_sim3d_load(const char *path, ipcu_stream_t stream, ipcu_sim3d **out);
+int64_t ipcu_sim3d_steps(const ipcu_sim3d *sim);
 
 #endif /* IPCU_SIM3D_H */

@@ -446,6 +446,8 @@ __device__ void coupled_update(const Job &j, int parity) {
     const double x0 = j.X0[2 * l], z0 = j.X0[2 * l + 1];
     const double rx = cth * x0 - sth * z0, rz = sth * x0 + cth * z0;
     const double fx = (double)sFT[2 * l] * j.dS[l], fz = (double)sFT[2 * l + 1] * j.dS[l];
+    j.fmark[2 * l] = (float)fx;
+    j.fmark[2 * l + 1] = (float)fz;
     acc[0] += fx;
     acc[1] += fz;
     acc[2] += rx * fz - rz * fx;

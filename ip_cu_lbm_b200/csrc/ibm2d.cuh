@@ -36,6 +36,7 @@ struct Job {
   int *org;          // [nl][2] stencil origin of the previous step's markers
   int *org2;         // [nl][2] ... and of the step before
   float *fext;       // [2][N] force density on the fluid (also fp.fext)
+  float *fmark;      // [nl][2] force each marker put on the fluid in the last update (F_l dS_l)
   uint8_t *flag;     // [tiles] (also fp.ibflag)
   int nl, iters;
   double m, I, rho_s, rho_f, grav;  // mass, moment of inertia, densities, gravity (-z)

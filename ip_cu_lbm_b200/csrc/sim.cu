@@ -53,6 +53,9 @@ struct ipcu_sim {
   int ntiles = 0;
   // area weights dx dz / dz^2 per column and row (conservation totals)
   float *twx = nullptr, *twz = nullptr;
+  // the attached body's description as given (snapshots re-attach it)
+  ipcu_ib_body2d ib_cfg;
+  std::vector<double> ib_X0, ib_dS;
 };
 
 // Macroscopic planes: S, u_x, u_z (+ p* with 16-bit storage)
@@ -304,6 +307,7 @@ void free_sim(ipcu_sim *s) {
     fr(s->ib->org2);
     fr(s->ib->fext);
     fr(s->ib->flag);
+    fr(s->ib->fmark);
     delete s->ib;
   }
   if (s->ready) cudaEventDestroy(s->ready);
@@ -791,7 +795,8 @@ extern "C" int ipcu_sim_ib_attach(ipcu_sim *s, const ipcu_ib_body2d *bd, const d
   std::vector<double> X0(markers, markers + 2 * n), dSv(dS, dS + n);
   bool ok = salloc(s, &j->body, sizeof(ib2d::Body)) && salloc(s, &j->org, sizeof(int) * 2 * n) &&
             salloc(s, &j->org2, sizeof(int) * 2 * n) &&
-            salloc(s, &j->fext, sizeof(float) * 2 * N) && salloc(s, &j->flag, (size_t)tx * tz);
+            salloc(s, &j->fext, sizeof(float) * 2 * N) && salloc(s, &j->flag, (size_t)tx * tz) &&
+            salloc(s, &j->fmark, sizeof(float) * 2 * n);
   double *dX0 = nullptr, *ddS = nullptr;
   ok = ok && salloc(s, &dX0, sizeof(double) * 2 * n) && salloc(s, &ddS, sizeof(double) * n);
   j->X0 = dX0;
@@ -804,6 +809,7 @@ extern "C" int ipcu_sim_ib_attach(ipcu_sim *s, const ipcu_ib_body2d *bd, const d
   if (e == cudaSuccess) e = cudaMemsetAsync(j->org, 0, sizeof(int) * 2 * n, s->stream);
   if (e == cudaSuccess) e = cudaMemsetAsync(j->org2, 0, sizeof(int) * 2 * n, s->stream);
   if (e == cudaSuccess) e = cudaMemsetAsync(j->fext, 0, sizeof(float) * 2 * N, s->stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(j->fmark, 0, sizeof(float) * 2 * n, s->stream);
   // the tiles whose halo may reach the initial markers' 4x4 stencils are
   // flagged from the start, as each update flags its successor's footprint:
   // the first fluid step then already stores the velocity the first update
@@ -825,6 +831,9 @@ extern "C" int ipcu_sim_ib_attach(ipcu_sim *s, const ipcu_ib_body2d *bd, const d
   if (e == cudaSuccess) e = cudaMemcpyAsync(j->flag, fl.data(), fl.size(), cudaMemcpyHostToDevice, s->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
   if (e != cudaSuccess) return IPCU_ERR_CUDA;
+  s->ib_cfg = *bd;
+  s->ib_X0.assign(markers, markers + 2 * n);
+  s->ib_dS.assign(dS, dS + n);
   j->nl = n;
   j->iters = bd->iters;
   j->m = bd->rho_s * bd->area;
@@ -851,6 +860,53 @@ extern "C" int ipcu_sim_ib_body(ipcu_sim *s, double *out) {
   const double v[9] = {b.X[0], b.X[1], b.U[0], b.U[1], b.th, b.om, b.Fib[0], b.Fib[1], b.Tib};
   std::memcpy(out, v, sizeof v);
   return IPCU_OK;
+}
+
+// Markers of the attached body as the reference's IB_csv writes them (ref:
+// function/ibm.cu:3-14): position, velocity and the force each marker put on
+// the fluid in the last update, 9 values per marker (x, y, z, u, v, w, Fx,
+// Fy, Fz; the body moves in the x-z plane, y = dz/2).
+extern "C" int32_t ipcu_sim_ib_markers(ipcu_sim *s, double *out, int32_t cap) {
+  if (!s || !out || !s->ib) return IPCU_ERR_ARG;
+  const int n = s->ib->nl;
+  if (cap < n) return IPCU_ERR_CAPACITY;
+  ib2d::Body b;
+  std::vector<float> fm(2 * (size_t)n);
+  if (cudaStreamSynchronize(s->stream) != cudaSuccess ||
+      cudaMemcpy(&b, s->ib->body, sizeof b, cudaMemcpyDeviceToHost) != cudaSuccess ||
+      cudaMemcpy(fm.data(), s->ib->fmark, sizeof(float) * fm.size(), cudaMemcpyDeviceToHost) != cudaSuccess)
+    return IPCU_ERR_CUDA;
+  const double c = std::cos(b.th), sn = std::sin(b.th);
+  for (int l = 0; l < n; l++) {
+    const double x0 = s->ib_X0[2 * l], z0 = s->ib_X0[2 * l + 1];
+    const double rx = c * x0 - sn * z0, rz = sn * x0 + c * z0;
+    double *o = out + 9 * (size_t)l;
+    o[0] = b.X[0] + rx;
+    o[1] = 0.5 * s->cfg.dz;
+    o[2] = b.X[1] + rz;
+    o[3] = b.U[0] - b.om * rz;
+    o[4] = 0.0;
+    o[5] = b.U[1] + b.om * rx;
+    o[6] = fm[2 * l];
+    o[7] = 0.0;
+    o[8] = fm[2 * l + 1];
+  }
+  return n;
+}
+
+extern "C" int ipcu_sim_write_ib_csv(ipcu_sim *s, const char *path) {
+  if (!s || !path || !s->ib) return IPCU_ERR_ARG;
+  const int n = s->ib->nl;
+  std::vector<double> m(9 * (size_t)n);
+  if (const int st = ipcu_sim_ib_markers(s, m.data(), n); st < 0) return st;
+  FILE *f = fopen(path, "w");
+  if (!f) return IPCU_ERR_IO;
+  fprintf(f, "x,y,z,velx,vely,velz,ax,ay,az\n");
+  for (int l = 0; l < n; l++) {
+    const double *o = m.data() + 9 * (size_t)l;
+    fprintf(f, "%g,%g,%g,%g,%g,%g,%g,%g,%g\n", o[0], o[1], o[2], o[3], o[4], o[5], o[6], o[7], o[8]);
+  }
+  return fclose(f) == 0 ? IPCU_OK : IPCU_ERR_IO;
 }
 
 extern "C" int64_t ipcu_sim_bytes_per_cell(const ipcu_sim *sim) {
@@ -1152,8 +1208,9 @@ extern "C" int ipcu_totals_noalloc_f32(const float *f, const float *mac, const f
 namespace {
 constexpr char kMagic[8] = {'I', 'P', 'C', 'U', 'S', 'I', 'M', '1'};
 // 2: 16-bit storage as equilibrium deviations + p* plane; 3: scalar kind and
-// phase-field parameters in the configuration, previous-step phi u planes
-constexpr int32_t kSnapVersion = 3;
+// phase-field parameters in the configuration, previous-step phi u planes;
+// 4: the moving body (description and device state) after the fluid state
+constexpr int32_t kSnapVersion = 4;
 template <class T>
 bool wr(FILE *f, const T *p, size_t n) { return fwrite(p, sizeof(T), n, f) == n; }
 template <class T>
@@ -1164,7 +1221,6 @@ extern "C" int64_t ipcu_sim_steps(const ipcu_sim *s) { return s ? s->steps : -1;
 
 extern "C" int ipcu_sim_save(ipcu_sim *s, const char *path) {
   if (!s || !path) return IPCU_ERR_ARG;
-  if (s->ib) return IPCU_ERR_UNSUPPORTED;  // the snapshot format holds no body
   if (int st = lean_fill(s)) return st;
   if (cudaStreamSynchronize(s->stream) != cudaSuccess) return IPCU_ERR_CUDA;
   const long long N = s->N;
@@ -1189,6 +1245,30 @@ extern "C" int ipcu_sim_save(ipcu_sim *s, const char *path) {
   if (ok && c.mrt) ok = wr(f, s->M.data(), 81) && wr(f, s->Minv.data(), 81) && wr(f, s->Srates.data(), 9);
   ok = ok && wr(f, fb.data(), fb.size()) && wr(f, gb.data(), gb.size()) && wr(f, mb.data(), mb.size()) &&
        wr(f, ob.data(), ob.size());
+  // the moving body: its description, then its device state as it stands
+  // (rigid-body state, the two previous stencil footprints, the force
+  // density on the fluid, the tile flags, the marker forces)
+  const int32_t has_body = s->ib ? 1 : 0;
+  ok = ok && wr(f, &has_body, 1);
+  if (ok && s->ib) {
+    const ib2d::Job &j = *s->ib;
+    const int32_t n = j.nl;
+    const size_t tiles = (size_t)s->ntiles;
+    ib2d::Body b;
+    std::vector<int> org(2 * n), org2(2 * n);
+    std::vector<float> fe(2 * N), fm(2 * n);
+    std::vector<uint8_t> fl(tiles);
+    ok = cudaMemcpy(&b, j.body, sizeof b, cudaMemcpyDeviceToHost) == cudaSuccess &&
+         cudaMemcpy(org.data(), j.org, sizeof(int) * 2 * n, cudaMemcpyDeviceToHost) == cudaSuccess &&
+         cudaMemcpy(org2.data(), j.org2, sizeof(int) * 2 * n, cudaMemcpyDeviceToHost) == cudaSuccess &&
+         cudaMemcpy(fe.data(), j.fext, sizeof(float) * 2 * N, cudaMemcpyDeviceToHost) == cudaSuccess &&
+         cudaMemcpy(fl.data(), j.flag, tiles, cudaMemcpyDeviceToHost) == cudaSuccess &&
+         cudaMemcpy(fm.data(), j.fmark, sizeof(float) * 2 * n, cudaMemcpyDeviceToHost) == cudaSuccess;
+    ok = ok && wr(f, &s->ib_cfg, 1) && wr(f, &n, 1) && wr(f, s->ib_X0.data(), 2 * (size_t)n) &&
+         wr(f, s->ib_dS.data(), (size_t)n) && wr(f, &b, 1) && wr(f, org.data(), org.size()) &&
+         wr(f, org2.data(), org2.size()) && wr(f, fe.data(), fe.size()) && wr(f, fl.data(), fl.size()) &&
+         wr(f, fm.data(), fm.size());
+  }
   ok = (fclose(f) == 0) && ok;
   return ok ? IPCU_OK : IPCU_ERR_IO;
 }
@@ -1202,7 +1282,8 @@ extern "C" int ipcu_sim_load(const char *path, ipcu_stream_t stream, ipcu_sim **
   int32_t ver = 0;
   ipcu_sim_config c;
   long long steps = 0;
-  bool ok = rd(f, mg, 8) && std::memcmp(mg, kMagic, 8) == 0 && rd(f, &ver, 1) && ver == kSnapVersion && rd(f, &c, 1) &&
+  bool ok = rd(f, mg, 8) && std::memcmp(mg, kMagic, 8) == 0 && rd(f, &ver, 1) && ver >= 3 && ver <= kSnapVersion &&
+            rd(f, &c, 1) &&
             rd(f, &steps, 1) && c.nx > 0 && c.nz > 0;
   std::vector<double> X(ok ? c.nx : 0), Z(ok ? c.nz : 0), DX(X.size()), DZ(Z.size()), M(81), Mi(81), S(9);
   ok = ok && rd(f, X.data(), X.size()) && rd(f, Z.data(), Z.size()) && rd(f, DX.data(), DX.size()) &&
@@ -1231,6 +1312,31 @@ extern "C" int ipcu_sim_load(const char *path, ipcu_stream_t stream, ipcu_sim **
   std::vector<float> mb((size_t)nmac(s) * N), ob(s->obuf[s->cur] ? 2 * N : 0);
   ok = rd(f, fb.data(), fb.size()) && rd(f, gb.data(), gb.size()) && rd(f, mb.data(), mb.size()) &&
        rd(f, ob.data(), ob.size());
+  // version 4: the moving body, re-attached and its device state restored
+  int32_t has_body = 0;
+  ipcu_ib_body2d bcfg;
+  int32_t nl = 0;
+  std::vector<double> X0, dSv;
+  ib2d::Body bst;
+  std::vector<int> org, org2;
+  std::vector<float> fe, fm;
+  std::vector<uint8_t> fl;
+  if (ok && ver >= 4) ok = rd(f, &has_body, 1);
+  if (ok && has_body) {
+    ok = rd(f, &bcfg, 1) && rd(f, &nl, 1) && nl > 0 && nl <= ib2d::kMaxMarkers;
+    if (ok) {
+      X0.resize(2 * (size_t)nl);
+      dSv.resize(nl);
+      org.resize(2 * (size_t)nl);
+      org2.resize(2 * (size_t)nl);
+      fe.resize(2 * N);
+      fm.resize(2 * (size_t)nl);
+      fl.resize((size_t)s->ntiles);
+      ok = rd(f, X0.data(), X0.size()) && rd(f, dSv.data(), dSv.size()) && rd(f, &bst, 1) &&
+           rd(f, org.data(), org.size()) && rd(f, org2.data(), org2.size()) && rd(f, fe.data(), fe.size()) &&
+           rd(f, fl.data(), fl.size()) && rd(f, fm.data(), fm.size());
+    }
+  }
   fclose(f);
   if (!ok) {
     ipcu_sim_destroy(s);
@@ -1248,6 +1354,22 @@ extern "C" int ipcu_sim_load(const char *path, ipcu_stream_t stream, ipcu_sim **
   if (lean_mark_all(s) != IPCU_OK) {
     ipcu_sim_destroy(s);
     return IPCU_ERR_CUDA;
+  }
+  if (has_body) {
+    st = ipcu_sim_ib_attach(s, &bcfg, X0.data(), dSv.data(), nl);
+    const ib2d::Job *j = s->ib;
+    if (st == IPCU_OK &&
+        (cudaMemcpy(j->body, &bst, sizeof bst, cudaMemcpyHostToDevice) != cudaSuccess ||
+         cudaMemcpy(j->org, org.data(), sizeof(int) * org.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
+         cudaMemcpy(j->org2, org2.data(), sizeof(int) * org2.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
+         cudaMemcpy(j->fext, fe.data(), sizeof(float) * fe.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
+         cudaMemcpy(j->flag, fl.data(), fl.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
+         cudaMemcpy(j->fmark, fm.data(), sizeof(float) * fm.size(), cudaMemcpyHostToDevice) != cudaSuccess))
+      st = IPCU_ERR_CUDA;
+    if (st != IPCU_OK) {
+      ipcu_sim_destroy(s);
+      return st;
+    }
   }
   s->steps = steps;
   *out = s;

@@ -363,3 +363,81 @@ extern "C" int64_t ipcu_sim3d_cells(const ipcu_sim3d *s) { return s ? s->N : 0; 
 extern "C" int64_t ipcu_sim3d_bytes_per_cell(const ipcu_sim3d *s) {
   return s ? 2 * 4 * (19 + 7 + 3) : 0;
 }
+
+// ---------------------------------------------------------------------------
+// Checkpoint / restore: configuration, axes, step count and the raw FP32
+// state f, g, F; a restored run continues bit-identically.
+namespace {
+constexpr char kMagic3[8] = {'I', 'P', 'C', 'U', 'S', '3', 'D', '1'};
+constexpr int32_t kSnap3Version = 1;
+template <class T>
+bool wr3(FILE *f, const T *p, size_t n) { return fwrite(p, sizeof(T), n, f) == n; }
+template <class T>
+bool rd3(FILE *f, T *p, size_t n) { return fread(p, sizeof(T), n, f) == n; }
+}  // namespace
+
+extern "C" int ipcu_sim3d_save(ipcu_sim3d *s, const char *path) {
+  if (!s || !path) return IPCU_ERR_ARG;
+  const long long N = s->N;
+  std::vector<float> f(19 * N), g(7 * N), F(3 * N);
+  if (cudaStreamSynchronize(s->stream) != cudaSuccess ||
+      cudaMemcpy(f.data(), s->f[s->cur], sizeof(float) * f.size(), cudaMemcpyDeviceToHost) != cudaSuccess ||
+      cudaMemcpy(g.data(), s->g[s->cur], sizeof(float) * g.size(), cudaMemcpyDeviceToHost) != cudaSuccess ||
+      cudaMemcpy(F.data(), s->F[s->cur], sizeof(float) * F.size(), cudaMemcpyDeviceToHost) != cudaSuccess)
+    return IPCU_ERR_CUDA;
+  FILE *fp = fopen(path, "wb");
+  if (!fp) return IPCU_ERR_IO;
+  const int32_t ns = s->ns;
+  bool ok = wr3(fp, kMagic3, 8) && wr3(fp, &kSnap3Version, 1) && wr3(fp, &s->cfg, 1) && wr3(fp, &ns, 1) &&
+            wr3(fp, &s->steps, 1) && wr3(fp, s->X.data(), s->X.size()) && wr3(fp, s->DX.data(), s->DX.size()) &&
+            wr3(fp, s->Y.data(), s->Y.size()) && wr3(fp, s->DY.data(), s->DY.size()) &&
+            wr3(fp, f.data(), f.size()) && wr3(fp, g.data(), g.size()) && wr3(fp, F.data(), F.size());
+  ok = (fclose(fp) == 0) && ok;
+  return ok ? IPCU_OK : IPCU_ERR_IO;
+}
+
+extern "C" int ipcu_sim3d_load(const char *path, ipcu_stream_t stream, ipcu_sim3d **out) {
+  if (!path || !out) return IPCU_ERR_ARG;
+  *out = nullptr;
+  FILE *fp = fopen(path, "rb");
+  if (!fp) return IPCU_ERR_IO;
+  char mg[8];
+  int32_t ver = 0, ns = 0;
+  ipcu_sim3d_config c;
+  long long steps = 0;
+  bool ok = rd3(fp, mg, 8) && std::memcmp(mg, kMagic3, 8) == 0 && rd3(fp, &ver, 1) && ver == kSnap3Version &&
+            rd3(fp, &c, 1) && rd3(fp, &ns, 1) && rd3(fp, &steps, 1) && c.nx > 0 && c.ny > 0 && c.nz > 0;
+  std::vector<double> X(ok ? c.nx : 0), DX(X.size()), Y(ok ? c.ny : 0), DY(Y.size());
+  ok = ok && rd3(fp, X.data(), X.size()) && rd3(fp, DX.data(), DX.size()) && rd3(fp, Y.data(), Y.size()) &&
+       rd3(fp, DY.data(), DY.size());
+  if (!ok) {
+    fclose(fp);
+    return IPCU_ERR_IO;
+  }
+  ipcu_sim3d_axes ax{X.data(), DX.data(), Y.data(), DY.data(), ns};
+  ipcu_sim3d *s = nullptr;
+  const int st = ipcu_sim3d_create_stretched(&c, ns ? &ax : nullptr, nullptr, stream, &s);
+  if (st != IPCU_OK) {
+    fclose(fp);
+    return st;
+  }
+  const long long N = s->N;
+  std::vector<float> f(19 * N), g(7 * N), F(3 * N);
+  ok = rd3(fp, f.data(), f.size()) && rd3(fp, g.data(), g.size()) && rd3(fp, F.data(), F.size());
+  fclose(fp);
+  if (!ok) {
+    ipcu_sim3d_destroy(s);
+    return IPCU_ERR_IO;
+  }
+  if (cudaMemcpy(s->f[s->cur], f.data(), sizeof(float) * f.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemcpy(s->g[s->cur], g.data(), sizeof(float) * g.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemcpy(s->F[s->cur], F.data(), sizeof(float) * F.size(), cudaMemcpyHostToDevice) != cudaSuccess) {
+    ipcu_sim3d_destroy(s);
+    return IPCU_ERR_CUDA;
+  }
+  s->steps = steps;
+  *out = s;
+  return IPCU_OK;
+}
+
+extern "C" int64_t ipcu_sim3d_steps(const ipcu_sim3d *s) { return s ? s->steps : -1; }

@@ -108,6 +108,20 @@ class Sim:
         _lib.check(_lib.lib().ipcu_sim_ib_body(self._h, out.ctypes.data), "ipcu_sim_ib_body")
         return dict(zip(("x", "z", "u", "w", "theta", "omega", "Fx", "Fz", "T"), out.tolist()))
 
+    def markers(self):
+        """Markers of the attached body, [n, 9]: x, y, z, u, v, w, Fx, Fy, Fz
+        (position, velocity, force on the fluid in the last update)."""
+        cap = 4096
+        out = np.zeros(9 * cap)
+        n = _lib.lib().ipcu_sim_ib_markers(self._h, out.ctypes.data, cap)
+        if n < 0:
+            _lib.check(n, "ipcu_sim_ib_markers")
+        return out.reshape(cap, 9)[:n].copy()
+
+    def write_ib_csv(self, path):
+        """The markers as the reference's IB_csv writes them (ibm.cu:3-14)."""
+        _lib.check(_lib.lib().ipcu_sim_write_ib_csv(self._h, str(path).encode()), "ipcu_sim_write_ib_csv")
+
     # ---------------------------------------------------------------- fields
     def get(self, field):
         n = self.N * (9 if field == "f" else (self.q_scalar if field == "g" else 1))

@@ -91,3 +91,25 @@ class Sim3D:
 
     def bytes_per_cell(self):
         return int(_lib.lib().ipcu_sim3d_bytes_per_cell(self._h))
+
+    def steps(self):
+        return int(_lib.lib().ipcu_sim3d_steps(self._h))
+
+    def save(self, path):
+        """Versioned binary snapshot (ipcu_sim3d_save)."""
+        _lib.check(_lib.lib().ipcu_sim3d_save(self._h, str(path).encode()), "ipcu_sim3d_save")
+
+    @classmethod
+    def load(cls, path, stream=None):
+        """Restores a simulation saved with `save`."""
+        h = ctypes.c_void_p()
+        _lib.check(_lib.lib().ipcu_sim3d_load(str(path).encode(), stream, ctypes.byref(h)), "ipcu_sim3d_load")
+        obj = cls.__new__(cls)
+        obj._h = h
+        cfg = _lib.Sim3DConfig()
+        with open(path, "rb") as fh:
+            head = fh.read(12 + ctypes.sizeof(cfg))
+        cfg = _lib.Sim3DConfig.from_buffer_copy(head[12:])
+        obj.nx, obj.ny, obj.nz = cfg.nx, cfg.ny, cfg.nz
+        obj.N = obj.nx * obj.ny * obj.nz
+        return obj
