@@ -117,9 +117,10 @@ int ipcu_totals_noalloc_f32(const float *f, const float *mac, const float *wx, c
 /* Time steps taken since creation or restore. */
 int64_t ipcu_sim_steps(const ipcu_sim *sim);
 /* Versioned binary snapshot (configuration, geometry, MRT matrices, step
- * count, raw state, and an attached moving body: its description and its
- * device state) and its restore into a new simulation; a restored run
- * continues bit-identically (replaces basic.cu:31-56 save_status). */
+ * count, raw state, and the attached moving bodies: their descriptions
+ * and device state) and its restore into a new simulation; a restored run
+ * continues bit-identically (replaces basic.cu:31-56 save_status). Version
+ * 5; versions 3 and 4 (at most one body) still load. */
 int ipcu_sim_save(ipcu_sim *sim, const char *path);
 int ipcu_sim_load(const char *path, ipcu_stream_t stream, ipcu_sim **out);
 /* Field CSV in the reference's column order and cell order (basic.cu:16-28). */
@@ -175,8 +176,9 @@ int ipcu_batch_sync(ipcu_batch *batch);
  * waits for it. A server keeps the host one tick ahead of the GPU with them. */
 int ipcu_batch_mark(ipcu_batch *batch);
 int ipcu_batch_wait_mark(ipcu_batch *batch, int mark);
-/* Moving immersed boundary: one rigid body per simulation (uniform
- * lattice, salinity or no scalar). Markers on the outline (body frame,
+/* Moving immersed boundaries: up to 16 rigid bodies per simulation, as the
+ * reference's IB_index loop over bodies (ref: function/ibm.cu:367-424)
+ * (uniform lattice, salinity or no scalar). Markers on the outline (body frame,
  * physical units) carry arc lengths dS; each step, after the fluid step,
  * multi-direct forcing with the reference's 4-point Peskin kernel
  * (ref: function/ibm.cu:61-66 weightFunction) makes the fluid follow the
@@ -189,7 +191,11 @@ int ipcu_batch_wait_mark(ipcu_batch *batch, int mark);
  * through the kernel-entry API above. The coupling is stable at density
  * ratios down to about one for bodies at least 4 cells thick (semi-axes
  * >= 4 dz): a thinner body lies wholly inside its own 4-point stencils and
- * its interior fluid no longer follows it. */
+ * its interior fluid no longer follows it. Bodies share the force density
+ * and are updated side by side: they must stay apart (no contact model, as
+ * in the reference); a body attached closer than 6 cells (outline to
+ * outline, the outlines taken as circles of the largest marker radius) to
+ * another is refused with IPCU_ERR_ARG. */
 typedef struct ipcu_ib_body2d {
   double xc, zc, theta;   /* centre (cell centres at (i + 1/2) dz) and angle */
   double u, w, omega;     /* initial velocity and angular velocity */
@@ -201,22 +207,29 @@ typedef struct ipcu_ib_body2d {
   int32_t iters;          /* multi-direct forcing iterations (3) */
   int32_t pad;
 } ipcu_ib_body2d;
-/* Attaches the body (n <= 512 markers, [n][2] x, z); IPCU_ERR_UNSUPPORTED
- * for stretched geometries and the phase field. Drops recorded graphs;
- * snapshots of a simulation with a body are refused. Status bit 8: the
- * body's stencils outgrew the kernel's window (the update was skipped). */
+/* Attaches one more body (n <= 512 markers, [n][2] x, z; it gets the next
+ * index, from 0); IPCU_ERR_UNSUPPORTED for stretched geometries and the
+ * phase field, IPCU_ERR_CAPACITY past 16 bodies. Drops recorded graphs.
+ * Status bit 8: a body's stencils outgrew the kernel's window (its update
+ * was skipped). */
 int ipcu_sim_ib_attach(ipcu_sim *sim, const ipcu_ib_body2d *body, const double *markers, const double *dS, int32_t n);
-/* Markers of the attached body, 9 values each (x, y, z, u, v, w, Fx, Fy,
- * Fz: position and velocity now, and the force the marker put on the fluid
- * in the last update; y = dz/2), cap >= the marker count; returns the
- * marker count (a negative status on error); and the same as a
- * CSV in the reference's IB_csv column order, header
- * "x,y,z,velx,vely,velz,ax,ay,az" (ref: function/ibm.cu:3-14). */
+/* Bodies attached. */
+int32_t ipcu_sim_ib_count(const ipcu_sim *sim);
+/* Markers of body `index`, 9 values each (x, y, z, u, v, w, Fx, Fy, Fz:
+ * position and velocity now, and the force the marker put on the fluid in
+ * the last update; y = dz/2), cap >= the marker count; returns the marker
+ * count (a negative status on error). ipcu_sim_ib_markers is body 0. The
+ * CSV holds every body's markers, body after body, in the reference's
+ * IB_csv column order, header "x,y,z,velx,vely,velz,ax,ay,az" (ref:
+ * function/ibm.cu:3-14). */
+int32_t ipcu_sim_ib_markers_at(ipcu_sim *sim, int32_t index, double *out, int32_t cap);
 int32_t ipcu_sim_ib_markers(ipcu_sim *sim, double *out, int32_t cap);
 int ipcu_sim_write_ib_csv(ipcu_sim *sim, const char *path);
-/* Body state: x, z, u, w, theta, omega and the IB force (x, z) and torque
- * the markers put on the fluid in the last step (9 values). Synchronises.
- * ipcu_sim_get serves the force density as fields "ibfx", "ibfz". */
+/* State of body `index`: x, z, u, w, theta, omega and the IB force (x, z)
+ * and torque the markers put on the fluid in the last step (9 values).
+ * Synchronises. ipcu_sim_ib_body is body 0. ipcu_sim_get serves the force
+ * density of all bodies as fields "ibfx", "ibfz". */
+int ipcu_sim_ib_body_at(ipcu_sim *sim, int32_t index, double *out);
 int ipcu_sim_ib_body(ipcu_sim *sim, double *out);
 /* A new non-blocking CUDA stream (it does not synchronise with the legacy
  * default stream) and its release; work still queued on a released stream

@@ -153,7 +153,10 @@ def _declare(L: ctypes.CDLL) -> None:
         "ipcu_sim_device_bytes": ([P], I64),
         "ipcu_sim_ib_attach": ([P, ctypes.POINTER(IBBody2D), P, P, ctypes.c_int32], I),
         "ipcu_sim_ib_body": ([P, P], I),
+        "ipcu_sim_ib_body_at": ([P, ctypes.c_int32, P], I),
+        "ipcu_sim_ib_count": ([P], ctypes.c_int32),
         "ipcu_sim_ib_markers": ([P, P, ctypes.c_int32], ctypes.c_int32),
+        "ipcu_sim_ib_markers_at": ([P, ctypes.c_int32, P, ctypes.c_int32], ctypes.c_int32),
         "ipcu_sim_write_ib_csv": ([P, ctypes.c_char_p], I),
         "ipcu_sim3d_save": ([P, ctypes.c_char_p], I),
         "ipcu_sim3d_load": ([ctypes.c_char_p, P, ctypes.POINTER(P)], I),

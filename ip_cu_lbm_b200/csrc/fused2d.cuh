@@ -67,12 +67,13 @@ struct alignas(64) Params {
   int8_t slipB9[16 * 9], slipK9[16 * 9];  // per wall class: owner neighbour and population
   int8_t slipB5[16 * 9], slipK5[16 * 9];
   unsigned *status;
-  // immersed boundary: force density [2][N] added to the cell force where the
-  // cell's tile is flagged in ibflag ([tiles z][ibtx]: some cell of the tile
-  // or of its halo carries a force); null without a body
+  // immersed boundaries: force density [2][N] added to the cell force where
+  // the cell's tile is flagged by some body in ibflag ([ibnb bodies][ntz][ibtx]:
+  // some cell of the tile or of its halo carries that body's force); null
+  // without a body
   const float *fext;
   const uint8_t *ibflag;
-  int ibtx;
+  int ibtx, ibnb;
   // Lean flow-only step (FP32 storage, TMA staging, no scalar lattice, S
   // uniform): the S plane is constant and never read or written; the
   // velocity planes of buffer b hold a tile's values only where

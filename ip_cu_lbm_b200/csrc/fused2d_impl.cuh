@@ -255,8 +255,12 @@ __device__ __forceinline__ void step_tile(const Params &p, int parity, int tile_
   // of the previous step may still be running (programmatic dependent
   // launch): a flagged tile waits for it before it reads anything. The flag
   // is read past L1 (the update sets it just before it lets this kernel go).
-  const bool ibt = p.fext != nullptr &&
-                   *reinterpret_cast<const volatile uint8_t *>(p.ibflag + tile_z * p.ibtx + tile_x) != 0;
+  bool ibt = false;
+  if (p.fext != nullptr) {
+    const long long tiles = (long long)p.ibtx * p.ntz;
+    for (int b = 0; b < p.ibnb; b++)
+      ibt |= *reinterpret_cast<const volatile uint8_t *>(p.ibflag + b * tiles + tile_z * p.ibtx + tile_x) != 0;
+  }
   if (ibt) asm volatile("griddepcontrol.wait;" ::: "memory");
   // lean step: which of the 3 x 3 tiles around this one hold their velocity
   // planes in the input buffer (bit (dz + 1) * 3 + (dx + 1)); the staged

@@ -1,5 +1,5 @@
-// Moving immersed boundary coupled to the fused 2-D solver (ibm2d.cu): one
-// rigid body per simulation, Lagrangian markers on its outline, multi-direct
+// Moving immersed boundaries coupled to the fused 2-D solver (ibm2d.cu):
+// rigid bodies (one CTA each), Lagrangian markers on their outlines, multi-direct
 // forcing with the reference's 4-point Peskin kernel (ref: function/ibm.cu:
 // 61-66 weightFunction) and an FP64 rigid-body update built on the
 // reference's update_IBbody / update_IBpoint (ref: function/ibm.cu:367-447).
@@ -35,9 +35,9 @@ struct Job {
   const double *dS;  // [nl] arc length per marker
   int *org;          // [nl][2] stencil origin of the previous step's markers
   int *org2;         // [nl][2] ... and of the step before
-  float *fext;       // [2][N] force density on the fluid (also fp.fext)
+  float *fext;       // [2][N] force density on the fluid, shared by the simulation's bodies (also fp.fext)
   float *fmark;      // [nl][2] force each marker put on the fluid in the last update (F_l dS_l)
-  uint8_t *flag;     // [tiles] (also fp.ibflag)
+  uint8_t *flag;     // [tiles] this body's slice of fp.ibflag
   int nl, iters;
   double m, I, rho_s, rho_f, grav;  // mass, moment of inertia, densities, gravity (-z)
   double semi_a, semi_b;            // ellipse semi-axes in the body frame (inside test)

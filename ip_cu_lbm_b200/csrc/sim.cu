@@ -43,9 +43,15 @@ struct ipcu_sim {
   std::vector<double> X, Z, DX, DZ;
   std::vector<double> M, Minv, Srates;  // MRT matrices as given (for snapshots)
   long long steps = 0;                  // time steps taken since creation / restore
-  // moving immersed boundary (null without a body): device state and the
-  // coupled update's parameters (fp filled per launch)
-  ib2d::Job *ib = nullptr;
+  // moving immersed boundaries (empty without a body): each body's device
+  // state and coupled-update parameters (fp filled per launch); the force
+  // density and the tile flags ([bodies][tiles]) they share; with several
+  // bodies, device copies of the job list per starting buffer parity
+  std::vector<ib2d::Job *> ibs;
+  float *ibfext = nullptr;
+  uint8_t *ibflags = nullptr;
+  ib2d::Job *d_jobs[2] = {nullptr, nullptr};
+  bool jobs_dirty = true;
   // lean flow-only step (f2d::Params::lean): per-parity tile flags of
   // stored velocity planes; lean_ok: the configuration allows it
   uint8_t *ustore[2] = {nullptr, nullptr};
@@ -53,9 +59,9 @@ struct ipcu_sim {
   int ntiles = 0;
   // area weights dx dz / dz^2 per column and row (conservation totals)
   float *twx = nullptr, *twz = nullptr;
-  // the attached body's description as given (snapshots re-attach it)
-  ipcu_ib_body2d ib_cfg;
-  std::vector<double> ib_X0, ib_dS;
+  // the attached bodies' descriptions as given (snapshots re-attach them)
+  std::vector<ipcu_ib_body2d> ib_cfg;
+  std::vector<std::vector<double>> ib_X0, ib_dS;
 };
 
 // Macroscopic planes: S, u_x, u_z (+ p* with 16-bit storage)
@@ -241,6 +247,7 @@ __global__ void k_totals_final(const double *part, int nb, double *out) {
 }
 
 constexpr int kTotBlocks = 296;
+constexpr int kMaxBodies = 16;  // bodies per simulation
 
 // A simulation's device memory comes from the device's stream-ordered pool
 // (cudaMallocAsync on the simulation's stream): creating and retiring many
@@ -299,17 +306,19 @@ void free_sim(ipcu_sim *s) {
   fr(s->ustore[1]);
   fr(s->twx);
   fr(s->twz);
-  if (s->ib) {
-    fr(s->ib->body);
-    fr((void *)s->ib->X0);
-    fr((void *)s->ib->dS);
-    fr(s->ib->org);
-    fr(s->ib->org2);
-    fr(s->ib->fext);
-    fr(s->ib->flag);
-    fr(s->ib->fmark);
-    delete s->ib;
+  for (ib2d::Job *j : s->ibs) {
+    fr(j->body);
+    fr((void *)j->X0);
+    fr((void *)j->dS);
+    fr(j->org);
+    fr(j->org2);
+    fr(j->fmark);
+    delete j;
   }
+  fr(s->ibfext);
+  fr(s->ibflags);
+  fr(s->d_jobs[0]);
+  fr(s->d_jobs[1]);
   if (s->ready) cudaEventDestroy(s->ready);
   delete s;
 }
@@ -340,6 +349,7 @@ int lean_mark_all(ipcu_sim *s) {
 }
 void drop_graphs(ipcu_sim *s) {
   cudaStreamSynchronize(s->stream);
+  s->jobs_dirty = true;  // the parameters changed: the device job lists follow
   for (int i = 0; i < 2; i++)
     if (s->graph[i]) {
       cudaGraphExecDestroy(s->graph[i]);
@@ -670,10 +680,13 @@ static int launch_one(ipcu_sim *s) {
   f2d::Params P = s->P;
   P.cur = s->cur;
   int st = f2d::launch_step(P, s->cfg.storage, s->cfg.q_scalar, s->cfg.geometry, s->stream);
-  if (st == IPCU_OK && s->ib) {
-    ib2d::Job j = *s->ib;
+  if (st == IPCU_OK && s->ibs.size() == 1) {
+    ib2d::Job j = *s->ibs[0];
     j.fp = P;
     st = ib2d::launch(j, 0, s->cfg.storage, s->cfg.q_scalar, s->stream);
+  } else if (st == IPCU_OK && s->ibs.size() > 1) {
+    // one CTA per body, side by side (bodies far enough apart never share a cell)
+    st = ib2d::launch_batched(s->d_jobs[s->cur], (int)s->ibs.size(), 0, s->cfg.storage, s->cfg.q_scalar, s->stream);
   }
   if (st == IPCU_OK) {
     s->cur ^= 1;
@@ -682,8 +695,32 @@ static int launch_one(ipcu_sim *s) {
   return st;
 }
 
+// Several bodies: the device job lists (one per starting buffer parity) hold
+// the simulation's current parameters (refreshed outside any capture).
+static int sync_jobs(ipcu_sim *s) {
+  const size_t nb = s->ibs.size();
+  if (nb < 2 || !s->jobs_dirty) return IPCU_OK;
+  std::vector<ib2d::Job> h(nb);
+  for (int c = 0; c < 2; c++) {
+    if (s->d_jobs[c]) cudaFreeAsync(s->d_jobs[c], s->stream);
+    s->d_jobs[c] = nullptr;
+    if (!salloc(s, &s->d_jobs[c], sizeof(ib2d::Job) * nb)) return IPCU_ERR_NOMEM;
+    for (size_t b = 0; b < nb; b++) {
+      h[b] = *s->ibs[b];
+      h[b].fp = s->P;
+      h[b].fp.cur = c;
+    }
+    if (cudaMemcpyAsync(s->d_jobs[c], h.data(), sizeof(ib2d::Job) * nb, cudaMemcpyHostToDevice, s->stream) !=
+        cudaSuccess)
+      return IPCU_ERR_CUDA;
+  }
+  s->jobs_dirty = false;
+  return IPCU_OK;
+}
+
 extern "C" int ipcu_sim_step(ipcu_sim *sim, int64_t nsteps) {
   if (!sim || nsteps < 0) return IPCU_ERR_ARG;
+  if (int st = sync_jobs(sim)) return st;
   for (int64_t i = 0; i < nsteps; i++) {
     int st = launch_one(sim);
     if (st) return st;
@@ -693,6 +730,7 @@ extern "C" int ipcu_sim_step(ipcu_sim *sim, int64_t nsteps) {
 
 extern "C" int ipcu_sim_step_graph(ipcu_sim *sim, int64_t nsteps, int32_t chunk) {
   if (!sim || nsteps < 0 || chunk < 2) return IPCU_ERR_ARG;
+  if (int st = sync_jobs(sim)) return st;
   if (chunk % 2) chunk++;  // even, so a replay returns to the same buffer parity
   if (sim->graph_chunk != chunk) {
     for (int i = 0; i < 2; i++)
@@ -751,10 +789,25 @@ extern "C" int ipcu_stream_destroy(ipcu_stream_t stream) {
 }
 
 // ---------------------------------------------------------------------------
-// Moving immersed boundary: one rigid body per simulation (ibm2d.cu).
-extern "C" int ipcu_sim_ib_attach(ipcu_sim *s, const ipcu_ib_body2d *bd, const double *markers, const double *dS,
-                                  int32_t n) {
-  if (!s || !bd || !markers || !dS || n <= 0 || s->ib) return IPCU_ERR_ARG;
+// Moving immersed boundaries (ibm2d.cu): up to kMaxBodies rigid bodies per
+// simulation, as the reference's IB_index loop over bodies (ref:
+// function/ibm.cu:367-424), each with its own markers, stencil footprints,
+// tile flags and previous orientation. They share the fluid's force density;
+// the body updates run side by side, so the bodies must stay apart (no
+// contact model, as in the reference): at attach the new body's outline must
+// be at least kBodyGap cells from every other body's.
+constexpr double kBodyGap = 6.0;  // two 4-point stencils and a cell of motion
+
+static double outline_radius(const double *markers, int n) {
+  double r = 0.0;
+  for (int l = 0; l < n; l++) r = std::max(r, std::hypot(markers[2 * l], markers[2 * l + 1]));
+  return r;
+}
+
+static int attach_body(ipcu_sim *s, const ipcu_ib_body2d *bd, const double *markers, const double *dS, int32_t n,
+                       bool check_gap) {
+  if (!s || !bd || !markers || !dS || n <= 0) return IPCU_ERR_ARG;
+  if ((int)s->ibs.size() >= kMaxBodies) return IPCU_ERR_CAPACITY;
   if (n > ib2d::kMaxMarkers) return IPCU_ERR_CAPACITY;
   if (s->cfg.geometry != IPCU_GEO_UNIFORM || s->cfg.scalar_kind == IPCU_SCALAR_PHASE) return IPCU_ERR_UNSUPPORTED;
   if (!(bd->rho_s > 0 && bd->rho_f > 0 && bd->area > 0 && bd->inertia > 0 && bd->semi_a > 0 && bd->semi_b > 0 &&
@@ -762,6 +815,16 @@ extern "C" int ipcu_sim_ib_attach(ipcu_sim *s, const ipcu_ib_body2d *bd, const d
     return IPCU_ERR_ARG;
   for (int i = 0; i < n; i++)
     if (!(dS[i] > 0) || !std::isfinite(markers[2 * i]) || !std::isfinite(markers[2 * i + 1])) return IPCU_ERR_ARG;
+  if (check_gap && !s->ibs.empty()) {
+    if (cudaStreamSynchronize(s->stream) != cudaSuccess) return IPCU_ERR_CUDA;
+    const double r = outline_radius(markers, n);
+    for (size_t b = 0; b < s->ibs.size(); b++) {
+      ib2d::Body o;
+      if (cudaMemcpy(&o, s->ibs[b]->body, sizeof o, cudaMemcpyDeviceToHost) != cudaSuccess) return IPCU_ERR_CUDA;
+      const double d = std::hypot(bd->xc - o.X[0], bd->zc - o.X[1]);
+      if (d < r + outline_radius(s->ib_X0[b].data(), s->ibs[b]->nl) + kBodyGap * s->cfg.dz) return IPCU_ERR_ARG;
+    }
+  }
   {
     static bool prepared[64] = {false};
     int dev = 0;
@@ -793,22 +856,37 @@ extern "C" int ipcu_sim_ib_attach(ipcu_sim *s, const ipcu_ib_body2d *bd, const d
   b0.th = bd->theta;
   b0.om = bd->omega;
   std::vector<double> X0(markers, markers + 2 * n), dSv(dS, dS + n);
+  const size_t tiles = (size_t)tx * tz;
+  const int nb = (int)s->ibs.size();  // bodies already attached
   bool ok = salloc(s, &j->body, sizeof(ib2d::Body)) && salloc(s, &j->org, sizeof(int) * 2 * n) &&
-            salloc(s, &j->org2, sizeof(int) * 2 * n) &&
-            salloc(s, &j->fext, sizeof(float) * 2 * N) && salloc(s, &j->flag, (size_t)tx * tz) &&
-            salloc(s, &j->fmark, sizeof(float) * 2 * n);
+            salloc(s, &j->org2, sizeof(int) * 2 * n) && salloc(s, &j->fmark, sizeof(float) * 2 * n);
   double *dX0 = nullptr, *ddS = nullptr;
   ok = ok && salloc(s, &dX0, sizeof(double) * 2 * n) && salloc(s, &ddS, sizeof(double) * n);
   j->X0 = dX0;
   j->dS = ddS;
-  s->ib = j;  // freed with the simulation from here on
+  s->ibs.push_back(j);  // freed with the simulation from here on
   if (!ok) return IPCU_ERR_NOMEM;
+  // the shared force density (first body), and the tile flags grown by one
+  // body's slice, the existing slices copied over
+  if (!s->ibfext) {
+    if (!salloc(s, &s->ibfext, sizeof(float) * 2 * N)) return IPCU_ERR_NOMEM;
+    if (cudaMemsetAsync(s->ibfext, 0, sizeof(float) * 2 * N, s->stream) != cudaSuccess) return IPCU_ERR_CUDA;
+  }
+  uint8_t *flags = nullptr;
+  if (!salloc(s, &flags, tiles * (nb + 1))) return IPCU_ERR_NOMEM;
+  if (nb > 0 && cudaMemcpyAsync(flags, s->ibflags, tiles * nb, cudaMemcpyDeviceToDevice, s->stream) != cudaSuccess)
+    return IPCU_ERR_CUDA;
+  if (s->ibflags) cudaFreeAsync(s->ibflags, s->stream);
+  s->ibflags = flags;
+  for (int b = 0; b <= nb; b++) {
+    s->ibs[b]->flag = flags + tiles * b;
+    s->ibs[b]->fext = s->ibfext;
+  }
   cudaError_t e = cudaMemcpyAsync(j->body, &b0, sizeof b0, cudaMemcpyHostToDevice, s->stream);
   if (e == cudaSuccess) e = cudaMemcpyAsync(dX0, X0.data(), sizeof(double) * 2 * n, cudaMemcpyHostToDevice, s->stream);
   if (e == cudaSuccess) e = cudaMemcpyAsync(ddS, dSv.data(), sizeof(double) * n, cudaMemcpyHostToDevice, s->stream);
   if (e == cudaSuccess) e = cudaMemsetAsync(j->org, 0, sizeof(int) * 2 * n, s->stream);
   if (e == cudaSuccess) e = cudaMemsetAsync(j->org2, 0, sizeof(int) * 2 * n, s->stream);
-  if (e == cudaSuccess) e = cudaMemsetAsync(j->fext, 0, sizeof(float) * 2 * N, s->stream);
   if (e == cudaSuccess) e = cudaMemsetAsync(j->fmark, 0, sizeof(float) * 2 * n, s->stream);
   // the tiles whose halo may reach the initial markers' 4x4 stencils are
   // flagged from the start, as each update flags its successor's footprint:
@@ -831,9 +909,9 @@ extern "C" int ipcu_sim_ib_attach(ipcu_sim *s, const ipcu_ib_body2d *bd, const d
   if (e == cudaSuccess) e = cudaMemcpyAsync(j->flag, fl.data(), fl.size(), cudaMemcpyHostToDevice, s->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
   if (e != cudaSuccess) return IPCU_ERR_CUDA;
-  s->ib_cfg = *bd;
-  s->ib_X0.assign(markers, markers + 2 * n);
-  s->ib_dS.assign(dS, dS + n);
+  s->ib_cfg.push_back(*bd);
+  s->ib_X0.emplace_back(markers, markers + 2 * n);
+  s->ib_dS.emplace_back(dS, dS + n);
   j->nl = n;
   j->iters = bd->iters;
   j->m = bd->rho_s * bd->area;
@@ -845,40 +923,53 @@ extern "C" int ipcu_sim_ib_attach(ipcu_sim *s, const ipcu_ib_body2d *bd, const d
   j->semi_b = bd->semi_b;
   j->dz = s->cfg.dz;
   j->dt = s->cfg.dt;
-  s->P.fext = j->fext;
-  s->P.ibflag = j->flag;
+  s->P.fext = s->ibfext;
+  s->P.ibflag = s->ibflags;
   s->P.ibtx = tx;
+  s->P.ibnb = nb + 1;
+  s->jobs_dirty = true;
   return IPCU_OK;
 }
 
-extern "C" int ipcu_sim_ib_body(ipcu_sim *s, double *out) {
-  if (!s || !out || !s->ib) return IPCU_ERR_ARG;
+extern "C" int ipcu_sim_ib_attach(ipcu_sim *s, const ipcu_ib_body2d *bd, const double *markers, const double *dS,
+                                  int32_t n) {
+  return attach_body(s, bd, markers, dS, n, true);
+}
+
+extern "C" int32_t ipcu_sim_ib_count(const ipcu_sim *s) { return s ? (int32_t)s->ibs.size() : 0; }
+
+extern "C" int ipcu_sim_ib_body_at(ipcu_sim *s, int32_t index, double *out) {
+  if (!s || !out || index < 0 || index >= (int)s->ibs.size()) return IPCU_ERR_ARG;
   ib2d::Body b;
   if (cudaStreamSynchronize(s->stream) != cudaSuccess ||
-      cudaMemcpy(&b, s->ib->body, sizeof b, cudaMemcpyDeviceToHost) != cudaSuccess)
+      cudaMemcpy(&b, s->ibs[index]->body, sizeof b, cudaMemcpyDeviceToHost) != cudaSuccess)
     return IPCU_ERR_CUDA;
   const double v[9] = {b.X[0], b.X[1], b.U[0], b.U[1], b.th, b.om, b.Fib[0], b.Fib[1], b.Tib};
   std::memcpy(out, v, sizeof v);
   return IPCU_OK;
 }
 
-// Markers of the attached body as the reference's IB_csv writes them (ref:
+extern "C" int ipcu_sim_ib_body(ipcu_sim *s, double *out) { return ipcu_sim_ib_body_at(s, 0, out); }
+
+// Markers of a body as the reference's IB_csv writes them (ref:
 // function/ibm.cu:3-14): position, velocity and the force each marker put on
 // the fluid in the last update, 9 values per marker (x, y, z, u, v, w, Fx,
 // Fy, Fz; the body moves in the x-z plane, y = dz/2).
-extern "C" int32_t ipcu_sim_ib_markers(ipcu_sim *s, double *out, int32_t cap) {
-  if (!s || !out || !s->ib) return IPCU_ERR_ARG;
-  const int n = s->ib->nl;
+extern "C" int32_t ipcu_sim_ib_markers_at(ipcu_sim *s, int32_t index, double *out, int32_t cap) {
+  if (!s || !out || index < 0 || index >= (int)s->ibs.size()) return IPCU_ERR_ARG;
+  const ib2d::Job *j = s->ibs[index];
+  const int n = j->nl;
   if (cap < n) return IPCU_ERR_CAPACITY;
   ib2d::Body b;
   std::vector<float> fm(2 * (size_t)n);
   if (cudaStreamSynchronize(s->stream) != cudaSuccess ||
-      cudaMemcpy(&b, s->ib->body, sizeof b, cudaMemcpyDeviceToHost) != cudaSuccess ||
-      cudaMemcpy(fm.data(), s->ib->fmark, sizeof(float) * fm.size(), cudaMemcpyDeviceToHost) != cudaSuccess)
+      cudaMemcpy(&b, j->body, sizeof b, cudaMemcpyDeviceToHost) != cudaSuccess ||
+      cudaMemcpy(fm.data(), j->fmark, sizeof(float) * fm.size(), cudaMemcpyDeviceToHost) != cudaSuccess)
     return IPCU_ERR_CUDA;
   const double c = std::cos(b.th), sn = std::sin(b.th);
+  const std::vector<double> &X0 = s->ib_X0[index];
   for (int l = 0; l < n; l++) {
-    const double x0 = s->ib_X0[2 * l], z0 = s->ib_X0[2 * l + 1];
+    const double x0 = X0[2 * l], z0 = X0[2 * l + 1];
     const double rx = c * x0 - sn * z0, rz = sn * x0 + c * z0;
     double *o = out + 9 * (size_t)l;
     o[0] = b.X[0] + rx;
@@ -894,16 +985,25 @@ extern "C" int32_t ipcu_sim_ib_markers(ipcu_sim *s, double *out, int32_t cap) {
   return n;
 }
 
+extern "C" int32_t ipcu_sim_ib_markers(ipcu_sim *s, double *out, int32_t cap) {
+  return ipcu_sim_ib_markers_at(s, 0, out, cap);
+}
+
+// every body's markers, body after body, in the IB_csv columns
 extern "C" int ipcu_sim_write_ib_csv(ipcu_sim *s, const char *path) {
-  if (!s || !path || !s->ib) return IPCU_ERR_ARG;
-  const int n = s->ib->nl;
-  std::vector<double> m(9 * (size_t)n);
-  if (const int st = ipcu_sim_ib_markers(s, m.data(), n); st < 0) return st;
+  if (!s || !path || s->ibs.empty()) return IPCU_ERR_ARG;
+  std::vector<double> m;
+  for (int b = 0; b < (int)s->ibs.size(); b++) {
+    const int n = s->ibs[b]->nl;
+    std::vector<double> mb(9 * (size_t)n);
+    if (const int st = ipcu_sim_ib_markers_at(s, b, mb.data(), n); st < 0) return st;
+    m.insert(m.end(), mb.begin(), mb.end());
+  }
   FILE *f = fopen(path, "w");
   if (!f) return IPCU_ERR_IO;
   fprintf(f, "x,y,z,velx,vely,velz,ax,ay,az\n");
-  for (int l = 0; l < n; l++) {
-    const double *o = m.data() + 9 * (size_t)l;
+  for (size_t l = 0; l < m.size() / 9; l++) {
+    const double *o = m.data() + 9 * l;
     fprintf(f, "%g,%g,%g,%g,%g,%g,%g,%g,%g\n", o[0], o[1], o[2], o[3], o[4], o[5], o[6], o[7], o[8]);
   }
   return fclose(f) == 0 ? IPCU_OK : IPCU_ERR_IO;
@@ -1051,11 +1151,11 @@ extern "C" int ipcu_sim_get(ipcu_sim *s, const char *field, double *out, int64_t
   const int q = s->cfg.q_scalar;
   const std::string fd(field);
   if (fd == "ibfx" || fd == "ibfz") {  // immersed-boundary force density
-    if (!s->ib) return IPCU_ERR_ARG;
+    if (s->ibs.empty()) return IPCU_ERR_ARG;
     if (n < N) return IPCU_ERR_CAPACITY;
     std::vector<float> m(N);
     if (cudaStreamSynchronize(s->stream) != cudaSuccess ||
-        cudaMemcpy(m.data(), s->ib->fext + (fd == "ibfz" ? N : 0), sizeof(float) * N, cudaMemcpyDeviceToHost) !=
+        cudaMemcpy(m.data(), s->ibfext + (fd == "ibfz" ? N : 0), sizeof(float) * N, cudaMemcpyDeviceToHost) !=
             cudaSuccess)
       return IPCU_ERR_CUDA;
     for (long long i = 0; i < N; i++) out[i] = m[i];
@@ -1210,7 +1310,7 @@ constexpr char kMagic[8] = {'I', 'P', 'C', 'U', 'S', 'I', 'M', '1'};
 // 2: 16-bit storage as equilibrium deviations + p* plane; 3: scalar kind and
 // phase-field parameters in the configuration, previous-step phi u planes;
 // 4: the moving body (description and device state) after the fluid state
-constexpr int32_t kSnapVersion = 4;
+constexpr int32_t kSnapVersion = 5;
 template <class T>
 bool wr(FILE *f, const T *p, size_t n) { return fwrite(p, sizeof(T), n, f) == n; }
 template <class T>
@@ -1245,29 +1345,32 @@ extern "C" int ipcu_sim_save(ipcu_sim *s, const char *path) {
   if (ok && c.mrt) ok = wr(f, s->M.data(), 81) && wr(f, s->Minv.data(), 81) && wr(f, s->Srates.data(), 9);
   ok = ok && wr(f, fb.data(), fb.size()) && wr(f, gb.data(), gb.size()) && wr(f, mb.data(), mb.size()) &&
        wr(f, ob.data(), ob.size());
-  // the moving body: its description, then its device state as it stands
-  // (rigid-body state, the two previous stencil footprints, the force
-  // density on the fluid, the tile flags, the marker forces)
-  const int32_t has_body = s->ib ? 1 : 0;
-  ok = ok && wr(f, &has_body, 1);
-  if (ok && s->ib) {
-    const ib2d::Job &j = *s->ib;
+  // the moving bodies: their count, then per body its description and its
+  // device state as it stands (rigid-body state, the two previous stencil
+  // footprints, its tile flags, the marker forces), then the force density
+  // the bodies put on the fluid
+  const int32_t nbodies = (int32_t)s->ibs.size();
+  ok = ok && wr(f, &nbodies, 1);
+  for (int bi = 0; ok && bi < nbodies; bi++) {
+    const ib2d::Job &j = *s->ibs[bi];
     const int32_t n = j.nl;
-    const size_t tiles = (size_t)s->ntiles;
     ib2d::Body b;
     std::vector<int> org(2 * n), org2(2 * n);
-    std::vector<float> fe(2 * N), fm(2 * n);
-    std::vector<uint8_t> fl(tiles);
+    std::vector<float> fm(2 * n);
+    std::vector<uint8_t> fl((size_t)s->ntiles);
     ok = cudaMemcpy(&b, j.body, sizeof b, cudaMemcpyDeviceToHost) == cudaSuccess &&
          cudaMemcpy(org.data(), j.org, sizeof(int) * 2 * n, cudaMemcpyDeviceToHost) == cudaSuccess &&
          cudaMemcpy(org2.data(), j.org2, sizeof(int) * 2 * n, cudaMemcpyDeviceToHost) == cudaSuccess &&
-         cudaMemcpy(fe.data(), j.fext, sizeof(float) * 2 * N, cudaMemcpyDeviceToHost) == cudaSuccess &&
-         cudaMemcpy(fl.data(), j.flag, tiles, cudaMemcpyDeviceToHost) == cudaSuccess &&
+         cudaMemcpy(fl.data(), j.flag, fl.size(), cudaMemcpyDeviceToHost) == cudaSuccess &&
          cudaMemcpy(fm.data(), j.fmark, sizeof(float) * 2 * n, cudaMemcpyDeviceToHost) == cudaSuccess;
-    ok = ok && wr(f, &s->ib_cfg, 1) && wr(f, &n, 1) && wr(f, s->ib_X0.data(), 2 * (size_t)n) &&
-         wr(f, s->ib_dS.data(), (size_t)n) && wr(f, &b, 1) && wr(f, org.data(), org.size()) &&
-         wr(f, org2.data(), org2.size()) && wr(f, fe.data(), fe.size()) && wr(f, fl.data(), fl.size()) &&
-         wr(f, fm.data(), fm.size());
+    ok = ok && wr(f, &s->ib_cfg[bi], 1) && wr(f, &n, 1) && wr(f, s->ib_X0[bi].data(), 2 * (size_t)n) &&
+         wr(f, s->ib_dS[bi].data(), (size_t)n) && wr(f, &b, 1) && wr(f, org.data(), org.size()) &&
+         wr(f, org2.data(), org2.size()) && wr(f, fl.data(), fl.size()) && wr(f, fm.data(), fm.size());
+  }
+  if (ok && nbodies > 0) {
+    std::vector<float> fe(2 * N);
+    ok = cudaMemcpy(fe.data(), s->ibfext, sizeof(float) * 2 * N, cudaMemcpyDeviceToHost) == cudaSuccess &&
+         wr(f, fe.data(), fe.size());
   }
   ok = (fclose(f) == 0) && ok;
   return ok ? IPCU_OK : IPCU_ERR_IO;
@@ -1312,30 +1415,42 @@ extern "C" int ipcu_sim_load(const char *path, ipcu_stream_t stream, ipcu_sim **
   std::vector<float> mb((size_t)nmac(s) * N), ob(s->obuf[s->cur] ? 2 * N : 0);
   ok = rd(f, fb.data(), fb.size()) && rd(f, gb.data(), gb.size()) && rd(f, mb.data(), mb.size()) &&
        rd(f, ob.data(), ob.size());
-  // version 4: the moving body, re-attached and its device state restored
-  int32_t has_body = 0;
-  ipcu_ib_body2d bcfg;
-  int32_t nl = 0;
-  std::vector<double> X0, dSv;
-  ib2d::Body bst;
-  std::vector<int> org, org2;
-  std::vector<float> fe, fm;
-  std::vector<uint8_t> fl;
-  if (ok && ver >= 4) ok = rd(f, &has_body, 1);
-  if (ok && has_body) {
-    ok = rd(f, &bcfg, 1) && rd(f, &nl, 1) && nl > 0 && nl <= ib2d::kMaxMarkers;
-    if (ok) {
-      X0.resize(2 * (size_t)nl);
-      dSv.resize(nl);
-      org.resize(2 * (size_t)nl);
-      org2.resize(2 * (size_t)nl);
-      fe.resize(2 * N);
-      fm.resize(2 * (size_t)nl);
-      fl.resize((size_t)s->ntiles);
-      ok = rd(f, X0.data(), X0.size()) && rd(f, dSv.data(), dSv.size()) && rd(f, &bst, 1) &&
-           rd(f, org.data(), org.size()) && rd(f, org2.data(), org2.size()) && rd(f, fe.data(), fe.size()) &&
-           rd(f, fl.data(), fl.size()) && rd(f, fm.data(), fm.size());
+  // versions 4 (one body, the force density inside its block) and 5 (a
+  // count of bodies, the force density after them): the moving bodies,
+  // re-attached and their device state restored
+  struct Saved {
+    ipcu_ib_body2d cfg;
+    int32_t nl = 0;
+    std::vector<double> X0, dS;
+    ib2d::Body b;
+    std::vector<int> org, org2;
+    std::vector<float> fm;
+    std::vector<uint8_t> fl;
+  };
+  int32_t nbodies = 0;
+  std::vector<Saved> bodies;
+  std::vector<float> fe;
+  if (ok && ver >= 4) ok = rd(f, &nbodies, 1) && nbodies >= 0 && nbodies <= kMaxBodies && (ver >= 5 || nbodies <= 1);
+  if (ok && nbodies > 0) {
+    bodies.resize(nbodies);
+    fe.resize(2 * N);
+    for (int bi = 0; ok && bi < nbodies; bi++) {
+      Saved &B = bodies[bi];
+      ok = rd(f, &B.cfg, 1) && rd(f, &B.nl, 1) && B.nl > 0 && B.nl <= ib2d::kMaxMarkers;
+      if (!ok) break;
+      const size_t nl = (size_t)B.nl;
+      B.X0.resize(2 * nl);
+      B.dS.resize(nl);
+      B.org.resize(2 * nl);
+      B.org2.resize(2 * nl);
+      B.fm.resize(2 * nl);
+      B.fl.resize((size_t)s->ntiles);
+      ok = rd(f, B.X0.data(), B.X0.size()) && rd(f, B.dS.data(), B.dS.size()) && rd(f, &B.b, 1) &&
+           rd(f, B.org.data(), B.org.size()) && rd(f, B.org2.data(), B.org2.size()) &&
+           (ver >= 5 || rd(f, fe.data(), fe.size())) && rd(f, B.fl.data(), B.fl.size()) &&
+           rd(f, B.fm.data(), B.fm.size());
     }
+    if (ok && ver >= 5) ok = rd(f, fe.data(), fe.size());
   }
   fclose(f);
   if (!ok) {
@@ -1355,21 +1470,26 @@ extern "C" int ipcu_sim_load(const char *path, ipcu_stream_t stream, ipcu_sim **
     ipcu_sim_destroy(s);
     return IPCU_ERR_CUDA;
   }
-  if (has_body) {
-    st = ipcu_sim_ib_attach(s, &bcfg, X0.data(), dSv.data(), nl);
-    const ib2d::Job *j = s->ib;
+  for (int bi = 0; bi < nbodies; bi++) {
+    const Saved &B = bodies[bi];
+    st = attach_body(s, &B.cfg, B.X0.data(), B.dS.data(), B.nl, false);
+    const ib2d::Job *j = st == IPCU_OK ? s->ibs[bi] : nullptr;
     if (st == IPCU_OK &&
-        (cudaMemcpy(j->body, &bst, sizeof bst, cudaMemcpyHostToDevice) != cudaSuccess ||
-         cudaMemcpy(j->org, org.data(), sizeof(int) * org.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
-         cudaMemcpy(j->org2, org2.data(), sizeof(int) * org2.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
-         cudaMemcpy(j->fext, fe.data(), sizeof(float) * fe.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
-         cudaMemcpy(j->flag, fl.data(), fl.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
-         cudaMemcpy(j->fmark, fm.data(), sizeof(float) * fm.size(), cudaMemcpyHostToDevice) != cudaSuccess))
+        (cudaMemcpy(j->body, &B.b, sizeof B.b, cudaMemcpyHostToDevice) != cudaSuccess ||
+         cudaMemcpy(j->org, B.org.data(), sizeof(int) * B.org.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
+         cudaMemcpy(j->org2, B.org2.data(), sizeof(int) * B.org2.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
+         cudaMemcpy(j->flag, B.fl.data(), B.fl.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
+         cudaMemcpy(j->fmark, B.fm.data(), sizeof(float) * B.fm.size(), cudaMemcpyHostToDevice) != cudaSuccess))
       st = IPCU_ERR_CUDA;
     if (st != IPCU_OK) {
       ipcu_sim_destroy(s);
       return st;
     }
+  }
+  if (nbodies > 0 &&
+      cudaMemcpy(s->ibfext, fe.data(), sizeof(float) * fe.size(), cudaMemcpyHostToDevice) != cudaSuccess) {
+    ipcu_sim_destroy(s);
+    return IPCU_ERR_CUDA;
   }
   s->steps = steps;
   *out = s;
@@ -1513,7 +1633,7 @@ static int batch_enqueue(ipcu_batch *b, ipcu_sim *const *sims, int n, const int6
   // group by (bodies first, kernel class), then by decreasing step count
   auto key = [&](int a) {
     const ipcu_sim_config &A = sims[a]->cfg;
-    return std::make_tuple(sims[a]->ib == nullptr, A.storage, A.q_scalar, A.geometry, A.scalar_kind, sims[a]->P.tma);
+    return std::make_tuple(sims[a]->ibs.empty(), A.storage, A.q_scalar, A.geometry, A.scalar_kind, sims[a]->P.tma);
   };
   std::stable_sort(order.begin(), order.end(), [&](int a, int c) {
     const auto ka = key(a), kc = key(c);
@@ -1540,8 +1660,8 @@ static int batch_enqueue(ipcu_batch *b, ipcu_sim *const *sims, int n, const int6
     const int tx = (s->nx + f2d::kTX - 1) / f2d::kTX, tz = (s->nz + f2d::kTZ - 1) / f2d::kTZ;
     for (int z = 0; z < tz; z++)
       for (int x = 0; x < tx; x++) hw.push_back({oi, x, z, 0});
-    if (s->ib) {
-      hj.push_back(*s->ib);
+    for (ib2d::Job *j : s->ibs) {
+      hj.push_back(*j);
       hj.back().fp = hp[oi];
     }
     Group &g = groups.back();
@@ -1643,13 +1763,21 @@ extern "C" int ipcu_batch_sync(ipcu_batch *b) {
   return cudaStreamSynchronize(b->stream) == cudaSuccess ? IPCU_OK : IPCU_ERR_CUDA;
 }
 
+// per body: tile flags, markers (X0, dS, two footprints, marker forces),
+// rigid-body state, and its entry in the two device job lists
+static long long ib_bytes(const ipcu_sim *s) {
+  long long t = 0;
+  for (const ib2d::Job *j : s->ibs)
+    t += (long long)s->ntiles + 40LL * j->nl + (long long)sizeof(ib2d::Body) +
+         (s->ibs.size() > 1 ? 2LL * (long long)sizeof(ib2d::Job) : 0);
+  return t;
+}
+
 extern "C" int64_t ipcu_sim_device_bytes(const ipcu_sim *s) {
   if (!s) return 0;
   const long long N = s->N;
   return 2 * ((long long)s->esz * (9 + std::max(s->cfg.q_scalar, 1)) * N + 4LL * (nmac(s) + (s->cfg.scalar_kind == IPCU_SCALAR_PHASE ? 2 : 0)) * N) +
          4LL * (3 * (s->nx + s->nz) + 2 * 5 * std::max(s->nx, s->nz)) + 2048 +
          (s->cfg.scalar_kind == IPCU_SCALAR_PHASE ? 4LL * (s->nx + s->nz) : 0) +  // 1/dx^2, 1/dz^2
-         (s->ib ? 8LL * N + ((s->nx + f2d::kTX - 1) / f2d::kTX) * ((s->nz + f2d::kTZ - 1) / f2d::kTZ) +
-                      40LL * s->ib->nl + (long long)sizeof(ib2d::Body)
-                : 0);  // immersed body: force density, tile flags, markers, body state
+         (s->ibs.empty() ? 0 : 8LL * N) + ib_bytes(s);  // immersed bodies: force density, per body below
 }

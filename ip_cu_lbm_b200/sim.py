@@ -91,7 +91,9 @@ class Sim:
                        iters=3, u=0.0, w=0.0, omega=0.0):
         """Attaches a rigid ellipse (semi-axes a along the body x axis, b along
         its z axis, physical units) with `markers` markers at equal arc length;
-        it settles under gravity by multi-direct forcing (ipcu_sim_ib_attach)."""
+        it settles under gravity by multi-direct forcing (ipcu_sim_ib_attach).
+        Each call adds a body (index 0, 1, ...); bodies must stay at least 6
+        cells apart."""
         X0, dS = ellipse_markers(a, b, markers)
         body = _lib.IBBody2D(xc=xc, zc=zc, theta=theta, u=u, w=w, omega=omega, rho_s=rho_s, rho_f=rho_f,
                              area=np.pi * a * b, inertia=np.pi * a * b * (a * a + b * b) / 4, semi_a=a, semi_b=b,
@@ -101,21 +103,26 @@ class Sim:
         _lib.check(_lib.lib().ipcu_sim_ib_attach(self._h, ctypes.byref(body), X0.ctypes.data, dS.ctypes.data,
                                                  len(dS)), "ipcu_sim_ib_attach")
 
-    def body(self):
-        """Body state: dict of x, z, u, w, theta, omega, Fx, Fz, T (the IB
-        force and torque on the fluid in the last step)."""
+    @property
+    def n_bodies(self):
+        """Bodies attached."""
+        return int(_lib.lib().ipcu_sim_ib_count(self._h))
+
+    def body(self, index=0):
+        """State of body `index`: dict of x, z, u, w, theta, omega, Fx, Fz, T
+        (the IB force and torque on the fluid in the last step)."""
         out = np.zeros(9)
-        _lib.check(_lib.lib().ipcu_sim_ib_body(self._h, out.ctypes.data), "ipcu_sim_ib_body")
+        _lib.check(_lib.lib().ipcu_sim_ib_body_at(self._h, int(index), out.ctypes.data), "ipcu_sim_ib_body_at")
         return dict(zip(("x", "z", "u", "w", "theta", "omega", "Fx", "Fz", "T"), out.tolist()))
 
-    def markers(self):
-        """Markers of the attached body, [n, 9]: x, y, z, u, v, w, Fx, Fy, Fz
+    def markers(self, index=0):
+        """Markers of body `index`, [n, 9]: x, y, z, u, v, w, Fx, Fy, Fz
         (position, velocity, force on the fluid in the last update)."""
         cap = 4096
         out = np.zeros(9 * cap)
-        n = _lib.lib().ipcu_sim_ib_markers(self._h, out.ctypes.data, cap)
+        n = _lib.lib().ipcu_sim_ib_markers_at(self._h, int(index), out.ctypes.data, cap)
         if n < 0:
-            _lib.check(n, "ipcu_sim_ib_markers")
+            _lib.check(n, "ipcu_sim_ib_markers_at")
         return out.reshape(cap, 9)[:n].copy()
 
     def write_ib_csv(self, path):

@@ -102,8 +102,13 @@ class Body2D:
 
 
 class IBBox:
-    def __init__(self, box: Box, body: Body2D, *, rho_f, gravity, iters=3):
-        self.b, self.body = box, body
+    """The coupled step for one body or a list of bodies (each with its own
+    markers, stencils and rigid-body state; they share the fluid's force
+    density and must stay apart, as the GPU path requires)."""
+
+    def __init__(self, box: Box, body, *, rho_f, gravity, iters=3):
+        self.bodies = list(body) if isinstance(body, (list, tuple)) else [body]
+        self.b, self.body = box, self.bodies[0]
         self.rho_f, self.g, self.iters = rho_f, gravity, iters
 
     def _stencil(self, X):
@@ -125,16 +130,22 @@ class IBBox:
             self._step()
 
     def _step(self):
-        b, body = self.b, self.body
+        b = self.b
         b.step(1)
-        X, Ub = body.markers()
-        K, I, W = self._stencil(X)
         rho = b.rho_of(b.S)
         # the fluid step's velocity carries half of the previous IB force;
         # MDF starts from the velocity without it and finds the whole force
         b.ux = b.ux - b.fext[0] * b.dt / (2 * rho)
         b.uz = b.uz - b.fext[1] * b.dt / (2 * rho)
         fib = np.zeros_like(b.fext)
+        for body in self.bodies:
+            self._couple(body, rho, fib)
+        b.fext = fib
+
+    def _couple(self, body, rho, fib):
+        b = self.b
+        X, Ub = body.markers()
+        K, I, W = self._stencil(X)
         Ft = np.zeros((len(X), 2))
         h2 = b.dz * b.dz
         for _ in range(self.iters):
@@ -148,7 +159,6 @@ class IBBox:
             b.uz = b.uz + df[1] * b.dt / (2 * rho)
             fib += df
             Ft += dF
-        b.fext = fib
         # body: reaction of the marker forces, buoyancy (ref: ibm.cu:383-396),
         # the change of the fluid momentum inside the body, forward Euler
         FdS = Ft * body.dS[:, None]

@@ -68,3 +68,18 @@ def test_settling_stable_near_unit_density_ratio():
         assert np.isfinite(body.U).all() and abs(body.th - np.pi / 4) < 0.05
         assert -0.01 < body.U[1] < 0  # sinking, well below the lattice speed
         assert np.abs(b.uz).max() < 0.01
+
+
+def test_body_list_of_one_equals_single_body():
+    """IBBox over a list of bodies reduces to the one-body step."""
+    M, Minv, S = d2q9_mrt()
+    X0, dS = ellipse_markers(6.0, 3.0, 32)
+    runs = []
+    for as_list in (False, True):
+        b = Box(40, 48, M=M, Minv=Minv, S=S, q_scalar=0, tau=0.56, rho_sal=0.0, g_bouss=0.0)
+        bd = Body2D(20.0, 30.0, X0, dS, rho_s=1.5, area=np.pi * 18.0, inertia_per_mass=45.0 / 4, theta=0.3)
+        bd.a_b = (6.0, 3.0)
+        IBBox(b, [bd] if as_list else bd, rho_f=1.0, gravity=1e-4, iters=3).step(5)
+        runs.append((b.ux.copy(), b.uz.copy(), np.array([*bd.X, *bd.U, bd.th, bd.om])))
+    for x, y in zip(*runs):
+        assert np.array_equal(x, y)
