@@ -725,97 +725,121 @@ def run_reference_2d(args):
 
 def run_serving(args):
     """Continuous-batching serving stream after the 512-request serving
-    configuration: 2-D requests in equal thirds -- lock exchange (salinity),
-    Rayleigh-Taylor (Allen-Cahn phase field), both on log-uniform grids
-    128x128 .. 1024x512, and falling-ellipse immersed-boundary cases on
-    log-uniform grids 192x576 .. 800x2400 -- each with U[200, 2000] steps (a
-    tenth of the configured 2,000-20,000 to keep the run at a few seconds),
-    FP16 storage, 150 GB admission budget. The configuration's 10 % of 3-D
-    sphere requests are not part of the stream (the 3-D path has no batched
-    kernel and no immersed body).
+    configuration: 60 % 2-D D2Q9 requests (half lock exchange with D2Q5
+    salinity, half Rayleigh-Taylor on the Allen-Cahn phase field) on
+    log-uniform grids 128x128 .. 1024x512, 30 % falling-ellipse
+    immersed-boundary requests on log-uniform grids 200x600 .. 800x2400, 10 %
+    3-D D3Q19 + D3Q7 stratified boxes on log-uniform 64x64x256 .. 128x128x512
+    (without the sphere: the 3-D path has no immersed body; FP32: it has no
+    16-bit storage), each with U[2000, 20000] steps (times --step-scale),
+    2-D in FP16 storage, 150 GB admission budget, graph-captured batched
+    launches with the autotuned grid per kernel class.
       * capacity: every request submitted at t = 0, served by continuous
         batching -> aggregate MLUPS (the headline value);
       * latency: Poisson arrivals at 80 % of that capacity -> p50/p99
         completion latency;
-      * baseline: the same jobs run one at a time in plain FP32.
+      * baseline: the same jobs run one at a time in plain FP32 through the
+        same API (Sim / Sim3D with graph replay).
     The served velocities are compared with the FP32 runs (rel-L2) for three
-    requests of each kind. The Rayleigh-Taylor runs amplify a 1e-7 relative
-    perturbation of the initial phase field to about 1e-3 in FP32 and in
-    FP64 alike, so their FP32 sensitivity to that perturbation is reported
-    beside their error."""
+    requests of each kind (the FP64-oracle errors of served requests are
+    measured by the serving tests at sizes the oracle finishes). The
+    Rayleigh-Taylor runs amplify a 1e-7 relative perturbation of the initial
+    phase field to about 1e-3 in FP32 and in FP64 alike, so their FP32
+    sensitivity to that perturbation is reported beside their error."""
     import torch
 
-    from ip_cu_lbm_b200 import Sim
-    from ip_cu_lbm_b200.serving import (Server, falling_ellipse_request, lock_exchange_request,
-                                        rayleigh_taylor_request)
+    from ip_cu_lbm_b200.serving import (Autotuner, Server, falling_ellipse_request, lock_exchange_request,
+                                        make_sim, rayleigh_taylor_request, stratified_box_request)
 
     torch.cuda.set_device(0)
     rng = np.random.default_rng(20261203)
     n = args.requests
-    kinds = ("LE", "RT", "IB")
-    kind = [kinds[i % 3] for i in range(n)]
-    nx2 = np.exp(rng.uniform(np.log(128), np.log(1024), n)).astype(int) // 32 * 32
-    nz2 = np.exp(rng.uniform(np.log(128), np.log(512), n)).astype(int) // 16 * 16
-    nxi = np.exp(rng.uniform(np.log(200), np.log(800), n)).astype(int) // 32 * 32
-    nx = np.where(np.array(kind) == "IB", nxi, nx2)
-    nz = np.where(np.array(kind) == "IB", 3 * nxi, nz2)
-    steps = rng.integers(200, 2001, n)
-    work = nx * nz * steps
+    counts = {"LE": int(round(0.3 * n)), "RT": int(round(0.3 * n)), "IB": int(round(0.3 * n))}
+    counts["3D"] = n - sum(counts.values())
+    kind = [k for k, c in counts.items() for _ in range(c)]
+    rng.shuffle(kind)
+    kinds = tuple(counts)
+    logu = lambda lo, hi: float(np.exp(rng.uniform(np.log(lo), np.log(hi))))
+    dims = []
+    for k in kind:
+        if k in ("LE", "RT"):
+            dims.append((int(logu(128, 1024)) // 32 * 32, 0, int(logu(128, 512)) // 16 * 16))
+        elif k == "IB":
+            nx = int(logu(200, 800)) // 8 * 8
+            dims.append((nx, 0, 3 * nx))
+        else:
+            sc = logu(1.0, 2.0)
+            dims.append((int(64 * sc) // 16 * 16, int(64 * sc) // 16 * 16, int(256 * sc) // 16 * 16))
+    steps = np.maximum(rng.integers(2000, 20001, n) * args.step_scale, 2).astype(int)
+    cells = np.array([nx * nz * (ny if ny else 1) for nx, ny, nz in dims])
+    work = cells * steps
     makers = {"LE": lock_exchange_request, "RT": rayleigh_taylor_request, "IB": falling_ellipse_request}
 
     def mk(i, t, storage):
-        return makers[kind[i]](i, int(nx[i]), int(nz[i]), int(steps[i]), arrival=t, storage=storage, seed=i)
+        nx, ny, nz = dims[i]
+        if kind[i] == "3D":
+            return stratified_box_request(i, nx, ny, nz, int(steps[i]), arrival=t, seed=i)
+        return makers[kind[i]](i, nx, nz, int(steps[i]), arrival=t, storage=storage, seed=i)
 
     def serial_run(r, s0=None):
-        s = Sim(r.nx, r.nz, s0=r.s0 if s0 is None else s0, **r.kwargs)
-        if r.body is not None:
-            s.attach_ellipse(**r.body)
-        s.step_graph(r.steps, chunk=200)
+        if s0 is not None:
+            r.s0 = s0
+        s = make_sim(r)
+        s.step_graph(r.steps) if r.is3d else s.step_graph(r.steps, chunk=200)
         u = np.stack([s.get("ux"), s.get("uz")])
         s.close()
         return u
 
-    # warm-up: one request through each path (kernel attributes, pools)
+    # warm-up: one small request of each kind through each path (kernel attributes, pools)
     for storage in ("f16", "f32"):
         w = Server(budget_bytes=150e9, tick_steps=200)
         w.run([lock_exchange_request(0, 128, 128, 200, storage=storage),
                rayleigh_taylor_request(1, 128, 128, 200, storage=storage),
-               falling_ellipse_request(2, 192, 576, 200, storage=storage)])
+               falling_ellipse_request(2, 200, 600, 200, storage=storage),
+               stratified_box_request(3, 64, 64, 256, 200)])
         w.close()
+    # autotuner: per kernel class, the grid of the persistent batched launch (untimed)
+    t0 = time.perf_counter()
+    tuner = Autotuner()
+    tuner.tune([mk(i, 0.0, "f16") for i in range(n) if kind[i] != "3D"])
+    tune_s = time.perf_counter() - t0
     # the stream-ordered memory pool grows once to the whole stream's size
     # (every request created and released, untimed), as in a long-running server
-    warm = []
-    for i in range(n):
-        r = mk(i, 0.0, "f16")
-        s = Sim(r.nx, r.nz, s0=r.s0, **r.kwargs)
-        if r.body is not None:
-            s.attach_ellipse(**r.body)
-        warm.append(s)
+    warm = [make_sim(mk(i, 0.0, "f16")) for i in range(n)]
     for s in warm:
         s.close()
     torch.cuda.synchronize()
     # capacity: everything submitted at once
-    srv = Server(budget_bytes=150e9, tick_steps=200)
-    cap = srv.run([mk(i, 0.0, "f16") for i in range(n)])
+    srv = Server(budget_bytes=150e9, tick_steps=200, autotuner=tuner)
+    reqs = [mk(i, 0.0, "f16") for i in range(n)]
+    with Clocks(0) as ck:
+        tc = time.perf_counter()
+        cap = srv.run(reqs)
+        ck.window(tc, time.perf_counter())
+    cap_clocks = ck.summary()
     served = {r.rid: r.result for r in srv.done}
     srv.close()
+    del reqs
     # latency under load: Poisson arrivals at 80 % of the measured capacity
     lam = 0.8 * cap["mlups"] * 1e6 / work.mean()
     arrivals = np.cumsum(rng.exponential(1 / lam, n))
     arrivals -= arrivals[0]
-    srv = Server(budget_bytes=150e9, tick_steps=200)
+    srv = Server(budget_bytes=150e9, tick_steps=200, autotuner=tuner)
     lat = srv.run([mk(i, float(arrivals[i]), "f16") for i in range(n)])
     srv.close()
     # serial plain FP32: the same jobs one at a time through the same API
     checked = [i for k in kinds for i in [j for j in range(n) if kind[j] == k][:3]]
     ref_u = {}
     torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    for i in range(n):
-        u = serial_run(mk(i, 0.0, "f32"))
-        if i in checked:
-            ref_u[i] = u
-    serial_s = time.perf_counter() - t0
+    with Clocks(0) as ck:
+        t0 = time.perf_counter()
+        for i in range(n):
+            u = serial_run(mk(i, 0.0, "f32"))
+            if i in checked:
+                ref_u[i] = u
+        serial_s = time.perf_counter() - t0
+        ck.window(t0, t0 + serial_s)
+    serial_clocks = ck.summary()
     serial = float(work.sum()) / serial_s / 1e6
     rel = lambda a, b: float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-30))
     errs = {k: [] for k in kinds}
@@ -827,22 +851,26 @@ def run_serving(args):
             r = mk(i, 0.0, "f32")
             pert = r.s0 * (1 + 1e-7 * np.random.default_rng(i).standard_normal(r.s0.shape))
             floor.append(rel(serial_run(r, pert), ref_u[i]))
-    mix = {k: int(sum(1 for x in kind if x == k)) for k in kinds}
     share = {k: round(float(work[np.array(kind) == k].sum() / work.sum()), 3) for k in kinds}
     print(json.dumps({
         "metric": "served-batch MLUPS", "value": round(cap["mlups"], 1), "unit": "MLUPS", "n_gpus": 1,
         "requests": n, "capacity_wall_s": round(cap["wall_s"], 3), "capacity_host_s": cap["host_s"],
+        "clocks": cap_clocks, "serial_clocks": serial_clocks,
+        "graph": cap["graph"], "autotune": {"ctas_per_sm": tuner.choice, "mlups": tuner.timings,
+                                            "seconds": round(tune_s, 2)},
         "p50_s": round(lat["p50_s"], 4), "p99_s": round(lat["p99_s"], 4),
-        "offered_mlups": round(lat["mlups"], 1), "arrival_rate_per_s": round(lam, 2),
-        "serial_fp32_mlups": round(serial, 1), "speedup_vs_serial_fp32": round(cap["mlups"] / serial, 3),
+        "offered_mlups": round(lat["mlups"], 1), "arrival_rate_per_s": round(lam, 3),
+        "serial_fp32_mlups": round(serial, 1), "serial_fp32_wall_s": round(serial_s, 3),
+        "speedup_vs_serial_fp32": round(cap["mlups"] / serial, 3),
         "max_rel_l2_velocity_vs_fp32": {k: (max(v) if v else None) for k, v in errs.items()},
         "rt_fp32_sensitivity_1e-7": max(floor) if floor else None,
-        "config": {"workload": "2-D requests in thirds: lock exchange (salinity) and Rayleigh-Taylor (Allen-Cahn) "
-                               "on log-uniform 128x128..1024x512, falling ellipse (immersed boundary) on "
-                               "log-uniform 192x576..800x2400; U[200,2000] steps; capacity = all submitted at t=0, "
-                               "latency = Poisson arrivals at 80% of capacity",
-                   "requests_per_kind": mix, "work_share": share,
-                   "storage": "f16 served / f32 serial", "budget_gb": 150, "tick_steps": 200},
+        "config": {"workload": "60% 2-D (lock exchange with salinity, Rayleigh-Taylor with Allen-Cahn) on "
+                               "log-uniform 128x128..1024x512, 30% falling ellipse (immersed boundary) on log-uniform "
+                               "200x600..800x2400, 10% 3-D D3Q19+D3Q7 stratified boxes (no sphere) on log-uniform "
+                               "64x64x256..128x128x512; U[2000,20000] steps x step_scale; capacity = all submitted "
+                               "at t=0, latency = Poisson arrivals at 80% of capacity",
+                   "requests_per_kind": counts, "work_share": share, "step_scale": args.step_scale,
+                   "storage": "2-D f16 served / f32 serial; 3-D f32 both", "budget_gb": 150, "tick_steps": 200},
         "higher_is_better": True}), flush=True)
 
 
@@ -858,6 +886,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--serving", action="store_true", help="run the continuous-batching serving stream instead")
     ap.add_argument("--requests", type=int, default=512)
+    ap.add_argument("--step-scale", type=float, default=1.0, help="serving: scales the U[2000,20000] step counts")
     ap.add_argument("--case", default="ib", choices=["ib", "2d", "3d"],
                     help="ib: the settling-ellipse immersed-boundary case (default); 2d: the nonuniform "
                          "two-layer 1024x256 case; 3d: the C4-sized 3-D box")

@@ -176,6 +176,16 @@ int ipcu_batch_sync(ipcu_batch *batch);
  * waits for it. A server keeps the host one tick ahead of the GPU with them. */
 int ipcu_batch_mark(ipcu_batch *batch);
 int ipcu_batch_wait_mark(ipcu_batch *batch, int mark);
+/* Graph mode (enable 1): each launch call's kernel sequence is captured into
+ * one CUDA graph and replayed, the executable graph updated in place while
+ * the sequence keeps its shape (IPCU_ERR_UNSUPPORTED on the legacy default
+ * stream). ipcu_batch_graph_stats: in-place updates and instantiations so far. */
+int ipcu_batch_set_graph(ipcu_batch *batch, int enable);
+int ipcu_batch_graph_stats(const ipcu_batch *batch, int64_t *updates, int64_t *instantiations);
+/* CTAs per SM of the batched grid for one kernel class (storage, scalar
+ * lattice, geometry, scalar kind); 0 restores the default (4). The
+ * autotuner of the serving loop sets it. */
+int ipcu_batch_set_ctas(ipcu_batch *batch, int storage, int q_scalar, int geometry, int scalar_kind, int ctas_per_sm);
 /* Moving immersed boundaries: up to 16 rigid bodies per simulation, as the
  * reference's IB_index loop over bodies (ref: function/ibm.cu:367-424)
  * (uniform lattice, salinity or no scalar). Markers on the outline (body frame,

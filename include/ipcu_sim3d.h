@@ -68,6 +68,10 @@ int ipcu_sim3d_set_state(ipcu_sim3d *sim, const double *f, const double *g, cons
 /* Raw FP32 state transfer, asynchronous (pinned host buffers): f, g, F. */
 int ipcu_sim3d_upload(ipcu_sim3d *sim, const float *f, const float *g, const float *F);
 int ipcu_sim3d_download(ipcu_sim3d *sim, float *f, float *g, float *F);
+/* S, u_x, u_y, u_z of every cell ([4][N] FP32, the values ipcu_sim3d_get
+ * serves) formed on the device and copied into `out` (pinned host or device
+ * memory), asynchronous on the simulation's stream. */
+int ipcu_sim3d_macro_async(ipcu_sim3d *sim, float *out);
 int ipcu_sim3d_sync(ipcu_sim3d *sim);
 /* Sticky error flags (bit 0: non-finite moment seen). Synchronises. */
 int ipcu_sim3d_status(ipcu_sim3d *sim, uint32_t *flags);

@@ -150,6 +150,9 @@ def _declare(L: ctypes.CDLL) -> None:
         "ipcu_batch_sync": ([P], I),
         "ipcu_batch_mark": ([P], I),
         "ipcu_batch_wait_mark": ([P, I], I),
+        "ipcu_batch_set_graph": ([P, I], I),
+        "ipcu_batch_graph_stats": ([P, P, P], I),
+        "ipcu_batch_set_ctas": ([P, I, I, I, I, I], I),
         "ipcu_sim_device_bytes": ([P], I64),
         "ipcu_sim_ib_attach": ([P, ctypes.POINTER(IBBody2D), P, P, ctypes.c_int32], I),
         "ipcu_sim_ib_body": ([P, P], I),
@@ -173,6 +176,7 @@ def _declare(L: ctypes.CDLL) -> None:
         "ipcu_sim3d_set_state": ([P, P, P, P], I),
         "ipcu_sim3d_upload": ([P, P, P, P], I),
         "ipcu_sim3d_download": ([P, P, P, P], I),
+        "ipcu_sim3d_macro_async": ([P, P], I),
         "ipcu_sim3d_sync": ([P], I),
         "ipcu_sim3d_status": ([P, ctypes.POINTER(ctypes.c_uint32)], I),
         "ipcu_sim3d_cells": ([P], I64),

@@ -5,6 +5,8 @@
 #include <cuda_fp16.h>
 
 #include <algorithm>
+#include <array>
+#include <map>
 #include <tuple>
 #include <cmath>
 #include <cstring>
@@ -1562,7 +1564,19 @@ struct ipcu_batch {
   f2d::WorkItem *d_work = nullptr;
   ib2d::Job *d_jobs = nullptr;  // coupled bodies of the listed simulations
   size_t cap_params = 0, cap_work = 0, cap_jobs = 0;
-  int grid_cap = 0;
+  int sms = 148;
+  // CTAs per SM of the batched grid, per kernel class (storage, scalar
+  // lattice, geometry, scalar kind); f2d::kMinBlocks where not set
+  std::map<std::array<int, 4>, int> ctas;
+  // graph mode: each enqueue's launches are captured into one CUDA graph and
+  // replayed; the executable graph is updated in place while the launch
+  // sequence keeps its shape, and re-instantiated when it changes. Replaced
+  // executables are released once the launch that used them has completed.
+  bool use_graph = false;
+  cudaGraphExec_t exec = nullptr;
+  cudaEvent_t exec_done = nullptr;  // recorded after the last launch of `exec`
+  std::vector<std::pair<cudaGraphExec_t, cudaEvent_t>> retired;
+  long long graph_updates = 0, graph_instantiations = 0;
 };
 
 extern "C" int ipcu_batch_create(ipcu_stream_t stream, ipcu_batch **out) {
@@ -1572,7 +1586,7 @@ extern "C" int ipcu_batch_create(ipcu_stream_t stream, ipcu_batch **out) {
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  b->grid_cap = sms * f2d::kMinBlocks;
+  b->sms = sms;
   bool ok = cudaEventCreateWithFlags(&b->done, cudaEventDisableTiming) == cudaSuccess;
   for (int i = 0; i < 4 && ok; i++) ok = cudaEventCreateWithFlags(&b->mark[i], cudaEventDisableTiming) == cudaSuccess;
   if (!ok) {
@@ -1589,6 +1603,12 @@ extern "C" void ipcu_batch_destroy(ipcu_batch *b) {
   cudaFree(b->d_params);
   cudaFree(b->d_work);
   cudaFree(b->d_jobs);
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  if (b->exec_done) cudaEventDestroy(b->exec_done);
+  for (auto &r : b->retired) {
+    cudaGraphExecDestroy(r.first);
+    cudaEventDestroy(r.second);
+  }
   if (b->done) cudaEventDestroy(b->done);
   for (int i = 0; i < 4; i++)
     if (b->mark[i]) cudaEventDestroy(b->mark[i]);
@@ -1608,6 +1628,55 @@ extern "C" void ipcu_batch_destroy(ipcu_batch *b) {
 // dependent of it (only the tiles the bodies flagged wait), and a class
 // without bodies follows one with bodies, so their fluid step runs beside
 // the body updates.
+// Graph mode: capture `launches` on the batch stream, bring the executable
+// graph up to date (in place when the captured sequence has the shape of the
+// previous one) and replay it.
+template <class F>
+static int batch_graph(ipcu_batch *b, F &&launches) {
+  // release replaced executables whose last launch has completed
+  for (size_t i = 0; i < b->retired.size();) {
+    if (cudaEventQuery(b->retired[i].second) == cudaSuccess) {
+      cudaGraphExecDestroy(b->retired[i].first);
+      cudaEventDestroy(b->retired[i].second);
+      b->retired.erase(b->retired.begin() + i);
+    } else {
+      cudaGetLastError();  // cudaErrorNotReady is not an error here
+      i++;
+    }
+  }
+  if (cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return IPCU_ERR_CUDA;
+  const int st = launches();
+  cudaGraph_t graph = nullptr;
+  const cudaError_t e = cudaStreamEndCapture(b->stream, &graph);
+  if (st != IPCU_OK || e != cudaSuccess) {
+    if (graph) cudaGraphDestroy(graph);
+    return st != IPCU_OK ? st : IPCU_ERR_CUDA;
+  }
+  bool ok = false;
+  if (b->exec) {
+    cudaGraphExecUpdateResultInfo info;
+    ok = cudaGraphExecUpdate(b->exec, graph, &info) == cudaSuccess;
+    if (ok) {
+      b->graph_updates++;
+    } else {
+      cudaGetLastError();
+      b->retired.emplace_back(b->exec, b->exec_done);  // in flight until exec_done completes
+      b->exec = nullptr;
+      b->exec_done = nullptr;
+    }
+  }
+  if (!ok) {
+    ok = cudaGraphInstantiate(&b->exec, graph, 0) == cudaSuccess &&
+         cudaEventCreateWithFlags(&b->exec_done, cudaEventDisableTiming) == cudaSuccess;
+    b->graph_instantiations++;
+  }
+  cudaGraphDestroy(graph);
+  if (!ok || cudaGraphLaunch(b->exec, b->stream) != cudaSuccess ||
+      cudaEventRecord(b->exec_done, b->stream) != cudaSuccess)
+    return IPCU_ERR_CUDA;
+  return IPCU_OK;
+}
+
 static int batch_enqueue(ipcu_batch *b, ipcu_sim *const *sims, int n, const int64_t *nsteps) {
   if (!b || (n > 0 && (!sims || !nsteps))) return IPCU_ERR_ARG;
   std::vector<int> order;
@@ -1695,22 +1764,31 @@ static int batch_enqueue(ipcu_batch *b, ipcu_sim *const *sims, int n, const int6
     int st = f2d::launch_batched(nullptr, nullptr, 0, 0, g.storage, g.qs, g.geo, g.pf, 0, b->stream, true, g.tma);
     if (st) return st;
   }
-  bool after_bodies = false;  // the last launch on the stream is a batch of body updates
-  for (int64_t k = 0; k < kmax; k++) {
-    for (Group &g : groups) {
-      while (g.live > 0 && g.mem[g.live - 1].steps <= k) g.live--;  // members done after k steps
-      if (g.live == 0) continue;
-      const int nw = g.mem[g.live - 1].w1 - g.w0, nj = g.mem[g.live - 1].j1 - g.j0;
-      const int grid = std::min(nw, b->grid_cap);
-      int st = f2d::launch_batched(b->d_params, b->d_work + g.w0, nw, (int)(k & 1), g.storage, g.qs, g.geo, g.pf, grid,
-                                   b->stream, false, g.tma != 0, after_bodies);
-      after_bodies = false;
-      if (!st && nj > 0) {
-        st = ib2d::launch_batched(b->d_jobs + g.j0, nj, (int)(k & 1), g.storage, g.qs, b->stream);
-        after_bodies = true;
+  auto launches = [&]() -> int {
+    bool after_bodies = false;  // the last launch on the stream is a batch of body updates
+    for (int64_t k = 0; k < kmax; k++) {
+      for (Group &g : groups) {
+        while (g.live > 0 && g.mem[g.live - 1].steps <= k) g.live--;  // members done after k steps
+        if (g.live == 0) continue;
+        const int nw = g.mem[g.live - 1].w1 - g.w0, nj = g.mem[g.live - 1].j1 - g.j0;
+        const auto it = b->ctas.find({g.storage, g.qs, g.geo, g.pf});
+        const int grid = std::min(nw, b->sms * (it == b->ctas.end() ? f2d::kMinBlocks : it->second));
+        int st = f2d::launch_batched(b->d_params, b->d_work + g.w0, nw, (int)(k & 1), g.storage, g.qs, g.geo, g.pf,
+                                     grid, b->stream, false, g.tma != 0, after_bodies);
+        after_bodies = false;
+        if (!st && nj > 0) {
+          st = ib2d::launch_batched(b->d_jobs + g.j0, nj, (int)(k & 1), g.storage, g.qs, b->stream);
+          after_bodies = true;
+        }
+        if (st) return st;
       }
-      if (st) return st;
     }
+    return IPCU_OK;
+  };
+  if (!b->use_graph) {
+    if (int st = launches()) return st;
+  } else if (int st = batch_graph(b, launches)) {
+    return st;
   }
   if (cudaEventRecord(b->done, b->stream) != cudaSuccess) return IPCU_ERR_CUDA;
   for (int i : order) {
@@ -1743,6 +1821,29 @@ extern "C" int ipcu_batch_launch(ipcu_batch *b, ipcu_sim *const *sims, int n, in
 extern "C" int ipcu_batch_launch_each(ipcu_batch *b, ipcu_sim *const *sims, const int64_t *nsteps, int n) {
   if (n < 0) return IPCU_ERR_ARG;
   return batch_enqueue(b, sims, n, nsteps);
+}
+
+extern "C" int ipcu_batch_set_graph(ipcu_batch *b, int enable) {
+  if (!b) return IPCU_ERR_ARG;
+  if (enable && b->stream == nullptr) return IPCU_ERR_UNSUPPORTED;  // the legacy stream cannot be captured
+  b->use_graph = enable != 0;
+  return IPCU_OK;
+}
+
+extern "C" int ipcu_batch_set_ctas(ipcu_batch *b, int storage, int q_scalar, int geometry, int scalar_kind,
+                                   int ctas_per_sm) {
+  if (!b || ctas_per_sm < 0 || ctas_per_sm > 32) return IPCU_ERR_ARG;
+  const std::array<int, 4> key = {storage, q_scalar, geometry, scalar_kind};
+  if (ctas_per_sm == 0) b->ctas.erase(key);
+  else b->ctas[key] = ctas_per_sm;
+  return IPCU_OK;
+}
+
+extern "C" int ipcu_batch_graph_stats(const ipcu_batch *b, int64_t *updates, int64_t *instantiations) {
+  if (!b || !updates || !instantiations) return IPCU_ERR_ARG;
+  *updates = b->graph_updates;
+  *instantiations = b->graph_instantiations;
+  return IPCU_OK;
 }
 
 extern "C" int ipcu_batch_mark(ipcu_batch *b) {

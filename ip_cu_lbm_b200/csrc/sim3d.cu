@@ -6,6 +6,7 @@
 #include <vector>
 
 #include "axis_tables.hpp"
+#include "d3q19.cuh"
 #include "fused3d.cuh"
 #include "fused3s.cuh"
 #include "ipcu_common.cuh"
@@ -37,16 +38,27 @@ constexpr int E19[19][3] = {{0, 0, 0}, {1, 0, 0}, {0, 1, 0}, {-1, 0, 0}, {0, -1,
                             {1, 1, 0}, {1, -1, 0}, {-1, 1, 0}, {-1, -1, 0}, {1, 0, 1}, {1, 0, -1}, {-1, 0, 1},
                             {-1, 0, -1}, {0, 1, 1}, {0, 1, -1}, {0, -1, 1}, {0, -1, -1}};
 
+// Device memory is stream-ordered on the simulation's stream (a server
+// creating and releasing simulations never synchronises the device): freed
+// after the work queued on that stream, allocated before it.
+template <class V>
+bool salloc3(ipcu_sim3d *s, V **p, size_t bytes) {
+  return cudaMallocAsync((void **)p, bytes, s->stream) == cudaSuccess;
+}
+
 void free3(ipcu_sim3d *s) {
   if (!s) return;
+  auto fr = [&](void *p) {
+    if (p) cudaFreeAsync(p, s->stream);
+  };
   for (int i = 0; i < 2; i++) {
     if (s->graph[i]) cudaGraphExecDestroy(s->graph[i]);
-    cudaFree(s->f[i]);
-    cudaFree(s->g[i]);
-    cudaFree(s->F[i]);
+    fr(s->f[i]);
+    fr(s->g[i]);
+    fr(s->F[i]);
   }
-  cudaFree(s->status);
-  cudaFree(s->tab);
+  fr(s->status);
+  fr(s->tab);
   delete s;
 }
 
@@ -112,13 +124,13 @@ extern "C" int ipcu_sim3d_create_stretched(const ipcu_sim3d_config *cfg, const i
   ensure_tables();
   const long long N = s->N;
   for (int i = 0; i < 2; i++)
-    if (cudaMalloc((void **)&s->f[i], sizeof(float) * 19 * N) != cudaSuccess ||
-        cudaMalloc((void **)&s->g[i], sizeof(float) * 7 * N) != cudaSuccess ||
-        cudaMalloc((void **)&s->F[i], sizeof(float) * 3 * N) != cudaSuccess) {
+    if (!salloc3(s, &s->f[i], sizeof(float) * 19 * N) || !salloc3(s, &s->g[i], sizeof(float) * 7 * N) ||
+        !salloc3(s, &s->F[i], sizeof(float) * 3 * N)) {
       free3(s);
       return IPCU_ERR_NOMEM;
     }
-  if (cudaMalloc((void **)&s->status, sizeof(unsigned)) != cudaSuccess) {
+  // the set-up below uses synchronous copies: the allocations land first
+  if (!salloc3(s, &s->status, sizeof(unsigned)) || cudaStreamSynchronize(s->stream) != cudaSuccess) {
     free3(s);
     return IPCU_ERR_NOMEM;
   }
@@ -162,7 +174,7 @@ extern "C" int ipcu_sim3d_create_stretched(const ipcu_sim3d_config *cfg, const i
     std::vector<float> all;
     all.reserve(total);
     for (auto *v : parts) all.insert(all.end(), v->begin(), v->end());
-    if (cudaMalloc((void **)&s->tab, sizeof(float) * total) != cudaSuccess ||
+    if (!salloc3(s, &s->tab, sizeof(float) * total) || cudaStreamSynchronize(s->stream) != cudaSuccess ||
         cudaMemcpy(s->tab, all.data(), sizeof(float) * total, cudaMemcpyHostToDevice) != cudaSuccess) {
       free3(s);
       return IPCU_ERR_NOMEM;
@@ -307,6 +319,44 @@ extern "C" int ipcu_sim3d_get(ipcu_sim3d *s, const char *field, double *out, int
     }
   }
   return IPCU_OK;
+}
+
+namespace {
+// S, u_x, u_y, u_z of every cell ([4][N]) from the current state, in the
+// float order of ipcu_sim3d_get (explicit rounding: the same values)
+__global__ void macro3d_kernel(const float *__restrict__ f, const float *__restrict__ g, const float *__restrict__ F,
+                               long long N, float c, float rsal, float rho0, float hdt, float *__restrict__ out) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < N; i += (long long)gridDim.x * blockDim.x) {
+    float j[3] = {0.f, 0.f, 0.f}, S = 0.f;
+#pragma unroll
+    for (int k = 0; k < 19; k++) {
+      const float v = f[k * N + i];
+      if (d3::cx(k)) j[0] = __fadd_rn(j[0], d3::cx(k) > 0 ? v : -v);
+      if (d3::cy(k)) j[1] = __fadd_rn(j[1], d3::cy(k) > 0 ? v : -v);
+      if (d3::cz(k)) j[2] = __fadd_rn(j[2], d3::cz(k) > 0 ? v : -v);
+    }
+#pragma unroll
+    for (int k = 0; k < 7; k++) S = __fadd_rn(S, g[k * N + i]);
+    const float h = __fdiv_rn(hdt, __fmaf_rn(S, rsal, rho0));
+    out[i] = S;
+#pragma unroll
+    for (int a = 0; a < 3; a++) out[(a + 1) * N + i] = __fadd_rn(__fmul_rn(c, j[a]), __fmul_rn(F[a * N + i], h));
+  }
+}
+}  // namespace
+
+extern "C" int ipcu_sim3d_macro_async(ipcu_sim3d *s, float *out) {
+  if (!s || !out) return IPCU_ERR_ARG;
+  const long long N = s->N;
+  float *d = nullptr;
+  if (cudaMallocAsync((void **)&d, sizeof(float) * 4 * N, s->stream) != cudaSuccess) return IPCU_ERR_NOMEM;
+  const int blocks = (int)std::min<long long>((N + 255) / 256, 148LL * 16);
+  macro3d_kernel<<<blocks, 256, 0, s->stream>>>(s->f[s->cur], s->g[s->cur], s->F[s->cur], N, s->P.c, s->P.rsal,
+                                                s->P.rho0, s->P.hdt, d);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaMemcpyAsync(out, d, sizeof(float) * 4 * N, cudaMemcpyDefault, s->stream);
+  cudaFreeAsync(d, s->stream);
+  return e == cudaSuccess ? IPCU_OK : IPCU_ERR_CUDA;
 }
 
 extern "C" int ipcu_sim3d_set_state(ipcu_sim3d *s, const double *f, const double *g, const double *F) {

@@ -66,6 +66,8 @@ class Sim:
         self._h = h
         self.N = self.nx * self.nz
         self.storage = storage
+        # (storage, scalar lattice, geometry, scalar kind): the batched kernel class
+        self.kernel_class = (int(cfg.storage), int(cfg.q_scalar), int(cfg.geometry), int(cfg.scalar_kind))
 
     # ---------------------------------------------------------------- lifecycle
     def close(self):

@@ -81,6 +81,18 @@ class Sim3D:
         P = lambda a: None if a is None else a.data_ptr()
         _lib.check(_lib.lib().ipcu_sim3d_download(self._h, P(f), P(g), P(F)), "ipcu_sim3d_download")
 
+    def macro_async(self, out):
+        """S, u_x, u_y, u_z ([4, N] FP32, the values of get) formed on the
+        device and copied into `out` (a pinned host or device tensor)
+        asynchronously on the simulation's stream."""
+        if out.numel() < 4 * self.N:
+            raise ValueError(f"out needs {4 * self.N} floats")
+        _lib.check(_lib.lib().ipcu_sim3d_macro_async(self._h, out.data_ptr()), "ipcu_sim3d_macro_async")
+
+    def device_bytes(self):
+        """Device bytes of the state (two buffers of f, g and the force planes)."""
+        return int(self.bytes_per_cell()) * self.N
+
     def sync(self):
         _lib.check(_lib.lib().ipcu_sim3d_sync(self._h), "ipcu_sim3d_sync")
 

@@ -9,6 +9,8 @@ from ip_cu_lbm_b200 import Sim
 from ip_cu_lbm_b200.serving import (Batch, Server, falling_ellipse_request, lock_exchange_request,
                                     rayleigh_taylor_request, request_bytes)
 
+from tests.helpers import rel_l2
+
 pytestmark = pytest.mark.gpu
 
 
@@ -155,3 +157,138 @@ def test_ragged_step_counts_in_one_call(cuda, storage):
         assert s.status() == 0
         ref.close()
         s.close()
+
+
+def test_graph_mode_batch_is_bit_identical(cuda):
+    """The batch's launches captured into a CUDA graph and replayed give the
+    launches' own results; ticks of the same shape update the executable
+    graph in place."""
+    from ip_cu_lbm_b200.serving import make_sim, new_stream
+    from ip_cu_lbm_b200 import _lib
+
+    reqs = [falling_ellipse_request(0, 192, 576, 0, storage="f16", seed=0),
+            lock_exchange_request(1, 96, 64, 0, storage="f16", seed=1),
+            rayleigh_taylor_request(2, 128, 128, 0, storage="f16", seed=2)]
+    st = new_stream()
+    plain, graphed = [make_sim(r) for r in reqs], [make_sim(r) for r in reqs]
+    a, g = Batch(st), Batch(st)
+    g.set_graph(True)
+    for k in range(4):  # same shape three times, then a ragged tick
+        n = [30, 30, 30] if k < 3 else [17, 30, 5]
+        a.launch_each(plain, n)
+        g.launch_each(graphed, n)
+    a.sync()
+    g.sync()
+    upd, inst = g.graph_stats()
+    assert inst == 2 and upd == 2, (upd, inst)
+    for s, t in zip(plain, graphed):
+        for k in ("S", "ux", "uz"):
+            assert np.array_equal(s.get(k), t.get(k)), k
+        s.close()
+        t.close()
+    a.close()
+    g.close()
+    with pytest.raises(RuntimeError):
+        Batch().set_graph(True)  # the legacy default stream cannot be captured
+    _lib.lib().ipcu_stream_destroy(st)
+
+
+def test_autotuned_grid_keeps_results(cuda):
+    """The autotuner times the candidate grids per kernel class; whatever it
+    picks, a served result equals the request run alone."""
+    from ip_cu_lbm_b200.serving import Autotuner
+
+    reqs = [lock_exchange_request(0, 96, 64, 60, storage="f16", seed=0),
+            falling_ellipse_request(1, 192, 576, 60, storage="f16", seed=1),
+            lock_exchange_request(2, 160, 48, 45, storage="f16", seed=2)]
+    tuner = Autotuner(steps=5)
+    choice = tuner.tune(reqs)
+    assert len(choice) == 2 and all(c in tuner.candidates for c in choice.values())
+    srv = Server(budget_bytes=2e9, tick_steps=20, autotuner=tuner)
+    srv.run(reqs)
+    srv.close()
+    for r in srv.done:
+        same = _alone(r, batched=True)
+        for k in ("S", "ux", "uz"):
+            assert np.array_equal(r.result[k], same[k]), (r.rid, k)
+
+
+def test_3d_requests_in_the_mix(cuda):
+    """3-D requests are admitted beside 2-D ones and replay their step graphs
+    on their own streams; each result is the 3-D simulation's own."""
+    from ip_cu_lbm_b200.serving import make_sim, stratified_box_request
+
+    reqs = [stratified_box_request(0, 64, 48, 80, 50, seed=0),
+            lock_exchange_request(1, 96, 64, 70, storage="f16", seed=1),
+            stratified_box_request(2, 32, 32, 64, 31, arrival=0.01, seed=2)]
+    srv = Server(budget_bytes=2e9, tick_steps=20)
+    stats = srv.run(reqs)
+    srv.close()
+    assert stats["requests"] == 3
+    for r in srv.done:
+        if not r.is3d:
+            continue
+        s = make_sim(r)
+        s.step(r.steps)
+        for k in ("S", "ux", "uy", "uz"):
+            assert np.array_equal(r.result[k], s.get(k).astype(np.float32)), (r.rid, k)
+        s.close()
+
+
+def test_served_fp16_against_fp64_oracle(cuda):
+    """Served FP16-storage requests of each 2-D kind, in one mix, against the
+    FP64 oracle (velocity rel-L2), the north star's bound 1e-3 for the lock
+    exchange and the falling ellipse. The Rayleigh-Taylor request is served
+    in FP32 as well: its FP32 error and the FP64 oracle's own response to a
+    1e-7 relative perturbation of the initial phase field are printed beside
+    the FP16 error. The instability amplifies any rounding: FP32 storage
+    lands as far from FP64 as FP16 does (2.4e-3 and 2.3e-3 at 300 steps), as
+    far as a 1e-7 perturbation moves FP64 itself (2.0e-3), so the FP16
+    error is held to twice the larger of the two."""
+    from oracle.ibm2d import Body2D, IBBox
+    from oracle.structured import Box
+    from ip_cu_lbm_b200 import cases
+
+    reqs = [lock_exchange_request(0, 128, 64, 400, storage="f16", seed=0),
+            rayleigh_taylor_request(1, 64, 96, 300, storage="f16", seed=1),
+            falling_ellipse_request(2, 96, 288, 300, storage="f16", seed=2),
+            rayleigh_taylor_request(3, 64, 96, 300, storage="f32", seed=1)]
+    srv = Server(budget_bytes=2e9, tick_steps=50)
+    srv.run(reqs)
+    srv.close()
+    M, Minv, S = cases.d2q9_mrt()
+    worst = {}
+    for r in sorted(srv.done, key=lambda r: r.rid):
+        kw = {k: v for k, v in r.kwargs.items() if k not in ("storage", "scalar")}
+        pf = r.kwargs.get("scalar") == "phase"
+        b = Box(r.nx, r.nz, M=M, Minv=Minv, S=S, phase_field=pf, **kw)
+        S0 = r.s0.reshape(r.nz, r.nx)
+        q = b.qs
+        if q:
+            wq = np.array([1 / 3] + [1 / 6] * 4) if q == 5 else np.array([4 / 9] + [1 / 9] * 4 + [1 / 36] * 4)
+            b.S = S0.copy()
+            b.g = wq[:, None, None] * S0[None]
+        if r.body is not None:
+            bd_ = r.body
+            X0, dS = cases.ellipse_markers(bd_["a"], bd_["b"], bd_["markers"])
+            bd = Body2D(bd_["xc"], bd_["zc"], X0, dS, rho_s=bd_["rho_s"], area=np.pi * bd_["a"] * bd_["b"],
+                        inertia_per_mass=(bd_["a"] ** 2 + bd_["b"] ** 2) / 4, theta=bd_["theta"])
+            bd.a_b = (bd_["a"], bd_["b"])
+            IBBox(b, bd, rho_f=bd_["rho_f"], gravity=bd_["gravity"], iters=bd_["iters"]).step(r.steps)
+        else:
+            b.step(r.steps)
+        e = rel_l2(np.stack([r.result["ux"], r.result["uz"]]), np.stack([b.ux, b.uz]))
+        name = ("IB" if r.body is not None else ("RT" if pf else "LE")) + ("32" if r.rid == 3 else "")
+        worst[name] = e
+        print(f"served {r.kwargs['storage']} {name} {r.nx}x{r.nz}, {r.steps} steps: velocity rel-L2 vs FP64 "
+              f"oracle {e:.2e}")
+        if r.rid == 3:
+            b2 = Box(r.nx, r.nz, M=M, Minv=Minv, S=S, phase_field=True, **kw)
+            S1 = S0 * (1 + 1e-7 * np.random.default_rng(0).standard_normal(S0.shape))
+            b2.S = S1.copy()
+            b2.g = wq[:, None, None] * S1[None]
+            b2.step(r.steps)
+            worst["sens"] = rel_l2(np.stack([b2.ux, b2.uz]), np.stack([b.ux, b.uz]))
+            print(f"FP64 oracle response to a 1e-7 relative perturbation of phi0: {worst['sens']:.2e}")
+    assert worst["LE"] <= 1e-3 and worst["IB"] <= 1e-3, worst
+    assert worst["RT"] <= 2 * max(worst["RT32"], worst["sens"]), worst
