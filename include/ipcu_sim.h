@@ -148,6 +148,16 @@ int ipcu_sim_totals(ipcu_sim *sim, double *sum_p, double *sum_s);
  * whether it is on. */
 int ipcu_sim_set_lean(ipcu_sim *sim, int enable);
 int ipcu_sim_lean(const ipcu_sim *sim);
+/* Push form of the lean step (on by default where allowed: bounce-back
+ * walls, uniform grid, two-moment MRT): each cell collides in registers and
+ * pushes its populations to the cells they stream into, no halo, no shared
+ * memory; a tile that applied a body force records that force instead of
+ * the velocity (the velocity stays recomputable bit for bit). Results equal
+ * the tile kernel's bit for bit. ipcu_sim_set_push(sim, 0) selects the
+ * tile form of the lean step (IPCU_ERR_UNSUPPORTED when enabling where not
+ * allowed); ipcu_sim_push reports whether the push form is selected. */
+int ipcu_sim_set_push(ipcu_sim *sim, int enable);
+int ipcu_sim_push(const ipcu_sim *sim);
 
 /* Batched stepping of many resident simulations (continuous-batching
  * serving): each call advances every listed simulation by nsteps with one

@@ -132,6 +132,8 @@ def _declare(L: ctypes.CDLL) -> None:
         "ipcu_sim_totals": ([P, ctypes.POINTER(D), ctypes.POINTER(D)], I),
         "ipcu_sim_set_lean": ([P, I], I),
         "ipcu_sim_lean": ([P], I),
+        "ipcu_sim_set_push": ([P, I], I),
+        "ipcu_sim_push": ([P], I),
         "ipcu_sim_upload": ([P, P, P, P], I),
         "ipcu_sim_download": ([P, P, P, P], I),
         "ipcu_sim_sync": ([P], I),

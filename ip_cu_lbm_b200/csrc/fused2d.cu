@@ -34,6 +34,7 @@ int launch_batched(const Params *ps, const WorkItem *work, int nwork, int parity
 }
 
 int launch_step(const Params &p, int storage, int qs, int geo, cudaStream_t s, bool prepare_only) {
+  if (p.lean && p.push && storage == IPCU_STORE_F32 && qs == 0 && !p.pf) return launch_push(p, s, prepare_only);
   switch (storage) {
     case IPCU_STORE_F32: return p.pf ? launch_pf_f32(p, qs, geo, s, prepare_only) : launch_f32(p, qs, geo, s, prepare_only);
     case IPCU_STORE_F16: return p.pf ? launch_pf_f16(p, qs, geo, s, prepare_only) : launch_f16(p, qs, geo, s, prepare_only);

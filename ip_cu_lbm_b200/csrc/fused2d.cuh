@@ -84,6 +84,17 @@ struct alignas(64) Params {
   uint8_t *ustore[2];
   int lean, ntx, ntz;
   float s_uni;
+  // Push form of the lean step (push2d.cu; bounce-back walls, two-moment
+  // MRT): each cell collides its own populations in registers and pushes
+  // them to the cells they stream into, so the velocity of the new state is
+  // never formed or stored.
+  int push;
+  // ib_uform (FP32 storage, no scalar lattice, uniform S): a body update
+  // leaves the velocity c j + (F0 + f_ib) dt / 2 rho in the cells it
+  // forced, with f_ib its new force density -- the state's velocity
+  // is then fma(F0 + f_ib, dt / 2 rho, c j) in every cell, f_ib as it
+  // stands (lean_velocity).
+  int ib_uform;
 };
 
 // p*, j_x, j_z of nine populations in the one summation order every kernel
@@ -107,6 +118,40 @@ __host__ __device__ __forceinline__ void moments9(const float (&f)[9], float &pr
 // prepare_only: set the kernel's shared-memory attribute (call once before any capture);
 // p.pf selects the phase-field kernels
 int launch_step(const Params &p, int storage, int qs, int geo, cudaStream_t s, bool prepare_only = false);
+// The push form of the lean flow-only step (FP32, no scalar lattice, uniform
+// grid and S, bounce-back, p.mrt == 2).
+int launch_push(const Params &p, cudaStream_t s, bool prepare_only = false);
+
+// Velocity of cell ci of buffer b of a lean simulation: the planes where
+// the step that wrote b stored them (ustore 1), elsewhere c j + F dt / 2 rho
+// from the populations with F = F0 + f_ib, F0 = (0, -S g') and f_ib the
+// immersed-boundary force density as it stands -- the force that step
+// applied, or, once a body update has run, the update's new force (ib_uform)
+// -- bit for bit the value the full step and the body update store.
+__device__ __forceinline__ void lean_velocity(const Params &p, int b, long long ci, long long N, float &ux,
+                                              float &uz) {
+  const int x = (int)(ci % p.nx), z = (int)(ci / p.nx);
+  if (p.ustore[b][(z / kTZ) * p.ntx + x / kTX] == 1) {
+    ux = p.mbuf[b][N + ci];
+    uz = p.mbuf[b][2 * N + ci];
+    return;
+  }
+  const float *fb = static_cast<const float *>(p.fbuf[b]);
+  float fv[9];
+#pragma unroll
+  for (int k = 0; k < 9; k++) fv[k] = fb[k * N + ci];
+  float pr, jx, jz;
+  moments9(fv, pr, jx, jz);
+  const float h0 = __fdividef(p.hdt, fmaf(p.s_uni, p.rho_sal_f, p.rho_base));
+  float Fx = 0.0f, Fz = 0.0f;
+  Fz -= __fmul_rn(p.s_uni, p.g_bouss_f);
+  if (p.fext != nullptr) {
+    Fx += p.fext[ci];
+    Fz += p.fext[N + ci];
+  }
+  ux = fmaf(Fx, h0, p.c * jx);
+  uz = fmaf(Fz, h0, p.c * jz);
+}
 
 // One work item of a batched step: simulation index and tile coordinates.
 struct WorkItem {

@@ -177,6 +177,54 @@ __device__ __forceinline__ void st(ST *p, long long i, float v, float scale) {
   }
 }
 
+// Two-moment MRT collision with forcing (unit non-shear rates, the
+// reference's S file): the non-shear moments relax to equilibrium in one
+// step, so
+//   f*_k = feq_k + Fk_k / 2 + (1 - 1/tau) (Minv_s M_s d)_k,  d = f - feq + Fk/2
+// (ref: collision.cu:115-150), whose shear moments reduce to (Lallemand-Luo
+// rows 7, 8)
+//   p_xx = (f1 + f3 - f2 - f4) - (u^2 - w^2)/c^2,  p_xz = (f5 + f7 - f6 - f8) - u w/c^2
+// (the forcing parts cancel pairwise); feq + Fk/2 is formed per opposite pair
+// from A = p* - 1.5 u^2 + 4.5 (e.u)^2, B = 3 e.u + e.F fden/2. uc, wc: u/c;
+// RES: f holds f - feq (16-bit storage), whose shear sums are the moments.
+// Shared by the tile kernel and the push kernel (push2d.cu); the sums of two
+// products are written as explicit fmas, so that both kernels round alike
+// whatever the compiler contracts around them.
+template <bool RES>
+__device__ __forceinline__ void collide_mrt2(const float (&f)[9], float pr, float uc, float wc, float fden, float Fx,
+                                             float Fz, float om_shear, float (&o)[9]) {
+  const float usq = fmaf(uc, uc, wc * wc);
+  const float P0 = fmaf(-1.5f, usq, pr);
+  const float hx = 0.5f * fden * Fx, hz = 0.5f * fden * Fz;
+  const float m7 = 0.25f * om_shear * (RES ? (f[1] + f[3]) - (f[2] + f[4])
+                                           : ((f[1] + f[3]) - (f[2] + f[4])) - fmaf(uc, uc, -(wc * wc)));
+  const float m8 = 0.25f * om_shear * (RES ? (f[5] + f[7]) - (f[6] + f[8])
+                                           : ((f[5] + f[7]) - (f[6] + f[8])) - uc * wc);
+  o[0] = w9(0) * P0;
+  {
+    const float A = fmaf(4.5f * uc, uc, P0), B = fmaf(3.0f, uc, hx);
+    o[1] = fmaf(w9(1), A + B, m7);
+    o[3] = fmaf(w9(3), A - B, m7);
+  }
+  {
+    const float A = fmaf(4.5f * wc, wc, P0), B = fmaf(3.0f, wc, hz);
+    o[2] = fmaf(w9(2), A + B, -m7);
+    o[4] = fmaf(w9(4), A - B, -m7);
+  }
+  {
+    const float eu = uc + wc;
+    const float A = fmaf(4.5f * eu, eu, P0), B = fmaf(3.0f, eu, hx + hz);
+    o[5] = fmaf(w9(5), A + B, m8);
+    o[7] = fmaf(w9(7), A - B, m8);
+  }
+  {
+    const float eu = wc - uc;
+    const float A = fmaf(4.5f * eu, eu, P0), B = fmaf(3.0f, eu, hz - hx);
+    o[6] = fmaf(w9(6), A + B, -m8);
+    o[8] = fmaf(w9(8), A - B, -m8);
+  }
+}
+
 // Clamp-free pull for an interior cell: lc is the cell's local index; W
 // holds the combined flux weights of its axis position for both signs of
 // the axis velocity (see axis_tables on the host), so the flux form is one
@@ -470,36 +518,11 @@ __device__ __forceinline__ void step_tile(const Params &p, int parity, int tile_
       //   p_xx = (f1 + f3 - f2 - f4) - (u^2 - w^2)/c^2, p_xz = (f5 + f7 - f6 - f8) - u w/c^2
       // (the forcing parts cancel pairwise); feq + Fk/2 is formed per
       // opposite pair from A = p* - 1.5 u^2 + 4.5 (e.u)^2, B = 3 e.u + e.F fden/2.
-      const float P0 = pr - 1.5f * usq;
-      const float hx = 0.5f * fden * Fx, hz = 0.5f * fden * Fz;
       // (16-bit storage holds f - feq already, whose shear sums are these)
-      const float m7 = 0.25f * om_shear * (RES ? (f[1] + f[3]) - (f[2] + f[4])
-                                               : ((f[1] + f[3]) - (f[2] + f[4])) - (uc * uc - wc * wc));
-      const float m8 = 0.25f * om_shear * (RES ? (f[5] + f[7]) - (f[6] + f[8])
-                                               : ((f[5] + f[7]) - (f[6] + f[8])) - uc * wc);
-      sf[e] = w9(0) * P0;
-      {
-        const float A = fmaf(4.5f * uc, uc, P0), B = fmaf(3.0f, uc, hx);
-        sf[1 * NE + e] = fmaf(w9(1), A + B, m7);
-        sf[3 * NE + e] = fmaf(w9(3), A - B, m7);
-      }
-      {
-        const float A = fmaf(4.5f * wc, wc, P0), B = fmaf(3.0f, wc, hz);
-        sf[2 * NE + e] = fmaf(w9(2), A + B, -m7);
-        sf[4 * NE + e] = fmaf(w9(4), A - B, -m7);
-      }
-      {
-        const float eu = uc + wc;
-        const float A = fmaf(4.5f * eu, eu, P0), B = fmaf(3.0f, eu, hx + hz);
-        sf[5 * NE + e] = fmaf(w9(5), A + B, m8);
-        sf[7 * NE + e] = fmaf(w9(7), A - B, m8);
-      }
-      {
-        const float eu = wc - uc;
-        const float A = fmaf(4.5f * eu, eu, P0), B = fmaf(3.0f, eu, hz - hx);
-        sf[6 * NE + e] = fmaf(w9(6), A + B, -m8);
-        sf[8 * NE + e] = fmaf(w9(8), A - B, -m8);
-      }
+      float o[9];
+      collide_mrt2<RES>(f, pr, uc, wc, fden, Fx, Fz, om_shear, o);
+#pragma unroll
+      for (int k = 0; k < 9; k++) sf[k * NE + e] = o[k];
     } else {
       // equilibrium (ref: collision.cu:3-14), d = f - feq + Fk/2; d goes to
       // shared memory (this cell's own slots) so that only the outputs stay

@@ -59,25 +59,14 @@ namespace ib2d {
 namespace {
 
 // Velocity of cell ci in buffer b, the one the fluid step wrote: its
-// velocity planes, or, after a lean flow-only step in a tile without a body
-// force, c j + F0 dt / 2 rho from the populations (the value that step
-// would have stored, bit for bit).
+// velocity planes, or, after a lean flow-only step, c j + F dt / 2 rho from
+// the populations and the force that step applied (f2d::lean_velocity: the
+// value the full step would have stored, bit for bit).
 __device__ __forceinline__ void vel_at(const f2d::Params &p, int b, const float *mac, long long ci, long long N,
                                        float &ux, float &uz) {
   if (p.lean) {
-    const int x = (int)(ci % p.nx), z = (int)(ci / p.nx);
-    if (!p.ustore[b][(z / f2d::kTZ) * p.ntx + x / f2d::kTX]) {
-      const float *fb = static_cast<const float *>(p.fbuf[b]);
-      float fv[9];
-#pragma unroll
-      for (int k = 0; k < 9; k++) fv[k] = fb[k * N + ci];
-      float pr, jx, jz;
-      f2d::moments9(fv, pr, jx, jz);
-      const float h0 = __fdividef(p.hdt, fmaf(p.s_uni, p.rho_sal_f, p.rho_base));
-      ux = fmaf(0.0f, h0, p.c * jx);
-      uz = fmaf(-(p.s_uni * p.g_bouss_f), h0, p.c * jz);
-      return;
-    }
+    f2d::lean_velocity(p, b, ci, N, ux, uz);
+    return;
   }
   ux = mac[N + ci];
   uz = mac[2 * N + ci];
@@ -403,7 +392,26 @@ __device__ void coupled_update(const Job &j, int parity) {
   const float ic = 1.0f / p.c;
   for (int s = tid; s < ns; s += kThreads) {
     const long long ci = sCell[s];
-    const float un = sU[s], wn = sW[s];
+    float un = sU[s], wn = sW[s];
+    if (!RES && p.ib_uform) {
+      // uniform S, no scalar lattice: the velocity the forcing leaves, in the
+      // form the lean steps recompute it (f2d::lean_velocity), c j + (F0 +
+      // f_ib) dt / 2 rho with this update's force f_ib
+      const float *fb = static_cast<const float *>(p.fbuf[b]);
+      float fv[9];
+#pragma unroll
+      for (int k = 0; k < 9; k++) fv[k] = fb[k * N + ci];
+      float pr, jx, jz;
+      f2d::moments9(fv, pr, jx, jz);
+      const float S = p.lean ? p.s_uni : mac[ci];
+      const float hf = __fdividef(p.hdt, fmaf(S, p.rho_sal_f, p.rho_base));
+      float Fx = 0.0f, Fz = 0.0f;
+      Fz -= __fmul_rn(S, p.g_bouss_f);
+      Fx += sFX[s];
+      Fz += sFZ[s];
+      un = fmaf(Fx, hf, p.c * jx);
+      wn = fmaf(Fz, hf, p.c * jz);
+    }
     if constexpr (RES) {
       // re-express the stored deviations about the new velocity
       ST *fb = static_cast<ST *>(p.fbuf[b]);

@@ -181,23 +181,19 @@ __global__ void k_init_g(const float *S, int q, float *g, long long N) {
 }
 
 // Lean flow-only step: completes the velocity planes of buffer b in the
-// tiles whose last step did not store them (ustore[b][tile] == 0), with the
-// value that step formed, c j + F0 dt / 2 rho from the populations.
+// tiles whose last step did not store them (ustore[b][tile] 0 or 2), with
+// the value that step formed, c j + F dt / 2 rho from the populations
+// (f2d::lean_velocity).
 __global__ void k_lean_fill(const __grid_constant__ f2d::Params P, int b) {
   const long long N = (long long)P.nx * P.nz;
-  const float *fb = static_cast<const float *>(P.fbuf[b]);
   float *mac = P.mbuf[b];
-  const float h0 = __fdividef(P.hdt, fmaf(P.s_uni, P.rho_sal_f, P.rho_base));
   IPCU_FOR(i, 0, N) {
     const int x = (int)(i % P.nx), z = (int)(i / P.nx);
-    if (P.ustore[b][(z / f2d::kTZ) * P.ntx + x / f2d::kTX]) continue;
-    float fv[9];
-#pragma unroll
-    for (int k = 0; k < 9; k++) fv[k] = fb[k * N + i];
-    float pr, jx, jz;
-    f2d::moments9(fv, pr, jx, jz);
-    mac[N + i] = fmaf(0.0f, h0, P.c * jx);
-    mac[2 * N + i] = fmaf(-(P.s_uni * P.g_bouss_f), h0, P.c * jz);
+    if (P.ustore[b][(z / f2d::kTZ) * P.ntx + x / f2d::kTX] == 1) continue;
+    float ux, uz;
+    f2d::lean_velocity(P, b, i, N, ux, uz);
+    mac[N + i] = ux;
+    mac[2 * N + i] = uz;
   }
 }
 
@@ -362,14 +358,13 @@ void drop_graphs(ipcu_sim *s) {
 // A new S plane was written to the current buffer: the lean step stays on
 // only while S is uniform at the value it was set up with.
 void lean_check_s(ipcu_sim *s, const float *S) {
-  if (!s->lean_ok) return;
+  if (!s->P.ib_uform) return;
   for (long long i = 0; i < s->N; i++)
     if (S[i] != s->P.s_uni) {
       s->lean_ok = false;
-      if (s->P.lean) {
-        s->P.lean = 0;
-        drop_graphs(s);
-      }
+      s->P.ib_uform = 0;
+      if (s->P.lean) s->P.lean = 0;
+      drop_graphs(s);
       return;
     }
 }
@@ -609,6 +604,7 @@ extern "C" int ipcu_sim_create(const ipcu_sim_config *cfg, const double *s0, ipc
     for (long long i = 1; s0 && i < s->N && uni; i++) uni = (float)s0[i] == s00;
     s->lean_ok = c.storage == IPCU_STORE_F32 && c.q_scalar == 0 && !pf && P.tma && uni;
     P.s_uni = s00;
+    P.ib_uform = (c.storage == IPCU_STORE_F32 && c.q_scalar == 0 && !pf && uni) ? 1 : 0;
     if (s->lean_ok) {
       if (!salloc(s, &s->ustore[0], (size_t)s->ntiles) || !salloc(s, &s->ustore[1], (size_t)s->ntiles)) {
         free_sim(s);
@@ -617,6 +613,8 @@ extern "C" int ipcu_sim_create(const ipcu_sim_config *cfg, const double *s0, ipc
       P.ustore[0] = s->ustore[0];
       P.ustore[1] = s->ustore[1];
       P.lean = 1;
+      // the push form: bounce-back walls on a uniform grid, two-moment MRT
+      P.push = (c.wall == IPCU_WALL_BB && c.geometry == IPCU_GEO_UNIFORM && P.mrt == 2) ? 1 : 0;
     }
   }
   {
@@ -1514,6 +1512,24 @@ extern "C" int ipcu_sim_set_lean(ipcu_sim *s, int enable) {
 }
 
 extern "C" int ipcu_sim_lean(const ipcu_sim *s) { return s && s->P.lean ? 1 : 0; }
+
+extern "C" int ipcu_sim_set_push(ipcu_sim *s, int enable) {
+  if (!s) return IPCU_ERR_ARG;
+  const bool ok = s->lean_ok && s->cfg.wall == IPCU_WALL_BB && s->cfg.geometry == IPCU_GEO_UNIFORM && s->P.mrt == 2;
+  if (enable && !ok) return IPCU_ERR_UNSUPPORTED;
+  if ((s->P.push != 0) == (enable != 0)) return IPCU_OK;
+  if (!enable && s->P.lean) {
+    // the tile form reads a tile's velocity planes wherever ustore is set:
+    // complete them and mark every tile
+    if (int st = lean_fill(s)) return st;
+    if (int st = lean_mark_all(s)) return st;
+  }
+  s->P.push = enable ? 1 : 0;
+  drop_graphs(s);
+  return IPCU_OK;
+}
+
+extern "C" int ipcu_sim_push(const ipcu_sim *s) { return s && s->P.lean && s->P.push ? 1 : 0; }
 
 // Field CSV in the reference's column order (ref: function/basic.cu:16-28):
 // "num_calc,N" then x,y,z,delx,dely,pressure,salinity,phi,rho,u,v,w,Fx,Fy,Fz

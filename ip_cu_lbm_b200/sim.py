@@ -163,6 +163,15 @@ class Sim:
         """True while the step kernel runs the lean flow-only step."""
         return bool(_lib.lib().ipcu_sim_lean(self._h))
 
+    def set_push(self, on=True):
+        """Selects the push form (on) or the tile form (off) of the lean step
+        (ipcu_sim_set_push)."""
+        _lib.check(_lib.lib().ipcu_sim_set_push(self._h, 1 if on else 0), "ipcu_sim_set_push")
+
+    def push(self):
+        """True while the lean step runs in its push form."""
+        return bool(_lib.lib().ipcu_sim_push(self._h))
+
     def bytes_per_cell(self):
         return int(_lib.lib().ipcu_sim_bytes_per_cell(self._h))
 

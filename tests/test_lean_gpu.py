@@ -149,3 +149,46 @@ def test_nonuniform_scalar_turns_lean_off(cuda):
     same(a, b)
     a.close()
     b.close()
+
+
+def test_push_form_is_the_default_and_matches_the_tile_form(cuda):
+    """The push form of the lean step (bounce-back, uniform grid, two-moment
+    MRT) against the tile form and the full step, with a settling body that
+    crosses tiles (so tiles switch between F0, a recorded body force and
+    stored planes), direct steps and graph replay, and a switch of form in
+    the middle of the run."""
+    M, Minv, S = d2q9_mrt()
+    kw = dict(q_scalar=0, geometry="uniform", wall="bb", tau=0.56, rho_sal=1e-3, g_bouss=1e-5, M=M, Minv=Minv, S=S)
+    runs = []
+    for mode in ("push", "tile", "full", "switch"):
+        s = Sim(160, 128, s0=np.full(160 * 128, 0.25), **kw)
+        s.attach_ellipse(58.0, 60.0, 8.0, 4.0, markers=48, theta=0.4, rho_s=5.0, gravity=1e-4, u=0.05, w=0.01)
+        assert s.lean() and s.push()
+        if mode == "tile":
+            s.set_push(False)
+            assert s.lean() and not s.push()
+        if mode == "full":
+            s.set_lean(False)
+        s.step(37)
+        if mode == "switch":
+            s.set_push(False)
+            s.step_graph(40, chunk=10)
+            s.set_push(True)
+        else:
+            s.step_graph(40, chunk=10)
+        s.step_graph(223, chunk=50)
+        runs.append(s)
+    ref = runs[2]
+    assert ref.body()["x"] > 64.0  # the body moved across the tile column boundary at x = 64
+    for s in runs[:2] + runs[3:]:
+        assert s.body() == ref.body()
+        same(s, ref)
+        assert s.status() == 0
+    for s in runs:
+        s.close()
+    # slip walls keep the tile form
+    s = Sim(64, 32, q_scalar=0, wall="slip", M=M, Minv=Minv, S=S)
+    assert s.lean() and not s.push()
+    with pytest.raises(Exception):
+        s.set_push(True)
+    s.close()
