@@ -128,14 +128,16 @@ def traffic3d(N, stretched):
     return int(d["dram_bytes_per_cell"] * N) if d else None
 
 
-def traffic_ib(args, lean):
+def traffic_ib(args, lean, push=False):
     """DRAM bytes per launch of the settling-ellipse fluid step (FP32,
-    800 x 3000; the lean flow-only step or the full one) from the committed
-    ncu summary (profiles/traffic.json), else None."""
+    800 x 3000; the push or tile form of the lean flow-only step, or the
+    full one) from the committed ncu summary (profiles/traffic.json), else
+    None."""
     p = os.path.join(ROOT, "profiles", "traffic.json")
     if args.storage != "f32" or not os.path.exists(p):
         return None
-    key = "step_kernel<float,0,uniform,TMA,lean>@800x3000" if lean else "step_kernel<float,0,uniform,TMA>@800x3000"
+    key = ("push_kernel@800x3000" if push else
+           "step_kernel<float,0,uniform,TMA,lean>@800x3000" if lean else "step_kernel<float,0,uniform,TMA>@800x3000")
     d = json.load(open(p)).get(key)
     return d["dram_bytes_per_launch"] if d else None
 
@@ -466,6 +468,26 @@ def run_ib(args):
     peak, peak_src = load_peaks()
     achieved = N * bpc / (step_ms / 1e3) / 1e9
     b = sim.body()
+    # the fluid step alone: the same box without the body (same kernel, same
+    # bytes), timed the same way
+    fluid = Sim(meta["nx"], meta["nz"], s0=S0.ravel(), stream=stream.cuda_stream, **params)
+    fev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    for w in range(args.warmup):
+        fluid.step_graph(inner, chunk=chunk)
+    R.barrier()
+    for k in range(args.steps):
+        flush.fill_(float(k))
+        fev[k][0].record(stream)
+        fluid.step_graph(inner, chunk=chunk)
+        fev[k][1].record(stream)
+    R.barrier()
+    fluid_ms = R.max(sum(a.elapsed_time(b) for a, b in fev))
+    fluid_step_ms = fluid_ms / (args.steps * inner)
+    fluid_gbs = N * bpc / (fluid_step_ms / 1e3) / 1e9
+    fluid_only = {"value": round(world * N * inner * args.steps / (fluid_ms / 1e3) / 1e6, 2), "unit": METRIC,
+                  "achieved_gbs": round(fluid_gbs, 1), "frac": round(fluid_gbs / peak, 4),
+                  "kernel": "push form" if fluid.push() else ("lean tile form" if fluid.lean() else "full step")}
+    fluid.close()
     # end to end through the C ABI: every bench step uploads the whole state
     # from pinned host memory, advances --inner steps and downloads the whole
     # state and the body (the state lives on the host between steps)
@@ -497,14 +519,18 @@ def run_ib(args):
         "config": ib_config(meta["nx"], meta["nz"]) if args.storage == "f32" else
         dict(ib_config(meta["nx"], meta["nz"]), storage=args.storage),
         "lbm_steps_per_step": inner, "parallelism": f"replicas x{world}",
-        "scheme": "fused collide-and-stream step (lean flow-only form: populations only, velocity planes near "
+        "scheme": "lean flow-only step in push form (each cell collides in registers and pushes its nine "
+                  "populations; 72 B/cell, no velocity planes) + multi-direct forcing (3 iterations, Peskin-4) with "
+                  "an FP64 rigid-body update, CUDA-graph replay" if sim.push() else
+                  "fused collide-and-stream step (lean flow-only form: populations only, velocity planes near "
                   "the body) + multi-direct forcing (3 iterations, Peskin-4) with an FP64 rigid-body update, "
                   "CUDA-graph replay" if sim.lean() else
                   "fused collide-and-stream step + multi-direct forcing (3 iterations, Peskin-4) with an FP64 "
                   "rigid-body update, CUDA-graph replay",
         "body_after": {k: round(v, 6) for k, v in b.items() if k in ("x", "z", "w", "theta")},
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                     "frac": round(achieved / peak, 4), "traffic": traffic_ib(args, sim.lean()), "bytes_per_cell": bpc,
+                     "frac": round(achieved / peak, 4), "traffic": traffic_ib(args, sim.lean(), sim.push()),
+                     "bytes_per_cell": bpc, "fluid_only": fluid_only,
                      "peak_source": peak_label(peak_src),
                      "note": "fluid step's algorithmic bytes / (fluid + immersed-boundary kernel time per step); "
                              "traffic = ncu dram read+write bytes of one fluid launch"},
