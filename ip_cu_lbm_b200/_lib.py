@@ -179,6 +179,7 @@ def _declare(L: ctypes.CDLL) -> None:
         "ipcu_sim3d_upload": ([P, P, P, P], I),
         "ipcu_sim3d_download": ([P, P, P, P], I),
         "ipcu_sim3d_macro_async": ([P, P], I),
+
         "ipcu_sim3d_sync": ([P], I),
         "ipcu_sim3d_status": ([P, ctypes.POINTER(ctypes.c_uint32)], I),
         "ipcu_sim3d_cells": ([P], I64),

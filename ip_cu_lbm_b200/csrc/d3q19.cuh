@@ -59,8 +59,10 @@ static_assert(check_tables(), "D3Q19 opposite / mirror tables");
 __device__ __forceinline__ void collide19(const float (&f)[19], const float (&g)[7], float pr, float S, float uc,
                                           float vc, float wc, float hx, float hy, float hz, float itau, float omg_s,
                                           bool mrt, float (&fo)[19], float (&go)[7]) {
-  const float usq = uc * uc + vc * vc + wc * wc;
-  const float P0 = pr - 1.5f * usq;
+  // (sums of two products as explicit fmas: every kernel that inlines this
+  // rounds alike, whatever the compiler contracts around it)
+  const float usq = fmaf(uc, uc, fmaf(vc, vc, wc * wc));
+  const float P0 = fmaf(-1.5f, usq, pr);
   if (mrt) {
     float a1 = 0.f, a2 = 0.f, a3 = 0.f, a4 = 0.f, a5 = 0.f;
 #pragma unroll
@@ -72,8 +74,8 @@ __device__ __forceinline__ void collide19(const float (&f)[19], const float (&g)
       if (m5(k)) a5 += m5(k) * f[k];
     }
     const float om = 1.0f - itau;
-    a1 = om * (a1 - (2.0f * uc * uc - vc * vc - wc * wc)) * (1.0f / 36.0f);
-    a2 = om * (a2 - (vc * vc - wc * wc)) * (1.0f / 12.0f);
+    a1 = om * (a1 - fmaf(2.0f * uc, uc, -fmaf(vc, vc, wc * wc))) * (1.0f / 36.0f);
+    a2 = om * (a2 - fmaf(vc, vc, -(wc * wc))) * (1.0f / 12.0f);
     a3 = om * (a3 - uc * vc) * 0.25f;
     a4 = om * (a4 - vc * wc) * 0.25f;
     a5 = om * (a5 - uc * wc) * 0.25f;

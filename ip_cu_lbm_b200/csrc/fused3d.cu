@@ -123,7 +123,7 @@ __global__ void __launch_bounds__(kThreads, 4) step3d_kernel(const __grid_consta
       const float S = sS[s0][ly][lx];
       const float rho = fmaf(S, p.rsal, p.rho0);
       const float h = __fdividef(p.hdt, rho);
-      const float uc = (c * jx + Fpx * h) * ic, vc = (c * jy + Fpy * h) * ic, wc = (c * jz + Fpz * h) * ic;
+      const float uc = fmaf(c, jx, Fpx * h) * ic, vc = fmaf(c, jy, Fpy * h) * ic, wc = fmaf(c, jz, Fpz * h) * ic;
       // force: buoyancy + pressure gradient, clamped central differences (ref: collision.cu:77-88)
       auto rs = [&](float s) { return fmaf(s, p.rsal, p.rho0); };
       const float gx = (x == 0 || x == nx - 1) ? p.gi_wall : p.gi_in;
@@ -132,7 +132,8 @@ __global__ void __launch_bounds__(kThreads, 4) step3d_kernel(const __grid_consta
       const float pc = pr * c2 / 3.0f;
       const float Fx = -pc * ((rs(sS[s0][ly][x + 1 < nx ? lx + 1 : lx]) - rs(sS[s0][ly][x > 0 ? lx - 1 : lx])) * gx);
       const float Fy = -pc * ((rs(sS[s0][y + 1 < ny ? ly + 1 : ly][lx]) - rs(sS[s0][y > 0 ? ly - 1 : ly][lx])) * gy);
-      const float Fz = -S * p.gb - pc * ((rs(sS[z + 1 < nz ? sp : s0][ly][lx]) - rs(sS[z > 0 ? sm : s0][ly][lx])) * gz);
+      const float Fz =
+          fmaf(-S, p.gb, -(pc * ((rs(sS[z + 1 < nz ? sp : s0][ly][lx]) - rs(sS[z > 0 ? sm : s0][ly][lx])) * gz)));
       // collision
       const float fden = __fdividef(p.fk3, rho);
       const float hx = 0.5f * fden * Fx, hy = 0.5f * fden * Fy, hz = 0.5f * fden * Fz;

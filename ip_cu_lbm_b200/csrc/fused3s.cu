@@ -32,6 +32,7 @@
 // L2): f [19][N], g [7][N] and the force F [3][N], 232 B per cell in FP32.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <type_traits>
 
 #include "d3q19.cuh"
@@ -80,6 +81,45 @@ __device__ __forceinline__ int pofs(int k, bool isg, int plane) {
 }
 
 
+// Collision of cell i (column gx, gy; its salinity S and the clamped
+// neighbours' along x, y and z; gz the z gradient factor of its plane): the
+// reference's moments -> Force -> collision on the D3Q19 / D3Q7 subsets
+// (ref: function/collision.cu:57-257). Returns true where the state is not
+// finite.
+__device__ __forceinline__ bool collide_cell(const Params3S &p, long long i, long long N, int gx, int gy, float S,
+                                             float Sxm, float Sxp, float Sym, float Syp, float Szm, float Szp,
+                                             float gz, float (&fo)[19], float (&go)[7], float &Fx, float &Fy,
+                                             float &Fz) {
+  const float c = p.c, ic = 1.0f / c, c2 = c * c;
+  float f[19], g[7];
+#pragma unroll
+  for (int k = 0; k < 19; k++) f[k] = p.f_in[k * N + i];
+#pragma unroll
+  for (int k = 0; k < 7; k++) g[k] = p.g_in[k * N + i];
+  const float Fpx = p.F_in[i], Fpy = p.F_in[N + i], Fpz = p.F_in[2 * N + i];
+  float pr = 0.f, jx = 0.f, jy = 0.f, jz = 0.f;
+#pragma unroll
+  for (int k = 0; k < 19; k++) {
+    pr += f[k];
+    if (cx(k)) jx += cx(k) * f[k];
+    if (cy(k)) jy += cy(k) * f[k];
+    if (cz(k)) jz += cz(k) * f[k];
+  }
+  auto rs = [&](float s) { return fmaf(s, p.rsal, p.rho0); };
+  const float rho = rs(S);
+  const float hh = __fdividef(p.hdt, rho);
+  const float uc = fmaf(c, jx, Fpx * hh) * ic, vc = fmaf(c, jy, Fpy * hh) * ic, wc = fmaf(c, jz, Fpz * hh) * ic;
+  // force: buoyancy + pressure gradient over clamped neighbours (ref: collision.cu:77-88)
+  const float pc = pr * c2 / 3.0f;
+  Fx = -pc * ((rs(Sxp) - rs(Sxm)) * __ldg(p.ax.ginv + gx));
+  Fy = -pc * ((rs(Syp) - rs(Sym)) * __ldg(p.ay.ginv + gy));
+  Fz = fmaf(-S, p.gb, -(pc * ((rs(Szp) - rs(Szm)) * gz)));
+  const float fden = __fdividef(p.fk3, rho);
+  collide19(f, g, pr, S, uc, vc, wc, 0.5f * fden * Fx, 0.5f * fden * Fy, 0.5f * fden * Fz, p.itau, p.omg_s,
+            p.mrt != 0, fo, go);
+  return !(isfinite(uc) && isfinite(vc) && isfinite(wc) && isfinite(S) && isfinite(pr));
+}
+
 // The wall path: populations of the boundary-layer cells (first and last
 // cell along x, y or z) whose source c - e lies outside the box bounce back,
 // f(c, k) = ftmp(c, -k), and the partner of that ftmp is across the wall:
@@ -88,26 +128,40 @@ __device__ __forceinline__ int pofs(int k, bool isg, int plane) {
 // are queued and taken as (population, cell) pairs, consecutive lanes on one
 // population, whose code is instantiated per population (compile-time
 // direction tables; only the mirror choice is decided at run time).
+//
+// Src is where the post-collision populations live (RingSrc: the kernel's
+// shared-memory plane rings, by z-motion class).
 template <int NS>
-struct Wall {
+struct RingSrc {
   using Gm = G<NS>;
-  static constexpr int h = Gm::h, RX = Gm::RX, RC = Gm::RC;
   const float *sm;
-  const Params3S *p;
-  int nx, ny, nz, rx0, ry0;
-
-  __device__ __forceinline__ int clx(int v) const { return min(max(v, 0), nx - 1); }
-  __device__ __forceinline__ int cly(int v) const { return min(max(v, 0), ny - 1); }
+  int rx0, ry0;
   // plane slot of the z-motion class CZ
   template <int CZ>
   __device__ __forceinline__ const float *slot(int plane) const {
-    return sm + (CZ > 0 ? Gm::UP0 + (plane % 3) * 6 * RC
-                        : (CZ < 0 ? Gm::DN0 + (plane & 1) * 6 * RC : Gm::MID0 + (plane & 1) * 14 * RC));
+    return sm + (CZ > 0 ? Gm::UP0 + (plane % 3) * 6 * Gm::RC
+                        : (CZ < 0 ? Gm::DN0 + (plane & 1) * 6 * Gm::RC : Gm::MID0 + (plane & 1) * 14 * Gm::RC));
   }
   // value of slot row `idx` (population within the class) at (gx, gy)
   __device__ __forceinline__ float V(const float *b, int idx, int gx, int gy) const {
-    return b[idx * RC + (gy - ry0) * RX + (gx - rx0)];
+    return b[idx * Gm::RC + (gy - ry0) * Gm::RX + (gx - rx0)];
   }
+};
+
+template <int NS, class Src>
+struct Wall {
+  static constexpr int h = NS / 2;
+  Src src;
+  const Params3S *p;
+  int nx, ny, nz;
+
+  __device__ __forceinline__ int clx(int v) const { return min(max(v, 0), nx - 1); }
+  __device__ __forceinline__ int cly(int v) const { return min(max(v, 0), ny - 1); }
+  template <int CZ>
+  __device__ __forceinline__ const float *slot(int plane) const {
+    return src.template slot<CZ>(plane);
+  }
+  __device__ __forceinline__ float V(const float *b, int idx, int gx, int gy) const { return src.V(b, idx, gx, gy); }
   __device__ __forceinline__ float Ix(const float *b, int idx, int s, int gx, int gy) const {
     const int sg = s == 0 ? 1 : -1;
     const float *w = p->ax.wA + ((long long)s * nx + gx) * NS;
@@ -179,10 +233,13 @@ struct Wall {
         return Ixy(b, i, sxi, syi, qx, qy);
       };
       const float axs = __ldg(p->ax.scout + clx(gx + ax)), ays = __ldg(p->ay.scout + cly(gy + ay));
-      const float fin = (axs * ays) * Q(3, gx, gy) + ays * (Q(2, gx + ax, gy) - axs * Q(3, gx + ax, gy)) +
-                        axs * (Q(1, gx, gy + ay) - ays * Q(3, gx, gy + ay));
-      const float fout =
-          axs * Q(1, gx + ax, gy + ay) + ays * Q(2, gx + ax, gy + ay) - (axs * ays) * Q(3, gx + ax, gy + ay);
+      // (explicit fmas: the rounding does not depend on what the compiler
+      // contracts around the call)
+      const float fin = fmaf(axs * ays, Q(3, gx, gy),
+                             fmaf(ays, fmaf(-axs, Q(3, gx + ax, gy), Q(2, gx + ax, gy)),
+                                  axs * fmaf(-ays, Q(3, gx, gy + ay), Q(1, gx, gy + ay))));
+      const float fout = fmaf(axs, Q(1, gx + ax, gy + ay),
+                              fmaf(ays, Q(2, gx + ax, gy + ay), -((axs * ays) * Q(3, gx + ax, gy + ay))));
       return Q(0, gx + ax, gy + ay) + (fin - fout);
     }
   }
@@ -217,7 +274,6 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) step3s_kernel(const __gr
   const int x0 = blockIdx.x * kTX, y0 = blockIdx.y * kTY;
   const int zb = blockIdx.z * p.zchunk, ze = min(zb + p.zchunk, nz);
   const int rx0 = x0 - H, ry0 = y0 - H;  // global coordinates of region cell (0, 0)
-  const float c = p.c, ic = 1.0f / c, c2 = c * c;
   auto clx = [&](int v) { return min(max(v, 0), nx - 1); };
   auto cly = [&](int v) { return min(max(v, 0), ny - 1); };
 
@@ -246,35 +302,11 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) step3s_kernel(const __gr
       const int gx = rx0 + lx, gy = ry0 + ly;
       if (gx < 0 || gx >= nx || gy < 0 || gy >= ny) continue;
       const long long i = (long long)q * P + (long long)gy * nx + gx;
-      float f[19], g[7];
-#pragma unroll
-      for (int k = 0; k < 19; k++) f[k] = p.f_in[k * N + i];
-#pragma unroll
-      for (int k = 0; k < 7; k++) g[k] = p.g_in[k * N + i];
-      const float Fpx = p.F_in[i], Fpy = p.F_in[N + i], Fpz = p.F_in[2 * N + i];
-      float pr = 0.f, jx = 0.f, jy = 0.f, jz = 0.f;
-#pragma unroll
-      for (int k = 0; k < 19; k++) {
-        pr += f[k];
-        if (cx(k)) jx += cx(k) * f[k];
-        if (cy(k)) jy += cy(k) * f[k];
-        if (cz(k)) jz += cz(k) * f[k];
-      }
       const int se = (ly + 1) * SX + lx + 1;  // ring slot of the cell
       const float S = Sq[se];
-      auto rs = [&](float s) { return fmaf(s, p.rsal, p.rho0); };
-      const float rho = rs(S);
-      const float hh = __fdividef(p.hdt, rho);
-      const float uc = (c * jx + Fpx * hh) * ic, vc = (c * jy + Fpy * hh) * ic, wc = (c * jz + Fpz * hh) * ic;
-      // force: buoyancy + pressure gradient over clamped neighbours (ref: collision.cu:77-88)
-      const float pc = pr * c2 / 3.0f;
-      const float Fx = -pc * ((rs(Sq[se + 1]) - rs(Sq[se - 1])) * __ldg(p.ax.ginv + gx));
-      const float Fy = -pc * ((rs(Sq[se + SX]) - rs(Sq[se - SX])) * __ldg(p.ay.ginv + gy));
-      const float Fz = -S * p.gb - pc * ((rs(q + 1 < nz ? Sp[se] : S) - rs(q > 0 ? Sm[se] : S)) * gz);
-      const float fden = __fdividef(p.fk3, rho);
-      float fo[19], go[7];
-      collide19(f, g, pr, S, uc, vc, wc, 0.5f * fden * Fx, 0.5f * fden * Fy, 0.5f * fden * Fz, p.itau, p.omg_s,
-                p.mrt != 0, fo, go);
+      float fo[19], go[7], Fx, Fy, Fz;
+      const bool bad = collide_cell(p, i, N, gx, gy, S, Sq[se - 1], Sq[se + 1], Sq[se - SX], Sq[se + SX],
+                                    q > 0 ? Sm[se] : S, q + 1 < nz ? Sp[se] : S, gz, fo, go, Fx, Fy, Fz);
       const int le = ly * RX + lx;
 #pragma unroll
       for (int k = 0; k < 19; k++) sm[pofs<NS>(k, false, q) + le] = fo[k];
@@ -286,7 +318,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) step3s_kernel(const __gr
         Fr[kTX * kTY] = Fy;
         Fr[2 * kTX * kTY] = Fz;
       }
-      if (!(isfinite(uc) && isfinite(vc) && isfinite(wc) && isfinite(S) && isfinite(pr))) atomicOr(p.status, 1u);
+      if (bad) atomicOr(p.status, 1u);
     }
   };
 
@@ -408,7 +440,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) step3s_kernel(const __gr
     // the wall cells of the plane: one (cell, population) pair per thread
     __syncthreads();
     {
-      const Wall<NS> wp{sm, &p, nx, ny, nz, rx0, ry0};
+      const Wall<NS, RingSrc<NS>> wp{RingSrc<NS>{sm, rx0, ry0}, &p, nx, ny, nz};
       const int nq = *qcount, nw = nq * 26;
 #pragma unroll 1
       for (int w = tid; w < nw; w += kThreads) {
@@ -429,6 +461,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) step3s_kernel(const __gr
 }
 
 size_t smem3s(int ns) { return ns == 5 ? G<5>::bytes : G<3>::bytes; }
+
 
 template <int NS>
 int launch_ns(const Params3S &p, cudaStream_t s, bool prep) {

@@ -373,6 +373,7 @@ extern "C" int ipcu_sim3d_set_state(ipcu_sim3d *s, const double *f, const double
                                                                                                       : IPCU_ERR_CUDA;
 }
 
+
 extern "C" int ipcu_sim3d_upload(ipcu_sim3d *s, const float *f, const float *g, const float *F) {
   if (!s) return IPCU_ERR_ARG;
   const long long N = s->N;
