@@ -83,6 +83,35 @@ int64_t ipcu_sim3d_bytes_per_cell(const ipcu_sim3d *sim);
  * continues bit-identically. */
 int ipcu_sim3d_save(ipcu_sim3d *sim, const char *path);
 int ipcu_sim3d_load(const char *path, ipcu_stream_t stream, ipcu_sim3d **out);
+/* Moving rigid sphere (one per simulation; the sphere of the reference's
+ * SphereFallSuzuki2018 driver): markers on its surface (body frame, [n][3],
+ * n <= 4096) carry areas dA; each step, after the fluid step, multi-direct
+ * forcing with the reference's 4-point Peskin kernel per axis (ref:
+ * function/ibm.cu:61-66 weightFunction; on stretched x and y axes the kernel
+ * is evaluated in cell-index space) makes the fluid follow the body at the
+ * markers, the force density enters the next fluid step, and the body moves
+ * by an FP64 momentum balance built on the reference's update_IBbody /
+ * update_IBpoint (ref: function/ibm.cu:367-447) in three dimensions:
+ * reaction of the IB force, buoyancy -(1 - rho_f/rho_s) m gravity along z,
+ * the change of the fluid momentum inside the sphere. Drops recorded
+ * graphs; snapshots of a simulation with a sphere are refused
+ * (IPCU_ERR_UNSUPPORTED). Status bit 8: the footprint outgrew the update's
+ * window (the update was skipped). */
+typedef struct ipcu_ib_sphere3d {
+  double xc, yc, zc;  /* centre (physical units; cell centres at the axes' x, y and (k + 1/2) dz) */
+  double u, v, w;     /* initial velocity */
+  double radius;
+  double rho_s, rho_f; /* sphere and fluid density */
+  double gravity;
+  int32_t iters;      /* multi-direct forcing iterations (3) */
+  int32_t pad;
+} ipcu_ib_sphere3d;
+int ipcu_sim3d_ib_attach(ipcu_sim3d *sim, const ipcu_ib_sphere3d *body, const double *markers, const double *dA,
+                         int32_t n);
+/* Sphere state: centre (3), velocity (3), angular velocity (3), and the IB
+ * force (3) and torque (3) the markers put on the fluid in the last step
+ * (15 values). Synchronises. */
+int ipcu_sim3d_ib_body(ipcu_sim3d *sim, double *out);
 int64_t ipcu_sim3d_steps(const ipcu_sim3d *sim);
 
 #endif /* IPCU_SIM3D_H */

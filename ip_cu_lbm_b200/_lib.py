@@ -83,6 +83,16 @@ class IBBody2D(ctypes.Structure):
     ]
 
 
+class IBSphere3D(ctypes.Structure):
+    """Mirror of ipcu_ib_sphere3d (include/ipcu_sim3d.h)."""
+    _fields_ = [
+        ("xc", ctypes.c_double), ("yc", ctypes.c_double), ("zc", ctypes.c_double),
+        ("u", ctypes.c_double), ("v", ctypes.c_double), ("w", ctypes.c_double),
+        ("radius", ctypes.c_double), ("rho_s", ctypes.c_double), ("rho_f", ctypes.c_double),
+        ("gravity", ctypes.c_double), ("iters", ctypes.c_int32), ("pad", ctypes.c_int32),
+    ]
+
+
 class Sim3DAxes(ctypes.Structure):
     """Mirror of ipcu_sim3d_axes (include/ipcu_sim3d.h)."""
     _fields_ = [("x", ctypes.c_void_p), ("wx", ctypes.c_void_p), ("y", ctypes.c_void_p), ("wy", ctypes.c_void_p),
@@ -166,6 +176,8 @@ def _declare(L: ctypes.CDLL) -> None:
         "ipcu_sim3d_save": ([P, ctypes.c_char_p], I),
         "ipcu_sim3d_load": ([ctypes.c_char_p, P, ctypes.POINTER(P)], I),
         "ipcu_sim3d_steps": ([P], I64),
+        "ipcu_sim3d_ib_attach": ([P, ctypes.POINTER(IBSphere3D), P, P, ctypes.c_int32], I),
+        "ipcu_sim3d_ib_body": ([P, P], I),
         "ipcu_stream_create": ([ctypes.POINTER(P)], I),
         "ipcu_stream_destroy": ([P], I),
         "ipcu_sim3d_create": ([ctypes.POINTER(Sim3DConfig), P, P, ctypes.POINTER(P)], I),

@@ -242,3 +242,15 @@ def ellipse_markers(a, b, n):
     s = np.concatenate([[0.0], np.cumsum(np.hypot(np.diff(x), np.diff(z)))])
     tt = np.interp(np.arange(n) * s[-1] / n, s, t)
     return np.stack([a * np.cos(tt), b * np.sin(tt)], 1), np.full(n, s[-1] / n)
+
+
+def sphere_markers(radius, n):
+    """Lagrangian markers of a sphere of the given radius in the body frame:
+    n points on a Fibonacci lattice (z = 1 - (2i + 1)/n, azimuth advancing by
+    the golden angle), each carrying the area 4 pi R^2 / n."""
+    i = np.arange(n)
+    z = 1.0 - (2.0 * i + 1.0) / n
+    rxy = np.sqrt(np.maximum(1.0 - z * z, 0.0))
+    phi = i * (np.pi * (3.0 - np.sqrt(5.0)))
+    r = radius * np.stack([rxy * np.cos(phi), rxy * np.sin(phi), z], 1)
+    return r, np.full(n, 4.0 * np.pi * radius * radius / n)

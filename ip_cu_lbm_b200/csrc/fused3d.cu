@@ -130,10 +130,15 @@ __global__ void __launch_bounds__(kThreads, 4) step3d_kernel(const __grid_consta
       const float gy = (y == 0 || y == ny - 1) ? p.gi_wall : p.gi_in;
       const float gz = (z == 0 || z == nz - 1) ? p.gi_wall : p.gi_in;
       const float pc = pr * c2 / 3.0f;
-      const float Fx = -pc * ((rs(sS[s0][ly][x + 1 < nx ? lx + 1 : lx]) - rs(sS[s0][ly][x > 0 ? lx - 1 : lx])) * gx);
-      const float Fy = -pc * ((rs(sS[s0][y + 1 < ny ? ly + 1 : ly][lx]) - rs(sS[s0][y > 0 ? ly - 1 : ly][lx])) * gy);
-      const float Fz =
+      float Fx = -pc * ((rs(sS[s0][ly][x + 1 < nx ? lx + 1 : lx]) - rs(sS[s0][ly][x > 0 ? lx - 1 : lx])) * gx);
+      float Fy = -pc * ((rs(sS[s0][y + 1 < ny ? ly + 1 : ly][lx]) - rs(sS[s0][y > 0 ? ly - 1 : ly][lx])) * gy);
+      float Fz =
           fmaf(-S, p.gb, -(pc * ((rs(sS[z + 1 < nz ? sp : s0][ly][lx]) - rs(sS[z > 0 ? sm : s0][ly][lx])) * gz)));
+      if (p.fext != nullptr) {  // immersed-boundary force density of the last body update
+        Fx += p.fext[i];
+        Fy += p.fext[N + i];
+        Fz += p.fext[2 * N + i];
+      }
       // collision
       const float fden = __fdividef(p.fk3, rho);
       const float hx = 0.5f * fden * Fx, hy = 0.5f * fden * Fy, hz = 0.5f * fden * Fz;

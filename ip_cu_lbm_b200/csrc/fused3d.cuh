@@ -17,6 +17,7 @@ struct Params3 {
   float gi_in, gi_wall;      // 1/(2dz + dz/1000), 1/(dz + dz/1000) (clamped central differences)
   int mrt;
   unsigned *status;
+  const float *fext;  // [3][N] immersed-boundary force density added to the force, or null
 };
 
 int launch3d(const Params3 &p, cudaStream_t s);

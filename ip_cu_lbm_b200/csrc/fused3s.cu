@@ -114,6 +114,11 @@ __device__ __forceinline__ bool collide_cell(const Params3S &p, long long i, lon
   Fx = -pc * ((rs(Sxp) - rs(Sxm)) * __ldg(p.ax.ginv + gx));
   Fy = -pc * ((rs(Syp) - rs(Sym)) * __ldg(p.ay.ginv + gy));
   Fz = fmaf(-S, p.gb, -(pc * ((rs(Szp) - rs(Szm)) * gz)));
+  if (p.fext != nullptr) {  // immersed-boundary force density of the last body update
+    Fx += p.fext[i];
+    Fy += p.fext[N + i];
+    Fz += p.fext[2 * N + i];
+  }
   const float fden = __fdividef(p.fk3, rho);
   collide19(f, g, pr, S, uc, vc, wc, 0.5f * fden * Fx, 0.5f * fden * Fy, 0.5f * fden * Fz, p.itau, p.omg_s,
             p.mrt != 0, fo, go);

@@ -31,6 +31,7 @@ struct Params3S {
   float giz_in, giz_wall;    // z (uniform): 1/(2dz + dz/1000), 1/(dz + dz/1000)
   int mrt;
   unsigned *status;
+  const float *fext;  // [3][N] immersed-boundary force density added to the force, or null
 };
 
 // ns: 3 (quadratic upwind) or 5 (the reference's stencil)

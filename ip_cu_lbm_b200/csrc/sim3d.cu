@@ -1,6 +1,7 @@
 // 3-D structured solver object (ipcu_sim3d_*): device-resident FP32 state,
 // stepping (direct or CUDA-graph replay), field I/O.
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -9,6 +10,7 @@
 #include "d3q19.cuh"
 #include "fused3d.cuh"
 #include "fused3s.cuh"
+#include "ibm3d.cuh"
 #include "ipcu_common.cuh"
 
 using namespace ipcu;
@@ -29,6 +31,10 @@ struct ipcu_sim3d {
   f3s::Params3S PS;
   float *tab = nullptr;
   std::vector<double> X, DX, Y, DY;
+  // an attached sphere (ibm3d.cu): its job with every device array, one
+  // block of memory for them, and the force density on the fluid
+  ib3d::Job *ib = nullptr;
+  void *ib_mem = nullptr;
 };
 
 namespace {
@@ -59,6 +65,8 @@ void free3(ipcu_sim3d *s) {
   }
   fr(s->status);
   fr(s->tab);
+  fr(s->ib_mem);
+  delete s->ib;
   delete s;
 }
 
@@ -84,6 +92,19 @@ int launch_one(const ipcu_sim3d *s, int cur, cudaStream_t st) {
   P.g_out = s->g[cur ^ 1];
   P.F_out = s->F[cur ^ 1];
   return f3s::launch3s(P, s->ns, st);
+}
+
+// fluid step, then the sphere's update on the state it wrote
+int launch_step(const ipcu_sim3d *s, int cur, cudaStream_t st) {
+  int e = launch_one(s, cur, st);
+  if (e == IPCU_OK && s->ib) {
+    ib3d::Job j = *s->ib;
+    j.f = s->f[cur ^ 1];
+    j.g = s->g[cur ^ 1];
+    j.F = s->F[cur ^ 1];
+    e = ib3d::launch(j, st);
+  }
+  return e;
 }
 
 }  // namespace
@@ -241,7 +262,7 @@ extern "C" void ipcu_sim3d_destroy(ipcu_sim3d *s) {
 extern "C" int ipcu_sim3d_step(ipcu_sim3d *s, int64_t nsteps) {
   if (!s || nsteps < 0) return IPCU_ERR_ARG;
   for (int64_t k = 0; k < nsteps; k++) {
-    const int st = launch_one(s, s->cur, s->stream);
+    const int st = launch_step(s, s->cur, s->stream);
     if (st != IPCU_OK) return st;
     s->cur ^= 1;
     s->steps++;
@@ -264,8 +285,8 @@ extern "C" int ipcu_sim3d_step_graph(ipcu_sim3d *s, int64_t nsteps) {
         cudaStreamDestroy(cs);
         return IPCU_ERR_CUDA;
       }
-      int st = launch_one(s, s->cur, cs);
-      if (st == IPCU_OK) st = launch_one(s, s->cur ^ 1, cs);
+      int st = launch_step(s, s->cur, cs);
+      if (st == IPCU_OK) st = launch_step(s, s->cur ^ 1, cs);
       const cudaError_t e = cudaStreamEndCapture(cs, &gr);
       cudaStreamDestroy(cs);
       if (st != IPCU_OK || e != cudaSuccess) return st != IPCU_OK ? st : IPCU_ERR_CUDA;
@@ -429,6 +450,7 @@ bool rd3(FILE *f, T *p, size_t n) { return fread(p, sizeof(T), n, f) == n; }
 
 extern "C" int ipcu_sim3d_save(ipcu_sim3d *s, const char *path) {
   if (!s || !path) return IPCU_ERR_ARG;
+  if (s->ib) return IPCU_ERR_UNSUPPORTED;  // the sphere's state is not part of the 3-D snapshot
   const long long N = s->N;
   std::vector<float> f(19 * N), g(7 * N), F(3 * N);
   if (cudaStreamSynchronize(s->stream) != cudaSuccess ||
@@ -492,3 +514,136 @@ extern "C" int ipcu_sim3d_load(const char *path, ipcu_stream_t stream, ipcu_sim3
 }
 
 extern "C" int64_t ipcu_sim3d_steps(const ipcu_sim3d *s) { return s ? s->steps : -1; }
+
+// ---------------------------------------------------------------------------
+// Moving sphere (ibm3d.cu): one per simulation.
+extern "C" int ipcu_sim3d_ib_attach(ipcu_sim3d *s, const ipcu_ib_sphere3d *bd, const double *markers, const double *dA,
+                                    int32_t n) {
+  if (!s || !bd || !markers || !dA || n <= 0) return IPCU_ERR_ARG;
+  if (s->ib) return IPCU_ERR_CAPACITY;
+  if (n > ib3d::kMaxMarkers) return IPCU_ERR_CAPACITY;
+  if (!(bd->radius > 0 && bd->rho_s > 0 && bd->rho_f > 0 && bd->iters >= 0 && bd->iters <= 64)) return IPCU_ERR_ARG;
+  for (int i = 0; i < 3 * n; i++)
+    if (!std::isfinite(markers[i])) return IPCU_ERR_ARG;
+  for (int i = 0; i < n; i++)
+    if (!(dA[i] > 0)) return IPCU_ERR_ARG;
+  const ipcu_sim3d_config &c = s->cfg;
+  const long long N = s->N;
+  const size_t W = ib3d::kMaxWin;
+  // one block: body, markers, scratch, axes, force density (8-byte aligned parts)
+  size_t off = 0;
+  auto take = [&](size_t bytes) {
+    const size_t o = off;
+    off += (bytes + 255) / 256 * 256;
+    return o;
+  };
+  const size_t o_body = take(sizeof(ib3d::Body)), o_r0 = take(sizeof(double) * 3 * n), o_dA = take(sizeof(double) * n);
+  const size_t o_xc = take(sizeof(double) * c.nx), o_yc = take(sizeof(double) * c.ny);
+  const size_t o_wx = take(sizeof(float) * c.nx), o_wy = take(sizeof(float) * c.ny);
+  const size_t o_morg = take(sizeof(int) * 3 * n), o_mw = take(sizeof(float) * 12 * n);
+  const size_t o_mub = take(sizeof(float) * 3 * n), o_mft = take(sizeof(float) * 3 * n), o_mdf = take(sizeof(float) * 3 * n);
+  const size_t o_cnt = take(sizeof(int) * (W + 1)), o_off = take(sizeof(int) * (W + 1)), o_cur = take(sizeof(int) * (W + 1));
+  const size_t o_list = take(sizeof(int) * 64 * (size_t)n);
+  const size_t o_wu = take(sizeof(float) * 3 * W), o_wf = take(sizeof(float) * 3 * W), o_wj = take(sizeof(float) * 3 * W);
+  const size_t o_wh = take(sizeof(float) * W), o_wv = take(sizeof(float) * W);
+  const size_t o_fext = take(sizeof(float) * 3 * (size_t)N);
+  char *mem = nullptr;
+  if (cudaStreamSynchronize(s->stream) != cudaSuccess) return IPCU_ERR_CUDA;
+  if (cudaMallocAsync((void **)&mem, off, s->stream) != cudaSuccess) return IPCU_ERR_NOMEM;
+  ib3d::Job *j = new ib3d::Job();
+  std::memset(j, 0, sizeof *j);
+  j->nx = c.nx;
+  j->ny = c.ny;
+  j->nz = c.nz;
+  j->c = s->P.c;
+  j->hdt = s->P.hdt;
+  j->rho0 = s->P.rho0;
+  j->rsal = s->P.rsal;
+  j->dz = c.dz;
+  j->dt = c.dt;
+  j->body = reinterpret_cast<ib3d::Body *>(mem + o_body);
+  j->r0 = reinterpret_cast<const double *>(mem + o_r0);
+  j->dA = reinterpret_cast<const double *>(mem + o_dA);
+  j->xc = reinterpret_cast<const double *>(mem + o_xc);
+  j->yc = reinterpret_cast<const double *>(mem + o_yc);
+  j->wx = reinterpret_cast<const float *>(mem + o_wx);
+  j->wy = reinterpret_cast<const float *>(mem + o_wy);
+  j->morg = reinterpret_cast<int *>(mem + o_morg);
+  j->mw = reinterpret_cast<float *>(mem + o_mw);
+  j->mub = reinterpret_cast<float *>(mem + o_mub);
+  j->mft = reinterpret_cast<float *>(mem + o_mft);
+  j->mdf = reinterpret_cast<float *>(mem + o_mdf);
+  j->cnt = reinterpret_cast<int *>(mem + o_cnt);
+  j->off = reinterpret_cast<int *>(mem + o_off);
+  j->cur = reinterpret_cast<int *>(mem + o_cur);
+  j->list = reinterpret_cast<int *>(mem + o_list);
+  j->wu = reinterpret_cast<float *>(mem + o_wu);
+  j->wf = reinterpret_cast<float *>(mem + o_wf);
+  j->wj = reinterpret_cast<float *>(mem + o_wj);
+  j->wh = reinterpret_cast<float *>(mem + o_wh);
+  j->wv = reinterpret_cast<float *>(mem + o_wv);
+  j->fext = reinterpret_cast<float *>(mem + o_fext);
+  j->status = s->status;
+  j->nl = n;
+  j->iters = bd->iters;
+  j->radius = bd->radius;
+  const double vol = 4.0 / 3.0 * M_PI * bd->radius * bd->radius * bd->radius;
+  j->m = bd->rho_s * vol;
+  j->I = 0.4 * j->m * bd->radius * bd->radius;
+  j->rho_s = bd->rho_s;
+  j->rho_f = bd->rho_f;
+  j->grav = bd->gravity;
+  ib3d::Body b0;
+  std::memset(&b0, 0, sizeof b0);
+  b0.X[0] = bd->xc;
+  b0.X[1] = bd->yc;
+  b0.X[2] = bd->zc;
+  b0.U[0] = bd->u;
+  b0.U[1] = bd->v;
+  b0.U[2] = bd->w;
+  b0.R[0] = b0.R[4] = b0.R[8] = 1.0;
+  std::vector<float> wxf(c.nx), wyf(c.ny);
+  for (int i = 0; i < c.nx; i++) wxf[i] = (float)s->DX[i];
+  for (int i = 0; i < c.ny; i++) wyf[i] = (float)s->DY[i];
+  cudaError_t e = cudaMemcpyAsync(j->body, &b0, sizeof b0, cudaMemcpyHostToDevice, s->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(mem + o_r0, markers, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, s->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(mem + o_dA, dA, sizeof(double) * n, cudaMemcpyHostToDevice, s->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(mem + o_xc, s->X.data(), sizeof(double) * c.nx, cudaMemcpyHostToDevice, s->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(mem + o_yc, s->Y.data(), sizeof(double) * c.ny, cudaMemcpyHostToDevice, s->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(mem + o_wx, wxf.data(), sizeof(float) * c.nx, cudaMemcpyHostToDevice, s->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(mem + o_wy, wyf.data(), sizeof(float) * c.ny, cudaMemcpyHostToDevice, s->stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(j->fext, 0, sizeof(float) * 3 * (size_t)N, s->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);  // the host vectors are released on return
+  if (e != cudaSuccess) {
+    cudaFreeAsync(mem, s->stream);
+    delete j;
+    return IPCU_ERR_CUDA;
+  }
+  // the step kernels add the force density; recorded graphs hold the old parameters
+  for (int i = 0; i < 2; i++)
+    if (s->graph[i]) {
+      cudaGraphExecDestroy(s->graph[i]);
+      s->graph[i] = nullptr;
+    }
+  s->P.fext = j->fext;
+  s->PS.fext = j->fext;
+  s->ib = j;
+  s->ib_mem = mem;
+  return IPCU_OK;
+}
+
+extern "C" int ipcu_sim3d_ib_body(ipcu_sim3d *s, double *out) {
+  if (!s || !out || !s->ib) return IPCU_ERR_ARG;
+  ib3d::Body b;
+  if (cudaStreamSynchronize(s->stream) != cudaSuccess ||
+      cudaMemcpy(&b, s->ib->body, sizeof b, cudaMemcpyDeviceToHost) != cudaSuccess)
+    return IPCU_ERR_CUDA;
+  for (int a = 0; a < 3; a++) {
+    out[a] = b.X[a];
+    out[3 + a] = b.U[a];
+    out[6 + a] = b.om[a];
+    out[9 + a] = b.Fib[a];
+    out[12 + a] = b.Tib[a];
+  }
+  return IPCU_OK;
+}

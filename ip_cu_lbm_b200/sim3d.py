@@ -96,6 +96,29 @@ class Sim3D:
     def sync(self):
         _lib.check(_lib.lib().ipcu_sim3d_sync(self._h), "ipcu_sim3d_sync")
 
+    # ---------------------------------------------------------------- moving sphere
+    def attach_sphere(self, xc, yc, zc, radius, *, markers=None, rho_s=1.5, rho_f=1.0, gravity=0.0, iters=3,
+                      u=0.0, v=0.0, w=0.0):
+        """Attaches a rigid sphere (physical units) with `markers` markers on
+        a Fibonacci lattice (default: about one per unit area, at least 64)
+        that settles under gravity by multi-direct forcing
+        (ipcu_sim3d_ib_attach)."""
+        from .cases import sphere_markers
+
+        n = int(markers) if markers else max(64, int(round(4.0 * np.pi * radius * radius)))
+        r0, dA = sphere_markers(radius, n)
+        self._sphere = (np.ascontiguousarray(r0, dtype=np.float64), np.ascontiguousarray(dA, dtype=np.float64))
+        body = _lib.IBSphere3D(xc=xc, yc=yc, zc=zc, u=u, v=v, w=w, radius=radius, rho_s=rho_s, rho_f=rho_f,
+                               gravity=gravity, iters=iters, pad=0)
+        _lib.check(_lib.lib().ipcu_sim3d_ib_attach(self._h, ctypes.byref(body), self._sphere[0].ctypes.data,
+                                                   self._sphere[1].ctypes.data, n), "ipcu_sim3d_ib_attach")
+
+    def body(self):
+        """Sphere state: dict of X (3), U (3), omega (3), Fib (3), Tib (3)."""
+        out = np.zeros(15)
+        _lib.check(_lib.lib().ipcu_sim3d_ib_body(self._h, out.ctypes.data), "ipcu_sim3d_ib_body")
+        return {"X": out[0:3], "U": out[3:6], "omega": out[6:9], "Fib": out[9:12], "Tib": out[12:15]}
+
     def status(self):
         fl = ctypes.c_uint32()
         _lib.lib().ipcu_sim3d_status(self._h, ctypes.byref(fl))

@@ -100,6 +100,7 @@ class Box3D:
         self.f = np.zeros((19,) + shape)
         self.g = np.zeros((7,) + shape)
         self.F = np.zeros((3,) + shape)  # force of the previous step
+        self.fext = np.zeros((3,) + shape)  # external force density (immersed boundary), added to F
         self.reg = dz / 1000
         self.stretched = x is not None or y is not None
         self.X = np.asarray(x if x is not None else (np.arange(nx) + 0.5) * dz, float)
@@ -266,7 +267,7 @@ class Box3D:
         p, S, rho, u = self.moments()
         gx, gy, gz = self._grad(rho)
         pc = p * c2 / 3
-        F = np.stack([-pc * gx, -pc * gy, -S * self.g_bouss - pc * gz])
+        F = np.stack([-pc * gx, -pc * gy, -S * self.g_bouss - pc * gz]) + self.fext
         uc = [a / c for a in u]
         eu = sum(E19[:, a].astype(float)[:, None, None, None] * uc[a][None] for a in range(3))
         us = sum(a * a for a in uc)
