@@ -328,9 +328,11 @@ def run_3d(args):
     3.8 GB > L2), x and y tanh-clustered toward the centreline (spacing ratio
     3) with the 3-point conservative flux form, z uniform (--uniform3d: the
     uniform box), D3Q19 MRT + D3Q7 salinity with a linear stratification,
-    bounce-back, FP32 (the configuration's falling sphere is not part of
-    it). A step is --inner LBM steps (default 20) replayed from a CUDA graph;
-    the inputs are far larger than L2, so no flush is needed."""
+    bounce-back, FP32, and the configuration's falling sphere (diameter 16
+    finest cells, 804 markers, density ratio 1.5; --no-sphere leaves it
+    out). A step is --inner LBM steps (default 20), each the fluid step and
+    the sphere's update, replayed from a CUDA graph; the inputs are far
+    larger than L2, so no flush is needed."""
     import torch
 
     from ip_cu_lbm_b200 import workloads
@@ -347,6 +349,9 @@ def run_3d(args):
         for k in ("x", "wx", "y", "wy", "ns"):
             kw.pop(k)
     sim = Sim3D(nx, ny, nz, s0=S0.ravel(), stream=stream.cuda_stream, **kw)
+    sphere = None if args.no_sphere else workloads.falling_sphere_3d(kw, nx, ny, nz)
+    if sphere:
+        sim.attach_sphere(**sphere)
     N, inner = sim.N, args.inner or 20
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     with Clocks(local) as clk:
@@ -390,7 +395,10 @@ def run_3d(args):
         "config": {"workload": (f"3-D uniform box {nx}x{ny}x{nz} D3Q19 MRT + D3Q7, bounce-back" if args.uniform3d else
                                 f"3-D box {nx}x{ny}x{nz}, x and y tanh-clustered toward the centreline (ratio 3, "
                                 "3-point conservative flux form, corner transport on the xy diagonals), z uniform, "
-                                "D3Q19 MRT + D3Q7 linear stratification, bounce-back; no body"),
+                                "D3Q19 MRT + D3Q7 linear stratification, bounce-back") +
+                               (f"; falling sphere, diameter 16 cells, 804 Fibonacci markers, density ratio 1.5, "
+                                f"multi-direct forcing x3, FP64 body update (released at z = {0.8 * nz:.0f})"
+                                if sphere else "; no body"),
                    "lbm_steps_per_step": inner, "cells": N, "storage": "f32", "parallelism": f"replicas x{world}",
                    "l2": f"inputs ({4 * 29 * N / 1e9:.2f} GB) larger than L2"},
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
@@ -400,8 +408,11 @@ def run_3d(args):
                                      "scaled by cells; it grows in proportion to the cells streamed"},
         "e2e": {"value": round(e2e, 2), "unit": METRIC,
                 "h2d_bytes_per_step": int(4 * (19 + 7 + 3) * N), "d2h_bytes_per_step": int(4 * 7 * N)},
-        "gpu_launches": args.steps * inner, "clocks": clk.summary(),
+        "gpu_launches": (2 if sphere else 1) * args.steps * inner, "clocks": clk.summary(),
     }
+    if sphere:
+        b = sim.body()
+        line["body_after"] = {"X": [round(v, 6) for v in b["X"]], "U": [float(f"{v:.6e}") for v in b["U"]]}
     if R.rank == 0:
         print(json.dumps(line), flush=True)
     R.close()
@@ -755,9 +766,9 @@ def run_serving(args):
     salinity, half Rayleigh-Taylor on the Allen-Cahn phase field) on
     log-uniform grids 128x128 .. 1024x512, 30 % falling-ellipse
     immersed-boundary requests on log-uniform grids 200x600 .. 800x2400, 10 %
-    3-D D3Q19 + D3Q7 stratified boxes on log-uniform 64x64x256 .. 128x128x512
-    (without the sphere: the 3-D path has no immersed body; FP32: it has no
-    16-bit storage), each with U[2000, 20000] steps (times --step-scale),
+    3-D D3Q19 + D3Q7 stratified boxes with a falling sphere on log-uniform
+    64x64x256 .. 128x128x512 (FP32: the 3-D path has no 16-bit storage),
+    each with U[2000, 20000] steps (times --step-scale),
     2-D in FP16 storage, 150 GB admission budget, graph-captured batched
     launches with the autotuned grid per kernel class.
       * capacity: every request submitted at t = 0, served by continuous
@@ -892,7 +903,8 @@ def run_serving(args):
         "rt_fp32_sensitivity_1e-7": max(floor) if floor else None,
         "config": {"workload": "60% 2-D (lock exchange with salinity, Rayleigh-Taylor with Allen-Cahn) on "
                                "log-uniform 128x128..1024x512, 30% falling ellipse (immersed boundary) on log-uniform "
-                               "200x600..800x2400, 10% 3-D D3Q19+D3Q7 stratified boxes (no sphere) on log-uniform "
+                               "200x600..800x2400, 10% 3-D D3Q19+D3Q7 stratified boxes with a falling sphere on "
+                               "log-uniform "
                                "64x64x256..128x128x512; U[2000,20000] steps x step_scale; capacity = all submitted "
                                "at t=0, latency = Poisson arrivals at 80% of capacity",
                    "requests_per_kind": counts, "work_share": share, "step_scale": args.step_scale,
@@ -918,6 +930,7 @@ def main():
                          "two-layer 1024x256 case; 3d: the C4-sized 3-D box")
     ap.add_argument("--dims", default="160,160,640", help="3-D box nx,ny,nz (--case 3d)")
     ap.add_argument("--uniform3d", action="store_true", help="--case 3d on a uniform box (no stretched axes)")
+    ap.add_argument("--no-sphere", action="store_true", help="--case 3d without the falling sphere")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -147,8 +147,8 @@ class Request:
 def request_bytes(req: Request) -> int:
     """Device bytes a request needs once admitted (same formula as
     ipcu_sim_device_bytes; 3-D: two FP32 buffers of f, g and the force planes)."""
-    if req.is3d:
-        return 2 * 4 * (19 + 7 + 3) * req.cells
+    if req.is3d:  # (a sphere adds its force density and about 4 MB of update scratch)
+        return 2 * 4 * (19 + 7 + 3) * req.cells + ((12 * req.cells + (4 << 20)) if req.body is not None else 0)
     f32 = req.kwargs.get("storage", "f32") == "f32"
     esz, nmac = (4, 3) if f32 else (2, 4)  # 16-bit storage keeps p* in a 4th FP32 plane
     pf = req.kwargs.get("scalar", "salinity") == "phase"
@@ -166,7 +166,10 @@ def request_bytes(req: Request) -> int:
 def make_sim(req: Request, stream=None):
     """The request's simulation (2-D Sim with its body, or Sim3D)."""
     if req.is3d:
-        return Sim3D(req.nx, req.ny, req.nz, s0=req.s0, stream=stream, **req.kwargs)
+        s = Sim3D(req.nx, req.ny, req.nz, s0=req.s0, stream=stream, **req.kwargs)
+        if req.body is not None:
+            s.attach_sphere(**req.body)
+        return s
     s = Sim(req.nx, req.nz, s0=req.s0, stream=stream, **req.kwargs)
     if req.body is not None:
         s.attach_ellipse(**req.body)
@@ -442,6 +445,8 @@ class Server:
                 shape = (r.nz, r.ny, r.nx)
                 r.result = {k: a[i * r.cells:(i + 1) * r.cells].reshape(shape).copy()
                             for i, k in enumerate(("S", "ux", "uy", "uz"))}
+                if r.body is not None:
+                    r.result["body"] = r.sim.body()
             else:
                 planes = {"S": 0, "ux": 1, "uz": 2, "p": 3}
                 r.result = {k: a[planes[k] * r.cells:(planes[k] + 1) * r.cells].reshape(r.nz, r.nx).copy()
@@ -557,14 +562,22 @@ def rayleigh_taylor_request(rid, nx, nz, steps, arrival=0.0, storage="f16", seed
     return Request(arrival=arrival, rid=rid, nx=nx, nz=nz, steps=steps, kwargs=kw, s0=phi0.ravel())
 
 
-def stratified_box_request(rid, nx, ny, nz, steps, arrival=0.0, seed=0):
-    """A 3-D request after the sphere configuration's fluid: D3Q19 MRT +
-    D3Q7 salinity with a linear stratification S = 1 - z/H (seeded 1e-4
-    noise), Boussinesq g' = 1e-5, rho = 1 + 1e-3 S, tau = 0.55, tau_s =
+def stratified_box_request(rid, nx, ny, nz, steps, arrival=0.0, seed=0, sphere=True):
+    """A 3-D falling-sphere request after the sphere configuration: D3Q19
+    MRT + D3Q7 salinity with a linear stratification S = 1 - z/H (seeded
+    1e-4 noise), Boussinesq g' = 1e-5, rho = 1 + 1e-3 S, tau = 0.55, tau_s =
     0.52, bounce-back walls, uniform grid, FP32 storage (the 3-D path has no
-    16-bit storage) and no immersed body (the 3-D path has none)."""
+    16-bit storage), and a sphere of diameter nx/8 (radius at least 4 cells)
+    with markers at about one per unit area, density ratio 1.5, released from
+    rest at 0.8 of the height with a seeded lateral offset of at most one
+    cell, gravity 2e-5 (sphere=False: the stratified box alone)."""
     rng = np.random.default_rng(seed)
     zz = np.broadcast_to((np.arange(nz) + 0.5)[:, None, None] / nz, (nz, ny, nx))
     S0 = 1.0 - zz + 1e-4 * rng.uniform(-1, 1, (nz, ny, nx))
     kw = dict(tau=0.55, taus=0.52, rho_sal=1e-3, g_bouss=1e-5)
-    return Request(arrival=arrival, rid=rid, nx=nx, nz=nz, ny=ny, steps=steps, kwargs=kw, s0=S0.ravel())
+    body = None
+    if sphere:
+        off = rng.uniform(-1.0, 1.0, 2)
+        body = dict(xc=nx / 2 + off[0], yc=ny / 2 + off[1], zc=0.8 * nz, radius=max(nx / 16.0, 4.0), rho_s=1.5,
+                    rho_f=1.0, gravity=2e-5, iters=3)
+    return Request(arrival=arrival, rid=rid, nx=nx, nz=nz, ny=ny, steps=steps, kwargs=kw, s0=S0.ravel(), body=body)

@@ -148,3 +148,21 @@ def clustered_box_3d(nx=160, ny=160, nz=640, ratio=3.0, seed=20261203):
     S0 = 1.0 - zz + 1e-4 * rng.uniform(-1, 1, (nz, ny, nx))
     kw = dict(tau=0.55, taus=0.52, rho_sal=1e-3, g_bouss=1e-5, x=x, wx=wx, y=y, wy=wy, ns=3)
     return kw, S0
+
+
+def falling_sphere_3d(kw, nx, ny, nz, seed=20261203, gravity=2e-5):
+    """The 3-D configuration's falling sphere for a box built by
+    clustered_box_3d (kw: its keyword arguments): diameter 16 finest cells
+    (radius 8 in the finest spacing), about 800 markers on a Fibonacci
+    lattice, density ratio 1.5, released from rest at 0.8 of the height on
+    the centreline with a seeded lateral offset of at most one cell, lattice
+    gravity 2e-5 (one value of the sweep). Returns Sim3D.attach_sphere
+    keyword arguments."""
+    rng = np.random.default_rng(seed)
+    x = kw.get("x", np.arange(nx) + 0.5)
+    y = kw.get("y", np.arange(ny) + 0.5)
+    off = rng.uniform(-1.0, 1.0, 2)
+    xc = 0.5 * (x[nx // 2 - 1] + x[nx // 2]) + off[0]
+    yc = 0.5 * (y[ny // 2 - 1] + y[ny // 2]) + off[1]
+    return dict(xc=float(xc), yc=float(yc), zc=0.8 * nz, radius=8.0, markers=804, rho_s=1.5, rho_f=1.0,
+                gravity=gravity, iters=3)

@@ -214,13 +214,15 @@ def test_autotuned_grid_keeps_results(cuda):
 
 
 def test_3d_requests_in_the_mix(cuda):
-    """3-D requests are admitted beside 2-D ones and replay their step graphs
-    on their own streams; each result is the 3-D simulation's own."""
+    """3-D requests (stratified boxes with a falling sphere, one without)
+    are admitted beside 2-D ones and replay their step graphs on their own
+    streams; each result -- fields and sphere -- is the 3-D simulation's
+    own."""
     from ip_cu_lbm_b200.serving import make_sim, stratified_box_request
 
     reqs = [stratified_box_request(0, 64, 48, 80, 50, seed=0),
             lock_exchange_request(1, 96, 64, 70, storage="f16", seed=1),
-            stratified_box_request(2, 32, 32, 64, 31, arrival=0.01, seed=2)]
+            stratified_box_request(2, 32, 32, 64, 31, arrival=0.01, seed=2, sphere=False)]
     srv = Server(budget_bytes=2e9, tick_steps=20)
     stats = srv.run(reqs)
     srv.close()
@@ -232,6 +234,10 @@ def test_3d_requests_in_the_mix(cuda):
         s.step(r.steps)
         for k in ("S", "ux", "uy", "uz"):
             assert np.array_equal(r.result[k], s.get(k).astype(np.float32)), (r.rid, k)
+        if r.body is not None:
+            b = s.body()
+            assert all(np.array_equal(r.result["body"][k], b[k]) for k in b)
+            assert b["U"][2] < 0  # the sphere sinks
         s.close()
 
 
