@@ -85,7 +85,7 @@ int ipcu_sim3d_save(ipcu_sim3d *sim, const char *path);
 int ipcu_sim3d_load(const char *path, ipcu_stream_t stream, ipcu_sim3d **out);
 /* Moving rigid sphere (one per simulation; the sphere of the reference's
  * SphereFallSuzuki2018 driver): markers on its surface (body frame, [n][3],
- * n <= 4096) carry areas dA; each step, after the fluid step, multi-direct
+ * n <= 1024) carry areas dA; each step, after the fluid step, multi-direct
  * forcing with the reference's 4-point Peskin kernel per axis (ref:
  * function/ibm.cu:61-66 weightFunction; on stretched x and y axes the kernel
  * is evaluated in cell-index space) makes the fluid follow the body at the

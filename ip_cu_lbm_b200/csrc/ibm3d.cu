@@ -25,7 +25,9 @@
 //      advances by the mean angular velocity (Rodrigues), the markers follow
 //      (ref: update_IBpoint, ibm.cu:426-447).
 // One CTA: the phases synchronise with block barriers; nothing waits on
-// another kernel.
+// another kernel. The marker arrays and the window's pair counts and offsets
+// live in shared memory (100 B per marker, 8 B per window cell); the
+// window's velocities and force sums and the pair lists in global scratch.
 #include <cuda_runtime.h>
 
 #include <climits>
@@ -85,7 +87,12 @@ __device__ void block_sum12(double (&v)[12], double *red) {
   for (int a = 0; a < 12; a++) v[a] = red[kWarps * 12 + a];
 }
 
+// dynamic shared memory of the update: the 227 KB a block may hold, less
+// room for its static shared memory (body state, reductions)
+constexpr size_t kSmem = 227 * 1024 - 4096;
+
 __global__ void __launch_bounds__(kThreads, 1) ib3d_kernel(const __grid_constant__ Job j) {
+  extern __shared__ __align__(16) unsigned char dsm[];
   __shared__ Body B;
   __shared__ int bnd[6], bnew[6], s_fail;
   __shared__ int wtot[kWarps];
@@ -94,6 +101,13 @@ __global__ void __launch_bounds__(kThreads, 1) ib3d_kernel(const __grid_constant
   const int nx = j.nx, ny = j.ny, nz = j.nz, nl = j.nl;
   const long long P = (long long)nx * ny, N = P * nz;
   const double dz = j.dz;
+  // shared memory: marker arrays, then the window's counts and offsets
+  float *sw = reinterpret_cast<float *>(dsm);  // [nl][12] weights
+  int *sorg = reinterpret_cast<int *>(sw + 12 * nl);  // [nl][3]
+  float *sub = reinterpret_cast<float *>(sorg + 3 * nl), *sft = sub + 3 * nl, *sdf = sft + 3 * nl;
+  float *sdA = sdf + 3 * nl;  // [nl]
+  int *soff = reinterpret_cast<int *>(sdA + nl);  // [W + 1]
+  const long long wcap = ((long long)kSmem - 100LL * nl) / 8 - 1;  // window cells that fit
   if (tid == 0) {
     B = *j.body;
     for (int a = 0; a < 3; a++) {
@@ -117,19 +131,20 @@ __global__ void __launch_bounds__(kThreads, 1) ib3d_kernel(const __grid_constant
     const double X = B.X[0] + rx, Y = B.X[1] + ry, Z = B.X[2] + rz;
     const double sx = index_coord(j.xc, nx, X), sy = index_coord(j.yc, ny, Y), sz = Z / dz - 0.5;
     const int i0 = (int)floor(sx) - 1, j0 = (int)floor(sy) - 1, k0 = (int)floor(sz) - 1;
-    j.morg[3 * l] = i0;
-    j.morg[3 * l + 1] = j0;
-    j.morg[3 * l + 2] = k0;
+    sorg[3 * l] = i0;
+    sorg[3 * l + 1] = j0;
+    sorg[3 * l + 2] = k0;
 #pragma unroll
     for (int a = 0; a < 4; a++) {
-      j.mw[12 * l + a] = peskin4((float)((double)(i0 + a) - sx));
-      j.mw[12 * l + 4 + a] = peskin4((float)((double)(j0 + a) - sy));
-      j.mw[12 * l + 8 + a] = peskin4((float)((double)(k0 + a) - sz));
+      sw[12 * l + a] = peskin4((float)((double)(i0 + a) - sx));
+      sw[12 * l + 4 + a] = peskin4((float)((double)(j0 + a) - sy));
+      sw[12 * l + 8 + a] = peskin4((float)((double)(k0 + a) - sz));
     }
-    j.mub[3 * l] = (float)(B.U[0] + (B.om[1] * rz - B.om[2] * ry));
-    j.mub[3 * l + 1] = (float)(B.U[1] + (B.om[2] * rx - B.om[0] * rz));
-    j.mub[3 * l + 2] = (float)(B.U[2] + (B.om[0] * ry - B.om[1] * rx));
-    j.mft[3 * l] = j.mft[3 * l + 1] = j.mft[3 * l + 2] = 0.f;
+    sub[3 * l] = (float)(B.U[0] + (B.om[1] * rz - B.om[2] * ry));
+    sub[3 * l + 1] = (float)(B.U[1] + (B.om[2] * rx - B.om[0] * rz));
+    sub[3 * l + 2] = (float)(B.U[2] + (B.om[0] * ry - B.om[1] * rx));
+    sft[3 * l] = sft[3 * l + 1] = sft[3 * l + 2] = 0.f;
+    sdA[l] = (float)j.dA[l];
     atomicMin(&bnew[0], i0);
     atomicMax(&bnew[1], i0 + 3);
     atomicMin(&bnew[2], j0);
@@ -156,7 +171,7 @@ __global__ void __launch_bounds__(kThreads, 1) ib3d_kernel(const __grid_constant
     bnd[4] = max(bnd[4], 0);
     bnd[5] = min(bnd[5], nz - 1);
     const long long W = (long long)(bnd[1] - bnd[0] + 1) * (bnd[3] - bnd[2] + 1) * (bnd[5] - bnd[4] + 1);
-    s_fail = (bnd[1] < bnd[0] || bnd[3] < bnd[2] || bnd[5] < bnd[4] || W > kMaxWin) ? 1 : 0;
+    s_fail = (bnd[1] < bnd[0] || bnd[3] < bnd[2] || bnd[5] < bnd[4] || W > kMaxWin || W > wcap) ? 1 : 0;
   }
   __syncthreads();
   if (s_fail) {
@@ -197,29 +212,28 @@ __global__ void __launch_bounds__(kThreads, 1) ib3d_kernel(const __grid_constant
     const int k = cw / (WX * WY), r = cw - k * (WX * WY), jj = r / WX, i = r - jj * WX;
     j.wh[cw] = h;
     j.wv[cw] = j.wx[wi0 + i] * j.wy[wj0 + jj] * (float)dz;
-    j.cnt[cw] = 0;
-    j.cur[cw] = 0;
+    soff[cw] = 0;
   }
   __syncthreads();
 
   // ---- 3. pairs: count per window cell, scan, list in pair order
   auto pair_cell = [&](int e) -> int {  // window index of pair e = 64 l + node, or -1 outside the box
     const int l = e >> 6, a = e & 63;
-    const int i = j.morg[3 * l] + (a & 3), jj = j.morg[3 * l + 1] + ((a >> 2) & 3), k = j.morg[3 * l + 2] + (a >> 4);
+    const int i = sorg[3 * l] + (a & 3), jj = sorg[3 * l + 1] + ((a >> 2) & 3), k = sorg[3 * l + 2] + (a >> 4);
     if (i < 0 || i >= nx || jj < 0 || jj >= ny || k < 0 || k >= nz) return -1;
     return ((k - wk0) * WY + (jj - wj0)) * WX + (i - wi0);
   };
   for (int e = tid; e < 64 * nl; e += kThreads) {
     const int cw = pair_cell(e);
-    if (cw >= 0) atomicAdd(&j.cnt[cw], 1);
+    if (cw >= 0) atomicAdd(&soff[cw], 1);
   }
   __syncthreads();
   {
-    // exclusive scan of cnt[0..W): consecutive chunks per thread, then across
-    // lanes and warps
+    // exclusive scan of the counts in place: consecutive chunks per thread,
+    // then across lanes and warps (the fill cursors start from the offsets)
     const int per = (W + kThreads - 1) / kThreads, b0 = tid * per, b1 = min(b0 + per, W);
     int sum = 0;
-    for (int q = b0; q < b1; q++) sum += j.cnt[q];
+    for (int q = b0; q < b1; q++) sum += soff[q];
     int x = sum;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
@@ -235,23 +249,25 @@ __global__ void __launch_bounds__(kThreads, 1) ib3d_kernel(const __grid_constant
         wtot[w] = run;
         run += t;
       }
-      j.off[W] = run;
+      soff[W] = run;
     }
     __syncthreads();
     int base = wtot[warp] + x - sum;
     for (int q = b0; q < b1; q++) {
-      j.off[q] = base;
-      base += j.cnt[q];
+      const int cq = soff[q];
+      soff[q] = base;
+      j.cur[q] = base;
+      base += cq;
     }
   }
   __syncthreads();
   for (int e = tid; e < 64 * nl; e += kThreads) {
     const int cw = pair_cell(e);
-    if (cw >= 0) j.list[j.off[cw] + atomicAdd(&j.cur[cw], 1)] = e;
+    if (cw >= 0) j.list[atomicAdd(&j.cur[cw], 1)] = e;
   }
   __syncthreads();
   for (int cw = tid; cw < W; cw += kThreads) {  // insertion sort of each cell's short list
-    const int a0 = j.off[cw], a1 = j.off[cw + 1];
+    const int a0 = soff[cw], a1 = soff[cw + 1];
     for (int a = a0 + 1; a < a1; a++) {
       const int v = j.list[a];
       int b2 = a - 1;
@@ -267,7 +283,7 @@ __global__ void __launch_bounds__(kThreads, 1) ib3d_kernel(const __grid_constant
   // ---- 4. multi-direct forcing
   const float two_rf_dt = (float)(2.0 * j.rho_f / j.dt);
   auto node_w = [&](int l, int a) {
-    return j.mw[12 * l + (a & 3)] * j.mw[12 * l + 4 + ((a >> 2) & 3)] * j.mw[12 * l + 8 + (a >> 4)];
+    return sw[12 * l + (a & 3)] * sw[12 * l + 4 + ((a >> 2) & 3)] * sw[12 * l + 8 + (a >> 4)];
   };
   for (int it = 0; it < j.iters; it++) {
     for (int l = tid; l < nl; l += kThreads) {
@@ -281,22 +297,22 @@ __global__ void __launch_bounds__(kThreads, 1) ib3d_kernel(const __grid_constant
       }
 #pragma unroll
       for (int q = 0; q < 3; q++) {
-        const float d = two_rf_dt * (j.mub[3 * l + q] - v[q]);
-        j.mdf[3 * l + q] = d;
-        j.mft[3 * l + q] += d;
+        const float d = two_rf_dt * (sub[3 * l + q] - v[q]);
+        sdf[3 * l + q] = d;
+        sft[3 * l + q] += d;
       }
     }
     __syncthreads();
     for (int cw = tid; cw < W; cw += kThreads) {
-      const int a0 = j.off[cw], a1 = j.off[cw + 1];
+      const int a0 = soff[cw], a1 = soff[cw + 1];
       if (a0 == a1) continue;
       float fx = 0.f, fy = 0.f, fz = 0.f;
       for (int a = a0; a < a1; a++) {
         const int e = j.list[a], l = e >> 6;
-        const float wd = node_w(l, e & 63) * (float)j.dA[l];
-        fx = fmaf(j.mdf[3 * l], wd, fx);
-        fy = fmaf(j.mdf[3 * l + 1], wd, fy);
-        fz = fmaf(j.mdf[3 * l + 2], wd, fz);
+        const float wd = node_w(l, e & 63) * sdA[l];
+        fx = fmaf(sdf[3 * l], wd, fx);
+        fy = fmaf(sdf[3 * l + 1], wd, fy);
+        fz = fmaf(sdf[3 * l + 2], wd, fz);
       }
       const float iv = 1.0f / j.wv[cw], h = j.wh[cw];
       fx *= iv;
@@ -336,8 +352,8 @@ __global__ void __launch_bounds__(kThreads, 1) ib3d_kernel(const __grid_constant
     const double rx = B.R[0] * r0x + B.R[1] * r0y + B.R[2] * r0z;
     const double ry = B.R[3] * r0x + B.R[4] * r0y + B.R[5] * r0z;
     const double rz = B.R[6] * r0x + B.R[7] * r0y + B.R[8] * r0z;
-    const double fx = (double)j.mft[3 * l] * j.dA[l], fy = (double)j.mft[3 * l + 1] * j.dA[l],
-                 fz = (double)j.mft[3 * l + 2] * j.dA[l];
+    const double fx = (double)sft[3 * l] * j.dA[l], fy = (double)sft[3 * l + 1] * j.dA[l],
+                 fz = (double)sft[3 * l + 2] * j.dA[l];
     acc[0] += fx;
     acc[1] += fy;
     acc[2] += fz;
@@ -422,10 +438,12 @@ __global__ void __launch_bounds__(kThreads, 1) ib3d_kernel(const __grid_constant
 
 }  // namespace
 
-int prepare() { return IPCU_OK; }
+int prepare() {
+  return status_from_cuda(cudaFuncSetAttribute(ib3d_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmem));
+}
 
 int launch(const Job &j, cudaStream_t s) {
-  ib3d_kernel<<<1, kThreads, 0, s>>>(j);
+  ib3d_kernel<<<1, kThreads, kSmem, s>>>(j);
   return status_from_cuda(cudaGetLastError());
 }
 

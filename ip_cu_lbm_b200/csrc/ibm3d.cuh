@@ -12,7 +12,7 @@ namespace ipcu {
 namespace ib3d {
 
 constexpr int kThreads = 1024;
-constexpr int kMaxMarkers = 4096;
+constexpr int kMaxMarkers = 1024;  // the marker arrays live in shared memory (100 B each)
 constexpr int kMaxWin = 65536;  // cells of the window box (old and new footprints)
 
 // Device-resident FP64 body state.
@@ -42,11 +42,9 @@ struct Job {
   const double *dA;  // [nl] area per marker
   int nl, iters;
   double m, I, rho_s, rho_f, grav, radius;
-  // scratch: markers (origins, weights, velocities, forces) and the window
-  int *morg;           // [nl][3]
-  float *mw;           // [nl][12] weights along x, y, z
-  float *mub, *mft, *mdf;  // [nl][3] body velocity at the marker, summed force, this iteration's force
-  int *cnt, *off, *cur;    // [kMaxWin + 1] pairs per window cell, their offsets, fill cursors
+  // global scratch of the window (the marker arrays and the pair offsets
+  // are in the kernel's shared memory)
+  int *cur;                // [kMaxWin + 1] fill cursors of the pair lists
   int *list;               // [64 nl] pairs (64 marker + node) by window cell
   float *wu, *wf, *wj;     // [3][kMaxWin] velocity u*, accumulated force density, momentum c j per window cell
   float *wh, *wv;          // [kMaxWin] dt / 2 rho and cell volume

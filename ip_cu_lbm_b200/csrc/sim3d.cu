@@ -527,6 +527,15 @@ extern "C" int ipcu_sim3d_ib_attach(ipcu_sim3d *s, const ipcu_ib_sphere3d *bd, c
     if (!std::isfinite(markers[i])) return IPCU_ERR_ARG;
   for (int i = 0; i < n; i++)
     if (!(dA[i] > 0)) return IPCU_ERR_ARG;
+  {
+    static bool prepared[64] = {false};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return IPCU_ERR_CUDA;
+    if (!prepared[dev]) {
+      if (int st = ib3d::prepare()) return st;
+      prepared[dev] = true;
+    }
+  }
   const ipcu_sim3d_config &c = s->cfg;
   const long long N = s->N;
   const size_t W = ib3d::kMaxWin;
@@ -540,9 +549,7 @@ extern "C" int ipcu_sim3d_ib_attach(ipcu_sim3d *s, const ipcu_ib_sphere3d *bd, c
   const size_t o_body = take(sizeof(ib3d::Body)), o_r0 = take(sizeof(double) * 3 * n), o_dA = take(sizeof(double) * n);
   const size_t o_xc = take(sizeof(double) * c.nx), o_yc = take(sizeof(double) * c.ny);
   const size_t o_wx = take(sizeof(float) * c.nx), o_wy = take(sizeof(float) * c.ny);
-  const size_t o_morg = take(sizeof(int) * 3 * n), o_mw = take(sizeof(float) * 12 * n);
-  const size_t o_mub = take(sizeof(float) * 3 * n), o_mft = take(sizeof(float) * 3 * n), o_mdf = take(sizeof(float) * 3 * n);
-  const size_t o_cnt = take(sizeof(int) * (W + 1)), o_off = take(sizeof(int) * (W + 1)), o_cur = take(sizeof(int) * (W + 1));
+  const size_t o_cur = take(sizeof(int) * (W + 1));
   const size_t o_list = take(sizeof(int) * 64 * (size_t)n);
   const size_t o_wu = take(sizeof(float) * 3 * W), o_wf = take(sizeof(float) * 3 * W), o_wj = take(sizeof(float) * 3 * W);
   const size_t o_wh = take(sizeof(float) * W), o_wv = take(sizeof(float) * W);
@@ -568,13 +575,6 @@ extern "C" int ipcu_sim3d_ib_attach(ipcu_sim3d *s, const ipcu_ib_sphere3d *bd, c
   j->yc = reinterpret_cast<const double *>(mem + o_yc);
   j->wx = reinterpret_cast<const float *>(mem + o_wx);
   j->wy = reinterpret_cast<const float *>(mem + o_wy);
-  j->morg = reinterpret_cast<int *>(mem + o_morg);
-  j->mw = reinterpret_cast<float *>(mem + o_mw);
-  j->mub = reinterpret_cast<float *>(mem + o_mub);
-  j->mft = reinterpret_cast<float *>(mem + o_mft);
-  j->mdf = reinterpret_cast<float *>(mem + o_mdf);
-  j->cnt = reinterpret_cast<int *>(mem + o_cnt);
-  j->off = reinterpret_cast<int *>(mem + o_off);
   j->cur = reinterpret_cast<int *>(mem + o_cur);
   j->list = reinterpret_cast<int *>(mem + o_list);
   j->wu = reinterpret_cast<float *>(mem + o_wu);
