@@ -76,6 +76,12 @@ __global__ void __launch_bounds__(kThreads, 4) step3d_kernel(const __grid_consta
   const int zb = blockIdx.z * p.zchunk, ze = min(zb + p.zchunk, nz);
   const int x = x0 + tx, y = y0 + ty;
   const bool own = x < nx && y < ny;
+  // the immersed-boundary force density is read only inside its box
+  int fb[6] = {0, 0, 0, 0, 0, 0};
+  if (p.fext != nullptr)
+#pragma unroll
+    for (int a = 0; a < 6; a++) fb[a] = p.fext_box[a];
+  const bool fcol = fb[3] > 0 && x >= fb[0] && x < fb[0] + fb[3] && y >= fb[1] && y < fb[1] + fb[4];
 
   // S of plane z (clamped into the box) for the ring slot z mod 3
   auto form_plane = [&](int z) {
@@ -134,7 +140,7 @@ __global__ void __launch_bounds__(kThreads, 4) step3d_kernel(const __grid_consta
       float Fy = -pc * ((rs(sS[s0][y + 1 < ny ? ly + 1 : ly][lx]) - rs(sS[s0][y > 0 ? ly - 1 : ly][lx])) * gy);
       float Fz =
           fmaf(-S, p.gb, -(pc * ((rs(sS[z + 1 < nz ? sp : s0][ly][lx]) - rs(sS[z > 0 ? sm : s0][ly][lx])) * gz)));
-      if (p.fext != nullptr) {  // immersed-boundary force density of the last body update
+      if (fcol && z >= fb[2] && z < fb[2] + fb[5]) {  // immersed-boundary force density of the last body update
         Fx += p.fext[i];
         Fy += p.fext[N + i];
         Fz += p.fext[2 * N + i];

@@ -18,6 +18,9 @@ struct Params3 {
   int mrt;
   unsigned *status;
   const float *fext;  // [3][N] immersed-boundary force density added to the force, or null
+  // the box outside which that density is zero (i0, j0, k0, wi, wj, wk; wi 0:
+  // none), device memory the body update rewrites
+  const int *fext_box;
 };
 
 int launch3d(const Params3 &p, cudaStream_t s);

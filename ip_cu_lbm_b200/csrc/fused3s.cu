@@ -89,7 +89,7 @@ __device__ __forceinline__ int pofs(int k, bool isg, int plane) {
 __device__ __forceinline__ bool collide_cell(const Params3S &p, long long i, long long N, int gx, int gy, float S,
                                              float Sxm, float Sxp, float Sym, float Syp, float Szm, float Szp,
                                              float gz, float (&fo)[19], float (&go)[7], float &Fx, float &Fy,
-                                             float &Fz) {
+                                             float &Fz, bool ext) {
   const float c = p.c, ic = 1.0f / c, c2 = c * c;
   float f[19], g[7];
 #pragma unroll
@@ -114,7 +114,7 @@ __device__ __forceinline__ bool collide_cell(const Params3S &p, long long i, lon
   Fx = -pc * ((rs(Sxp) - rs(Sxm)) * __ldg(p.ax.ginv + gx));
   Fy = -pc * ((rs(Syp) - rs(Sym)) * __ldg(p.ay.ginv + gy));
   Fz = fmaf(-S, p.gb, -(pc * ((rs(Szp) - rs(Szm)) * gz)));
-  if (p.fext != nullptr) {  // immersed-boundary force density of the last body update
+  if (ext) {  // immersed-boundary force density of the last body update (inside its box)
     Fx += p.fext[i];
     Fy += p.fext[N + i];
     Fz += p.fext[2 * N + i];
@@ -282,6 +282,12 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) step3s_kernel(const __gr
   auto clx = [&](int v) { return min(max(v, 0), nx - 1); };
   auto cly = [&](int v) { return min(max(v, 0), ny - 1); };
 
+  // the immersed-boundary force density is read only inside its box
+  int fb[6] = {0, 0, 0, 0, 0, 0};
+  if (p.fext != nullptr)
+#pragma unroll
+    for (int a = 0; a < 6; a++) fb[a] = p.fext_box[a];
+
   // salinity S = sum g of plane q (clamped into the box), region + 1 cell
   auto form_S = [&](int q) {
     const int qz = min(max(q, 0), nz - 1);
@@ -310,8 +316,10 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) step3s_kernel(const __gr
       const int se = (ly + 1) * SX + lx + 1;  // ring slot of the cell
       const float S = Sq[se];
       float fo[19], go[7], Fx, Fy, Fz;
+      const bool ext = fb[3] > 0 && gx >= fb[0] && gx < fb[0] + fb[3] && gy >= fb[1] && gy < fb[1] + fb[4] &&
+                       q >= fb[2] && q < fb[2] + fb[5];
       const bool bad = collide_cell(p, i, N, gx, gy, S, Sq[se - 1], Sq[se + 1], Sq[se - SX], Sq[se + SX],
-                                    q > 0 ? Sm[se] : S, q + 1 < nz ? Sp[se] : S, gz, fo, go, Fx, Fy, Fz);
+                                    q > 0 ? Sm[se] : S, q + 1 < nz ? Sp[se] : S, gz, fo, go, Fx, Fy, Fz, ext);
       const int le = ly * RX + lx;
 #pragma unroll
       for (int k = 0; k < 19; k++) sm[pofs<NS>(k, false, q) + le] = fo[k];

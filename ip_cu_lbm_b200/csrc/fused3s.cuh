@@ -32,6 +32,9 @@ struct Params3S {
   int mrt;
   unsigned *status;
   const float *fext;  // [3][N] immersed-boundary force density added to the force, or null
+  // the box outside which that density is zero (i0, j0, k0, wi, wj, wk; wi 0:
+  // none), device memory the body update rewrites
+  const int *fext_box;
 };
 
 // ns: 3 (quadratic upwind) or 5 (the reference's stencil)

@@ -11,9 +11,12 @@
 namespace ipcu {
 namespace ib3d {
 
-constexpr int kThreads = 1024;
-constexpr int kMaxMarkers = 1024;  // the marker arrays live in shared memory (100 B each)
-constexpr int kMaxWin = 65536;  // cells of the window box (old and new footprints)
+constexpr int kThreads = 1024;    // the set-up and the final body step (one CTA each)
+constexpr int kMaxMarkers = 1024;
+constexpr int kMaxWin = 65536;    // cells of the window box (old and new footprints)
+constexpr int kSlots = 64;        // (marker, node) contributions a window cell may hold
+constexpr int kMaxBins = 32768;   // stencil-origin bins
+constexpr int kParts = 256;       // CTAs of the partial FP64 sums
 
 // Device-resident FP64 body state.
 struct Body {
@@ -21,8 +24,17 @@ struct Body {
   double R[9];               // orientation (body frame -> lab), row major
   double P[3], L[3];         // fluid momentum and angular momentum inside the body, previous step
   double Fib[3], Tib[3];     // force and torque the markers put on the fluid, previous step
-  int win[6];                // window box of the last update (i0, j0, k0, wi, wj, wk); wi = 0: none
+  int win[6];                // cells holding the IB force (i0, j0, k0, wi, wj, wk); wi = 0: none
   int have_prev;
+  int pad;
+};
+
+// The current update's geometry, written by its set-up kernel and read by
+// the rest: window box, stencil-origin bin box, and whether to go on.
+struct Plan {
+  int win[6];        // i0, j0, k0, WX, WY, WZ
+  int olo[3], on[3]; // first stencil origin and bins per axis
+  int W, NB, ok;
   int pad;
 };
 
@@ -42,12 +54,17 @@ struct Job {
   const double *dA;  // [nl] area per marker
   int nl, iters;
   double m, I, rho_s, rho_f, grav, radius;
-  // global scratch of the window (the marker arrays and the pair offsets
-  // are in the kernel's shared memory)
-  int *cur;                // [kMaxWin + 1] fill cursors of the pair lists
-  int *list;               // [64 nl] pairs (64 marker + node) by window cell
+  // global scratch (L2-resident)
+  Plan *plan;
+  int *morg;               // [nl][3] stencil origins
+  float *mw;               // [nl][12] Peskin weights along x, y, z
+  float *mub, *mft, *mdf;  // [nl][3] body velocity at the marker, summed force, this iteration's force
+  int *bstart, *blist;     // [kMaxBins + 1], [nl] markers by stencil-origin bin, in index order
   float *wu, *wf, *wj;     // [3][kMaxWin] velocity u*, accumulated force density, momentum c j per window cell
   float *wh, *wv;          // [kMaxWin] dt / 2 rho and cell volume
+  int *ccnt;               // [kMaxWin] contributions per window cell
+  int *clist;              // [kMaxWin][kSlots] its contributions (marker << 6 | node)
+  double *part;            // [kParts][12] partial FP64 sums
   unsigned *status;
 };
 

@@ -549,10 +549,13 @@ extern "C" int ipcu_sim3d_ib_attach(ipcu_sim3d *s, const ipcu_ib_sphere3d *bd, c
   const size_t o_body = take(sizeof(ib3d::Body)), o_r0 = take(sizeof(double) * 3 * n), o_dA = take(sizeof(double) * n);
   const size_t o_xc = take(sizeof(double) * c.nx), o_yc = take(sizeof(double) * c.ny);
   const size_t o_wx = take(sizeof(float) * c.nx), o_wy = take(sizeof(float) * c.ny);
-  const size_t o_cur = take(sizeof(int) * (W + 1));
-  const size_t o_list = take(sizeof(int) * 64 * (size_t)n);
+  const size_t o_plan = take(sizeof(ib3d::Plan)), o_morg = take(sizeof(int) * 3 * n), o_mw = take(sizeof(float) * 12 * n);
+  const size_t o_mub = take(sizeof(float) * 3 * n), o_mft = take(sizeof(float) * 3 * n), o_mdf = take(sizeof(float) * 3 * n);
+  const size_t o_bstart = take(sizeof(int) * (ib3d::kMaxBins + 1)), o_blist = take(sizeof(int) * n);
+  const size_t o_part = take(sizeof(double) * 12 * ib3d::kParts);
   const size_t o_wu = take(sizeof(float) * 3 * W), o_wf = take(sizeof(float) * 3 * W), o_wj = take(sizeof(float) * 3 * W);
   const size_t o_wh = take(sizeof(float) * W), o_wv = take(sizeof(float) * W);
+  const size_t o_ccnt = take(sizeof(int) * W), o_clist = take(sizeof(int) * W * ib3d::kSlots);
   const size_t o_fext = take(sizeof(float) * 3 * (size_t)N);
   char *mem = nullptr;
   if (cudaStreamSynchronize(s->stream) != cudaSuccess) return IPCU_ERR_CUDA;
@@ -575,13 +578,22 @@ extern "C" int ipcu_sim3d_ib_attach(ipcu_sim3d *s, const ipcu_ib_sphere3d *bd, c
   j->yc = reinterpret_cast<const double *>(mem + o_yc);
   j->wx = reinterpret_cast<const float *>(mem + o_wx);
   j->wy = reinterpret_cast<const float *>(mem + o_wy);
-  j->cur = reinterpret_cast<int *>(mem + o_cur);
-  j->list = reinterpret_cast<int *>(mem + o_list);
+  j->plan = reinterpret_cast<ib3d::Plan *>(mem + o_plan);
+  j->morg = reinterpret_cast<int *>(mem + o_morg);
+  j->mw = reinterpret_cast<float *>(mem + o_mw);
+  j->mub = reinterpret_cast<float *>(mem + o_mub);
+  j->mft = reinterpret_cast<float *>(mem + o_mft);
+  j->mdf = reinterpret_cast<float *>(mem + o_mdf);
+  j->bstart = reinterpret_cast<int *>(mem + o_bstart);
+  j->blist = reinterpret_cast<int *>(mem + o_blist);
+  j->part = reinterpret_cast<double *>(mem + o_part);
   j->wu = reinterpret_cast<float *>(mem + o_wu);
   j->wf = reinterpret_cast<float *>(mem + o_wf);
   j->wj = reinterpret_cast<float *>(mem + o_wj);
   j->wh = reinterpret_cast<float *>(mem + o_wh);
   j->wv = reinterpret_cast<float *>(mem + o_wv);
+  j->ccnt = reinterpret_cast<int *>(mem + o_ccnt);
+  j->clist = reinterpret_cast<int *>(mem + o_clist);
   j->fext = reinterpret_cast<float *>(mem + o_fext);
   j->status = s->status;
   j->nl = n;
@@ -627,6 +639,7 @@ extern "C" int ipcu_sim3d_ib_attach(ipcu_sim3d *s, const ipcu_ib_sphere3d *bd, c
     }
   s->P.fext = j->fext;
   s->PS.fext = j->fext;
+  s->P.fext_box = s->PS.fext_box = j->body->win;
   s->ib = j;
   s->ib_mem = mem;
   return IPCU_OK;
