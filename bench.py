@@ -328,7 +328,8 @@ def run_3d(args):
     3.8 GB > L2), x and y tanh-clustered toward the centreline (spacing ratio
     3) with the 3-point conservative flux form, z uniform (--uniform3d: the
     uniform box), D3Q19 MRT + D3Q7 salinity with a linear stratification,
-    bounce-back, FP32, and the configuration's falling sphere (diameter 16
+    bounce-back, FP32 (--storage f16 / bf16: 16-bit population storage,
+    FP32 arithmetic), and the configuration's falling sphere (diameter 16
     finest cells, 804 markers, density ratio 1.5; --no-sphere leaves it
     out). A step is --inner LBM steps (default 20), each the fluid step and
     the sphere's update, replayed from a CUDA graph; the inputs are far
@@ -348,7 +349,7 @@ def run_3d(args):
     if args.uniform3d:
         for k in ("x", "wx", "y", "wy", "ns"):
             kw.pop(k)
-    sim = Sim3D(nx, ny, nz, s0=S0.ravel(), stream=stream.cuda_stream, **kw)
+    sim = Sim3D(nx, ny, nz, s0=S0.ravel(), stream=stream.cuda_stream, storage=args.storage, **kw)
     sphere = None if args.no_sphere else workloads.falling_sphere_3d(kw, nx, ny, nz)
     if sphere:
         sim.attach_sphere(**sphere)
@@ -373,10 +374,14 @@ def run_3d(args):
     bpc = sim.bytes_per_cell()
     peak, peak_src = load_peaks()
     achieved = N * bpc / (launch_ms / 1e3) / 1e9
-    # end to end: upload the state from pinned host memory, advance, read back the force and salinity planes
-    hf = torch.empty(19 * N, dtype=torch.float32, pin_memory=True)
-    hg = torch.empty(7 * N, dtype=torch.float32, pin_memory=True)
+    # end to end: upload the state from pinned host memory (16-bit storage:
+    # the force planes), advance, read back the salinity planes (16-bit: S
+    # and u, formed on the device)
+    f32 = args.storage == "f32"
+    hf = torch.empty(19 * N, dtype=torch.float32, pin_memory=True) if f32 else None
+    hg = torch.empty(7 * N, dtype=torch.float32, pin_memory=True) if f32 else None
     hF = torch.empty(3 * N, dtype=torch.float32, pin_memory=True)
+    hm = None if f32 else torch.empty(4 * N, dtype=torch.float32, pin_memory=True)
     sim.download(hf, hg, hF)
     sim.sync()
     R.barrier()
@@ -384,10 +389,15 @@ def run_3d(args):
     for _ in range(max(3, args.steps)):
         sim.upload(hf, hg, hF)
         sim.step_graph(inner)
-        sim.download(None, hg, None)
+        if f32:
+            sim.download(None, hg, None)
+        else:
+            sim.macro_async(hm)
         sim.sync()
     R.barrier()
     e2e = world * N * inner * max(3, args.steps) / R.max(time.perf_counter() - t0) / 1e6
+    h2d = 4 * (19 + 7 + 3) * N if f32 else 4 * 3 * N
+    d2h = 4 * 7 * N if f32 else 4 * 4 * N
     line = {
         "metric": METRIC, "value": round(value, 2), "unit": METRIC, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(total_ms / args.steps, 4), "higher_is_better": True,
@@ -399,16 +409,21 @@ def run_3d(args):
                                (f"; falling sphere, diameter 16 cells, 804 Fibonacci markers, density ratio 1.5, "
                                 f"multi-direct forcing x3, FP64 body update (released at z = {0.8 * nz:.0f})"
                                 if sphere else "; no body"),
-                   "lbm_steps_per_step": inner, "cells": N, "storage": "f32", "parallelism": f"replicas x{world}",
-                   "l2": f"inputs ({4 * 29 * N / 1e9:.2f} GB) larger than L2"},
+                   "lbm_steps_per_step": inner, "cells": N, "storage": args.storage,
+                   "parallelism": f"replicas x{world}",
+                   "l2": f"inputs ({bpc / 2 * N / 1e9:.2f} GB) larger than L2"},
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                     "frac": round(achieved / peak, 4), "traffic": traffic3d(N, not args.uniform3d), "bytes_per_cell": bpc,
+                     "frac": round(achieved / peak, 4),
+                     "traffic": traffic3d(N, not args.uniform3d) if f32 else None, "bytes_per_cell": bpc,
                      "peak_source": peak_label(peak_src),
                      "traffic_note": "DRAM read+write bytes per launch from the 128^3 ncu capture (profiles/traffic.json), "
                                      "scaled by cells; it grows in proportion to the cells streamed"},
         "e2e": {"value": round(e2e, 2), "unit": METRIC,
-                "h2d_bytes_per_step": int(4 * (19 + 7 + 3) * N), "d2h_bytes_per_step": int(4 * 7 * N)},
-        "gpu_launches": (2 if sphere else 1) * args.steps * inner, "clocks": clk.summary(),
+                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
+        # the fluid step, and the sphere's update: set-up, window, (interpolate, spread) per iteration,
+        # write-back, body step
+        "gpu_launches": (1 + (4 + 2 * sphere["iters"] if sphere else 0)) * args.steps * inner,
+        "clocks": clk.summary(),
     }
     if sphere:
         b = sim.body()

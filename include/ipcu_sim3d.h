@@ -18,6 +18,17 @@
  * resident in HBM. D3Q7 weights 1/4, 1/8 (cs^2 = 1/4), equilibrium
  * w_k S (1 + 4 e_k.u/c). The reference has no D3Q19/D3Q7 path: this mode
  * has no reference counterpart beyond the shared kernel rules.
+ *
+ * 16-bit storage (storage IPCU_STORE_F16 / IPCU_STORE_BF16; collision,
+ * streaming and forcing stay FP32): each cell keeps five reference values
+ * r [5][N] (p, u_x/c, u_y/c, u_z/c, S: what its collision formed in the step
+ * that wrote it) in the storage type, and its populations as deviations
+ * from the linear equilibria of that reference,
+ * f_k - w_k (p + 3 e_k.u) and g_k - w_k S (1 + 4 e_k.u), scaled by 2^12
+ * (FP16) or 1 (BF16): 148 B per cell and step against 232 B. Every box,
+ * uniform or stretched, runs the flux-form kernel (stencil 3 unless the
+ * axes say otherwise). Status bit 2: a stored magnitude beyond the format's
+ * range. Raw transfer (upload/download) of f and g is FP32-only.
  */
 #ifndef IPCU_SIM3D_H
 #define IPCU_SIM3D_H
@@ -30,6 +41,8 @@ typedef struct ipcu_sim3d_config {
   double tau, taus;     /* relaxation times of f and of the salinity */
   double rho0, rho_sal; /* rho = rho0 + rho_sal S */
   double g_bouss;       /* buoyancy -g_bouss S along z */
+  int32_t storage;      /* IPCU_STORE_* (16-bit: see below) */
+  int32_t pad;
 } ipcu_sim3d_config;
 
 typedef struct ipcu_sim3d ipcu_sim3d;
@@ -65,7 +78,8 @@ int ipcu_sim3d_step_graph(ipcu_sim3d *sim, int64_t nsteps);
 int ipcu_sim3d_get(ipcu_sim3d *sim, const char *field, double *out, int64_t n);
 /* Overwrites f (19 N), g (7 N), F (3 N) from host FP64 arrays (NULL keeps). */
 int ipcu_sim3d_set_state(ipcu_sim3d *sim, const double *f, const double *g, const double *F);
-/* Raw FP32 state transfer, asynchronous (pinned host buffers): f, g, F. */
+/* Raw FP32 state transfer, asynchronous (pinned host buffers): f, g, F.
+ * With 16-bit storage only F (IPCU_ERR_UNSUPPORTED for f or g). */
 int ipcu_sim3d_upload(ipcu_sim3d *sim, const float *f, const float *g, const float *F);
 int ipcu_sim3d_download(ipcu_sim3d *sim, float *f, float *g, float *F);
 /* S, u_x, u_y, u_z of every cell ([4][N] FP32, the values ipcu_sim3d_get
@@ -76,11 +90,12 @@ int ipcu_sim3d_sync(ipcu_sim3d *sim);
 /* Sticky error flags (bit 0: non-finite moment seen). Synchronises. */
 int ipcu_sim3d_status(ipcu_sim3d *sim, uint32_t *flags);
 int64_t ipcu_sim3d_cells(const ipcu_sim3d *sim);
-/* Algorithmic bytes per cell and step: f, g, F each read and written once. */
+/* Algorithmic bytes per cell and step: f, g, F (16-bit: and the reference
+ * planes) each read and written once. */
 int64_t ipcu_sim3d_bytes_per_cell(const ipcu_sim3d *sim);
 /* Versioned binary snapshot (configuration, axes, stencil, step count, raw
- * FP32 state) and its restore into a new simulation; a restored run
- * continues bit-identically. */
+ * state in its storage type) and its restore into a new simulation; a
+ * restored run continues bit-identically. */
 int ipcu_sim3d_save(ipcu_sim3d *sim, const char *path);
 int ipcu_sim3d_load(const char *path, ipcu_stream_t stream, ipcu_sim3d **out);
 /* Moving rigid sphere (one per simulation; the sphere of the reference's

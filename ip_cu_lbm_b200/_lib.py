@@ -105,6 +105,7 @@ class Sim3DConfig(ctypes.Structure):
         ("nx", ctypes.c_int32), ("ny", ctypes.c_int32), ("nz", ctypes.c_int32), ("mrt", ctypes.c_int32),
         ("dz", ctypes.c_double), ("dt", ctypes.c_double), ("tau", ctypes.c_double), ("taus", ctypes.c_double),
         ("rho0", ctypes.c_double), ("rho_sal", ctypes.c_double), ("g_bouss", ctypes.c_double),
+        ("storage", ctypes.c_int32), ("pad", ctypes.c_int32),
     ]
 
 

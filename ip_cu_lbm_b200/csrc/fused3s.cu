@@ -38,13 +38,14 @@
 #include "d3q19.cuh"
 #include "fused3s.cuh"
 #include "ipcu_common.cuh"
+#include "store3d.cuh"
 
 namespace ipcu {
 namespace f3s {
 
 using namespace d3;
 
-template <int NS>
+template <int NS, bool R16 = false>
 struct G {
   static constexpr int h = NS / 2;
   static constexpr int H = h + 1;  // halo: nodes of the stencils around the partners
@@ -56,7 +57,10 @@ struct G {
   static constexpr int S0 = DN0 + 2 * 6 * RC;                   // [3][SC]
   static constexpr int FR0 = S0 + 3 * SC;                       // [2][3][kTX * kTY] force of the tile cells
   static constexpr int Q0 = FR0 + 2 * 3 * kTX * kTY;            // wall-cell queue: count + kTX * kTY cells
-  static constexpr int NF = Q0 + 4 + kTX * kTY;
+  // 16-bit storage: [2][4][kTX * kTY] reference values (p, u/c) of the tile
+  // cells in the storage type, two to a slot
+  static constexpr int RF0 = Q0 + 4 + kTX * kTY;
+  static constexpr int NF = RF0 + (R16 ? 4 * kTX * kTY : 0);
   static constexpr size_t bytes = sizeof(float) * (size_t)NF;
 };
 
@@ -81,21 +85,36 @@ __device__ __forceinline__ int pofs(int k, bool isg, int plane) {
 }
 
 
+// salinity S = sum g of cell i, in the order of load_cell's values
+template <class T>
+__device__ __forceinline__ float cell_S(const Params3S &p, long long i, long long N) {
+  float S = 0.f;
+  if constexpr (std::is_same<T, float>::value) {
+    const float *gi = static_cast<const float *>(p.g_in);
+#pragma unroll
+    for (int k = 0; k < 7; k++) S += gi[k * N + i];
+  } else {
+    const T *gi = static_cast<const T *>(p.g_in), *ri = static_cast<const T *>(p.r_in);
+    const s3::Ref r{0.f, s3::to_f(ri[N + i]), s3::to_f(ri[2 * N + i]), s3::to_f(ri[3 * N + i]), s3::to_f(ri[4 * N + i])};
+#pragma unroll
+    for (int k = 0; k < 7; k++) S += s3::dec(gi[k * N + i], p.inv_scale, s3::rg(k, r));
+  }
+  return S;
+}
+
 // Collision of cell i (column gx, gy; its salinity S and the clamped
 // neighbours' along x, y and z; gz the z gradient factor of its plane): the
 // reference's moments -> Force -> collision on the D3Q19 / D3Q7 subsets
-// (ref: function/collision.cu:57-257). Returns true where the state is not
-// finite.
+// (ref: function/collision.cu:57-257). mo: the cell's pressure and u/c.
+// Returns true where the state is not finite.
+template <class T>
 __device__ __forceinline__ bool collide_cell(const Params3S &p, long long i, long long N, int gx, int gy, float S,
                                              float Sxm, float Sxp, float Sym, float Syp, float Szm, float Szp,
                                              float gz, float (&fo)[19], float (&go)[7], float &Fx, float &Fy,
-                                             float &Fz, bool ext) {
+                                             float &Fz, bool ext, float (&mo)[4]) {
   const float c = p.c, ic = 1.0f / c, c2 = c * c;
   float f[19], g[7];
-#pragma unroll
-  for (int k = 0; k < 19; k++) f[k] = p.f_in[k * N + i];
-#pragma unroll
-  for (int k = 0; k < 7; k++) g[k] = p.g_in[k * N + i];
+  s3::load_cell<T>(p.f_in, p.g_in, p.r_in, i, N, p.inv_scale, f, g);
   const float Fpx = p.F_in[i], Fpy = p.F_in[N + i], Fpz = p.F_in[2 * N + i];
   float pr = 0.f, jx = 0.f, jy = 0.f, jz = 0.f;
 #pragma unroll
@@ -122,6 +141,10 @@ __device__ __forceinline__ bool collide_cell(const Params3S &p, long long i, lon
   const float fden = __fdividef(p.fk3, rho);
   collide19(f, g, pr, S, uc, vc, wc, 0.5f * fden * Fx, 0.5f * fden * Fy, 0.5f * fden * Fz, p.itau, p.omg_s,
             p.mrt != 0, fo, go);
+  mo[0] = pr;
+  mo[1] = uc;
+  mo[2] = vc;
+  mo[3] = wc;
   return !(isfinite(uc) && isfinite(vc) && isfinite(wc) && isfinite(S) && isfinite(pr));
 }
 
@@ -268,9 +291,10 @@ struct Wall {
   }
 };
 
-template <int NS>
+template <int NS, class T>
 __global__ void __launch_bounds__(kThreads, kMinBlocks) step3s_kernel(const __grid_constant__ Params3S p) {
-  using Gm = G<NS>;
+  constexpr bool R16 = !std::is_same<T, float>::value;
+  using Gm = G<NS, R16>;
   constexpr int h = Gm::h, H = Gm::H, RX = Gm::RX, RC = Gm::RC, SX = Gm::SX, SC = Gm::SC;
   extern __shared__ __align__(16) float sm[];
   const int nx = p.nx, ny = p.ny, nz = p.nz;
@@ -295,10 +319,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) step3s_kernel(const __gr
     for (int e = tid; e < SC; e += kThreads) {
       const int ly = e / SX, lx = e - ly * SX;
       const long long i = (long long)qz * P + (long long)cly(ry0 - 1 + ly) * nx + clx(rx0 - 1 + lx);
-      float S = 0.f;
-#pragma unroll
-      for (int k = 0; k < 7; k++) S += p.g_in[k * N + i];
-      dst[e] = S;
+      dst[e] = cell_S<T>(p, i, N);
     }
   };
 
@@ -315,11 +336,11 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) step3s_kernel(const __gr
       const long long i = (long long)q * P + (long long)gy * nx + gx;
       const int se = (ly + 1) * SX + lx + 1;  // ring slot of the cell
       const float S = Sq[se];
-      float fo[19], go[7], Fx, Fy, Fz;
+      float fo[19], go[7], Fx, Fy, Fz, mo[4];
       const bool ext = fb[3] > 0 && gx >= fb[0] && gx < fb[0] + fb[3] && gy >= fb[1] && gy < fb[1] + fb[4] &&
                        q >= fb[2] && q < fb[2] + fb[5];
-      const bool bad = collide_cell(p, i, N, gx, gy, S, Sq[se - 1], Sq[se + 1], Sq[se - SX], Sq[se + SX],
-                                    q > 0 ? Sm[se] : S, q + 1 < nz ? Sp[se] : S, gz, fo, go, Fx, Fy, Fz, ext);
+      const bool bad = collide_cell<T>(p, i, N, gx, gy, S, Sq[se - 1], Sq[se + 1], Sq[se - SX], Sq[se + SX],
+                                       q > 0 ? Sm[se] : S, q + 1 < nz ? Sp[se] : S, gz, fo, go, Fx, Fy, Fz, ext, mo);
       const int le = ly * RX + lx;
 #pragma unroll
       for (int k = 0; k < 19; k++) sm[pofs<NS>(k, false, q) + le] = fo[k];
@@ -330,6 +351,11 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) step3s_kernel(const __gr
         Fr[0] = Fx;
         Fr[kTX * kTY] = Fy;
         Fr[2 * kTX * kTY] = Fz;
+        if constexpr (R16) {  // the reference the cell's stored populations will be encoded against
+          T *rf = reinterpret_cast<T *>(sm + Gm::RF0) + (q & 1) * 4 * kTX * kTY + (ly - H) * kTX + (lx - H);
+#pragma unroll
+          for (int a = 0; a < 4; a++) rf[a * kTX * kTY] = s3::from_f<T>(mo[a]);
+        }
       }
       if (bad) atomicOr(p.status, 1u);
     }
@@ -389,6 +415,37 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) step3s_kernel(const __gr
     return acc;
   };
 
+  // ---- storage of the output populations. 16-bit: the reference of tile
+  // cell `cell` of plane z (its collision's p and u/c from shared memory, S
+  // from the salinity ring) in the storage type; i >= 0 also writes the
+  // cell's reference planes
+  auto tile_ref = [&](int cell, int z, long long i) -> s3::Ref {
+    s3::Ref R{};
+    if constexpr (R16) {
+      const T *rf = reinterpret_cast<const T *>(sm + Gm::RF0) + (z & 1) * 4 * kTX * kTY + cell;
+      const int se = (cell / kTX + H + 1) * SX + cell % kTX + H + 1;
+      const T Sh = s3::from_f<T>(sm[Gm::S0 + (z % 3) * SC + se]);
+      R = s3::Ref{s3::to_f(rf[0]), s3::to_f(rf[kTX * kTY]), s3::to_f(rf[2 * kTX * kTY]), s3::to_f(rf[3 * kTX * kTY]),
+                  s3::to_f(Sh)};
+      if (i >= 0) {
+        T *ro = static_cast<T *>(p.r_out);
+#pragma unroll
+        for (int a = 0; a < 4; a++) ro[a * N + i] = rf[a * kTX * kTY];
+        ro[4 * N + i] = Sh;
+      }
+    }
+    return R;
+  };
+  auto put = [&](bool isg, int k, long long i, float v, const s3::Ref &R, float &amax) {
+    if constexpr (R16) {
+      const float x = s3::mul(s3::add(v, -(isg ? s3::rg(k, R) : s3::rf(k, R))), p.scale);
+      amax = fmaxf(amax, fabsf(x));
+      static_cast<T *>(isg ? p.g_out : p.f_out)[k * N + i] = s3::from_f<T>(x);
+    } else {
+      static_cast<float *>(isg ? p.g_out : p.f_out)[k * N + i] = v;
+    }
+  };
+
   // ---- march along z: planes zb - 1 (its upward populations) and zb first
   if (zb > 0) {
     form_S(zb - 2);
@@ -429,26 +486,32 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) step3s_kernel(const __gr
       p.F_out[N + i] = Fr[kTX * kTY];
       p.F_out[2 * N + i] = Fr[2 * kTX * kTY];
       if (xlo || xhi || ylo || yhi || zlo || zhi) queue[atomicAdd(qcount, 1)] = tid;
-      float pr = 0.f, S = 0.f;
+      float pr = 0.f, S = 0.f, amax = 0.f;
+      s3::Ref R{};
+      if constexpr (R16) {  // the cell's reference planes
+        R = tile_ref(tid, z, i);
+        amax = fmaxf(fmaxf(fabsf(R.p), fabsf(R.S)), fmaxf(fmaxf(fabsf(R.ux), fabsf(R.uy)), fabsf(R.uz)));
+      }
       auto all = [&](auto tag) {
 #pragma unroll
         for (int k = 0; k < 19; k++)
           if (src_in(k)) {
             const float v = fast(k, false, z, tag);
-            p.f_out[k * N + i] = v;
+            put(false, k, i, v, R, amax);
             pr += v;
           }
 #pragma unroll
         for (int k = 0; k < 7; k++)
           if (src_in(k)) {
             const float v = fast(k, true, z, tag);
-            p.g_out[k * N + i] = v;
+            put(true, k, i, v, R, amax);
             S += v;
           }
       };
       if (inx && iny) all(std::false_type{});
       else all(std::true_type{});
       if (!(isfinite(pr) && isfinite(S))) atomicOr(p.status, 1u);
+      if (R16 && !(amax <= p.store_max)) atomicOr(p.status, 4u);
     }
     // the wall cells of the plane: one (cell, population) pair per thread
     __syncthreads();
@@ -464,32 +527,41 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) step3s_kernel(const __gr
         if (sx >= 0 && sx < nx && sy >= 0 && sy < ny && sz >= 0 && sz < nz) continue;  // done above
         const float v = wp.bounce_any(kk, z, gx, gy);
         const long long i = (long long)z * P + (long long)gy * nx + gx;
-        if (kk >= 19) p.g_out[(kk - 19) * N + i] = v;
-        else p.f_out[kk * N + i] = v;
+        float amax = 0.f;
+        s3::Ref R{};
+        if constexpr (R16) R = tile_ref(cell, z, -1);
+        put(kk >= 19, k, i, v, R, amax);
         if (!isfinite(v)) atomicOr(p.status, 1u);
+        if (R16 && !(amax <= p.store_max)) atomicOr(p.status, 4u);
       }
     }
     __syncthreads();  // the next collide overwrites the oldest ring slots
   }
 }
 
-size_t smem3s(int ns) { return ns == 5 ? G<5>::bytes : G<3>::bytes; }
-
-
-template <int NS>
+template <int NS, class T>
 int launch_ns(const Params3S &p, cudaStream_t s, bool prep) {
-  constexpr size_t sm = G<NS>::bytes;
+  constexpr size_t sm = G<NS, !std::is_same<T, float>::value>::bytes;
+  static_assert(sm <= 227 * 1024, "shared memory of the 3-D step");
   if (prep)
     return status_from_cuda(
-        cudaFuncSetAttribute(step3s_kernel<NS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        cudaFuncSetAttribute(step3s_kernel<NS, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
   dim3 grid((p.nx + kTX - 1) / kTX, (p.ny + kTY - 1) / kTY, (p.nz + p.zchunk - 1) / p.zchunk);
-  step3s_kernel<NS><<<grid, kThreads, sm, s>>>(p);
+  step3s_kernel<NS, T><<<grid, kThreads, sm, s>>>(p);
   return status_from_cuda(cudaGetLastError());
 }
 
+template <int NS>
+int launch_st(const Params3S &p, cudaStream_t s, bool prep) {
+  if (p.store == IPCU_STORE_F32) return launch_ns<NS, float>(p, s, prep);
+  if (p.store == IPCU_STORE_F16) return launch_ns<NS, __half>(p, s, prep);
+  if (p.store == IPCU_STORE_BF16) return launch_ns<NS, __nv_bfloat16>(p, s, prep);
+  return IPCU_ERR_ARG;
+}
+
 int launch3s(const Params3S &p, int ns, cudaStream_t s, bool prepare_only) {
-  if (ns == 3) return launch_ns<3>(p, s, prepare_only);
-  if (ns == 5) return launch_ns<5>(p, s, prepare_only);
+  if (ns == 3) return launch_st<3>(p, s, prepare_only);
+  if (ns == 5) return launch_st<5>(p, s, prepare_only);
   return IPCU_ERR_UNSUPPORTED;
 }
 

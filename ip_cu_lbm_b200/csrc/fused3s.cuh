@@ -22,8 +22,19 @@ struct Axis {
 
 struct Params3S {
   int nx, ny, nz, zchunk;  // z cells per CTA
-  const float *f_in, *g_in, *F_in;
-  float *f_out, *g_out, *F_out;
+  // populations f [19][N] and g [7][N] in the storage type (FP32, or the
+  // 16-bit deviations of store3d.cuh), the force F [3][N] in FP32
+  const void *f_in, *g_in;
+  const float *F_in;
+  void *f_out, *g_out;
+  float *F_out;
+  // 16-bit storage: the reference planes [5][N] (p, u_x/c, u_y/c, u_z/c, S)
+  // of the state read and of the state written, the deviations' scale, and
+  // the largest finite stored magnitude (status bit 2 beyond it)
+  int store;  // IPCU_STORE_*
+  const void *r_in;
+  void *r_out;
+  float scale, inv_scale, store_max;
   Axis ax, ay;
   float c, dt, itau, omg_s;  // 1/tau, 1 - 1/tau_s
   float fk3, hdt;            // 3 dt / c, dt / 2
@@ -37,9 +48,9 @@ struct Params3S {
   const int *fext_box;
 };
 
-// ns: 3 (quadratic upwind) or 5 (the reference's stencil)
+// ns: 3 (quadratic upwind) or 5 (the reference's stencil); p.store selects
+// the storage instantiation
 int launch3s(const Params3S &p, int ns, cudaStream_t s, bool prepare_only = false);
-size_t smem3s(int ns);
 
 }  // namespace f3s
 }  // namespace ipcu

@@ -36,6 +36,7 @@
 #include "d3q19.cuh"
 #include "ibm3d.cuh"
 #include "ipcu_common.cuh"
+#include "store3d.cuh"
 
 namespace ipcu {
 namespace ib3d {
@@ -216,15 +217,19 @@ __global__ void __launch_bounds__(256) ib3d_window_kernel(const __grid_constant_
     const int gi = pl.win[0] + i, gj = pl.win[1] + jj, gk = pl.win[2] + k;
     const long long ci = (long long)gk * P + (long long)gj * j.nx + gi;
     float jx = 0.f, jy = 0.f, jzm = 0.f, S = 0.f;
+    float f[19], g[7];
+    if (j.store == IPCU_STORE_F16) s3::load_cell<__half>(j.f, j.g, j.r, ci, N, j.inv_scale, f, g);
+    else if (j.store == IPCU_STORE_BF16) s3::load_cell<__nv_bfloat16>(j.f, j.g, j.r, ci, N, j.inv_scale, f, g);
+    else s3::load_cell<float>(j.f, j.g, j.r, ci, N, j.inv_scale, f, g);
 #pragma unroll
     for (int q = 0; q < 19; q++) {
-      const float v = j.f[q * N + ci];
+      const float v = f[q];
       if (d3::cx(q)) jx += d3::cx(q) * v;
       if (d3::cy(q)) jy += d3::cy(q) * v;
       if (d3::cz(q)) jzm += d3::cz(q) * v;
     }
 #pragma unroll
-    for (int q = 0; q < 7; q++) S += j.g[q * N + ci];
+    for (int q = 0; q < 7; q++) S += g[q];
     const float h = __fdividef(j.hdt, fmaf(S, j.rsal, j.rho0));
     const float cj[3] = {c * jx, c * jy, c * jzm};
 #pragma unroll

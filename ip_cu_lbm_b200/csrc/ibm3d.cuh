@@ -41,7 +41,10 @@ struct Plan {
 // One coupled sphere after a fluid step: the buffers of the state that step
 // wrote and the body's own arrays.
 struct Job {
-  const float *f, *g;  // populations of the state [19][N], [7][N]
+  const void *f, *g;  // populations of the state [19][N], [7][N] in its storage type
+  const void *r;      // 16-bit storage: the state's reference planes [5][N]
+  int store;          // IPCU_STORE_*
+  float inv_scale;    // 16-bit storage: 1 / the deviations' scale
   float *F;            // its force planes [3][N] (corrected in place: the next step's velocity)
   float *fext;         // [3][N] force density on the fluid (zero outside the window)
   int nx, ny, nz;

@@ -1,6 +1,8 @@
-// 3-D structured solver object (ipcu_sim3d_*): device-resident FP32 state,
-// stepping (direct or CUDA-graph replay), field I/O.
+// 3-D structured solver object (ipcu_sim3d_*): device-resident state (FP32,
+// or 16-bit deviations from a per-cell reference, store3d.cuh), stepping
+// (direct or CUDA-graph replay), field I/O.
 #include <algorithm>
+#include <cstddef>
 #include <cmath>
 #include <cstring>
 #include <string>
@@ -12,6 +14,7 @@
 #include "fused3s.cuh"
 #include "ibm3d.cuh"
 #include "ipcu_common.cuh"
+#include "store3d.cuh"
 
 using namespace ipcu;
 
@@ -19,7 +22,12 @@ struct ipcu_sim3d {
   ipcu_sim3d_config cfg;
   long long N;
   cudaStream_t stream;
-  float *f[2] = {nullptr, nullptr}, *g[2] = {nullptr, nullptr}, *F[2] = {nullptr, nullptr};
+  // populations in the storage type, FP32 force planes, and with 16-bit
+  // storage the reference planes [5][N]
+  void *f[2] = {nullptr, nullptr}, *g[2] = {nullptr, nullptr}, *r[2] = {nullptr, nullptr};
+  float *F[2] = {nullptr, nullptr};
+  int store = IPCU_STORE_F32;
+  float scale = 1.0f, inv_scale = 1.0f;
   unsigned *status = nullptr;
   int cur = 0;
   f3d::Params3 P;
@@ -61,6 +69,7 @@ void free3(ipcu_sim3d *s) {
     if (s->graph[i]) cudaGraphExecDestroy(s->graph[i]);
     fr(s->f[i]);
     fr(s->g[i]);
+    fr(s->r[i]);
     fr(s->F[i]);
   }
   fr(s->status);
@@ -72,11 +81,11 @@ void free3(ipcu_sim3d *s) {
 
 f3d::Params3 params_for(const ipcu_sim3d *s, int cur) {
   f3d::Params3 P = s->P;
-  P.f_in = s->f[cur];
-  P.g_in = s->g[cur];
+  P.f_in = static_cast<const float *>(s->f[cur]);
+  P.g_in = static_cast<const float *>(s->g[cur]);
   P.F_in = s->F[cur];
-  P.f_out = s->f[cur ^ 1];
-  P.g_out = s->g[cur ^ 1];
+  P.f_out = static_cast<float *>(s->f[cur ^ 1]);
+  P.g_out = static_cast<float *>(s->g[cur ^ 1]);
   P.F_out = s->F[cur ^ 1];
   return P;
 }
@@ -91,6 +100,8 @@ int launch_one(const ipcu_sim3d *s, int cur, cudaStream_t st) {
   P.f_out = s->f[cur ^ 1];
   P.g_out = s->g[cur ^ 1];
   P.F_out = s->F[cur ^ 1];
+  P.r_in = s->r[cur];
+  P.r_out = s->r[cur ^ 1];
   return f3s::launch3s(P, s->ns, st);
 }
 
@@ -101,10 +112,99 @@ int launch_step(const ipcu_sim3d *s, int cur, cudaStream_t st) {
     ib3d::Job j = *s->ib;
     j.f = s->f[cur ^ 1];
     j.g = s->g[cur ^ 1];
+    j.r = s->r[cur ^ 1];
     j.F = s->F[cur ^ 1];
     e = ib3d::launch(j, st);
   }
   return e;
+}
+
+// ---- host side of the storage formats (store3d.cuh): the FP32 state of
+// buffer `cur` written into / read from the simulation's storage layout
+template <class T>
+void encode3(const ipcu_sim3d *s, const float *f, const float *g, const float *F, std::vector<T> &fh,
+             std::vector<T> &gh, std::vector<T> &rh) {
+  const long long N = s->N;
+  const float c = s->P.c, ic = 1.0f / c;
+  fh.resize(19 * N);
+  gh.resize(7 * N);
+  rh.resize(5 * N);
+  for (long long i = 0; i < N; i++) {
+    // the reference: the cell's pressure, u/c and salinity
+    float pr = 0.f, j[3] = {0.f, 0.f, 0.f}, S = 0.f;
+    for (int k = 0; k < 19; k++) {
+      const float v = f[k * N + i];
+      pr += v;
+      for (int a = 0; a < 3; a++)
+        if (E19[k][a]) j[a] += E19[k][a] * v;
+    }
+    for (int k = 0; k < 7; k++) S += g[k * N + i];
+    const float h = s->P.hdt / std::fmaf(S, s->P.rsal, s->P.rho0);
+    const float ref[5] = {pr, std::fmaf(c, j[0], F[i] * h) * ic, std::fmaf(c, j[1], F[N + i] * h) * ic,
+                          std::fmaf(c, j[2], F[2 * N + i] * h) * ic, S};
+    for (int a = 0; a < 5; a++) rh[a * N + i] = s3::from_f<T>(ref[a]);
+    const s3::Ref R = s3::ref_of(rh.data(), i, N);
+    for (int k = 0; k < 19; k++) fh[k * N + i] = s3::enc<T>(f[k * N + i], s->scale, s3::rf(k, R));
+    for (int k = 0; k < 7; k++) gh[k * N + i] = s3::enc<T>(g[k * N + i], s->scale, s3::rg(k, R));
+  }
+}
+
+template <class T>
+int put16(ipcu_sim3d *s, const float *f, const float *g, const float *F) {
+  std::vector<T> fh, gh, rh;
+  encode3(s, f, g, F, fh, gh, rh);
+  const int b = s->cur;
+  const bool ok = cudaMemcpy(s->f[b], fh.data(), 2 * fh.size(), cudaMemcpyHostToDevice) == cudaSuccess &&
+                  cudaMemcpy(s->g[b], gh.data(), 2 * gh.size(), cudaMemcpyHostToDevice) == cudaSuccess &&
+                  cudaMemcpy(s->r[b], rh.data(), 2 * rh.size(), cudaMemcpyHostToDevice) == cudaSuccess;
+  return ok ? IPCU_OK : IPCU_ERR_CUDA;
+}
+
+template <class T>
+int get16(ipcu_sim3d *s, float *f, float *g) {
+  const long long N = s->N;
+  std::vector<T> fh(19 * N), gh(7 * N), rh(5 * N);
+  const int b = s->cur;
+  if (cudaMemcpy(fh.data(), s->f[b], 2 * fh.size(), cudaMemcpyDeviceToHost) != cudaSuccess ||
+      cudaMemcpy(gh.data(), s->g[b], 2 * gh.size(), cudaMemcpyDeviceToHost) != cudaSuccess ||
+      cudaMemcpy(rh.data(), s->r[b], 2 * rh.size(), cudaMemcpyDeviceToHost) != cudaSuccess)
+    return IPCU_ERR_CUDA;
+  float fo[19], go[7];
+  for (long long i = 0; i < N; i++) {
+    s3::load_cell<T>(fh.data(), gh.data(), rh.data(), i, N, s->inv_scale, fo, go);
+    for (int k = 0; k < 19; k++) f[k * N + i] = fo[k];
+    for (int k = 0; k < 7; k++) g[k * N + i] = go[k];
+  }
+  return IPCU_OK;
+}
+
+// FP32 state (f [19][N], g [7][N], F [3][N]) into buffer `cur`; synchronises
+int put_state(ipcu_sim3d *s, const float *f, const float *g, const float *F) {
+  const long long N = s->N;
+  if (cudaStreamSynchronize(s->stream) != cudaSuccess ||
+      cudaMemcpy(s->F[s->cur], F, sizeof(float) * 3 * N, cudaMemcpyHostToDevice) != cudaSuccess)
+    return IPCU_ERR_CUDA;
+  if (s->store == IPCU_STORE_F16) return put16<__half>(s, f, g, F);
+  if (s->store == IPCU_STORE_BF16) return put16<__nv_bfloat16>(s, f, g, F);
+  const bool ok = cudaMemcpy(s->f[s->cur], f, sizeof(float) * 19 * N, cudaMemcpyHostToDevice) == cudaSuccess &&
+                  cudaMemcpy(s->g[s->cur], g, sizeof(float) * 7 * N, cudaMemcpyHostToDevice) == cudaSuccess;
+  return ok ? IPCU_OK : IPCU_ERR_CUDA;
+}
+
+// buffer `cur` as FP32 arrays; synchronises
+int get_state(ipcu_sim3d *s, std::vector<float> &f, std::vector<float> &g, std::vector<float> &F) {
+  const long long N = s->N;
+  f.resize(19 * N);
+  g.resize(7 * N);
+  F.resize(3 * N);
+  if (cudaStreamSynchronize(s->stream) != cudaSuccess ||
+      cudaMemcpy(F.data(), s->F[s->cur], sizeof(float) * F.size(), cudaMemcpyDeviceToHost) != cudaSuccess)
+    return IPCU_ERR_CUDA;
+  if (s->store == IPCU_STORE_F16) return get16<__half>(s, f.data(), g.data());
+  if (s->store == IPCU_STORE_BF16) return get16<__nv_bfloat16>(s, f.data(), g.data());
+  const bool ok = cudaMemcpy(f.data(), s->f[s->cur], sizeof(float) * f.size(), cudaMemcpyDeviceToHost) == cudaSuccess &&
+                  cudaMemcpy(g.data(), s->g[s->cur], sizeof(float) * g.size(), cudaMemcpyDeviceToHost) == cudaSuccess;
+  return ok ? IPCU_OK : IPCU_ERR_CUDA;
 }
 
 }  // namespace
@@ -123,6 +223,11 @@ extern "C" int ipcu_sim3d_create_stretched(const ipcu_sim3d_config *cfg, const i
     return IPCU_ERR_ARG;
   const bool stretched = axes && (axes->x || axes->wx || axes->y || axes->wy);
   if (stretched && axes->ns != 3 && axes->ns != 5) return IPCU_ERR_ARG;
+  if (c.storage != IPCU_STORE_F32 && c.storage != IPCU_STORE_F16 && c.storage != IPCU_STORE_BF16) return IPCU_ERR_ARG;
+  // 16-bit storage runs the flux-form kernel on every box (stencil 3 unless
+  // the axes name one)
+  const bool flux = stretched || c.storage != IPCU_STORE_F32;
+  const int ns = stretched ? axes->ns : (axes && axes->ns == 5 ? 5 : 3);
   std::vector<double> X(c.nx), DX(c.nx), Y(c.ny), DY(c.ny);
   for (int i = 0; i < c.nx; i++) {
     X[i] = stretched && axes->x ? axes->x[i] : (i + 0.5) * c.dz;
@@ -144,9 +249,17 @@ extern "C" int ipcu_sim3d_create_stretched(const ipcu_sim3d_config *cfg, const i
   s->stream = (cudaStream_t)stream;
   ensure_tables();
   const long long N = s->N;
+  s->store = c.storage;
+  // FP16 scales the deviations by 2^12 (they span about 1e-9 .. 1e-1 in
+  // lattice units: FP16's normal range from 1.5e-8 up to 16); BF16 has
+  // FP32's range
+  s->scale = c.storage == IPCU_STORE_F16 ? 4096.0f : 1.0f;
+  s->inv_scale = 1.0f / s->scale;
+  const size_t es = c.storage == IPCU_STORE_F32 ? sizeof(float) : 2;
   for (int i = 0; i < 2; i++)
-    if (!salloc3(s, &s->f[i], sizeof(float) * 19 * N) || !salloc3(s, &s->g[i], sizeof(float) * 7 * N) ||
-        !salloc3(s, &s->F[i], sizeof(float) * 3 * N)) {
+    if (!salloc3(s, &s->f[i], es * 19 * N) || !salloc3(s, &s->g[i], es * 7 * N) ||
+        !salloc3(s, &s->F[i], sizeof(float) * 3 * N) ||
+        (c.storage != IPCU_STORE_F32 && !salloc3(s, &s->r[i], 2 * 5 * N))) {
       free3(s);
       return IPCU_ERR_NOMEM;
     }
@@ -182,9 +295,9 @@ extern "C" int ipcu_sim3d_create_stretched(const ipcu_sim3d_config *cfg, const i
   P.gi_wall = 1.0f / ((float)c.dz + reg);
   P.mrt = c.mrt ? 1 : 0;
   P.status = s->status;
-  if (stretched) {
+  if (flux) {
     // flux-form and gradient tables of both axes, one device block
-    s->ns = axes->ns;
+    s->ns = ns;
     std::vector<float> wx, six, sox, wcx, wy, siy, soy, wcy;
     axis_tables(X, DX, c.dz, s->ns, wx, six, sox, wcx);
     axis_tables(Y, DY, c.dz, s->ns, wy, siy, soy, wcy);
@@ -230,6 +343,10 @@ extern "C" int ipcu_sim3d_create_stretched(const ipcu_sim3d_config *cfg, const i
     Q.giz_wall = P.gi_wall;
     Q.mrt = P.mrt;
     Q.status = s->status;
+    Q.store = s->store;
+    Q.scale = s->scale;
+    Q.inv_scale = s->inv_scale;
+    Q.store_max = c.storage == IPCU_STORE_F16 ? 65504.0f : 3.0e38f;
     const int st = f3s::launch3s(Q, s->ns, s->stream, true);
     if (st != IPCU_OK) {
       free3(s);
@@ -237,16 +354,13 @@ extern "C" int ipcu_sim3d_create_stretched(const ipcu_sim3d_config *cfg, const i
     }
   }
   // state at rest: f = 0, g = w_k S0, F = 0
-  std::vector<float> g0(7 * N);
+  std::vector<float> f0(19 * N, 0.0f), g0(7 * N), F0(3 * N, 0.0f);
   for (long long i = 0; i < N; i++) {
     const double S = s0 ? s0[i] : 0.0;
     for (int k = 0; k < 7; k++) g0[k * N + i] = (float)(w7d(k) * S);
   }
   if (cudaMemsetAsync(s->status, 0, sizeof(unsigned), s->stream) != cudaSuccess ||
-      cudaMemsetAsync(s->f[0], 0, sizeof(float) * 19 * N, s->stream) != cudaSuccess ||
-      cudaMemsetAsync(s->F[0], 0, sizeof(float) * 3 * N, s->stream) != cudaSuccess ||
-      cudaMemcpyAsync(s->g[0], g0.data(), sizeof(float) * 7 * N, cudaMemcpyHostToDevice, s->stream) != cudaSuccess ||
-      cudaStreamSynchronize(s->stream) != cudaSuccess) {
+      put_state(s, f0.data(), g0.data(), F0.data()) != IPCU_OK) {
     free3(s);
     return IPCU_ERR_CUDA;
   }
@@ -309,12 +423,8 @@ extern "C" int ipcu_sim3d_get(ipcu_sim3d *s, const char *field, double *out, int
   if (fd != "f" && fd != "g" && fd != "F" && fd != "S" && fd != "p" && fd != "ux" && fd != "uy" && fd != "uz")
     return IPCU_ERR_ARG;
   if (n < need) return IPCU_ERR_CAPACITY;
-  std::vector<float> f(19 * N), g(7 * N), F(3 * N);
-  if (cudaStreamSynchronize(s->stream) != cudaSuccess ||
-      cudaMemcpy(f.data(), s->f[s->cur], sizeof(float) * f.size(), cudaMemcpyDeviceToHost) != cudaSuccess ||
-      cudaMemcpy(g.data(), s->g[s->cur], sizeof(float) * g.size(), cudaMemcpyDeviceToHost) != cudaSuccess ||
-      cudaMemcpy(F.data(), s->F[s->cur], sizeof(float) * F.size(), cudaMemcpyDeviceToHost) != cudaSuccess)
-    return IPCU_ERR_CUDA;
+  std::vector<float> f, g, F;
+  if (int st = get_state(s, f, g, F)) return st;
   const std::vector<float> *raw = fd == "f" ? &f : (fd == "g" ? &g : (fd == "F" ? &F : nullptr));
   if (raw) {
     for (long long i = 0; i < need; i++) out[i] = (*raw)[i];
@@ -345,19 +455,22 @@ extern "C" int ipcu_sim3d_get(ipcu_sim3d *s, const char *field, double *out, int
 namespace {
 // S, u_x, u_y, u_z of every cell ([4][N]) from the current state, in the
 // float order of ipcu_sim3d_get (explicit rounding: the same values)
-__global__ void macro3d_kernel(const float *__restrict__ f, const float *__restrict__ g, const float *__restrict__ F,
-                               long long N, float c, float rsal, float rho0, float hdt, float *__restrict__ out) {
+template <class T>
+__global__ void macro3d_kernel(const void *__restrict__ fs, const void *__restrict__ gs, const void *__restrict__ rs,
+                               float inv_scale, const float *__restrict__ F, long long N, float c, float rsal,
+                               float rho0, float hdt, float *__restrict__ out) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < N; i += (long long)gridDim.x * blockDim.x) {
-    float j[3] = {0.f, 0.f, 0.f}, S = 0.f;
+    float j[3] = {0.f, 0.f, 0.f}, S = 0.f, f[19], g[7];
+    s3::load_cell<T>(fs, gs, rs, i, N, inv_scale, f, g);
 #pragma unroll
     for (int k = 0; k < 19; k++) {
-      const float v = f[k * N + i];
+      const float v = f[k];
       if (d3::cx(k)) j[0] = __fadd_rn(j[0], d3::cx(k) > 0 ? v : -v);
       if (d3::cy(k)) j[1] = __fadd_rn(j[1], d3::cy(k) > 0 ? v : -v);
       if (d3::cz(k)) j[2] = __fadd_rn(j[2], d3::cz(k) > 0 ? v : -v);
     }
 #pragma unroll
-    for (int k = 0; k < 7; k++) S = __fadd_rn(S, g[k * N + i]);
+    for (int k = 0; k < 7; k++) S = __fadd_rn(S, g[k]);
     const float h = __fdiv_rn(hdt, __fmaf_rn(S, rsal, rho0));
     out[i] = S;
 #pragma unroll
@@ -372,8 +485,14 @@ extern "C" int ipcu_sim3d_macro_async(ipcu_sim3d *s, float *out) {
   float *d = nullptr;
   if (cudaMallocAsync((void **)&d, sizeof(float) * 4 * N, s->stream) != cudaSuccess) return IPCU_ERR_NOMEM;
   const int blocks = (int)std::min<long long>((N + 255) / 256, 148LL * 16);
-  macro3d_kernel<<<blocks, 256, 0, s->stream>>>(s->f[s->cur], s->g[s->cur], s->F[s->cur], N, s->P.c, s->P.rsal,
-                                                s->P.rho0, s->P.hdt, d);
+  const int b = s->cur;
+  auto go = [&](auto kern) {
+    kern<<<blocks, 256, 0, s->stream>>>(s->f[b], s->g[b], s->r[b], s->inv_scale, s->F[b], N, s->P.c, s->P.rsal,
+                                        s->P.rho0, s->P.hdt, d);
+  };
+  if (s->store == IPCU_STORE_F16) go(macro3d_kernel<__half>);
+  else if (s->store == IPCU_STORE_BF16) go(macro3d_kernel<__nv_bfloat16>);
+  else go(macro3d_kernel<float>);
   cudaError_t e = cudaGetLastError();
   if (e == cudaSuccess) e = cudaMemcpyAsync(out, d, sizeof(float) * 4 * N, cudaMemcpyDefault, s->stream);
   cudaFreeAsync(d, s->stream);
@@ -382,21 +501,22 @@ extern "C" int ipcu_sim3d_macro_async(ipcu_sim3d *s, float *out) {
 
 extern "C" int ipcu_sim3d_set_state(ipcu_sim3d *s, const double *f, const double *g, const double *F) {
   if (!s) return IPCU_ERR_ARG;
-  const long long N = s->N;
-  auto put = [&](const double *src, float *dst, long long n) -> bool {
-    if (!src) return true;
-    std::vector<float> v(n);
-    for (long long i = 0; i < n; i++) v[i] = (float)src[i];
-    return cudaMemcpy(dst, v.data(), sizeof(float) * n, cudaMemcpyHostToDevice) == cudaSuccess;
+  std::vector<float> fv, gv, Fv;
+  if (int st = get_state(s, fv, gv, Fv)) return st;  // the parts kept
+  auto put = [&](const double *src, std::vector<float> &dst) {
+    if (src)
+      for (size_t i = 0; i < dst.size(); i++) dst[i] = (float)src[i];
   };
-  if (cudaStreamSynchronize(s->stream) != cudaSuccess) return IPCU_ERR_CUDA;
-  return put(f, s->f[s->cur], 19 * N) && put(g, s->g[s->cur], 7 * N) && put(F, s->F[s->cur], 3 * N) ? IPCU_OK
-                                                                                                      : IPCU_ERR_CUDA;
+  put(f, fv);
+  put(g, gv);
+  put(F, Fv);
+  return put_state(s, fv.data(), gv.data(), Fv.data());
 }
 
 
 extern "C" int ipcu_sim3d_upload(ipcu_sim3d *s, const float *f, const float *g, const float *F) {
   if (!s) return IPCU_ERR_ARG;
+  if (s->store != IPCU_STORE_F32 && (f || g)) return IPCU_ERR_UNSUPPORTED;
   const long long N = s->N;
   cudaError_t e = cudaSuccess;
   if (f) e = cudaMemcpyAsync(s->f[s->cur], f, sizeof(float) * 19 * N, cudaMemcpyHostToDevice, s->stream);
@@ -407,6 +527,7 @@ extern "C" int ipcu_sim3d_upload(ipcu_sim3d *s, const float *f, const float *g, 
 
 extern "C" int ipcu_sim3d_download(ipcu_sim3d *s, float *f, float *g, float *F) {
   if (!s) return IPCU_ERR_ARG;
+  if (s->store != IPCU_STORE_F32 && (f || g)) return IPCU_ERR_UNSUPPORTED;
   const long long N = s->N;
   cudaError_t e = cudaSuccess;
   if (f) e = cudaMemcpyAsync(f, s->f[s->cur], sizeof(float) * 19 * N, cudaMemcpyDeviceToHost, s->stream);
@@ -433,38 +554,54 @@ extern "C" int ipcu_sim3d_status(ipcu_sim3d *s, uint32_t *flags) {
 extern "C" int64_t ipcu_sim3d_cells(const ipcu_sim3d *s) { return s ? s->N : 0; }
 
 extern "C" int64_t ipcu_sim3d_bytes_per_cell(const ipcu_sim3d *s) {
-  return s ? 2 * 4 * (19 + 7 + 3) : 0;
+  if (!s) return 0;
+  return s->store == IPCU_STORE_F32 ? 2 * 4 * (19 + 7 + 3) : 2 * (2 * (19 + 7 + 5) + 4 * 3);
 }
 
 // ---------------------------------------------------------------------------
-// Checkpoint / restore: configuration, axes, step count and the raw FP32
-// state f, g, F; a restored run continues bit-identically.
+// Checkpoint / restore: configuration, axes, step count and the raw state in
+// its storage type (f, g, with 16-bit storage the reference planes, F); a
+// restored run continues bit-identically. Version 1 files (FP32 only, the
+// configuration without its storage field) still load.
 namespace {
 constexpr char kMagic3[8] = {'I', 'P', 'C', 'U', 'S', '3', 'D', '1'};
-constexpr int32_t kSnap3Version = 1;
+constexpr int32_t kSnap3Version = 2;
+constexpr size_t kCfgV1 = offsetof(ipcu_sim3d_config, storage);
 template <class T>
 bool wr3(FILE *f, const T *p, size_t n) { return fwrite(p, sizeof(T), n, f) == n; }
 template <class T>
 bool rd3(FILE *f, T *p, size_t n) { return fread(p, sizeof(T), n, f) == n; }
+
+// the raw arrays of buffer `cur`: device pointer and bytes
+std::vector<std::pair<void *, size_t>> raw_parts(ipcu_sim3d *s) {
+  const long long N = s->N;
+  const int b = s->cur;
+  const size_t es = s->store == IPCU_STORE_F32 ? sizeof(float) : 2;
+  std::vector<std::pair<void *, size_t>> v = {{s->f[b], es * 19 * N}, {s->g[b], es * 7 * N}};
+  if (s->store != IPCU_STORE_F32) v.push_back({s->r[b], 2 * 5 * (size_t)N});
+  v.push_back({s->F[b], sizeof(float) * 3 * N});
+  return v;
+}
 }  // namespace
 
 extern "C" int ipcu_sim3d_save(ipcu_sim3d *s, const char *path) {
   if (!s || !path) return IPCU_ERR_ARG;
   if (s->ib) return IPCU_ERR_UNSUPPORTED;  // the sphere's state is not part of the 3-D snapshot
-  const long long N = s->N;
-  std::vector<float> f(19 * N), g(7 * N), F(3 * N);
-  if (cudaStreamSynchronize(s->stream) != cudaSuccess ||
-      cudaMemcpy(f.data(), s->f[s->cur], sizeof(float) * f.size(), cudaMemcpyDeviceToHost) != cudaSuccess ||
-      cudaMemcpy(g.data(), s->g[s->cur], sizeof(float) * g.size(), cudaMemcpyDeviceToHost) != cudaSuccess ||
-      cudaMemcpy(F.data(), s->F[s->cur], sizeof(float) * F.size(), cudaMemcpyDeviceToHost) != cudaSuccess)
-    return IPCU_ERR_CUDA;
+  const auto parts = raw_parts(s);
+  std::vector<std::vector<char>> host(parts.size());
+  if (cudaStreamSynchronize(s->stream) != cudaSuccess) return IPCU_ERR_CUDA;
+  for (size_t a = 0; a < parts.size(); a++) {
+    host[a].resize(parts[a].second);
+    if (cudaMemcpy(host[a].data(), parts[a].first, parts[a].second, cudaMemcpyDeviceToHost) != cudaSuccess)
+      return IPCU_ERR_CUDA;
+  }
   FILE *fp = fopen(path, "wb");
   if (!fp) return IPCU_ERR_IO;
   const int32_t ns = s->ns;
   bool ok = wr3(fp, kMagic3, 8) && wr3(fp, &kSnap3Version, 1) && wr3(fp, &s->cfg, 1) && wr3(fp, &ns, 1) &&
             wr3(fp, &s->steps, 1) && wr3(fp, s->X.data(), s->X.size()) && wr3(fp, s->DX.data(), s->DX.size()) &&
-            wr3(fp, s->Y.data(), s->Y.size()) && wr3(fp, s->DY.data(), s->DY.size()) &&
-            wr3(fp, f.data(), f.size()) && wr3(fp, g.data(), g.size()) && wr3(fp, F.data(), F.size());
+            wr3(fp, s->Y.data(), s->Y.size()) && wr3(fp, s->DY.data(), s->DY.size());
+  for (auto &h : host) ok = ok && wr3(fp, h.data(), h.size());
   ok = (fclose(fp) == 0) && ok;
   return ok ? IPCU_OK : IPCU_ERR_IO;
 }
@@ -477,9 +614,11 @@ extern "C" int ipcu_sim3d_load(const char *path, ipcu_stream_t stream, ipcu_sim3
   char mg[8];
   int32_t ver = 0, ns = 0;
   ipcu_sim3d_config c;
+  std::memset(&c, 0, sizeof c);
   long long steps = 0;
-  bool ok = rd3(fp, mg, 8) && std::memcmp(mg, kMagic3, 8) == 0 && rd3(fp, &ver, 1) && ver == kSnap3Version &&
-            rd3(fp, &c, 1) && rd3(fp, &ns, 1) && rd3(fp, &steps, 1) && c.nx > 0 && c.ny > 0 && c.nz > 0;
+  bool ok = rd3(fp, mg, 8) && std::memcmp(mg, kMagic3, 8) == 0 && rd3(fp, &ver, 1) && (ver == 1 || ver == 2) &&
+            rd3(fp, reinterpret_cast<char *>(&c), ver == 1 ? kCfgV1 : sizeof c) && rd3(fp, &ns, 1) &&
+            rd3(fp, &steps, 1) && c.nx > 0 && c.ny > 0 && c.nz > 0;
   std::vector<double> X(ok ? c.nx : 0), DX(X.size()), Y(ok ? c.ny : 0), DY(Y.size());
   ok = ok && rd3(fp, X.data(), X.size()) && rd3(fp, DX.data(), DX.size()) && rd3(fp, Y.data(), Y.size()) &&
        rd3(fp, DY.data(), DY.size());
@@ -487,6 +626,8 @@ extern "C" int ipcu_sim3d_load(const char *path, ipcu_stream_t stream, ipcu_sim3
     fclose(fp);
     return IPCU_ERR_IO;
   }
+  // ns 0: the uniform box kernel; else the flux-form kernel on the saved
+  // axes (a 16-bit box without stretched axes saved its uniform ones)
   ipcu_sim3d_axes ax{X.data(), DX.data(), Y.data(), DY.data(), ns};
   ipcu_sim3d *s = nullptr;
   const int st = ipcu_sim3d_create_stretched(&c, ns ? &ax : nullptr, nullptr, stream, &s);
@@ -494,19 +635,16 @@ extern "C" int ipcu_sim3d_load(const char *path, ipcu_stream_t stream, ipcu_sim3
     fclose(fp);
     return st;
   }
-  const long long N = s->N;
-  std::vector<float> f(19 * N), g(7 * N), F(3 * N);
-  ok = rd3(fp, f.data(), f.size()) && rd3(fp, g.data(), g.size()) && rd3(fp, F.data(), F.size());
+  const auto parts = raw_parts(s);
+  for (auto &pt : parts) {
+    std::vector<char> h(pt.second);
+    ok = ok && rd3(fp, h.data(), h.size()) &&
+         cudaMemcpy(pt.first, h.data(), h.size(), cudaMemcpyHostToDevice) == cudaSuccess;
+  }
   fclose(fp);
   if (!ok) {
     ipcu_sim3d_destroy(s);
     return IPCU_ERR_IO;
-  }
-  if (cudaMemcpy(s->f[s->cur], f.data(), sizeof(float) * f.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
-      cudaMemcpy(s->g[s->cur], g.data(), sizeof(float) * g.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
-      cudaMemcpy(s->F[s->cur], F.data(), sizeof(float) * F.size(), cudaMemcpyHostToDevice) != cudaSuccess) {
-    ipcu_sim3d_destroy(s);
-    return IPCU_ERR_CUDA;
   }
   s->steps = steps;
   *out = s;
@@ -596,6 +734,8 @@ extern "C" int ipcu_sim3d_ib_attach(ipcu_sim3d *s, const ipcu_ib_sphere3d *bd, c
   j->clist = reinterpret_cast<int *>(mem + o_clist);
   j->fext = reinterpret_cast<float *>(mem + o_fext);
   j->status = s->status;
+  j->store = s->store;
+  j->inv_scale = s->inv_scale;
   j->nl = n;
   j->iters = bd->iters;
   j->radius = bd->radius;

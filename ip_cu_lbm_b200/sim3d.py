@@ -14,16 +14,24 @@ class Sim3D:
     as numpy arrays shaped [nz, ny, nx] (x fastest), or [q, nz, ny, nx]."""
 
     def __init__(self, nx, ny, nz, *, mrt=True, dz=1.0, dt=1.0, tau=0.55, taus=0.51, rho0=1.0, rho_sal=0.0,
-                 g_bouss=0.0, s0=None, stream=None, x=None, wx=None, y=None, wy=None, ns=3):
+                 g_bouss=0.0, s0=None, stream=None, x=None, wx=None, y=None, wy=None, ns=3, storage="f32"):
         """x, wx / y, wy: cell centres and widths of stretched x / y axes
         (z stays uniform), streamed with the ns-point conservative flux form
-        (ipcu_sim3d_create_stretched); all None: the uniform box kernel."""
+        (ipcu_sim3d_create_stretched); all None: the uniform box kernel.
+        storage: "f32", or "f16" / "bf16" (populations stored as 16-bit
+        deviations from a per-cell reference equilibrium; every box then
+        runs the flux-form kernel)."""
         self.nx, self.ny, self.nz = int(nx), int(ny), int(nz)
         self.N = self.nx * self.ny * self.nz
         cfg = _lib.Sim3DConfig()
         cfg.nx, cfg.ny, cfg.nz, cfg.mrt = self.nx, self.ny, self.nz, 1 if mrt else 0
         cfg.dz, cfg.dt, cfg.tau, cfg.taus = dz, dt, tau, taus
         cfg.rho0, cfg.rho_sal, cfg.g_bouss = rho0, rho_sal, g_bouss
+        stores = {"f32": 0, "f16": 1, "bf16": 2}
+        if storage not in stores:
+            raise ValueError(f"storage must be one of {sorted(stores)}")
+        cfg.storage = stores[storage]
+        self.storage = storage
         s0p = None
         if s0 is not None:
             self._s0 = np.ascontiguousarray(s0, dtype=np.float64).reshape(-1)
@@ -146,5 +154,7 @@ class Sim3D:
             head = fh.read(12 + ctypes.sizeof(cfg))
         cfg = _lib.Sim3DConfig.from_buffer_copy(head[12:])
         obj.nx, obj.ny, obj.nz = cfg.nx, cfg.ny, cfg.nz
+        version = int.from_bytes(head[8:12], "little")
+        obj.storage = {0: "f32", 1: "f16", 2: "bf16"}[cfg.storage if version >= 2 else 0]
         obj.N = obj.nx * obj.ny * obj.nz
         return obj

@@ -1,0 +1,186 @@
+"""16-bit storage of the 3-D solver (Sim3D(storage="f16" / "bf16"):
+populations stored as FP16/BF16 deviations from the linear equilibria of a
+per-cell reference (p, u/c, S in the storage type), collision, streaming
+and forcing in FP32) against
+  * the FP64 oracle (oracle/structured3d.py): a lock exchange on clustered
+    x and y axes and the stratified clustered box, velocity rel-L2 <= 1e-3
+    with FP16 (the precision bar for 16-bit storage), the BF16 format's own
+    floor (8 significant bits) at <= 1e-2;
+  * the FP32 path on the same inputs;
+  * the falling sphere against its FP64 oracle;
+with the rest state kept exactly, graph replay equal to direct steps, a
+snapshot that resumes bit for bit, the uniform box on the flux-form kernel,
+and the host encode/decode round trip."""
+import numpy as np
+import pytest
+
+from ip_cu_lbm_b200.sim3d import Sim3D
+from ip_cu_lbm_b200.workloads import clustered_box_3d
+from oracle.ibm3d import IBBox3D, Sphere3D
+from oracle.structured3d import W7, Box3D
+from helpers import rel_l2
+
+pytestmark = pytest.mark.gpu
+
+TOL_U = {"f16": 1e-3, "bf16": 1e-2}
+
+
+def clustered(n, ratio=3.0):
+    xi = (np.arange(n) + 0.5) / n
+    w = 1.0 + (ratio - 1.0) * np.abs(2.0 * xi - 1.0) ** 2
+    w = w / w.min()
+    return np.cumsum(w) - w / 2, w
+
+
+def lock(nx, ny, nz):
+    """Lock exchange across x on clustered x and y axes: S = 1 left of the
+    gate, 0 right of it, Boussinesq g' = 1e-4 (rho = 1 + 1e-3 S)."""
+    X, WX = clustered(nx)
+    Y, WY = clustered(ny)
+    S0 = np.broadcast_to((X < X[-1] / 2).astype(float)[None, None, :], (nz, ny, nx)).copy()
+    kw = dict(tau=0.56, taus=0.52, g_bouss=1e-4, rho_sal=1e-3, x=X, wx=WX, y=Y, wy=WY, ns=3)
+    return kw, S0
+
+
+def run(kw, S0, steps, storage):
+    nz, ny, nx = S0.shape
+    s = Sim3D(nx, ny, nz, s0=S0, storage=storage, **kw)
+    s.step(steps)
+    return s
+
+
+def oracle(kw, S0, steps):
+    nz, ny, nx = S0.shape
+    b = Box3D(nx, ny, nz, **kw)
+    b.g = W7[:, None, None, None] * S0[None]
+    b.step(steps)
+    return b
+
+
+@pytest.mark.parametrize("storage", ["f16", "bf16"])
+def test_lock_exchange_16bit_against_fp64_oracle(cuda, storage):
+    kw, S0 = lock(40, 20, 24)
+    steps = 200
+    s = run(kw, S0, steps, storage)
+    ref = run(kw, S0, steps, "f32")
+    b = oracle(kw, S0, steps)
+    p, S, rho, u = b.moments()
+    errs = {n: rel_l2(s.get(n), r) for n, r in (("ux", u[0]), ("uy", u[1]), ("uz", u[2]), ("S", S))}
+    e32 = {n: rel_l2(ref.get(n), r) for n, r in (("ux", u[0]), ("uz", u[2]), ("S", S))}
+    print(f"lock exchange {storage}: " + ", ".join(f"{k} {v:.2e}" for k, v in errs.items()) +
+          f"; FP32 ux {e32['ux']:.2e} uz {e32['uz']:.2e}; |u|max {np.abs(u[0]).max():.2e}")
+    assert s.status() == 0
+    assert errs["ux"] <= TOL_U[storage] and errs["uz"] <= TOL_U[storage], errs
+    assert errs["S"] <= TOL_U[storage] / 10, errs
+    assert s.bytes_per_cell() == 148 and ref.bytes_per_cell() == 232
+    s.close()
+    ref.close()
+
+
+def test_stratified_box_fp16_against_fp64_oracle(cuda):
+    kw, S0 = clustered_box_3d(24, 24, 48)
+    steps = 200
+    s = run(kw, S0, steps, "f16")
+    b = oracle(kw, S0, steps)
+    p, S, rho, u = b.moments()
+    eu = max(rel_l2(s.get(n), r) for n, r in (("ux", u[0]), ("uy", u[1]), ("uz", u[2])))
+    eS = rel_l2(s.get("S"), S)
+    print(f"stratified box f16: u {eu:.2e}, S {eS:.2e} (|u|max {np.abs(u[2]).max():.2e})")
+    assert s.status() == 0 and eu <= 1e-3 and eS <= 1e-4, (eu, eS)
+    s.close()
+
+
+@pytest.mark.parametrize("storage", ["f16", "bf16"])
+def test_rest_state_kept_exactly(cuda, storage):
+    n = (20, 12, 16)
+    S0 = np.full(n[::-1], 0.5)
+    s = Sim3D(*n, s0=S0, storage=storage, tau=0.56, taus=0.52, rho_sal=1e-3, g_bouss=0.0)
+    s.step(50)
+    assert np.all(s.get("f") == 0.0)
+    assert np.all(s.get("S") == 0.5)
+    for c in ("ux", "uy", "uz"):
+        assert np.all(s.get(c) == 0.0)
+    assert s.status() == 0
+    s.close()
+
+
+def test_graph_and_snapshot_bitwise(cuda, tmp_path):
+    kw, S0 = lock(36, 20, 16)
+    a = Sim3D(36, 20, 16, s0=S0, storage="f16", **kw)
+    b = Sim3D(36, 20, 16, s0=S0, storage="f16", **kw)
+    a.step(40)
+    b.step_graph(40)
+    assert np.array_equal(a.get("f"), b.get("f")) and np.array_equal(a.get("g"), b.get("g"))
+    a.save(tmp_path / "s16.ipcu3")
+    a.step(20)
+    c = Sim3D.load(tmp_path / "s16.ipcu3")
+    assert c.storage == "f16" and c.steps() == 40 and c.bytes_per_cell() == 148
+    c.step(20)
+    for fld in ("f", "g", "F"):
+        assert np.array_equal(a.get(fld), c.get(fld)), fld
+    with pytest.raises(RuntimeError):  # raw transfer is FP32-only
+        import torch
+
+        a.download(f=torch.empty(19 * a.N))
+    for s in (a, b, c):
+        s.close()
+
+
+def test_uniform_box_runs_flux_form(cuda):
+    """Without axes a 16-bit box runs the flux-form kernel on uniform axes:
+    the same bits as with the uniform axes given."""
+    nx, ny, nz = 24, 16, 20
+    S0 = np.broadcast_to(1.0 - (np.arange(nz) + 0.5)[:, None, None] / nz, (nz, ny, nx)).copy()
+    kw = dict(tau=0.56, taus=0.52, rho_sal=1e-3, g_bouss=1e-4)
+    a = Sim3D(nx, ny, nz, s0=S0, storage="f16", **kw)
+    b = Sim3D(nx, ny, nz, s0=S0, storage="f16", x=np.arange(nx) + 0.5, wx=np.ones(nx), y=np.arange(ny) + 0.5,
+              wy=np.ones(ny), ns=3, **kw)
+    f32 = Sim3D(nx, ny, nz, s0=S0, **kw)
+    for s in (a, b, f32):
+        s.step(60)
+    assert np.array_equal(a.get("f"), b.get("f"))
+    assert rel_l2(a.get("uz"), f32.get("uz")) < 1e-3
+    for s in (a, b, f32):
+        s.close()
+
+
+@pytest.mark.parametrize("storage", ["f16", "bf16"])
+def test_set_state_round_trip(cuda, storage):
+    nx, ny, nz = 16, 12, 10
+    rng = np.random.default_rng(4)
+    f = 1e-3 * rng.standard_normal((19, nz, ny, nx))
+    g = W7[:, None, None, None] * (0.5 + 0.1 * rng.standard_normal((1, nz, ny, nx)))
+    s = Sim3D(nx, ny, nz, storage=storage)
+    s.set_state(f=f, g=g, F=np.zeros((3, nz, ny, nx)))
+    tol = 2.0 ** -11 if storage == "f16" else 2.0 ** -8
+    # each value within the format's relative precision of its deviation from the reference
+    assert np.abs(s.get("f") - f).max() <= tol * 2e-3 * 3
+    assert np.abs(s.get("g") - g).max() <= tol * 0.1
+    s.close()
+
+
+def test_falling_sphere_fp16(cuda):
+    """The sphere on a 16-bit box: its motion against the FP64 oracle. The
+    velocity field near the markers is sensitive to any perturbation of the
+    coupled update (a perturbation grows over the run), so the field is held
+    to 1e-2 here and the body to 1e-4."""
+    from test_sphere3d_gpu import NM, NX, NY, NZ, PHYS, R, axes, centre
+
+    kw = axes(True)
+    xc, yc = centre(kw)
+    steps = 60
+    s = Sim3D(NX, NY, NZ, storage="f16", **PHYS, **kw)
+    s.attach_sphere(xc, yc, 22.0, R, markers=NM, rho_s=1.5, gravity=1e-4)
+    s.step(steps)
+    b = Box3D(NX, NY, NZ, **PHYS, **kw)
+    sp = Sphere3D(xc, yc, 22.0, R, NM, rho_s=1.5)
+    IBBox3D(b, sp, rho_f=1.0, gravity=1e-4).step(steps)
+    d = s.body()
+    dvel = np.abs(d["U"] - sp.U).max() / np.abs(sp.U).max()
+    dpos = np.abs(d["X"] - sp.X).max() / np.abs(sp.X - [xc, yc, 22.0]).max()
+    u = b.moments()[3]
+    eu = max(rel_l2(s.get(n), r) for n, r in (("ux", u[0]), ("uy", u[1]), ("uz", u[2])))
+    print(f"sphere f16: body velocity rel {dvel:.2e}, position rel {dpos:.2e}, field {eu:.2e}")
+    assert s.status() == 0 and sp.U[2] < 0
+    assert dvel < 1e-4 and dpos < 1e-4 and eu < 1e-2, (dvel, dpos, eu)
+    s.close()
