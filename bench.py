@@ -117,14 +117,15 @@ def measured_traffic(args):
     return d["dram_bytes_per_launch"] if d else None
 
 
-def traffic3d(N, stretched):
+def traffic3d(N, stretched, storage="f32"):
     """DRAM bytes per launch of the 3-D step at N cells, scaled from the
     committed 128^3 ncu capture of the same kernel (profiles/traffic.json),
     else None."""
     p = os.path.join(ROOT, "profiles", "traffic.json")
     if not os.path.exists(p):
         return None
-    d = json.load(open(p)).get("step3s_kernel<3>@128x128x128" if stretched else "step3d_kernel@128x128x128")
+    key = {"f32": "step3s_kernel<3>@128x128x128", "f16": "step3s_kernel<3,__half>@128x128x128"}.get(storage)
+    d = json.load(open(p)).get(key if stretched or storage != "f32" else "step3d_kernel@128x128x128") if key else None
     return int(d["dram_bytes_per_cell"] * N) if d else None
 
 
@@ -414,7 +415,7 @@ def run_3d(args):
                    "l2": f"inputs ({bpc / 2 * N / 1e9:.2f} GB) larger than L2"},
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4),
-                     "traffic": traffic3d(N, not args.uniform3d) if f32 else None, "bytes_per_cell": bpc,
+                     "traffic": traffic3d(N, not args.uniform3d, args.storage), "bytes_per_cell": bpc,
                      "peak_source": peak_label(peak_src),
                      "traffic_note": "DRAM read+write bytes per launch from the 128^3 ncu capture (profiles/traffic.json), "
                                      "scaled by cells; it grows in proportion to the cells streamed"},
