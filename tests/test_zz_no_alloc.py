@@ -6,7 +6,8 @@ not enter the driver's allocator.
 For them the library keeps the reduction's scratch in a fixed device array.
 This file checks, through the C ABI, that two calls in a row return the same
 totals as the allocating path (ipcu_sim_totals, same FP64 reduction) within
-1e-12 relative, and that fields beyond the fixed scratch are rejected. It is
+1e-12 relative, that a call captured in a CUDA graph replays to the same
+totals, and that fields beyond the fixed scratch are rejected. It is
 collected last (test_zz_...) so a failure here comes after every other test,
 and it runs alone in a fresh process as well as after the others.
 """
@@ -60,6 +61,21 @@ def test_noalloc_totals_match_allocating_path(cuda):
         got_p, got_s = out.cpu().tolist()
         assert abs(got_s - ref_s) <= 1e-12 * abs(ref_s), (call, got_s, ref_s)
         assert abs(got_p - ref_p) <= 1e-12 * p_scale, (call, got_p, ref_p, p_scale)
+    # the launches can be captured once the scratch address is resolved: a
+    # graph replay gives the same totals
+    graph = torch.cuda.CUDAGraph()
+    cs = torch.cuda.Stream(cuda)
+    with torch.cuda.graph(graph, stream=cs):
+        rc = fn(f_ptr, mac_ptr, wx_d.data_ptr(), wz_d.data_ptr(), nx, nz, out.data_ptr(), cs.cuda_stream)
+    assert rc == 0, f"captured call: status {rc}"
+    out.fill_(float("nan"))
+    torch.cuda.synchronize()
+    graph.replay()
+    torch.cuda.synchronize()
+    got_p, got_s = out.cpu().tolist()
+    assert abs(got_s - ref_s) <= 1e-12 * abs(ref_s), ("replay", got_s, ref_s)
+    assert abs(got_p - ref_p) <= 1e-12 * p_scale, ("replay", got_p, ref_p, p_scale)
+    del graph
     # beyond the fixed scratch: rejected before any launch
     rc = fn(f_ptr, mac_ptr, wx_d.data_ptr(), wz_d.data_ptr(), 8192, 4097, out.data_ptr(), stream.cuda_stream)
     assert rc == -4, rc  # IPCU_ERR_CAPACITY
