@@ -322,22 +322,22 @@ __device__ void coupled_update(const Job &j, int parity) {
   __syncthreads();
   for (int s = tid; s < ns; s += kThreads) sCur[s] = sOff[s];
   __syncthreads();
+  // each slot's pairs, first in arrival order (into the window map, free
+  // from here on), then each pair at its rank in pair order: the lists come
+  // out sorted, so every sum over them runs in a fixed order
+  short *sTmp = sMap;
   for (int e = tid; e < 16 * nl; e += kThreads) {
     const int s = sPS[e];
-    if (s >= 0) sList[atomicAdd(&sCur[s], 1)] = (short)e;
+    if (s >= 0) sTmp[atomicAdd(&sCur[s], 1)] = (short)e;
   }
   __syncthreads();
-  for (int s = tid; s < ns; s += kThreads) {  // insertion sort of each slot's short list
+  for (int e = tid; e < 16 * nl; e += kThreads) {
+    const int s = sPS[e];
+    if (s < 0) continue;
     const int a0 = sOff[s], a1 = sOff[s + 1];
-    for (int a = a0 + 1; a < a1; a++) {
-      const short v = sList[a];
-      int b2 = a - 1;
-      while (b2 >= a0 && sList[b2] > v) {
-        sList[b2 + 1] = sList[b2];
-        b2--;
-      }
-      sList[b2 + 1] = v;
-    }
+    int r = 0;
+    for (int a = a0; a < a1; a++) r += sTmp[a] < e;
+    sList[a0 + r] = (short)e;
   }
   __syncthreads();
 
@@ -345,30 +345,43 @@ __device__ void coupled_update(const Job &j, int parity) {
   const int g = tid >> 4, q = tid & 15, qa = q & 3, qc = q >> 2;
   auto slot_of = [&](int l) -> int { return sPS[16 * l + q]; };
   const float two_rf_dt = (float)(2.0 * j.rho_f / j.dt);
-  for (int it = 0; it < j.iters; it++) {
-    for (int lb = 0; lb < nl; lb += kGroups) {
-      const int l = lb + g;
-      float vx = 0.f, vz = 0.f;
-      if (l < nl) {
-        const int s = slot_of(l);
-        if (s >= 0) {
-          const float w = sWX[4 * l + qa] * sWZ[4 * l + qc];
-          vx = w * sU[s];
-          vz = w * sW[s];
-        }
+  // the velocity a 16-lane group interpolates at marker l (lane q's node)
+  auto node_vel = [&](int l, float &vx, float &vz) {
+    vx = vz = 0.f;
+    if (l < nl) {
+      const int s = slot_of(l);
+      if (s >= 0) {
+        const float w = sWX[4 * l + qa] * sWZ[4 * l + qc];
+        vx = w * sU[s];
+        vz = w * sW[s];
       }
+    }
+  };
+  auto marker_force = [&](int l, float vx, float vz) {
+    if (l < nl && q == 0) {
+      const float dfx = two_rf_dt * (sUB[2 * l] - vx), dfz = two_rf_dt * (sUB[2 * l + 1] - vz);
+      sDF[2 * l] = dfx;
+      sDF[2 * l + 1] = dfz;
+      sFT[2 * l] += dfx;
+      sFT[2 * l + 1] += dfz;
+    }
+  };
+  for (int it = 0; it < j.iters; it++) {
+    // two markers per group at a time: independent reductions in flight
+    for (int lb = 0; lb < nl; lb += 2 * kGroups) {
+      const int l1 = lb + g, l2 = lb + kGroups + g;
+      float vx1, vz1, vx2, vz2;
+      node_vel(l1, vx1, vz1);
+      node_vel(l2, vx2, vz2);
 #pragma unroll
       for (int o = 8; o > 0; o >>= 1) {
-        vx += __shfl_xor_sync(0xffffffffu, vx, o, 16);
-        vz += __shfl_xor_sync(0xffffffffu, vz, o, 16);
+        vx1 += __shfl_xor_sync(0xffffffffu, vx1, o, 16);
+        vz1 += __shfl_xor_sync(0xffffffffu, vz1, o, 16);
+        vx2 += __shfl_xor_sync(0xffffffffu, vx2, o, 16);
+        vz2 += __shfl_xor_sync(0xffffffffu, vz2, o, 16);
       }
-      if (l < nl && q == 0) {
-        const float dfx = two_rf_dt * (sUB[2 * l] - vx), dfz = two_rf_dt * (sUB[2 * l + 1] - vz);
-        sDF[2 * l] = dfx;
-        sDF[2 * l + 1] = dfz;
-        sFT[2 * l] += dfx;
-        sFT[2 * l + 1] += dfz;
-      }
+      marker_force(l1, vx1, vz1);
+      marker_force(l2, vx2, vz2);
     }
     __syncthreads();
     for (int s = tid; s < ns; s += kThreads) {
