@@ -106,9 +106,11 @@ struct Layout {
   static constexpr size_t LIST = CUR + 4 * kMaxSlots;                // short [16 nl] pairs l*16+q by slot
   static constexpr size_t PS = LIST + 2 * 16 * kMaxMarkers;          // short [16 nl] slot of each pair (-1 outside)
   static constexpr size_t MAP = PS + 2 * 16 * kMaxMarkers;           // short [window] slot of a window cell
-  static constexpr size_t RED = (MAP + 2 * kMaxWindow + 15) / 16 * 16;  // double [kWarps][6]
+  static constexpr size_t WL = (MAP + 2 * kMaxWindow + 15) / 16 * 16;  // float [16 nl] spread weight of each list entry
+  static constexpr size_t RED = WL + 4 * 16 * kMaxMarkers;              // double [kWarps][6]
   static constexpr size_t BYTES = RED + 8 * 6 * kWarps;
 };
+static_assert(Layout::BYTES + 2048 <= 227 * 1024, "the update's dynamic and static shared memory");
 
 template <class ST, int QS>
 __device__ void coupled_update(const Job &j, int parity) {
@@ -132,6 +134,7 @@ __device__ void coupled_update(const Job &j, int parity) {
   short *sList = reinterpret_cast<short *>(sm + Layout::LIST);
   short *sPS = reinterpret_cast<short *>(sm + Layout::PS);
   short *sMap = reinterpret_cast<short *>(sm + Layout::MAP);
+  float *sWL = reinterpret_cast<float *>(sm + Layout::WL);
   double *sRed = reinterpret_cast<double *>(sm + Layout::RED);
   __shared__ Body B;
   __shared__ int bnd[4];   // window bounds imin, imax, kmin, kmax
@@ -165,6 +168,26 @@ __device__ void coupled_update(const Job &j, int parity) {
   if (have_prev) asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
   const double cth = cos(B.th), sth = sin(B.th);
 
+  // window bounds: each thread's own, then one shared atomic per warp
+  int bx[12] = {INT_MAX, INT_MIN, INT_MAX, INT_MIN, INT_MAX, INT_MIN, INT_MAX, INT_MIN,
+                INT_MAX, INT_MIN, INT_MAX, INT_MIN};
+  auto take_box = [&](int *box, int i0, int k0) {
+    box[0] = min(box[0], i0);
+    box[1] = max(box[1], i0 + 3);
+    box[2] = min(box[2], k0);
+    box[3] = max(box[3], k0 + 3);
+  };
+  auto merge_box = [&](const int *box, int *dst) {
+    const int a = __reduce_min_sync(0xffffffffu, box[0]), b2 = __reduce_max_sync(0xffffffffu, box[1]);
+    const int c = __reduce_min_sync(0xffffffffu, box[2]), d = __reduce_max_sync(0xffffffffu, box[3]);
+    if (lane == 0) {
+      atomicMin(&dst[0], a);
+      atomicMax(&dst[1], b2);
+      atomicMin(&dst[2], c);
+      atomicMax(&dst[3], d);
+    }
+  };
+
   // ---- 1. markers: position, velocity, stencil origin and weights
   for (int l = tid; l < nl; l += kThreads) {
     const double x0 = j.X0[2 * l], z0 = j.X0[2 * l + 1];
@@ -183,25 +206,12 @@ __device__ void coupled_update(const Job &j, int parity) {
     sUB[2 * l + 1] = (float)(B.U[1] + B.om * rx);
     sFT[2 * l] = sFT[2 * l + 1] = 0.f;
     sDS[l] = (float)(j.dS[l] * idz * idz);
-    atomicMin(&bnd[0], i0);
-    atomicMax(&bnd[1], i0 + 3);
-    atomicMin(&bnd[2], k0);
-    atomicMax(&bnd[3], k0 + 3);
-    if (have_prev2) {
-      const int oi = j.org2[2 * l], ok = j.org2[2 * l + 1];
-      atomicMin(&bnd2[0], oi);
-      atomicMax(&bnd2[1], oi + 3);
-      atomicMin(&bnd2[2], ok);
-      atomicMax(&bnd2[3], ok + 3);
-    }
-    if (have_prev) {
-      const int oi = j.org[2 * l], ok = j.org[2 * l + 1];
-      atomicMin(&bnd[0], oi);
-      atomicMax(&bnd[1], oi + 3);
-      atomicMin(&bnd[2], ok);
-      atomicMax(&bnd[3], ok + 3);
-    }
+    take_box(bx, i0, k0);
+    if (have_prev2) take_box(bx + 4, j.org2[2 * l], j.org2[2 * l + 1]);
+    if (have_prev) take_box(bx, j.org[2 * l], j.org[2 * l + 1]);
   }
+  merge_box(bx, bnd);
+  merge_box(bx + 4, bnd2);
   __syncthreads();
   const int wi0 = bnd[0], wk0 = bnd[2], WW = bnd[1] - bnd[0] + 1, WH = bnd[3] - bnd[2] + 1;
   if (nl == 0 || (long long)WW * WH > kMaxWindow) {
@@ -338,6 +348,8 @@ __device__ void coupled_update(const Job &j, int parity) {
     int r = 0;
     for (int a = a0; a < a1; a++) r += sTmp[a] < e;
     sList[a0 + r] = (short)e;
+    const int l = e >> 4;
+    sWL[a0 + r] = sWX[4 * l + (e & 3)] * sWZ[4 * l + ((e >> 2) & 3)] * sDS[l];  // kernel weight x marker area
   }
   __syncthreads();
 
@@ -387,8 +399,8 @@ __device__ void coupled_update(const Job &j, int parity) {
     for (int s = tid; s < ns; s += kThreads) {
       float fx = 0.f, fz = 0.f;
       for (int a = sOff[s]; a < sOff[s + 1]; a++) {
-        const int e = sList[a], l = e >> 4, qq = e & 15;
-        const float wd = sWX[4 * l + (qq & 3)] * sWZ[4 * l + (qq >> 2)] * sDS[l];
+        const int l = sList[a] >> 4;
+        const float wd = sWL[a];
         fx = fmaf(sDF[2 * l], wd, fx);
         fz = fmaf(sDF[2 * l + 1], wd, fz);
       }
@@ -556,11 +568,9 @@ __device__ void coupled_update(const Job &j, int parity) {
       const int pi = (int)floor(X * idz - 0.5) - 1, pk = (int)floor(Z * idz - 0.5) - 1;
       sPI[2 * l] = pi;
       sPI[2 * l + 1] = pk;
-      atomicMin(&bnd3[0], pi);
-      atomicMax(&bnd3[1], pi + 3);
-      atomicMin(&bnd3[2], pk);
-      atomicMax(&bnd3[3], pk + 3);
+      take_box(bx + 8, pi, pk);
     }
+    merge_box(bx + 8, bnd3);
   }
   __syncthreads();
   const int lo_i = min(min(wi0, bnd2[0]), bnd3[0]), hi_i = max(max(wi0 + WW - 1, bnd2[1]), bnd3[1]);
