@@ -10,8 +10,9 @@
 //   2. the cells of the previous and the new stencils get shared-memory
 //      slots (a window map over their bounding box); the old force's half
 //      is taken out of u there and f_ib restarts at zero;
-//   3. multi-direct forcing, `iters` times: U*_l = sum phi u (16 lanes per
-//      marker, shuffle reduction), dF_l = 2 rho_f (U_b,l - U*_l) / dt,
+//   3. multi-direct forcing, `iters` times: U*_l = sum phi u (one thread
+//      per marker, a fixed pairwise sum over its 16 nodes), dF_l = 2 rho_f
+//      (U_b,l - U*_l) / dt,
 //      spread df = dF_l phi dS_l / dz^2 onto f_ib and df dt / 2 rho onto u,
 //      F_l += dF_l; each slot gathers its (marker, cell) pairs from a list
 //      sorted by pair index, so every sum runs in a fixed order and a
@@ -73,7 +74,6 @@ __device__ __forceinline__ void vel_at(const f2d::Params &p, int b, const float 
 }
 
 constexpr int kWarps = kThreads / 32;
-constexpr int kGroups = kThreads / 16;  // 16 lanes (one 4x4 stencil) per marker
 constexpr int kTileMap = 1024;          // tiles tracked around the footprints for the flag clean-up
 
 // 4-point Peskin kernel (ref: function/ibm.cu:61-66), r in lattice spacings
@@ -354,46 +354,40 @@ __device__ void coupled_update(const Job &j, int parity) {
   __syncthreads();
 
   // ---- 3. multi-direct forcing
-  const int g = tid >> 4, q = tid & 15, qa = q & 3, qc = q >> 2;
-  auto slot_of = [&](int l) -> int { return sPS[16 * l + q]; };
   const float two_rf_dt = (float)(2.0 * j.rho_f / j.dt);
-  // the velocity a 16-lane group interpolates at marker l (lane q's node)
-  auto node_vel = [&](int l, float &vx, float &vz) {
-    vx = vz = 0.f;
-    if (l < nl) {
-      const int s = slot_of(l);
-      if (s >= 0) {
-        const float w = sWX[4 * l + qa] * sWZ[4 * l + qc];
-        vx = w * sU[s];
-        vz = w * sW[s];
+  for (int it = 0; it < j.iters; it++) {
+    // one thread per marker: the velocity at its 16 nodes, summed in a
+    // fixed pairwise order (explicit rounding: the order and the roundings
+    // do not depend on the compiler), then the marker's force
+    for (int l = tid; l < nl; l += kThreads) {
+      float wx[4], wz[4], vx[16], vz[16];
+#pragma unroll
+      for (int a = 0; a < 4; a++) {
+        wx[a] = sWX[4 * l + a];
+        wz[a] = sWZ[4 * l + a];
       }
-    }
-  };
-  auto marker_force = [&](int l, float vx, float vz) {
-    if (l < nl && q == 0) {
-      const float dfx = two_rf_dt * (sUB[2 * l] - vx), dfz = two_rf_dt * (sUB[2 * l + 1] - vz);
+#pragma unroll
+      for (int q = 0; q < 16; q++) {
+        const int s = sPS[16 * l + q];
+        vx[q] = vz[q] = 0.f;
+        if (s >= 0) {
+          const float w = __fmul_rn(wx[q & 3], wz[q >> 2]);
+          vx[q] = __fmul_rn(w, sU[s]);
+          vz[q] = __fmul_rn(w, sW[s]);
+        }
+      }
+#pragma unroll
+      for (int o = 8; o > 0; o >>= 1)
+#pragma unroll
+        for (int q = 0; q < o; q++) {
+          vx[q] = __fadd_rn(vx[q], vx[q + o]);
+          vz[q] = __fadd_rn(vz[q], vz[q + o]);
+        }
+      const float dfx = two_rf_dt * (sUB[2 * l] - vx[0]), dfz = two_rf_dt * (sUB[2 * l + 1] - vz[0]);
       sDF[2 * l] = dfx;
       sDF[2 * l + 1] = dfz;
       sFT[2 * l] += dfx;
       sFT[2 * l + 1] += dfz;
-    }
-  };
-  for (int it = 0; it < j.iters; it++) {
-    // two markers per group at a time: independent reductions in flight
-    for (int lb = 0; lb < nl; lb += 2 * kGroups) {
-      const int l1 = lb + g, l2 = lb + kGroups + g;
-      float vx1, vz1, vx2, vz2;
-      node_vel(l1, vx1, vz1);
-      node_vel(l2, vx2, vz2);
-#pragma unroll
-      for (int o = 8; o > 0; o >>= 1) {
-        vx1 += __shfl_xor_sync(0xffffffffu, vx1, o, 16);
-        vz1 += __shfl_xor_sync(0xffffffffu, vz1, o, 16);
-        vx2 += __shfl_xor_sync(0xffffffffu, vx2, o, 16);
-        vz2 += __shfl_xor_sync(0xffffffffu, vz2, o, 16);
-      }
-      marker_force(l1, vx1, vz1);
-      marker_force(l2, vx2, vz2);
     }
     __syncthreads();
     for (int s = tid; s < ns; s += kThreads) {
