@@ -151,6 +151,19 @@ __device__ void coupled_update(const Job &j, int parity) {
   float *mac = p.mbuf[b];
   const double dz = j.dz, idz = 1.0 / dz;
 
+  // this thread's marker (nl <= kMaxMarkers = kThreads: at most one),
+  // loaded while thread 0 fetches the body
+  double px0 = 0.0, pz0 = 0.0, pdS = 0.0;
+  int porg[4] = {0, 0, 0, 0};
+  if (tid < nl) {
+    px0 = j.X0[2 * tid];
+    pz0 = j.X0[2 * tid + 1];
+    pdS = j.dS[tid];
+    porg[0] = j.org[2 * tid];
+    porg[1] = j.org[2 * tid + 1];
+    porg[2] = j.org2[2 * tid];
+    porg[3] = j.org2[2 * tid + 1];
+  }
   if (tid == 0) {
     B = *j.body;
     bnd[0] = bnd[2] = bnd2[0] = bnd2[2] = bnd3[0] = bnd3[2] = INT_MAX;
@@ -189,8 +202,10 @@ __device__ void coupled_update(const Job &j, int parity) {
   };
 
   // ---- 1. markers: position, velocity, stencil origin and weights
-  for (int l = tid; l < nl; l += kThreads) {
-    const double x0 = j.X0[2 * l], z0 = j.X0[2 * l + 1];
+  static_assert(kMaxMarkers <= kThreads, "one marker per thread at most");
+  if (tid < nl) {
+    const int l = tid;
+    const double x0 = px0, z0 = pz0;
     const double rx = cth * x0 - sth * z0, rz = sth * x0 + cth * z0;
     const double X = B.X[0] + rx, Z = B.X[1] + rz;
     const double xs = X * idz - 0.5, zs = Z * idz - 0.5;  // in cell-index units
@@ -205,10 +220,10 @@ __device__ void coupled_update(const Job &j, int parity) {
     sUB[2 * l] = (float)(B.U[0] - B.om * rz);
     sUB[2 * l + 1] = (float)(B.U[1] + B.om * rx);
     sFT[2 * l] = sFT[2 * l + 1] = 0.f;
-    sDS[l] = (float)(j.dS[l] * idz * idz);
+    sDS[l] = (float)(pdS * idz * idz);
     take_box(bx, i0, k0);
-    if (have_prev2) take_box(bx + 4, j.org2[2 * l], j.org2[2 * l + 1]);
-    if (have_prev) take_box(bx, j.org[2 * l], j.org[2 * l + 1]);
+    if (have_prev2) take_box(bx + 4, porg[2], porg[3]);
+    if (have_prev) take_box(bx, porg[0], porg[1]);
   }
   merge_box(bx, bnd);
   merge_box(bx + 4, bnd2);
@@ -489,23 +504,45 @@ __device__ void coupled_update(const Job &j, int parity) {
     const int bw = ib - ia + 1, bh = kb - ka + 1;
     const double dA = dz * dz;
     if (bw > 0 && bh > 0) {
-      for (int e = tid; e < bw * bh; e += kThreads) {
-        const int i = ia + e % bw, k = ka + e / bw;
-        const double dx = (i + 0.5) * dz - B.X[0], dzz = (k + 0.5) * dz - B.X[1];
-        const double xb = cth * dx + sth * dzz, zb = -sth * dx + cth * dzz;
-        const double xa = xb * ra, zc = zb * rb;
-        const double F = xa * xa + zc * zc - 1.0;
-        const double G = 2.0 * hypot(xa * ra, zc * rb);
-        const double al = fmin(fmax(0.5 - F / fmax(G, 1e-300) * idz, 0.0), 1.0) * dA;
-        if (al > 0.0) {
-          const long long ci = (long long)k * nx + i;
-          float uxf, uzf;
-          vel_at(p, b, mac, ci, N, uxf, uzf);
-          const double ux = uxf, uz = uzf;
-          acc[3] += al * ux;
-          acc[4] += al * uz;
-          acc[5] += al * (dx * uz - dzz * ux);
+      // kC cells per thread at a time: their fractions first, then all
+      // their velocity loads in flight together, then the sums in cell order
+      constexpr int kC = 4;
+      for (int e0 = tid; e0 < bw * bh; e0 += kC * kThreads) {
+        double al[kC], dxs[kC], dzs[kC];
+        long long cis[kC];
+#pragma unroll
+        for (int c = 0; c < kC; c++) {
+          const int e = e0 + c * kThreads;
+          al[c] = 0.0;
+          dxs[c] = dzs[c] = 0.0;
+          cis[c] = 0;
+          if (e < bw * bh) {
+            const int i = ia + e % bw, k = ka + e / bw;
+            const double dx = (i + 0.5) * dz - B.X[0], dzz = (k + 0.5) * dz - B.X[1];
+            const double xb = cth * dx + sth * dzz, zb = -sth * dx + cth * dzz;
+            const double xa = xb * ra, zc = zb * rb;
+            const double F = xa * xa + zc * zc - 1.0;
+            const double G = 2.0 * hypot(xa * ra, zc * rb);
+            al[c] = fmin(fmax(0.5 - F / fmax(G, 1e-300) * idz, 0.0), 1.0) * dA;
+            dxs[c] = dx;
+            dzs[c] = dzz;
+            cis[c] = (long long)k * nx + i;
+          }
         }
+        float uxf[kC], uzf[kC];
+#pragma unroll
+        for (int c = 0; c < kC; c++) {
+          uxf[c] = uzf[c] = 0.f;
+          if (al[c] > 0.0) vel_at(p, b, mac, cis[c], N, uxf[c], uzf[c]);
+        }
+#pragma unroll
+        for (int c = 0; c < kC; c++)
+          if (al[c] > 0.0) {
+            const double ux = uxf[c], uz = uzf[c];
+            acc[3] += al[c] * ux;
+            acc[4] += al[c] * uz;
+            acc[5] += al[c] * (dxs[c] * uz - dzs[c] * ux);
+          }
       }
     }
   }
