@@ -356,12 +356,13 @@ __device__ void coupled_update(const Job &j, int parity) {
     if (s >= 0) sTmp[atomicAdd(&sCur[s], 1)] = (short)e;
   }
   __syncthreads();
-  for (int e = tid; e < 16 * nl; e += kThreads) {
-    const int s = sPS[e];
-    if (s < 0) continue;
+  // (one thread per list position: neighbouring lanes mostly share a slot,
+  // so they scan the same entries together)
+  for (int a = tid; a < sOff[ns]; a += kThreads) {
+    const int e = sTmp[a], s = sPS[e];
     const int a0 = sOff[s], a1 = sOff[s + 1];
     int r = 0;
-    for (int a = a0; a < a1; a++) r += sTmp[a] < e;
+    for (int b2 = a0; b2 < a1; b2++) r += sTmp[b2] < e;
     sList[a0 + r] = (short)e;
     const int l = e >> 4;
     sWL[a0 + r] = sWX[4 * l + (e & 3)] * sWZ[4 * l + ((e >> 2) & 3)] * sDS[l];  // kernel weight x marker area
