@@ -9,7 +9,7 @@ import pytest
 from conftest import ROOT
 from ip_cu_lbm_b200 import _abi, _lib
 
-HEADERS = [os.path.join(ROOT, "include", h) for h in ("ipcu.h", "ipcu_sim.h")]
+HEADERS = [os.path.join(ROOT, "include", h) for h in ("ipcu.h", "ipcu_sim.h", "ipcu_sim3d.h")]
 
 
 def declared_symbols():
@@ -66,3 +66,42 @@ def test_reference_harness_exports():
         precs = ("f32",) if k in _abi.REF_FLOAT_ONLY else ("f32", "f64")
         for p in precs:
             assert hasattr(L, f"ref_{k}_{p}"), k
+
+
+# the ctypes mirrors of the header's structs, field by field
+MIRRORS = [("ipcu_sim_config", "SimConfig"), ("ipcu_ib_body2d", "IBBody2D"), ("ipcu_ib_sphere3d", "IBSphere3D"),
+           ("ipcu_sim3d_axes", "Sim3DAxes"), ("ipcu_sim3d_config", "Sim3DConfig")]
+
+
+def test_ctypes_mirrors_match_the_header_layout(tmp_path):
+    """Size and every field offset of each mirrored struct, as the C
+    compiler lays them out from include/ipcu.h (gcc on the host)."""
+    import shutil
+    import subprocess
+
+    gcc = shutil.which("gcc")
+    if gcc is None:
+        pytest.skip("no host C compiler")
+    lines = ["#include <stdio.h>", "#include <stddef.h>", '#include "ipcu.h"', "int main(void) {"]
+    for cname, pyname in MIRRORS:
+        cls = getattr(_lib, pyname)
+        lines.append(f'  printf("{pyname} size %zu\\n", sizeof({cname}));')
+        for fname, _ in cls._fields_:
+            lines.append(f'  printf("{pyname} {fname} %zu\\n", offsetof({cname}, {fname}));')
+    lines += ["  return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "layout"
+    subprocess.run([gcc, "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split("\n")
+    got = {}
+    for ln in out:
+        if ln.strip():
+            name, field, val = ln.split()
+            got[(name, field)] = int(val)
+    for _, pyname in MIRRORS:
+        cls = getattr(_lib, pyname)
+        assert got[(pyname, "size")] == ctypes.sizeof(cls), pyname
+        for fname, _ in cls._fields_:
+            assert got[(pyname, fname)] == getattr(cls, fname).offset, (pyname, fname)
+
