@@ -30,6 +30,12 @@
 // salinity planes one cell wider feeds the density gradient. Every stored
 // value is read from HBM once and written once per step (halo re-reads hit
 // L2): f [19][N], g [7][N] and the force F [3][N], 232 B per cell in FP32.
+//
+// With 16-bit storage (store3d.cuh) the kernel decodes a cell's populations
+// where it loads them (the collision of tile and halo cells, the salinity
+// ring) and encodes them where it stores them, against the reference (p,
+// u/c, S) that the cell's collision of this step left in shared memory;
+// 148 B per cell.
 #include <cuda_runtime.h>
 
 #include <algorithm>
