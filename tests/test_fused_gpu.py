@@ -134,7 +134,7 @@ def test_fused_matches_structured_oracle(cuda, geo, qs, wall):
 
 @pytest.mark.parametrize("storage", ["f16", "bf16"])
 def test_reduced_precision_storage_error(cuda, storage):
-    """FP16 shifted storage with FP32 arithmetic stays within 1e-3 rel-L2 of
+    """FP16 and BF16 storage with FP32 arithmetic stay within 1e-3 rel-L2 of
     the FP64 oracle on the nonuniform (z-stretched, 3-point upwind) case."""
     M, Minv, S = cases.d2q9_mrt()
     nx, nz = 64, 32
@@ -149,8 +149,8 @@ def test_reduced_precision_storage_error(cuda, storage):
     s.step(200)
     eu = rel_l2(np.stack([s.get("ux"), s.get("uz")]), np.stack([b.ux, b.uz]))
     es = rel_l2(s.get("S"), b.S)
-    limit = 1e-3 if storage == "f16" else 1e-2
-    assert eu <= limit and es <= limit, (eu, es)
+    print(f"{storage} storage, 200 steps: velocity {eu:.2e}, salinity {es:.2e}")
+    assert eu <= 1e-3 and es <= 1e-3, (eu, es)
 
 
 def test_rest_state_exact(cuda):
