@@ -32,13 +32,13 @@ def clustered(n, ratio=3.0):
     return np.cumsum(w) - w / 2, w
 
 
-def lock(nx, ny, nz):
+def lock(nx, ny, nz, ns=3):
     """Lock exchange across x on clustered x and y axes: S = 1 left of the
     gate, 0 right of it, Boussinesq g' = 1e-4 (rho = 1 + 1e-3 S)."""
     X, WX = clustered(nx)
     Y, WY = clustered(ny)
     S0 = np.broadcast_to((X < X[-1] / 2).astype(float)[None, None, :], (nz, ny, nx)).copy()
-    kw = dict(tau=0.56, taus=0.52, g_bouss=1e-4, rho_sal=1e-3, x=X, wx=WX, y=Y, wy=WY, ns=3)
+    kw = dict(tau=0.56, taus=0.52, g_bouss=1e-4, rho_sal=1e-3, x=X, wx=WX, y=Y, wy=WY, ns=ns)
     return kw, S0
 
 
@@ -75,6 +75,21 @@ def test_lock_exchange_16bit_against_fp64_oracle(cuda, storage):
     assert s.bytes_per_cell() == 148 and ref.bytes_per_cell() == 232
     s.close()
     ref.close()
+
+
+def test_lock_exchange_fp16_five_point_stencil(cuda):
+    """The reference's 5-point stencil (the largest shared-memory layout of
+    the 16-bit kernel) against the FP64 oracle."""
+    kw, S0 = lock(40, 20, 16, ns=5)
+    steps = 100
+    s = run(kw, S0, steps, "f16")
+    b = oracle(kw, S0, steps)
+    p, S, rho, u = b.moments()
+    eu = max(rel_l2(s.get(n), r) for n, r in (("ux", u[0]), ("uz", u[2])))
+    eS = rel_l2(s.get("S"), S)
+    print(f"lock exchange f16, 5-point stencil: u {eu:.2e}, S {eS:.2e}")
+    assert s.status() == 0 and eu <= 1e-3 and eS <= 1e-4, (eu, eS)
+    s.close()
 
 
 def test_stratified_box_fp16_against_fp64_oracle(cuda):
