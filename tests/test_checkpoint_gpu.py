@@ -119,3 +119,34 @@ def test_3d_restore_continues_bit_identically(cuda, tmp_path):
     b.step(10)
     for fld in ("f", "g", "F"):
         assert np.array_equal(a.get(fld), b.get(fld)), fld
+
+
+def test_3d_version_1_snapshot_still_loads(cuda, tmp_path):
+    """A version 1 file (FP32 state, the configuration without its storage
+    field) restores and continues bit for bit: written here by taking a
+    version 2 file apart (magic, version, configuration, then the rest)."""
+    import ctypes
+
+    from ip_cu_lbm_b200 import _lib
+    from ip_cu_lbm_b200.sim3d import Sim3D
+
+    nx, ny, nz = 24, 16, 10
+    S0 = np.linspace(0.2, 0.8, nx * ny * nz)
+    a = Sim3D(nx, ny, nz, tau=0.58, taus=0.53, rho_sal=1e-3, g_bouss=1e-4, s0=S0)
+    a.step(10)
+    v2 = tmp_path / "v2.ipcu3"
+    a.save(v2)
+    raw = v2.read_bytes()
+    cfg = ctypes.sizeof(_lib.Sim3DConfig)
+    storage_at = _lib.Sim3DConfig.storage.offset
+    assert int.from_bytes(raw[8:12], "little") == 2
+    v1 = raw[:8] + (1).to_bytes(4, "little") + raw[12:12 + storage_at] + raw[12 + cfg:]
+    (tmp_path / "v1.ipcu3").write_bytes(v1)
+    a.step(10)
+    b = Sim3D.load(tmp_path / "v1.ipcu3")
+    assert b.storage == "f32" and b.steps() == 10
+    b.step(10)
+    for fld in ("f", "g", "F"):
+        assert np.array_equal(a.get(fld), b.get(fld)), fld
+    a.close()
+    b.close()
