@@ -33,9 +33,9 @@
 //
 // With 16-bit storage (store3d.cuh) the kernel decodes a cell's populations
 // where it loads them (the collision of tile and halo cells, the salinity
-// ring) and encodes them where it stores them, against the reference (p,
-// u/c, S) that the cell's collision of this step left in shared memory;
-// 148 B per cell.
+// ring) and encodes them where it stores them, against the reference of
+// each cell: the p and u/c its collision of this step left in shared memory
+// and its salinity from the ring; 148 B per cell.
 #include <cuda_runtime.h>
 
 #include <algorithm>
