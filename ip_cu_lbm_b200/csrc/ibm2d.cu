@@ -144,6 +144,9 @@ __device__ void coupled_update(const Job &j, int parity) {
   __shared__ int nslot, fail;
 
   const f2d::Params &p = j.fp;
+  // launched as a programmatic dependent of the fluid step: nothing is read
+  // before that step has completed (a no-op for an ordinary launch)
+  asm volatile("griddepcontrol.wait;" ::: "memory");
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int nx = p.nx, nz = p.nz, nl = j.nl;
   const long long N = (long long)nx * nz;
@@ -679,8 +682,23 @@ int prep_q() {
 
 template <class ST, int QS>
 int go(const Job *jp, const Job *jobs, int njobs, int parity, cudaStream_t s) {
-  if (jp) ib_kernel<ST, QS><<<1, kThreads, Layout::BYTES, s>>>(*jp, parity);
-  else ib_kernel_batched<ST, QS><<<njobs, kThreads, Layout::BYTES, s>>>(jobs, parity);
+  if (jp) {
+    // a programmatic dependent of the fluid step before it: its launch
+    // overlaps that step's last wave, and it waits (griddepcontrol.wait,
+    // first thing) for the step to complete before it reads anything
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.gridDim = dim3(1);
+    cfg.blockDim = dim3(kThreads);
+    cfg.dynamicSmemBytes = Layout::BYTES;
+    cfg.stream = s;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    return status_from_cuda(cudaLaunchKernelEx(&cfg, ib_kernel<ST, QS>, *jp, parity));
+  }
+  ib_kernel_batched<ST, QS><<<njobs, kThreads, Layout::BYTES, s>>>(jobs, parity);
   return status_from_cuda(cudaGetLastError());
 }
 

@@ -38,6 +38,9 @@ __global__ void __launch_bounds__(kThreads, 6) push_kernel(const __grid_constant
   float *__restrict__ f_out = static_cast<float *>(p.fbuf[bo]);
   const int tile = tile_z * p.ntx + tile_x;
 
+  // the body update after this step may be scheduled once every CTA of it
+  // has started (it waits for this step's completion before it reads)
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
   bool ibt = false;
   if (p.fext != nullptr) {
     const long long tiles = (long long)p.ibtx * p.ntz;
