@@ -20,7 +20,9 @@
 // ustore marks are per tile); 256 threads, two rows each. With a body the
 // kernel is a programmatic dependent of the previous body update: flagged
 // tiles wait for it (griddepcontrol.wait) before they read the force, the
-// rest run beside it.
+// rest run beside it. It also releases the next body update, which waits
+// for this step to complete before it reads anything, as soon as all its
+// CTAs have started.
 #include "fused2d_impl.cuh"
 
 namespace ipcu {
