@@ -146,9 +146,12 @@ class Request:
 
 def request_bytes(req: Request) -> int:
     """Device bytes a request needs once admitted (same formula as
-    ipcu_sim_device_bytes; 3-D: two FP32 buffers of f, g and the force planes)."""
+    ipcu_sim_device_bytes; 3-D: two buffers of f, g, the FP32 force planes
+    and, with 16-bit storage, the reference planes, as
+    ipcu_sim3d_bytes_per_cell counts them)."""
     if req.is3d:  # (a sphere adds its force density and about 4 MB of update scratch)
-        return 2 * 4 * (19 + 7 + 3) * req.cells + ((12 * req.cells + (4 << 20)) if req.body is not None else 0)
+        per_cell = 232 if req.kwargs.get("storage", "f32") == "f32" else 148
+        return per_cell * req.cells + ((12 * req.cells + (4 << 20)) if req.body is not None else 0)
     f32 = req.kwargs.get("storage", "f32") == "f32"
     esz, nmac = (4, 3) if f32 else (2, 4)  # 16-bit storage keeps p* in a 4th FP32 plane
     pf = req.kwargs.get("scalar", "salinity") == "phase"
@@ -562,12 +565,13 @@ def rayleigh_taylor_request(rid, nx, nz, steps, arrival=0.0, storage="f16", seed
     return Request(arrival=arrival, rid=rid, nx=nx, nz=nz, steps=steps, kwargs=kw, s0=phi0.ravel())
 
 
-def stratified_box_request(rid, nx, ny, nz, steps, arrival=0.0, seed=0, sphere=True):
+def stratified_box_request(rid, nx, ny, nz, steps, arrival=0.0, seed=0, sphere=True, storage="f32"):
     """A 3-D falling-sphere request after the sphere configuration: D3Q19
     MRT + D3Q7 salinity with a linear stratification S = 1 - z/H (seeded
     1e-4 noise), Boussinesq g' = 1e-5, rho = 1 + 1e-3 S, tau = 0.55, tau_s =
-    0.52, bounce-back walls, uniform grid, FP32 storage (the 3-D path has no
-    16-bit storage), and a sphere of diameter nx/8 (radius at least 4 cells)
+    0.52, bounce-back walls, uniform grid, FP32 storage by default (the 3-D
+    kernel is issue-bound: 16-bit storage saves memory, not time), and a
+    sphere of diameter nx/8 (radius at least 4 cells)
     with markers at about one per unit area, density ratio 1.5, released from
     rest at 0.8 of the height with a seeded lateral offset of at most one
     cell, gravity 2e-5 (sphere=False: the stratified box alone)."""
@@ -575,6 +579,8 @@ def stratified_box_request(rid, nx, ny, nz, steps, arrival=0.0, seed=0, sphere=T
     zz = np.broadcast_to((np.arange(nz) + 0.5)[:, None, None] / nz, (nz, ny, nx))
     S0 = 1.0 - zz + 1e-4 * rng.uniform(-1, 1, (nz, ny, nx))
     kw = dict(tau=0.55, taus=0.52, rho_sal=1e-3, g_bouss=1e-5)
+    if storage != "f32":
+        kw["storage"] = storage
     body = None
     if sphere:
         off = rng.uniform(-1.0, 1.0, 2)
