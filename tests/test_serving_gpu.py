@@ -214,19 +214,20 @@ def test_autotuned_grid_keeps_results(cuda):
 
 
 def test_3d_requests_in_the_mix(cuda):
-    """3-D requests (stratified boxes with a falling sphere, one without)
-    are admitted beside 2-D ones and replay their step graphs on their own
-    streams; each result -- fields and sphere -- is the 3-D simulation's
-    own."""
+    """3-D requests (stratified boxes with a falling sphere, one without,
+    one with FP16 storage) are admitted beside 2-D ones and replay their
+    step graphs on their own streams; each result -- fields and sphere -- is
+    the 3-D simulation's own."""
     from ip_cu_lbm_b200.serving import make_sim, stratified_box_request
 
     reqs = [stratified_box_request(0, 64, 48, 80, 50, seed=0),
             lock_exchange_request(1, 96, 64, 70, storage="f16", seed=1),
-            stratified_box_request(2, 32, 32, 64, 31, arrival=0.01, seed=2, sphere=False)]
+            stratified_box_request(2, 32, 32, 64, 31, arrival=0.01, seed=2, sphere=False),
+            stratified_box_request(3, 32, 32, 48, 25, arrival=0.02, seed=3, storage="f16")]
     srv = Server(budget_bytes=2e9, tick_steps=20)
     stats = srv.run(reqs)
     srv.close()
-    assert stats["requests"] == 3
+    assert stats["requests"] == 4
     for r in srv.done:
         if not r.is3d:
             continue
