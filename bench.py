@@ -783,7 +783,8 @@ def run_serving(args):
     log-uniform grids 128x128 .. 1024x512, 30 % falling-ellipse
     immersed-boundary requests on log-uniform grids 200x600 .. 800x2400, 10 %
     3-D D3Q19 + D3Q7 stratified boxes with a falling sphere on log-uniform
-    64x64x256 .. 128x128x512 (FP32: the 3-D path has no 16-bit storage),
+    64x64x256 .. 128x128x512 (FP32: the issue-bound 3-D kernel runs 16-bit
+    storage at 0.9x the FP32 speed),
     each with U[2000, 20000] steps (times --step-scale),
     2-D in FP16 storage, 150 GB admission budget, graph-captured batched
     launches with the autotuned grid per kernel class.
